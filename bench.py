@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the 3D stratified ray fan (ray-steps/s) on B200.
+
+One step = one full ray fan through one seeded synthetic atmosphere:
+inclinations 0.5..60 deg every 0.1 deg (596, FP64-accumulated as the
+reference CLI does) x azimuths 0..357 deg every 3 deg (120) = 71,520 rays,
+10 bounces, 2000 km range, amplitude on (18 equations), FP64.  Steps cycle
+through four atmosphere seeds.  ray-steps = accepted RK4 steps (the sum of
+prop_rk4's returned k in the reference).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU, each tracing its own fans (weak scaling, no
+data-path collective); value = all ranks' ray-steps / max over ranks of the
+device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "ray-steps/s"
+UNIT = "ray-steps/s"
+SEEDS = (1, 2, 3, 4)
+FAN = dict(incl=(0.5, 60.01, 0.1), az=(0.0, 357.0, 3.0), bounces=10, rng_max=2000.0)
+# Algorithmic FP64 work of one RK4 ray-step with amplitude (4 RHS stages of the
+# 12 varying equations, the midpoint travel-time increment and one
+# Sutherland-Bass evaluation), counting add/sub/mul as 1, FMA as 2,
+# div/sqrt/reciprocal as 4 and exp/exp10/log/cbrt as 20 FLOPs.
+FLOPS_PER_STEP = 2600.0
+L2_FLUSH_BYTES = 256 << 20
+
+
+def config_dict(extra=None):
+    d = {"workload": "3d-strat-fan-71520rays-10bnc-2000km-fp64-amp",
+         "rays_per_step": 71520, "incl_deg": list(FAN["incl"]), "az_deg": list(FAN["az"]),
+         "bounces": FAN["bounces"], "max_rng_km": FAN["rng_max"], "calc_amp": True,
+         "profiles": "seeded synthetic zTuvdp, 751 levels 0-150 km, seeds 1-4 (one per step, cycling)",
+         "l2": "flushed (256 MiB write) between timed steps"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def write_profiles(d):
+    from infraga_b200 import synth
+    return [synth.write_met(os.path.join(d, f"gen{s}.met"), s) for s in SEEDS]
+
+
+def fan_angles():
+    from infraga_b200 import synth
+    return synth.fan_angles(*FAN["incl"], *FAN["az"])
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU legs
+def ref_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "iga_ref_3d_fast")
+    return p if os.path.exists(p) else None
+
+
+def parse_ref_steps(text):
+    for line in text.splitlines():
+        if line.startswith("# rays"):
+            parts = line.split()
+            return int(parts[4]), float(parts[6])
+    raise RuntimeError("reference driver output without a summary line")
+
+
+def cpu_sample_reference(met, az_list, incl_step, procs):
+    """Run the reference solver (oracle/_ref, compiled from the reference
+    sources) as `procs` concurrent single-threaded processes, one azimuth each.
+    Returns (ray-steps, wall seconds)."""
+    exe = ref_binary()
+    cmds = [[exe, "prop", met, "incl_min=0.5", f"incl_max={FAN['incl'][1]}", f"incl_step={incl_step}",
+             f"azimuth={az}", f"bounces={FAN['bounces']}", f"max_rng={FAN['rng_max']}", "write_rays=false"]
+            for az in az_list[:procs]]
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for c in cmds]
+    outs = [p.communicate()[0] for p in ps]
+    wall = time.perf_counter() - t0
+    steps = sum(parse_ref_steps(o)[0] for o in outs)
+    return steps, wall
+
+
+def cpu_sample_port(met, az_list, incl_step, threads):
+    from infraga_b200 import synth
+    from oracle import oracle
+    th, ph = [], []
+    for az in az_list:
+        a, b = synth.fan_angles(0.5, FAN["incl"][1], incl_step, az, az, 1.0)
+        th.append(a); ph.append(b)
+    th, ph = np.concatenate(th), np.concatenate(ph)
+    t0 = time.perf_counter()
+    _, steps = oracle.fan_3d(met, th, ph, bounces=FAN["bounces"], rng_max=FAN["rng_max"], write_rays=0,
+                             n_threads=threads)
+    return int(steps.sum()), time.perf_counter() - t0
+
+
+def cpu_baseline(met):
+    """Bounded single-core sample: one azimuth (90 deg), every 20th inclination
+    (30 rays), same fan settings."""
+    if ref_binary():
+        steps, wall = cpu_sample_reference(met, [90.0], 2.0, 1)
+        kind = "reference"
+    else:
+        steps, wall = cpu_sample_port(met, [90.0], 2.0, 1)
+        kind = "port"
+    return {"value": steps / wall, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"1 azimuth (90 deg) x 30 inclinations (0.5..60 step 2), seed {SEEDS[0]}, "
+                      f"{steps} ray-steps in {wall:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    tmp = tempfile.mkdtemp(prefix="iga_bench_")
+    mets = write_profiles(tmp)
+    az_all = [float(a) for a in np.arange(0.0, 360.0, 3.0)]
+    kind = "reference" if ref_binary() else "port"
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        met = mets[i % len(mets)]
+        az = [az_all[(i * cores + j) % len(az_all)] for j in range(cores)]
+        if kind == "reference":
+            steps, wall = cpu_sample_reference(met, az, 2.0, cores)
+        else:
+            steps, wall = cpu_sample_port(met, az, 2.0, cores)
+        if i >= args.warmup:
+            per_step.append((steps, wall))
+    tot_steps = sum(s for s, _ in per_step)
+    tot_t = sum(w for _, w in per_step)
+    value = tot_steps / tot_t
+    sample = (f"{cores} concurrent single-threaded processes, one azimuth each, 30 inclinations "
+              f"(0.5..60 step 2) per azimuth, same fan settings; {tot_steps} ray-steps over {args.steps} steps")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict({"reference_sample": sample}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def fp64_peak_tflops(torch):
+    """Measured FP64 throughput of cuBLAS DGEMM (torch.matmul, 8192^3), best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import infraga_b200 as ig
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    tmp = tempfile.mkdtemp(prefix=f"iga_bench_{rank}_")
+    mets = write_profiles(tmp)
+    atmos = [ig.Atmosphere.load(m) for m in mets]
+    th, ph = fan_angles()
+    n = th.size
+    params = [a.default_params(bounces=FAN["bounces"], rng_max=FAN["rng_max"], write_rays=0) for a in atmos]
+    nb = FAN["bounces"] + 1
+    d_th = torch.tensor(th, dtype=torch.float64, device=dev)
+    d_ph = torch.tensor(ph, dtype=torch.float64, device=dev)
+    d_arr = torch.empty((n, nb, 12), dtype=torch.float64, device=dev)
+    d_n = torch.empty(n, dtype=torch.int32, device=dev)
+    d_steps = torch.empty(n, dtype=torch.int64, device=dev)
+    d_stat = torch.empty(n, dtype=torch.int32, device=dev)
+    d_ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        k = (i + rank) % len(atmos)
+        ig.fan_run_device(atmos[k], params[k], d_th.data_ptr(), d_ph.data_ptr(), n, d_arr.data_ptr(),
+                          d_n.data_ptr(), d_steps.data_ptr(), d_stat.data_ptr(), d_ws.data_ptr(), stream.cuda_stream)
+
+    peak = fp64_peak_tflops(torch)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    steps_acc = torch.zeros((), dtype=torch.int64, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        step(args.warmup + i)
+        evs[i][1].record(stream)
+        steps_acc += d_steps.sum()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall0
+    clocks = sampler.stop()
+    kern_s = sum(s.elapsed_time(e) for s, e in evs) * 1e-3
+    my_steps = int(steps_acc.item())
+
+    tot_steps, max_t = my_steps, kern_s
+    if world > 1:
+        t = torch.tensor([float(my_steps), kern_s], dtype=torch.float64, device=dev)
+        s = t.clone()
+        dist.all_reduce(s[:1], op=dist.ReduceOp.SUM)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
+        tot_steps, max_t = int(s[0].item()), float(t[1].item())
+    value = tot_steps / max_t
+
+    # e2e: the public host-buffer API (H2D of launch angles from pinned memory,
+    # kernel, D2H of the arrival records), wall-clocked per call.
+    th_p = torch.from_numpy(th).pin_memory().numpy()
+    ph_p = torch.from_numpy(ph).pin_memory().numpy()
+    e2e_steps, e2e_t, d2h = 0, 0.0, 0
+    ig.fan_run(atmos[0], params[0], th_p, ph_p)   # warm the handle's buffers
+    for i in range(args.steps):
+        k = (i + rank) % len(atmos)
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ig.fan_run(atmos[k], params[k], th_p, ph_p)
+        e2e_t += time.perf_counter() - t0
+        e2e_steps += r["total_steps"]
+        d2h = r["arrivals"].nbytes + n * (4 + 4 + 8)
+    if world > 1:
+        t = torch.tensor([float(e2e_steps), e2e_t], dtype=torch.float64, device=dev)
+        s = t.clone()
+        dist.all_reduce(s[:1], op=dist.ReduceOp.SUM)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
+        e2e_steps, e2e_t = int(s[0].item()), float(t[1].item())
+
+    result = None
+    if rank == 0:
+        achieved = FLOPS_PER_STEP * my_steps / kern_s / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * max_t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict({"parallelism": f"independent fans per GPU x{world}",
+                                   "ray_steps_per_step": tot_steps / args.steps / world}),
+            "e2e": {"value": e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n,
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (best of 5)",
+                         "flops_per_step": FLOPS_PER_STEP},
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(mets[0])
+        result = line
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    for a in atmos:
+        a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0 if result is not None or rank != 0 else 1
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

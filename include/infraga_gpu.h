@@ -1,0 +1,166 @@
+/*
+ * infraga_gpu.h — C ABI of the B200 ray-fan / eigenray library
+ * (libinfraga_gpu.so).
+ *
+ * The reference has no library boundary: its CLI mains call the geoac/atmo
+ * C++ namespace functions directly, one ray at a time, on global state.
+ * Each entry point below replaces a group of those calls for a whole batch
+ * of rays; the comment on each names the reference interface it replaces
+ * (paths relative to the reference project).
+ *
+ * Conventions: plain C types only; the caller owns every input and output
+ * array; the library owns device copies of atmospheres (handle lifetime =
+ * create .. destroy).  Every function returns IGA_OK (0) or a negative
+ * iga_status; no exceptions cross the ABI.  Handles are immutable after
+ * creation and may be shared between threads.
+ */
+#ifndef INFRAGA_GPU_H_
+#define INFRAGA_GPU_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IGA_ABI_VERSION 1
+
+/* ---- status codes ---- */
+enum iga_status {
+    IGA_OK = 0,
+    IGA_E_INVALID = -1,      /* bad argument or parameter */
+    IGA_E_IO = -2,           /* profile / terrain file missing or malformed */
+    IGA_E_NOMEM = -3,        /* host or device allocation failed */
+    IGA_E_CUDA = -4,         /* CUDA runtime error (see iga_last_cuda_error) */
+    IGA_E_NODEVICE = -5,     /* no CUDA device / extension not usable */
+    IGA_E_TRUNCATED = -6,    /* output capacity too small; n_out holds the needed count */
+    IGA_E_UNSUPPORTED = -7   /* combination not implemented (e.g. terrain on this geometry) */
+};
+
+/* ---- per-ray termination status (why a ray stopped) ---- */
+enum iga_ray_status {
+    IGA_RAY_BOUNCES = 0,     /* all requested bounces traced */
+    IGA_RAY_ESCAPED = 1,     /* left the region: range, x/y, altitude or s_max (break_check) */
+    IGA_RAY_LOW_TURN = 2,    /* turning height below turn_ht_min (main.infraga.3d.cpp:503) */
+    IGA_RAY_SHORT = 3,       /* ground reached in < 2 steps (main.infraga.3d.cpp:507) */
+    IGA_RAY_NONFINITE = 4,   /* state became NaN/Inf */
+    IGA_RAY_STEPCAP = 5      /* s_max/ds_min steps without a stop (prop_rk4 array bound) */
+};
+
+/* geometry / precision selectors */
+enum iga_geometry { IGA_GEOM_3D = 0, IGA_GEOM_SPH = 1 };
+enum iga_precision { IGA_FP64 = 0, IGA_FP32C = 1 };
+
+/* Columns of an arrival row, in the reference's .arrivals.dat order
+ * (main.infraga.3d.cpp:362-374): incl, az, n_b, x_0, y_0, time, cel,
+ * turning ht, arrival incl, back az, trans. coeff. [dB], absorption [dB]. */
+#define IGA_ARRIVAL_COLS 12
+
+typedef struct iga_atmo_s* iga_atmo_t;
+
+/* One stratified profile already in solver units (the values set_region
+ * stores after conversion, atmo_io.3d.strat.cpp:106-124). */
+typedef struct iga_profile {
+    int n;                   /* number of altitude knots (>= 3) */
+    const double* z;         /* [n] km, increasing */
+    const double* c;         /* [n] km/s adiabatic sound speed */
+    const double* u;         /* [n] km/s east wind */
+    const double* v;         /* [n] km/s north wind */
+    const double* rho;       /* [n] g/cm^3 */
+} iga_profile;
+
+/* Ray-fan parameters: the geoac globals (geoac.params.3d.cpp:27-41), the
+ * topo::z0 ground height and the run_prop locals (main.infraga.3d.cpp:206-215). */
+typedef struct iga_fan_params {
+    int geometry;            /* IGA_GEOM_3D */
+    int precision;           /* IGA_FP64 or IGA_FP32C */
+    int bounces;             /* reflections to follow (>= 0) */
+    int calc_amp;            /* 1: 18 equations with the Jacobian auxiliaries */
+    int write_rays;          /* 1: sum time/absorption per step like the CLI's
+                                write_rays=true path (all segments but the last of
+                                each bounce, main.infraga.3d.cpp:451-453) */
+    int reserved;
+    double src[3];           /* source x, y [km], altitude [km] */
+    double ds_min, ds_max, s_max;
+    double alt_max, rng_max, x_min, x_max, y_min, y_max;
+    double z_grnd;           /* topo::z0 */
+    double freq;             /* Hz */
+    double tweak_abs;        /* atmo::tweak_abs (abs_coeff=) */
+    double turn_ht_min;      /* km */
+} iga_fan_params;
+
+/* ---- library / device ---- */
+const char* iga_strerror(int status);
+const char* iga_last_cuda_error(void);   /* thread-local text of the last CUDA failure */
+int iga_version(void);                    /* IGA_ABI_VERSION */
+int iga_device_count(int* count);
+
+/* ---- atmospheres ---- */
+
+/* Replaces set_region(atmo_file, format, invert_winds)
+ * (src/atmo/atmo_io.3d.strat.cpp:55-143 and atmo_io.sph.strat.cpp): parses a
+ * .met profile ("zTuvdp", "zuvwTdp" or "zcuvd"), builds the FP64 natural cubic
+ * spline slopes (interp::set, src/util/interpolation.cpp:103-136) on the host
+ * and uploads the tables to the current CUDA device. */
+int iga_atmo_load(const char* met_path, const char* format, int reverse_winds, iga_atmo_t* out);
+
+/* Same as iga_atmo_load from arrays already in solver units. */
+int iga_atmo_create(const iga_profile* profile, iga_atmo_t* out);
+
+/* Propagation limits the reference derives from the profile
+ * (geoac::set_limits, atmo_io.3d.strat.cpp:24-37): z_ground = first knot,
+ * z_top = last knot. */
+int iga_atmo_limits(iga_atmo_t atmo, double* z_ground, double* z_top);
+
+int iga_atmo_destroy(iga_atmo_t atmo);
+
+/* Defaults of run_prop after set_region for a flat-ground 3D run
+ * (main.infraga.3d.cpp:206-215, geoac.params.3d.cpp:27-41,
+ * atmo_io.3d.strat.cpp:24-37): bounces 10, calc_amp 1, write_rays 0,
+ * ds 0.001..0.05, s_max 1000, alt_max = z_top, rng_max 2000, x/y +-2000,
+ * z_grnd = z_ground, freq 0.1, tweak_abs 1, turn_ht_min 0.2. */
+int iga_fan_params_default(iga_atmo_t atmo, iga_fan_params* params);
+
+/* ---- ray fans ---- */
+
+/* Replaces the per-ray loop body of run_prop (src/main.infraga.3d.cpp:421-541):
+ * geoac::set_initial, prop_rk4 (src/util/rk4solver.cpp:14-85), travel_time,
+ * atten, amp and set_refl (src/geoac/geoac.eqset.3d.strat.cpp) for every ray
+ * of a fan at once.  theta_deg/phi_deg are the launch inclination and the
+ * azimuth (degrees clockwise from north, as on the command line) of each ray.
+ *
+ * Host buffers.  arrivals receives up to `cap` rows of IGA_ARRIVAL_COLS
+ * doubles, ordered by ray then bounce (the reference's file order);
+ * *n_out = rows produced (if > cap, rows past cap are dropped and
+ * IGA_E_TRUNCATED is returned).  ray_index (nullable, cap ints) gets the ray
+ * of each row; ray_steps (nullable, n_rays) the accepted RK4 steps of each
+ * ray (the sum of prop_rk4's returned k); ray_status (nullable, n_rays) an
+ * iga_ray_status; total_steps (nullable) the sum over all rays. */
+int iga_fan_run(iga_atmo_t atmo, const iga_fan_params* params,
+                const double* theta_deg, const double* phi_deg, int n_rays,
+                double* arrivals, int cap, int* n_out, int* ray_index,
+                long long* ray_steps, int* ray_status, long long* total_steps);
+
+/* Bytes of device workspace iga_fan_run_device needs (ray queue counters). */
+size_t iga_fan_workspace_bytes(void);
+
+/* Device-resident form of iga_fan_run for callers that keep inputs and
+ * outputs in device memory.  All pointers are device pointers on the
+ * atmosphere's device; the launch is asynchronous on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).
+ *   d_arrivals  [n_rays * (bounces + 1) * IGA_ARRIVAL_COLS] doubles; row j of
+ *               ray i at (i * (bounces + 1) + j)
+ *   d_n_arr     [n_rays] ints, arrivals of each ray
+ *   d_ray_steps [n_rays] long longs
+ *   d_ray_status[n_rays] ints (nullable)
+ *   d_workspace iga_fan_workspace_bytes() bytes, 16-byte aligned; the call
+ *               resets it on `stream` before the launch */
+int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
+                       const double* d_theta_deg, const double* d_phi_deg, int n_rays,
+                       double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
+                       int* d_ray_status, void* d_workspace, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INFRAGA_GPU_H_ */

@@ -1,0 +1,209 @@
+"""ctypes binding of libinfraga_gpu.so (the C ABI in include/infraga_gpu.h).
+
+There is no CPU fallback: if the shared library is missing or cannot be
+loaded, every call raises ``NativeLibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libinfraga_gpu.so")
+ARRIVAL_COLS = 12
+
+IGA_OK, IGA_E_INVALID, IGA_E_IO, IGA_E_NOMEM, IGA_E_CUDA, IGA_E_NODEVICE, IGA_E_TRUNCATED, IGA_E_UNSUPPORTED = \
+    0, -1, -2, -3, -4, -5, -6, -7
+GEOM_3D, GEOM_SPH = 0, 1
+FP64, FP32C = 0, 1
+RAY_STATUS = {0: "bounces", 1: "escaped", 2: "low_turn", 3: "short", 4: "nonfinite", 5: "stepcap"}
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+class IgaError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {strerror(code)} ({code}) {last_cuda_error()}".rstrip())
+
+
+class FanParams(ctypes.Structure):
+    """Mirror of iga_fan_params."""
+    _fields_ = [
+        ("geometry", ctypes.c_int), ("precision", ctypes.c_int), ("bounces", ctypes.c_int),
+        ("calc_amp", ctypes.c_int), ("write_rays", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("src", ctypes.c_double * 3),
+        ("ds_min", ctypes.c_double), ("ds_max", ctypes.c_double), ("s_max", ctypes.c_double),
+        ("alt_max", ctypes.c_double), ("rng_max", ctypes.c_double),
+        ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+        ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+        ("z_grnd", ctypes.c_double), ("freq", ctypes.c_double), ("tweak_abs", ctypes.c_double),
+        ("turn_ht_min", ctypes.c_double),
+    ]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("z", ctypes.POINTER(ctypes.c_double)), ("c", ctypes.POINTER(ctypes.c_double)),
+                ("u", ctypes.POINTER(ctypes.c_double)), ("v", ctypes.POINTER(ctypes.c_double)),
+                ("rho", ctypes.POINTER(ctypes.c_double))]
+
+
+_lib = None
+_P = ctypes.POINTER
+_D = ctypes.c_double
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+_VP = ctypes.c_void_p
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "iga_strerror": (ctypes.c_char_p, [_I]),
+    "iga_last_cuda_error": (ctypes.c_char_p, []),
+    "iga_version": (_I, []),
+    "iga_device_count": (_I, [_P(_I)]),
+    "iga_atmo_load": (_I, [ctypes.c_char_p, ctypes.c_char_p, _I, _P(_VP)]),
+    "iga_atmo_create": (_I, [_P(Profile), _P(_VP)]),
+    "iga_atmo_limits": (_I, [_VP, _P(_D), _P(_D)]),
+    "iga_atmo_destroy": (_I, [_VP]),
+    "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
+    "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL)]),
+    "iga_fan_workspace_bytes": (ctypes.c_size_t, []),
+    "iga_fan_run_device": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+}
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib():
+    """Load libinfraga_gpu.so (building it first only if the sources are present and it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        try:
+            from . import build as _build
+            _build.build_lib()
+        except Exception as e:  # pragma: no cover - depends on toolchain
+            raise NativeLibraryError(f"libinfraga_gpu.so is missing and could not be built: {e}") from e
+    try:
+        L = ctypes.CDLL(LIB_PATH)
+    except OSError as e:
+        raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def strerror(code: int) -> str:
+    return lib().iga_strerror(code).decode()
+
+
+def last_cuda_error() -> str:
+    return lib().iga_last_cuda_error().decode()
+
+
+def _check(rc: int, what: str):
+    if rc != IGA_OK:
+        raise IgaError(rc, what)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_P(_D))
+
+
+class Atmosphere:
+    """A stratified atmosphere resident on the current CUDA device
+    (the reference's set_region, atmo_io.3d.strat.cpp:55-143)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, met_path: str, fmt: str = "zTuvdp", reverse_winds: bool = False) -> "Atmosphere":
+        h = _VP()
+        _check(lib().iga_atmo_load(str(met_path).encode(), fmt.encode(), int(reverse_winds), ctypes.byref(h)),
+               f"iga_atmo_load({met_path})")
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, z, c, u, v, rho) -> "Atmosphere":
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (z, c, u, v, rho)]
+        pr = Profile(len(arrs[0]), *[_dptr(a) for a in arrs])
+        h = _VP()
+        _check(lib().iga_atmo_create(ctypes.byref(pr), ctypes.byref(h)), "iga_atmo_create")
+        return cls(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def limits(self):
+        lo, hi = _D(), _D()
+        _check(lib().iga_atmo_limits(self._h, ctypes.byref(lo), ctypes.byref(hi)), "iga_atmo_limits")
+        return lo.value, hi.value
+
+    def default_params(self, **overrides) -> FanParams:
+        p = FanParams()
+        _check(lib().iga_fan_params_default(self._h, ctypes.byref(p)), "iga_fan_params_default")
+        for k, v in overrides.items():
+            if k == "src":
+                p.src = (_D * 3)(*v)
+            else:
+                setattr(p, k, v)
+        return p
+
+    def close(self):
+        if self._h:
+            lib().iga_atmo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg):
+    """Trace a ray fan (host buffers).  Returns a dict with ``arrivals``
+    [n_rows, 12] in the reference's .arrivals.dat column order, ``ray_index``,
+    ``ray_steps``, ``ray_status`` and ``total_steps``."""
+    th = np.ascontiguousarray(theta_deg, dtype=np.float64)
+    ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
+    n = int(th.size)
+    cap = n * (params.bounces + 1)
+    arr = np.zeros((max(cap, 1), ARRIVAL_COLS), dtype=np.float64)
+    ray_index = np.zeros(max(cap, 1), dtype=np.int32)
+    steps = np.zeros(max(n, 1), dtype=np.int64)
+    status = np.zeros(max(n, 1), dtype=np.int32)
+    n_out = _I()
+    tot = _LL()
+    rc = lib().iga_fan_run(atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph), n, _dptr(arr), cap,
+                           ctypes.byref(n_out), ray_index.ctypes.data_as(_P(_I)), steps.ctypes.data_as(_P(_LL)),
+                           status.ctypes.data_as(_P(_I)), ctypes.byref(tot))
+    _check(rc, "iga_fan_run")
+    m = n_out.value
+    return {"arrivals": arr[:m], "ray_index": ray_index[:m], "ray_steps": steps[:n], "ray_status": status[:n],
+            "total_steps": int(tot.value)}
+
+
+def fan_workspace_bytes() -> int:
+    return int(lib().iga_fan_workspace_bytes())
+
+
+def fan_run_device(atmo: Atmosphere, params: FanParams, d_theta: int, d_phi: int, n_rays: int, d_arrivals: int,
+                   d_n_arr: int, d_steps: int, d_status: int, d_workspace: int, stream: int = 0) -> None:
+    """Device-pointer form (pointers as integers, e.g. ``tensor.data_ptr()``)."""
+    rc = lib().iga_fan_run_device(atmo.handle, ctypes.byref(params), _VP(d_theta), _VP(d_phi), int(n_rays),
+                                  _VP(d_arrivals), _VP(d_n_arr), _VP(d_steps), _VP(d_status) if d_status else None,
+                                  _VP(d_workspace), _VP(stream) if stream else None)
+    _check(rc, "iga_fan_run_device")

@@ -1,0 +1,308 @@
+// C ABI of libinfraga_gpu.so (declared in include/infraga_gpu.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/infraga_gpu.h"
+#include "atmo_host.h"
+#include "fan3d.cuh"
+
+using iga::StratProfile;
+
+struct iga_atmo_s {
+    int device = 0;
+    StratProfile prof;
+    double* d_knots = nullptr;
+    // reusable device buffers of the host-buffer entry points
+    std::mutex mu;
+    void* d_buf = nullptr;
+    size_t d_buf_bytes = 0;
+};
+
+namespace {
+
+thread_local std::string g_cuda_err;
+thread_local std::string g_err;
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_cuda_err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return IGA_E_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return IGA_E_NODEVICE;
+    return IGA_E_CUDA;
+}
+
+#define IGA_CUDA(call, what)                         \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+int upload(iga_atmo_s* h) {
+    int dev;
+    IGA_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    h->device = dev;
+    const size_t bytes = h->prof.table.size() * sizeof(double);
+    IGA_CUDA(cudaMalloc(&h->d_knots, bytes), "cudaMalloc(knots)");
+    IGA_CUDA(cudaMemcpy(h->d_knots, h->prof.table.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(knots)");
+    return IGA_OK;
+}
+
+// Boundary-layer scaling and its z-derivative at altitude z over flat ground
+// z0 (topo::bndlyr_sc / bndlyr_dsc, atmo_state.3d.strat.cpp:85-109).
+void bl_host(double z, double z0, double bl, double& sc, double& dsc_z) {
+    sc = 1.0; dsc_z = 0.0;
+    if (z < z0 + 2.0) {
+        const double X = std::exp(-(z - z0) / bl);
+        sc = (1.0 - X) / (1.0 + X);
+        dsc_z = -2.0 * (-X / bl) / std::pow(1.0 + X, 2);
+    }
+}
+
+int validate(const iga_fan_params* p, int n_rays) {
+    if (!p || n_rays < 0) return IGA_E_INVALID;
+    if (p->geometry != IGA_GEOM_3D) return IGA_E_UNSUPPORTED;
+    if (p->precision != IGA_FP64 && p->precision != IGA_FP32C) return IGA_E_INVALID;
+    if (p->bounces < 0 || !(p->ds_min > 0.0) || !(p->ds_max >= p->ds_min) || !(p->s_max > 0.0)) return IGA_E_INVALID;
+    if (!std::isfinite(p->s_max / p->ds_min) || p->s_max / p->ds_min > 2.0e9) return IGA_E_INVALID;
+    if (!(p->freq > 0.0) || !(p->tweak_abs >= 0.0)) return IGA_E_INVALID;
+    for (int i = 0; i < 3; i++) if (!std::isfinite(p->src[i])) return IGA_E_INVALID;
+    return IGA_OK;
+}
+
+int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const StratProfile& P = h->prof;
+    memset(&a, 0, sizeof(a));
+    a.knots = h->d_knots;
+    a.n_knots = (int)P.z.size();
+    a.uniform = P.uniform ? 1 : 0;
+    a.z_lo = P.z.front();
+    a.z_hi = P.z.back();
+    a.inv_dz = P.inv_dz;
+    a.bounces = p->bounces;
+    a.write_rays = p->write_rays ? 1 : 0;
+    a.length = (int)(p->s_max / p->ds_min);
+    a.src_x = p->src[0];
+    a.src_y = p->src[1];
+    a.z0 = p->z_grnd;
+    a.src_z = std::max(p->src[2], a.z0);   // z_src = max(z_src, topo::z) (main.infraga.3d.cpp:306)
+    a.ds_min = p->ds_min; a.ds_max = p->ds_max; a.s_max = p->s_max;
+    a.alt_max = p->alt_max; a.rng_max = p->rng_max;
+    a.x_min = p->x_min; a.x_max = p->x_max; a.y_min = p->y_min; a.y_max = p->y_max;
+    a.z_bl = a.z0 + 2.0;
+    a.bl = 0.1;
+    a.inv_bl = 1.0 / a.bl;
+    a.freq = p->freq; a.tweak_abs = p->tweak_abs; a.turn_ht_min = p->turn_ht_min;
+    double f, d1, d2, sc, dsc;
+    iga::spline_eval(P.z, P.c, P.cs, a.src_z, f, d1, d2); a.c0 = f;
+    bl_host(a.src_z, a.z0, a.bl, sc, dsc);
+    iga::spline_eval(P.z, P.u, P.us, a.src_z, f, d1, d2); a.u0s = f * sc;
+    iga::spline_eval(P.z, P.v, P.vs, a.src_z, f, d1, d2); a.v0s = f * sc;
+    iga::spline_eval(P.z, P.rho, P.rhos, a.src_z, f, d1, d2); a.rho0 = f;
+    iga::spline_eval(P.z, P.c, P.cs, a.z0, f, d1, d2); a.c_gnd = f; a.dcz_g = d1;
+    bl_host(a.z0, a.z0, a.bl, sc, dsc);
+    iga::spline_eval(P.z, P.u, P.us, a.z0, f, d1, d2); a.duz_g = f * dsc + d1 * sc;
+    iga::spline_eval(P.z, P.v, P.vs, a.z0, f, d1, d2); a.dvz_g = f * dsc + d1 * sc;
+    a.c_ratio = a.c_gnd / a.c0;
+    a.sb.x0_low = std::pow(10.0, -0.67887);
+    a.sb.x1_low = std::pow(10.0, -0.10744);
+    a.sb.x2 = std::pow(10.0, -3.3979);
+    return IGA_OK;
+}
+
+int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
+               double* d_arr, int* d_n, long long* d_steps, int* d_status, void* d_ws, cudaStream_t st) {
+    iga::Fan3DArgs a;
+    int rc = build_args(h, p, a);
+    if (rc) return rc;
+    a.theta_deg = d_th; a.phi_deg = d_ph; a.n_rays = n_rays;
+    a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status;
+    a.queue = static_cast<unsigned int*>(d_ws);
+    IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
+    if (n_rays == 0) return IGA_OK;
+    IGA_CUDA(iga::launch_fan3d_fp64(a, p->calc_amp != 0, st, nullptr), "fan3d kernel launch");
+    return IGA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* iga_strerror(int status) {
+    switch (status) {
+        case IGA_OK: return "ok";
+        case IGA_E_INVALID: return "invalid argument";
+        case IGA_E_IO: return g_err.empty() ? "profile or terrain file error" : g_err.c_str();
+        case IGA_E_NOMEM: return "out of memory";
+        case IGA_E_CUDA: return "CUDA error";
+        case IGA_E_NODEVICE: return "no usable CUDA device";
+        case IGA_E_TRUNCATED: return "output capacity too small";
+        case IGA_E_UNSUPPORTED: return "unsupported configuration";
+        default: return "unknown status";
+    }
+}
+
+const char* iga_last_cuda_error(void) { return g_cuda_err.c_str(); }
+
+int iga_version(void) { return IGA_ABI_VERSION; }
+
+int iga_device_count(int* count) {
+    if (!count) return IGA_E_INVALID;
+    *count = 0;
+    IGA_CUDA(cudaGetDeviceCount(count), "cudaGetDeviceCount");
+    return IGA_OK;
+}
+
+int iga_atmo_load(const char* met_path, const char* format, int reverse_winds, iga_atmo_t* out) {
+    if (!met_path || !out) return IGA_E_INVALID;
+    *out = nullptr;
+    iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
+    if (!h) return IGA_E_NOMEM;
+    int rc = iga::load_met(met_path, format ? format : "zTuvdp", reverse_winds != 0, h->prof, g_err);
+    if (rc == IGA_OK) rc = upload(h);
+    if (rc != IGA_OK) { iga_atmo_destroy(h); return rc; }
+    *out = h;
+    return IGA_OK;
+}
+
+int iga_atmo_create(const iga_profile* pr, iga_atmo_t* out) {
+    if (!pr || !out || pr->n < 3 || !pr->z || !pr->c || !pr->u || !pr->v || !pr->rho) return IGA_E_INVALID;
+    *out = nullptr;
+    iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
+    if (!h) return IGA_E_NOMEM;
+    h->prof.z.assign(pr->z, pr->z + pr->n);
+    h->prof.c.assign(pr->c, pr->c + pr->n);
+    h->prof.u.assign(pr->u, pr->u + pr->n);
+    h->prof.v.assign(pr->v, pr->v + pr->n);
+    h->prof.rho.assign(pr->rho, pr->rho + pr->n);
+    int rc = iga::finalize_profile(h->prof, g_err);
+    if (rc == IGA_OK) rc = upload(h);
+    if (rc != IGA_OK) { iga_atmo_destroy(h); return rc; }
+    *out = h;
+    return IGA_OK;
+}
+
+int iga_atmo_limits(iga_atmo_t h, double* z_ground, double* z_top) {
+    if (!h) return IGA_E_INVALID;
+    if (z_ground) *z_ground = h->prof.z.front();
+    if (z_top) *z_top = h->prof.z.back();
+    return IGA_OK;
+}
+
+int iga_atmo_destroy(iga_atmo_t h) {
+    if (!h) return IGA_OK;
+    if (h->d_knots) cudaFree(h->d_knots);
+    if (h->d_buf) cudaFree(h->d_buf);
+    delete h;
+    return IGA_OK;
+}
+
+int iga_fan_params_default(iga_atmo_t h, iga_fan_params* p) {
+    if (!h || !p) return IGA_E_INVALID;
+    memset(p, 0, sizeof(*p));
+    p->geometry = IGA_GEOM_3D;
+    p->precision = IGA_FP64;
+    p->bounces = 10;
+    p->calc_amp = 1;
+    p->write_rays = 0;
+    p->ds_min = 0.001; p->ds_max = 0.05; p->s_max = 1000.0;
+    p->alt_max = h->prof.z.back();
+    p->rng_max = 2000.0;
+    p->x_min = -2000.0; p->x_max = 2000.0; p->y_min = -2000.0; p->y_max = 2000.0;
+    p->z_grnd = h->prof.z.front();
+    p->freq = 0.1; p->tweak_abs = 1.0; p->turn_ht_min = 0.2;
+    return IGA_OK;
+}
+
+size_t iga_fan_workspace_bytes(void) { return 256; }
+
+int iga_fan_run_device(iga_atmo_t h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
+                       double* d_arr, int* d_n, long long* d_steps, int* d_status, void* d_ws, void* stream) {
+    if (!h) return IGA_E_INVALID;
+    int rc = validate(p, n_rays);
+    if (rc) return rc;
+    if (n_rays > 0 && (!d_th || !d_ph || !d_arr || !d_n || !d_steps)) return IGA_E_INVALID;
+    if (!d_ws || (reinterpret_cast<uintptr_t>(d_ws) & 15)) return IGA_E_INVALID;
+    if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_ws, static_cast<cudaStream_t>(stream));
+}
+
+int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, const double* phi_deg, int n_rays,
+                double* arrivals, int cap, int* n_out, int* ray_index, long long* ray_steps, int* ray_status,
+                long long* total_steps) {
+    if (!h || !n_out) return IGA_E_INVALID;
+    *n_out = 0;
+    int rc = validate(p, n_rays);
+    if (rc) return rc;
+    if (n_rays > 0 && (!theta_deg || !phi_deg)) return IGA_E_INVALID;
+    if (cap > 0 && !arrivals) return IGA_E_INVALID;
+    if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    if (total_steps) *total_steps = 0;
+    if (n_rays == 0) return IGA_OK;
+
+    const int nb = p->bounces + 1;
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t b_ws = align(iga_fan_workspace_bytes());
+    const size_t b_ang = align(sizeof(double) * (size_t)n_rays);
+    const size_t b_arr = align(sizeof(double) * 12 * (size_t)nb * n_rays);
+    const size_t b_n = align(sizeof(int) * (size_t)n_rays);
+    const size_t b_st = align(sizeof(long long) * (size_t)n_rays);
+    const size_t need = b_ws + 2 * b_ang + b_arr + 2 * b_n + b_st;
+
+    std::lock_guard<std::mutex> lock(h->mu);
+    if (h->d_buf_bytes < need) {
+        if (h->d_buf) cudaFree(h->d_buf);
+        h->d_buf = nullptr;
+        h->d_buf_bytes = 0;
+        IGA_CUDA(cudaMalloc(&h->d_buf, need), "cudaMalloc(fan buffers)");
+        h->d_buf_bytes = need;
+    }
+    char* base = static_cast<char*>(h->d_buf);
+    void* d_ws = base; base += b_ws;
+    double* d_th = reinterpret_cast<double*>(base); base += b_ang;
+    double* d_ph = reinterpret_cast<double*>(base); base += b_ang;
+    double* d_arr = reinterpret_cast<double*>(base); base += b_arr;
+    int* d_n = reinterpret_cast<int*>(base); base += b_n;
+    int* d_stat = reinterpret_cast<int*>(base); base += b_n;
+    long long* d_steps = reinterpret_cast<long long*>(base);
+
+    cudaStream_t st = 0;
+    IGA_CUDA(cudaMemcpyAsync(d_th, theta_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D theta");
+    IGA_CUDA(cudaMemcpyAsync(d_ph, phi_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D phi");
+    rc = run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_stat, d_ws, st);
+    if (rc) return rc;
+    std::vector<int> n_arr(n_rays), stat(n_rays);
+    std::vector<long long> steps(n_rays);
+    std::vector<double> rows((size_t)12 * nb * n_rays);
+    IGA_CUDA(cudaMemcpyAsync(n_arr.data(), d_n, sizeof(int) * n_rays, cudaMemcpyDeviceToHost, st), "D2H n_arr");
+    IGA_CUDA(cudaMemcpyAsync(stat.data(), d_stat, sizeof(int) * n_rays, cudaMemcpyDeviceToHost, st), "D2H status");
+    IGA_CUDA(cudaMemcpyAsync(steps.data(), d_steps, sizeof(long long) * n_rays, cudaMemcpyDeviceToHost, st), "D2H steps");
+    IGA_CUDA(cudaMemcpyAsync(rows.data(), d_arr, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H arrivals");
+    IGA_CUDA(cudaStreamSynchronize(st), "fan kernel");
+
+    long long tot = 0;
+    int w = 0;
+    for (int i = 0; i < n_rays; i++) {
+        tot += steps[i];
+        if (ray_steps) ray_steps[i] = steps[i];
+        if (ray_status) ray_status[i] = stat[i];
+        for (int j = 0; j < n_arr[i]; j++, w++) {
+            if (w < cap) {
+                memcpy(arrivals + (size_t)w * 12, &rows[((size_t)i * nb + j) * 12], 12 * sizeof(double));
+                if (ray_index) ray_index[w] = i;
+            }
+        }
+    }
+    *n_out = w;
+    if (total_steps) *total_steps = tot;
+    return w > cap ? IGA_E_TRUNCATED : IGA_OK;
+}
+
+}  // extern "C"

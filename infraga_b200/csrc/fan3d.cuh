@@ -1,0 +1,50 @@
+// Launch arguments shared by the 3D stratified fan kernels and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "device_common.cuh"
+
+namespace iga {
+
+// Everything a fan launch needs, by value (kernel parameter space).
+struct Fan3DArgs {
+    // atmosphere knot table (device, kStride doubles per knot)
+    const double* knots;
+    int n_knots;
+    int uniform;
+    double z_lo, z_hi, inv_dz;
+    // rays
+    const double* theta_deg;
+    const double* phi_deg;
+    int n_rays;
+    int bounces;
+    int write_rays;
+    int length;              // int(s_max / ds_min): prop_rk4's row budget
+    // outputs
+    double* arrivals;        // [n_rays][bounces+1][12]
+    int* n_arr;
+    long long* ray_steps;
+    int* ray_status;         // nullable
+    unsigned int* queue;     // [0] next ray (device ray queue)
+    // geometry / limits
+    double src_x, src_y, src_z;
+    double ds_min, ds_max, s_max;
+    double alt_max, rng_max, x_min, x_max, y_min, y_max;
+    double z0;               // flat ground height (topo::z0)
+    double z_bl;             // boundary-layer top (topo::z_bndlyr = z0 + 2)
+    double bl;               // topo::bndlyr_param
+    double inv_bl;
+    double freq, tweak_abs, turn_ht_min;
+    // per-launch constants evaluated on the host (source and ground point)
+    double c0;               // c at the source
+    double u0s, v0s;         // winds at the source (boundary-layer scaled)
+    double rho0;             // rho at the source
+    double c_gnd;            // c at the ground height
+    double dcz_g, duz_g, dvz_g;   // z-derivatives of c, u, v at the ground (set_refl)
+    double c_ratio;          // c_gnd / c0 (arrival inclination)
+    SBConst sb;
+};
+
+cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
+}  // namespace iga

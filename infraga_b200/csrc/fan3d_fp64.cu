@@ -1,0 +1,390 @@
+// FP64 ray-fan kernel: 3D Cartesian, stratified atmosphere, flat ground.
+//
+// One thread traces one ray at a time through all of its bounces; threads
+// pull rays from a device queue (persistent grid), so a warp keeps all 32
+// lanes busy while rays remain even though ray lengths differ by 10-100x.
+// The loop body is one RK4 step; the rare events (ground hit, arrival record,
+// reflection, new ray) are handled inside it, so lanes that hit the ground
+// never wait for the rest of the warp to finish their bounce.
+//
+// Physics follows the reference 3D stratified equation set
+// (src/geoac/geoac.eqset.3d.strat.cpp) and its RK4 driver
+// (src/util/rk4solver.cpp:14-85); see the per-function notes below.  Without
+// terrain the reference's d(nu_x)/ds, d(nu_y)/ds and the x/y components of
+// the mu equations are identically zero (eval_src_eq, lines 353, 367, 382),
+// and its flat-ground reflection leaves them unchanged, so those six values
+// are per-ray constants here and only 12 of the 18 equations are integrated.
+//
+// The 1D spline table (altitude knots, interleaved c/u/v/rho values and
+// slopes) is staged in shared memory once per CTA.
+#include "fan3d.cuh"
+
+namespace iga {
+
+namespace {
+
+// Evolving state: 0 x, 1 y, 2 z, 3 nu_z, 4-6 X_th, 7 mu_th_z, 8-10 X_ph, 11 mu_ph_z.
+template <bool AMP> struct Dim { static constexpr int n = AMP ? 12 : 4; };
+
+struct RayConst {
+    double nx, ny;             // nu_x, nu_y
+    double mtx, mty, mpx, mpy; // mu_th_{x,y}, mu_ph_{x,y}
+};
+
+// Right-hand side of the ray (and, with AMP, auxiliary) equations at state y:
+// update_refs (geoac.eqset.3d.strat.cpp:225-328) + eval_src_eq (:333-389)
+// with atmo::calc_uvw (atmo_state.3d.strat.cpp:462-734) on flat ground.
+template <bool AMP>
+__device__ __forceinline__ void rhs(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                    const double* y, const RayConst& rc, double* f) {
+    const double z = y[2];
+    const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    double c, cz, czz = 0.0, u0, u0z, u0zz = 0.0, v0, v0z, v0zz = 0.0;
+    if (AMP) {
+        cubic_f2(r0, q, 2, c, cz, czz);
+        cubic_f2(r0, q, 4, u0, u0z, u0zz);
+        cubic_f2(r0, q, 6, v0, v0z, v0zz);
+    } else {
+        cubic_f1(r0, q, 2, c, cz);
+        cubic_f1(r0, q, 4, u0, u0z);
+        cubic_f1(r0, q, 6, v0, v0z);
+    }
+    // no-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-(z-zg)/bl)
+    const double Xb = exp(-(z - a.z0) * a.inv_bl);
+    const double opX = 1.0 + Xb;
+    const double iop = 1.0 / opX;
+    const double sc0 = (1.0 - Xb) * iop;
+    const double dX2 = -Xb * a.inv_bl;
+    const double dsc2 = -2.0 * dX2 * (iop * iop);
+    const double u = u0 * sc0, v = v0 * sc0;
+    const double uz = u0z * sc0 + u0 * dsc2;
+    const double vz = v0z * sc0 + v0 * dsc2;
+
+    const double nz = y[3];
+    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nz * nz);
+    const double inum = 1.0 / num;
+    const double cgx = c * rc.nx * inum + u;
+    const double cgy = c * rc.ny * inum + v;
+    const double cgz = c * nz * inum;
+    const double cgm = sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
+    const double icg = 1.0 / cgm;
+    f[0] = cgx * icg;
+    f[1] = cgy * icg;
+    f[2] = cgz * icg;
+    const double Kz = num * cz + rc.nx * uz + rc.ny * vz;
+    f[3] = -icg * Kz;
+    if (AMP) {
+        const double ddX22 = Xb * (a.inv_bl * a.inv_bl);
+        const double ddsc22 = -2.0 * (ddX22 * (iop * iop) - 2.0 * dX2 * dX2 * (iop * iop * iop));
+        const double uzz = u0zz * sc0 + 2.0 * u0z * dsc2 + u0 * ddsc22;
+        const double vzz = v0zz * sc0 + 2.0 * v0z * dsc2 + v0 * ddsc22;
+        const double Xtz = y[6], Xpz = y[10], mtz = y[7], mpz = y[11];
+        const double dc3 = Xtz * cz, dc4 = Xpz * cz;
+        const double du3 = Xtz * uz, du4 = Xpz * uz;
+        // The reference adds the azimuth variation of v into dv[3] and
+        // leaves dv[4] at zero (geoac.eqset.3d.strat.cpp:298).
+        const double dv3 = Xtz * vz + Xpz * vz;
+        const double dnu0 = (rc.nx * rc.mtx + rc.ny * rc.mty + nz * mtz) * inum;
+        const double dnu1 = (rc.nx * rc.mpx + rc.ny * rc.mpy + nz * mpz) * inum;
+        const double cin = c * inum, cin2 = cin * inum;
+        const double g0x = rc.nx * inum * dc3 + cin * rc.mtx - cin2 * rc.nx * dnu0 + du3;
+        const double g0y = rc.ny * inum * dc3 + cin * rc.mty - cin2 * rc.ny * dnu0 + dv3;
+        const double g0z = nz * inum * dc3 + cin * mtz - cin2 * nz * dnu0;
+        const double g1x = rc.nx * inum * dc4 + cin * rc.mpx - cin2 * rc.nx * dnu1 + du4;
+        const double g1y = rc.ny * inum * dc4 + cin * rc.mpy - cin2 * rc.ny * dnu1;
+        const double g1z = nz * inum * dc4 + cin * mpz - cin2 * nz * dnu1;
+        const double dm0 = (cgx * g0x + cgy * g0y + cgz * g0z) * icg;
+        const double dm1 = (cgx * g1x + cgy * g1y + cgz * g1z) * icg;
+        const double icg2 = icg * icg;
+        f[4] = g0x * icg - cgx * icg2 * dm0;
+        f[5] = g0y * icg - cgy * icg2 * dm0;
+        f[6] = g0z * icg - cgz * icg2 * dm0;
+        f[8] = g1x * icg - cgx * icg2 * dm1;
+        f[9] = g1y * icg - cgy * icg2 * dm1;
+        f[10] = g1z * icg - cgz * icg2 * dm1;
+        f[7] = dm0 * icg2 * Kz - icg * (dnu0 * cz + num * (Xtz * czz) + rc.mtx * uz + rc.mty * vz + rc.nx * (Xtz * uzz) + rc.ny * (Xtz * vzz));
+        f[11] = dm1 * icg2 * Kz - icg * (dnu1 * cz + num * (Xpz * czz) + rc.mpx * uz + rc.mpy * vz + rc.nx * (Xpz * uzz) + rc.ny * (Xpz * vzz));
+    }
+}
+
+// Boundary-layer scaling of atmo::u/v (bndlyr_sc, atmo_state.3d.strat.cpp:85-92).
+__device__ __forceinline__ double bl_scale(const Fan3DArgs& a, double z) {
+    if (z < a.z_bl) {
+        const double X = exp(-(z - a.z0) * a.inv_bl);
+        return (1.0 - X) / (1.0 + X);
+    }
+    return 1.0;
+}
+
+// Travel-time and absorption increments of the segment y0 -> y1, evaluated at
+// the segment midpoint (travel_time :486-511, atten :688-699, SB_alpha).
+__device__ __forceinline__ void seg_increment(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                              const double* y0, const double* y1, const RayConst& rc,
+                                              double& dt, double& da) {
+    const double dx = y1[0] - y0[0], dy = y1[1] - y0[1], dz = y1[2] - y0[2];
+    const double zm = y0[2] + dz * 0.5;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double nzm = y0[3] + (y1[3] - y0[3]) * 0.5;
+    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
+    const double ze = fmin(fmax(zm, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    const double c = cubic_f(r0, q, 2);
+    const double sc = bl_scale(a, zm);
+    const double u = cubic_f(r0, q, 4) * sc;
+    const double v = cubic_f(r0, q, 6) * sc;
+    const double rho = cubic_f(r0, q, 8);
+    const double inum = 1.0 / num;
+    const double cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
+    dt = ds / sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
+    da = sb_alpha_cart(c, rho, zm, a.freq, a.tweak_abs, a.sb) * ds;
+}
+
+// geoac::amp with geoac::jacobian at the below-ground row
+// (geoac.eqset.3d.strat.cpp:704-748).
+__device__ double amp_db(const double* __restrict__ tab, const Fan3DArgs& a, int& seg, const double* y,
+                         const RayConst& rc, double theta, double phi) {
+    const double zk = y[2];
+    const double ze = fmin(fmax(zk, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    const double c = cubic_f(r0, q, 2);
+    const double sc = bl_scale(a, zk);
+    const double wx = cubic_f(r0, q, 4) * sc, wy = cubic_f(r0, q, 6) * sc;
+    const double rho = cubic_f(r0, q, 8);
+    const double nz = y[3];
+    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nz * nz);
+    const double num0 = 1.0 - (rc.nx * a.u0s + rc.ny * a.v0s) / a.c0;
+    const double cgx = c * rc.nx / num + wx, cgy = c * rc.ny / num + wy, cgz = c * nz / num;
+    const double ct = cos(theta), st = sin(theta);
+    const double g0x = a.c0 * ct * cos(phi) + a.u0s, g0y = a.c0 * ct * sin(phi) + a.v0s, g0z = a.c0 * st;
+    const double cgm = sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
+    const double cgm0 = sqrt(g0x * g0x + g0y * g0y + g0z * g0z);
+    const double ex = cgx / cgm, ey = cgy / cgm, ez = cgz / cgm;
+    const double Xt[3] = {y[4], y[5], y[6]}, Xp[3] = {y[8], y[9], y[10]};
+    const double jac = ex * (Xt[1] * Xp[2] - Xp[1] * Xt[2]) - Xt[0] * (ey * Xp[2] - ez * Xp[1]) + Xp[0] * (ey * Xt[2] - ez * Xt[1]);
+    const double numr = rho * num * (c * c * c) * cgm0 * ct;
+    const double den = a.rho0 * num0 * (a.c0 * a.c0 * a.c0) * cgm * jac;
+    return 20.0 * log10(sqrt(fabs(numr / den)));
+}
+
+// Launch state of a ray: geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105).
+template <bool AMP>
+__device__ __forceinline__ void ray_init(const Fan3DArgs& a, double theta, double phi, double* y, RayConst& rc) {
+    const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
+    const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
+    const double n0x = ct * cp, n0y = ct * sp, n0z = st;
+    const double ms = 1.0 + (n0x * mx + n0y * my + n0z * 0.0);
+    const double ims = 1.0 / ms, ims2 = ims * ims;
+    y[0] = a.src_x; y[1] = a.src_y; y[2] = a.src_z;
+    rc.nx = n0x * ims; rc.ny = n0y * ims; y[3] = n0z * ims;
+    if (AMP) {
+        const double tx = -st * cp, ty = -st * sp, tz = ct;
+        const double px = -ct * sp, py = ct * cp, pz = 0.0;
+        const double tm = tx * mx + ty * my + tz * 0.0;
+        const double pm = px * mx + py * my + pz * 0.0;
+        rc.mtx = tx * ims - n0x * ims2 * tm;
+        rc.mty = ty * ims - n0y * ims2 * tm;
+        y[7] = tz * ims - n0z * ims2 * tm;
+        rc.mpx = px * ims - n0x * ims2 * pm;
+        rc.mpy = py * ims - n0y * ims2 * pm;
+        y[11] = pz * ims - n0z * ims2 * pm;
+        y[4] = y[5] = y[6] = 0.0;
+        y[8] = y[9] = y[10] = 0.0;
+    } else {
+        rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0;
+    }
+}
+
+template <bool AMP, bool SMEM>
+__global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
+    constexpr int N = Dim<AMP>::n;
+    extern __shared__ double s_tab[];
+    const double* tab;
+    if (SMEM) {
+        const int tot = a.n_knots * kStride;
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
+        __syncthreads();
+        tab = s_tab;
+    } else {
+        tab = a.knots;
+    }
+
+    const int nb = a.bounces + 1;
+    const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
+
+    int ray = (int)atomicAdd(a.queue, 1u);
+    if (ray >= a.n_rays) return;
+
+    double y[N], pm1[N];
+    RayConst rc;
+    double theta, phi;
+    int seg, bnc, kb, na;
+    long long steps;
+    double s, tt, att, seg_tt, seg_att, pend_t, pend_a, zmax;
+    bool have_pend;
+
+    auto start_ray = [&](int r) {
+        theta = a.theta_deg[r] * kPi / 180.0;
+        phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
+        ray_init<AMP>(a, theta, phi, y, rc);
+        seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+        bnc = 0; kb = 0; na = 0; steps = 0;
+        s = 0.0; tt = 0.0; att = 0.0; seg_tt = 0.0; seg_att = 0.0; pend_t = 0.0; pend_a = 0.0;
+        zmax = a.z0;
+        have_pend = false;
+#pragma unroll
+        for (int i = 0; i < N; i++) pm1[i] = y[i];
+    };
+    start_ray(ray);
+
+    while (true) {
+        // ---- one RK4 step (rk4solver.cpp:30-55) ----
+        zmax = fmax(zmax, y[2]);
+        double ds = a.ds_max;   // set_ds (geoac.eqset.3d.strat.cpp:214-220)
+        if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - a.z0) / 0.2);
+        s += ds;
+        double acc[N], stg[N], f[N];
+        rhs<AMP>(tab, a, seg, y, rc, f);
+#pragma unroll
+        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
+        rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
+        rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
+        rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+        kb++;
+
+        double dt, da;
+        seg_increment(tab, a, seg, y, acc, rc, dt, da);
+        if (a.write_rays) {
+            if (have_pend) { tt += pend_t; att += pend_a; }
+            pend_t = dt; pend_a = da; have_pend = true;
+        } else {
+            seg_tt += dt; seg_att += da;
+        }
+
+        // ---- stop checks (rk4solver.cpp:57-75, break/ground_check :438-453) ----
+        const double rx = acc[0] - a.src_x, ry = acc[1] - a.src_y;
+        bool esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) ||
+                   (acc[0] > a.x_max) || (acc[0] < a.x_min) || (acc[1] > a.y_max) || (acc[1] < a.y_min) ||
+                   (acc[2] > a.alt_max);
+        const bool gnd = !esc && (acc[2] < a.z0);
+        bool capped = false, bad = false;
+        if (!esc && !gnd) {
+            if (kb >= a.length - 1) { capped = true; esc = true; }
+            else if (!isfinite(acc[2]) || !isfinite(acc[3])) { bad = true; esc = true; }
+        }
+        if (!esc && !gnd) {
+#pragma unroll
+            for (int i = 0; i < N; i++) { pm1[i] = y[i]; y[i] = acc[i]; }
+            continue;
+        }
+
+        // ---- end of a bounce segment (main.infraga.3d.cpp:436-538) ----
+        const int K = capped ? a.length : kb;
+        steps += K;
+        if (!a.write_rays) { tt += seg_tt; att += seg_att; }
+        int status = -1;
+        if (zmax < a.z0 + a.turn_ht_min) status = 2;
+        else if (esc) status = bad ? 4 : (capped ? 5 : 1);
+        else if (K < 2) status = 3;
+        if (status < 0) {
+            // arrival record from the first below-ground row
+            double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
+            const double incl = -asin(a.c_ratio * acc[3]) * 180.0 / kPi;
+            double baz = 90.0 - atan2(-rc.ny, -rc.nx) * 180.0 / kPi;
+            if (baz < -180.0) baz += 360.0;
+            else if (baz > 180.0) baz -= 360.0;
+            const double ex = acc[0] - a.src_x, ey = acc[1] - a.src_y;
+            out[0] = a.theta_deg[ray];
+            out[1] = a.phi_deg[ray];
+            out[2] = (double)bnc;
+            out[3] = acc[0];
+            out[4] = acc[1];
+            out[5] = tt;
+            out[6] = sqrt(ex * ex + ey * ey) / tt;
+            out[7] = zmax;
+            out[8] = incl;
+            out[9] = baz;
+            out[10] = AMP ? amp_db(tab, a, seg, acc, rc, theta, phi) : 0.0;
+            out[11] = -2.0 * att;
+            na++;
+            // reflection from rows k-2 (pm1) and k-1 (y): geoac::approx_intercept
+            // and geoac::set_refl (geoac.eqset.3d.strat.cpp:110-209), flat ground
+            const double dz_grnd = a.z0 - y[2];
+            const double dz_k = y[2] - pm1[2];
+            double p[N];
+#pragma unroll
+            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - pm1[i]) / dz_k * dz_grnd;
+            y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
+            if (AMP) {
+                y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
+                y[8] = p[8]; y[9] = p[9]; y[10] = -p[10];
+                const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
+                const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
+                const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + rc.nx * a.duz_g + rc.ny * a.dvz_g);
+                y[7] = -p[7] + (-2.0 * dnuz_ds) * ds0_dth;
+                y[11] = -p[11] + (-2.0 * dnuz_ds) * ds0_dph;
+            }
+#pragma unroll
+            for (int i = 0; i < N; i++) pm1[i] = y[i];
+            bnc++;
+            if (bnc > a.bounces) status = 0;
+        }
+        if (status < 0) {
+            s = 0.0; kb = 0; seg_tt = 0.0; seg_att = 0.0; have_pend = false;
+            continue;
+        }
+        // ray finished: record and take the next one from the queue
+        a.n_arr[ray] = na;
+        a.ray_steps[ray] = steps;
+        if (a.ray_status) a.ray_status[ray] = status;
+        ray = (int)atomicAdd(a.queue, 1u);
+        if (ray >= a.n_rays) break;
+        start_ray(ray);
+    }
+}
+
+template <bool AMP, bool SMEM>
+cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    auto kern = fan3d_fp64_kernel<AMP, SMEM>;
+    const size_t smem = SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0;
+    cudaError_t e;
+    if (SMEM) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, n_sm = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long want = ((long long)a.n_rays + 127) / 128;
+    long long grid = (long long)n_sm * per_sm;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    if (grid_used) *grid_used = (int)grid;
+    kern<<<(unsigned)grid, 128, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
+    const size_t smem = (size_t)a.n_knots * kStride * sizeof(double);
+    const bool fits = smem <= 96 * 1024;
+    if (calc_amp) return fits ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<true, false>(a, stream, grid_used);
+    return fits ? launch_impl<false, true>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
+}
+
+}  // namespace iga

@@ -1,0 +1,71 @@
+"""Regenerates the golden fixtures in this directory from the reference solver
+itself (oracle/_ref, compiled from the reference sources by oracle/Makefile).
+
+    python tests/golden/make_golden.py        # needs the reference sources (make -C oracle ref)
+
+Each fixture is the full-precision output of the reference's own solver
+functions driven by oracle/harness/*.cpp: one line per arrival
+(%.17g, the 12 .arrivals.dat columns), ``R`` lines with each ray's RK4 step
+count, and a ``#`` summary line.  Profiles are seeded synthetic ones
+(infraga_b200.synth), also stored here so the fixtures do not depend on the
+random generator.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from infraga_b200 import synth  # noqa: E402
+
+PROFILES = os.path.join(HERE, "profiles")
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+# name -> (binary, mode, profile seed, argv key=value list)
+CASES = {
+    "3d_c0_rays": ("iga_ref_3d", "prop", 0, ["incl_min=1", "incl_max=45", "incl_step=1", "azimuth=90", "bounces=5",
+                                             "max_rng=1000", "write_rays=true"]),
+    "3d_c0_bulk": ("iga_ref_3d", "prop", 0, ["incl_min=1", "incl_max=45", "incl_step=1", "azimuth=90", "bounces=5",
+                                             "max_rng=1000", "write_rays=false"]),
+    "3d_noamp": ("iga_ref_3d", "prop", 1, ["incl_min=2", "incl_max=40", "incl_step=2", "az_min=0", "az_max=300",
+                                           "az_step=60", "bounces=3", "max_rng=800", "calc_amp=false",
+                                           "write_rays=false"]),
+    "3d_fan_sub": ("iga_ref_3d", "prop", 2, ["incl_min=0.5", "incl_max=60.01", "incl_step=3.5", "az_min=0",
+                                             "az_max=270", "az_step=90", "bounces=10", "max_rng=2000",
+                                             "write_rays=false"]),
+    "3d_elevated": ("iga_ref_3d", "prop", 3, ["incl_min=-30", "incl_max=30", "incl_step=5", "azimuth=45",
+                                              "bounces=2", "src_alt=10", "max_rng=600", "write_rays=false"]),
+    "3d_zgrnd": ("iga_ref_3d", "prop", 4, ["incl_min=5", "incl_max=35", "incl_step=5", "azimuth=200", "bounces=3",
+                                           "z_grnd=0.5", "freq=0.5", "abs_coeff=0.3", "turn_ht_min=10",
+                                           "max_rng=900", "write_rays=true"]),
+}
+
+
+def profile_path(seed: int) -> str:
+    return os.path.join(PROFILES, f"gen{seed}.met")
+
+
+def main():
+    os.makedirs(PROFILES, exist_ok=True)
+    for seed in range(5):
+        synth.write_met(profile_path(seed), seed)
+    meta = {}
+    for name, (binary, mode, seed, args) in CASES.items():
+        exe = os.path.join(REF, binary)
+        cmd = [exe, mode, profile_path(seed), *args]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(os.path.join(HERE, name + ".txt"), "w") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": binary, "mode": mode, "seed": seed, "args": args}
+        print(name, r.stdout.strip().splitlines()[-1])
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

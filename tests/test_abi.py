@@ -1,0 +1,57 @@
+"""The C ABI library loads, exports every function include/*.h declares, and
+fails with a status code (not a crash, not a CPU fallback) without a GPU."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+import infraga_b200 as ig
+from infraga_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(iga_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_functions():
+    assert "iga_fan_run" in declared_functions()
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_symbol_exported(name):
+    L = ig.lib()
+    assert hasattr(L, name), f"{name} declared in include/ but not exported by libinfraga_gpu.so"
+
+
+def test_binding_covers_header():
+    assert set(declared_functions()) <= set(_lib.exported_symbols())
+
+
+def test_status_strings():
+    for code in (0, -1, -2, -3, -4, -5, -6, -7):
+        assert _lib.strerror(code)
+
+
+def test_invalid_arguments_rejected_without_device():
+    L = ig.lib()
+    n = ctypes.c_int()
+    assert L.iga_fan_run(None, None, None, None, 0, None, 0, ctypes.byref(n), None, None, None, None) == _lib.IGA_E_INVALID
+    assert L.iga_atmo_load(None, b"zTuvdp", 0, None) == _lib.IGA_E_INVALID
+
+
+def test_no_silent_cpu_fallback_when_no_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(ig.IgaError):
+        ig.Atmosphere.load(os.path.join(ROOT, "tests", "golden", "profiles", "gen0.met"))

@@ -1,0 +1,171 @@
+"""GPU parity of the 3D stratified ray fan (FP64) through the C ABI, against
+the reference's full-precision output (tests/golden) and the CPU oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import infraga_b200 as ig
+from infraga_b200 import _lib, synth
+from tests._cases import FP64_ATOL, FP64_RTOL, case_setup, compare_arrivals, load_cases, parse_golden, profile_path
+
+pytestmark = pytest.mark.gpu
+
+CASES = {k: v for k, v in load_cases().items() if v["binary"] == "iga_ref_3d" and v["mode"] == "prop"}
+
+
+@pytest.fixture(scope="module")
+def dev():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    ig.lib()
+    return torch
+
+
+def run_case(args, seed, **over):
+    th, ph, p = case_setup(args)
+    p.update(over)
+    atmo = ig.Atmosphere.load(profile_path(seed))
+    params = atmo.default_params(**p)
+    return th, ph, p, ig.fan_run(atmo, params, th, ph)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fan_matches_reference_golden(dev, name):
+    c = CASES[name]
+    th, ph, p, r = run_case(c["args"], c["seed"])
+    ref, ref_steps = parse_golden(name)
+    np.testing.assert_array_equal(r["ray_steps"], ref_steps)
+    ok, msg = compare_arrivals(r["arrivals"], ref)
+    assert ok, msg
+    assert r["total_steps"] == int(ref_steps.sum())
+
+
+def test_fan_matches_oracle_random_rays(dev, oracle_mod):
+    rng = np.random.default_rng(7)
+    th = rng.uniform(0.5, 60.0, 160)
+    ph = rng.uniform(0.0, 360.0, 160)
+    met = profile_path(1)
+    kw = dict(bounces=4, rng_max=1500.0, write_rays=0, n_threads=8)
+    ref, ref_steps = oracle_mod.fan_3d(met, th, ph, **kw)
+    atmo = ig.Atmosphere.load(met)
+    params = atmo.default_params(bounces=4, rng_max=1500.0, write_rays=0)
+    r = ig.fan_run(atmo, params, th, ph)
+    np.testing.assert_array_equal(r["ray_steps"], ref_steps)
+    ok, msg = compare_arrivals(r["arrivals"], ref)
+    assert ok, msg
+
+
+def test_noamp_matches_oracle(dev, oracle_mod):
+    th, ph = synth.fan_angles(1, 50, 7, 0, 315, 45)
+    met = profile_path(3)
+    ref, ref_steps = oracle_mod.fan_3d(met, th, ph, bounces=2, calc_amp=0, write_rays=1, n_threads=8)
+    atmo = ig.Atmosphere.load(met)
+    r = ig.fan_run(atmo, atmo.default_params(bounces=2, calc_amp=0, write_rays=1), th, ph)
+    np.testing.assert_array_equal(r["ray_steps"], ref_steps)
+    ok, msg = compare_arrivals(r["arrivals"], ref)
+    assert ok, msg
+    assert np.all(r["arrivals"][:, 10] == 0.0)
+
+
+def test_deterministic_and_order_independent(dev):
+    th, ph = synth.fan_angles(0.5, 60.01, 1.5, 0, 350, 10)
+    atmo = ig.Atmosphere.load(profile_path(2))
+    params = atmo.default_params(bounces=3)
+    a = ig.fan_run(atmo, params, th, ph)
+    b = ig.fan_run(atmo, params, th, ph)
+    np.testing.assert_array_equal(a["arrivals"], b["arrivals"])
+    perm = np.random.default_rng(3).permutation(th.size)
+    c = ig.fan_run(atmo, params, th[perm], ph[perm])
+    np.testing.assert_array_equal(c["ray_steps"], a["ray_steps"][perm])
+    # per-ray rows are identical whatever the ray order
+    for j in (0, 17, th.size - 1):
+        i = perm[j]
+        np.testing.assert_array_equal(c["arrivals"][c["ray_index"] == j], a["arrivals"][a["ray_index"] == i])
+
+
+def test_full_size_fan_subsample_and_invariants(dev, oracle_mod):
+    """71,520-ray fan (0.5..60 deg x 0..357 deg, 10 bounces, 2000 km): every
+    ray finishes with a valid status, per-ray steps add up, and a fixed
+    subsample of rays equals the oracle's."""
+    th, ph = synth.fan_angles(0.5, 60.01, 0.1, 0, 357, 3)
+    assert th.size == 71520
+    met = profile_path(1)
+    atmo = ig.Atmosphere.load(met)
+    params = atmo.default_params(bounces=10, rng_max=2000.0, write_rays=0)
+    r = ig.fan_run(atmo, params, th, ph)
+    assert r["total_steps"] == int(r["ray_steps"].sum()) > 0
+    assert np.isin(r["ray_status"], [0, 1, 2, 3]).all()
+    assert np.isfinite(r["arrivals"][:, :10]).all()
+    idx = np.arange(0, th.size, 1489)
+    ref, ref_steps = oracle_mod.fan_3d(met, th[idx], ph[idx], bounces=10, rng_max=2000.0, write_rays=0, n_threads=8)
+    np.testing.assert_array_equal(r["ray_steps"][idx], ref_steps)
+    sel = np.concatenate([np.nonzero(r["ray_index"] == i)[0] for i in idx])
+    ok, msg = compare_arrivals(r["arrivals"][sel], ref)
+    assert ok, msg
+
+
+def test_device_entry_matches_host_entry(dev):
+    torch = dev
+    th, ph = synth.fan_angles(2, 40, 4, 30, 330, 60)
+    atmo = ig.Atmosphere.load(profile_path(0))
+    params = atmo.default_params(bounces=3)
+    host = ig.fan_run(atmo, params, th, ph)
+    n = th.size
+    nb = params.bounces + 1
+    d_th = torch.tensor(th, dtype=torch.float64, device="cuda")
+    d_ph = torch.tensor(ph, dtype=torch.float64, device="cuda")
+    d_arr = torch.full((n, nb, 12), float("nan"), dtype=torch.float64, device="cuda")
+    d_n = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_steps = torch.zeros(n, dtype=torch.int64, device="cuda")
+    d_stat = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device="cuda")
+    ig.fan_run_device(atmo, params, d_th.data_ptr(), d_ph.data_ptr(), n, d_arr.data_ptr(), d_n.data_ptr(),
+                      d_steps.data_ptr(), d_stat.data_ptr(), d_ws.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    n_arr = d_n.cpu().numpy()
+    arr = d_arr.cpu().numpy()
+    rows = np.concatenate([arr[i, :n_arr[i]] for i in range(n)])
+    np.testing.assert_array_equal(rows, host["arrivals"])
+    np.testing.assert_array_equal(d_steps.cpu().numpy(), host["ray_steps"])
+
+
+def test_edge_cases(dev):
+    atmo = ig.Atmosphere.load(profile_path(0))
+    params = atmo.default_params(bounces=0)
+    r = ig.fan_run(atmo, params, np.zeros(0), np.zeros(0))
+    assert r["arrivals"].shape[0] == 0 and r["total_steps"] == 0
+    r = ig.fan_run(atmo, params, np.array([10.0]), np.array([90.0]))
+    assert r["arrivals"].shape[0] <= 1
+    # truncation is reported, with the needed count
+    th, ph = synth.fan_angles(5, 30, 5, 90, 90, 1)
+    p = atmo.default_params(bounces=3)
+    n_out = ctypes.c_int()
+    buf = np.zeros((2, 12))
+    rc = ig.lib().iga_fan_run(atmo.handle, ctypes.byref(p), th.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              ph.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), th.size,
+                              buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2, ctypes.byref(n_out),
+                              None, None, None, None)
+    assert rc == _lib.IGA_E_TRUNCATED and n_out.value > 2
+    # invalid parameters are rejected before any launch
+    bad = atmo.default_params(ds_min=0.0)
+    with pytest.raises(ig.IgaError):
+        ig.fan_run(atmo, bad, th, ph)
+    with pytest.raises(ig.IgaError):
+        ig.Atmosphere.load("/nonexistent/profile.met")
+
+
+def test_atmosphere_from_arrays_matches_file(dev):
+    z = np.arange(0, 150.2, 0.2)
+    from infraga_b200.synth import profile_columns
+    zz, T, u, v, rho, p = profile_columns(0)
+    c = np.sqrt(0.1 * 1.4 * p / rho) / 1000.0
+    a1 = ig.Atmosphere.from_arrays(zz, c, u / 1000.0, v / 1000.0, rho)
+    a2 = ig.Atmosphere.load(profile_path(0))
+    th, ph = synth.fan_angles(3, 33, 10, 90, 90, 1)
+    r1 = ig.fan_run(a1, a1.default_params(bounces=2), th, ph)
+    r2 = ig.fan_run(a2, a2.default_params(bounces=2), th, ph)
+    assert z.size == zz.size
+    ok, msg = compare_arrivals(r1["arrivals"], r2["arrivals"], atol=FP64_ATOL * 10, rtol=FP64_RTOL * 10)
+    assert ok, msg
