@@ -1,12 +1,13 @@
 #!/usr/bin/env python
 """Benchmark of the 3D stratified ray fan (ray-steps/s) on B200.
 
-One step = one full ray fan through one seeded synthetic atmosphere:
-inclinations 0.5..60 deg every 0.1 deg (596, FP64-accumulated as the
-reference CLI does) x azimuths 0..357 deg every 3 deg (120) = 71,520 rays,
-10 bounces, 2000 km range, amplitude on (18 equations), FP64.  Steps cycle
-through four atmosphere seeds.  ray-steps = accepted RK4 steps (the sum of
-prop_rk4's returned k in the reference).
+One step = the large 3D fan workload: four seeded synthetic atmospheres,
+each traced with inclinations 0.5..60 deg every 0.1 deg (596, FP64-accumulated
+as the reference CLI does) x azimuths 0..357 deg every 3 deg (120) = 71,520
+rays, 10 bounces, 2000 km range, amplitude on (18 equations), FP64 --
+286,080 rays per step, the four fans running concurrently on four CUDA
+streams.  ray-steps = accepted RK4 steps (the sum of prop_rk4's returned k
+in the reference).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -45,10 +46,11 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def config_dict(extra=None):
-    d = {"workload": "3d-strat-fan-71520rays-10bnc-2000km-fp64-amp",
-         "rays_per_step": 71520, "incl_deg": list(FAN["incl"]), "az_deg": list(FAN["az"]),
+    n = n_fan_rays()
+    d = {"workload": f"3d-strat-fan-4x{n}rays-10bnc-2000km-fp64-amp",
+         "rays_per_step": 4 * n, "rays_per_fan": n, "incl_deg": list(FAN["incl"]), "az_deg": list(FAN["az"]),
          "bounces": FAN["bounces"], "max_rng_km": FAN["rng_max"], "calc_amp": True,
-         "profiles": "seeded synthetic zTuvdp, 751 levels 0-150 km, seeds 1-4 (one per step, cycling)",
+         "profiles": "seeded synthetic zTuvdp, 751 levels 0-150 km, seeds 1-4 (one fan each per step)",
          "l2": "flushed (256 MiB write) between timed steps"}
     if extra:
         d.update(extra)
@@ -63,6 +65,10 @@ def write_profiles(d):
 def fan_angles():
     from infraga_b200 import synth
     return synth.fan_angles(*FAN["incl"], *FAN["az"])
+
+
+def n_fan_rays():
+    return fan_angles()[0].size
 
 
 # ---------------------------------------------------------------- clocks
@@ -247,22 +253,29 @@ def run_ours(args):
     nb = FAN["bounces"] + 1
     d_th = torch.tensor(th, dtype=torch.float64, device=dev)
     d_ph = torch.tensor(ph, dtype=torch.float64, device=dev)
-    d_arr = torch.empty((n, nb, 12), dtype=torch.float64, device=dev)
-    d_n = torch.empty(n, dtype=torch.int32, device=dev)
-    d_steps = torch.empty(n, dtype=torch.int64, device=dev)
-    d_stat = torch.empty(n, dtype=torch.int32, device=dev)
-    d_ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)
+    bufs = [dict(arr=torch.empty((n, nb, 12), dtype=torch.float64, device=dev),
+                 n=torch.empty(n, dtype=torch.int32, device=dev),
+                 st=torch.empty(n, dtype=torch.int64, device=dev),
+                 stat=torch.empty(n, dtype=torch.int32, device=dev),
+                 ws=torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)) for _ in atmos]
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream()
+    main = torch.cuda.current_stream()
+    side = [torch.cuda.Stream(device=dev) for _ in atmos]
 
-    def step(i):
-        k = (i + rank) % len(atmos)
-        ig.fan_run_device(atmos[k], params[k], d_th.data_ptr(), d_ph.data_ptr(), n, d_arr.data_ptr(),
-                          d_n.data_ptr(), d_steps.data_ptr(), d_stat.data_ptr(), d_ws.data_ptr(), stream.cuda_stream)
+    def step():
+        # the four seed fans of the workload, concurrently on four streams
+        for k, a in enumerate(atmos):
+            side[k].wait_stream(main)
+            b = bufs[k]
+            ig.fan_run_device(a, params[k], d_th.data_ptr(), d_ph.data_ptr(), n, b["arr"].data_ptr(),
+                              b["n"].data_ptr(), b["st"].data_ptr(), b["stat"].data_ptr(), b["ws"].data_ptr(),
+                              side[k].cuda_stream)
+        for k in range(len(atmos)):
+            main.wait_stream(side[k])
 
-    peak = fp64_peak_tflops(torch)
-    for i in range(args.warmup):
-        step(i)
+    peak = fp64_peak_tflops(torch) if not args.no_peak else None
+    for _ in range(args.warmup):
+        step()
     torch.cuda.synchronize()
 
     props = torch.cuda.get_device_properties(dev)
@@ -277,10 +290,11 @@ def run_ours(args):
     t_wall0 = time.perf_counter()
     for i in range(args.steps):
         flush.zero_()
-        evs[i][0].record(stream)
-        step(args.warmup + i)
-        evs[i][1].record(stream)
-        steps_acc += d_steps.sum()
+        evs[i][0].record(main)
+        step()
+        evs[i][1].record(main)
+        for b in bufs:
+            steps_acc += b["st"].sum()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -298,21 +312,31 @@ def run_ours(args):
         tot_steps, max_t = int(s[0].item()), float(t[1].item())
     value = tot_steps / max_t
 
-    # e2e: the public host-buffer API (H2D of launch angles from pinned memory,
-    # kernel, D2H of the arrival records), wall-clocked per call.
+    # e2e: the public host-buffer C ABI (iga_fan_run: H2D of the launch angles
+    # from pinned memory, kernel, D2H of the arrival records), one host thread
+    # per seed fan so the four calls overlap on the GPU, wall-clocked per step.
     th_p = torch.from_numpy(th).pin_memory().numpy()
     ph_p = torch.from_numpy(ph).pin_memory().numpy()
     e2e_steps, e2e_t, d2h = 0, 0.0, 0
-    ig.fan_run(atmos[0], params[0], th_p, ph_p)   # warm the handle's buffers
-    for i in range(args.steps):
-        k = (i + rank) % len(atmos)
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = ig.fan_run(atmos[k], params[k], th_p, ph_p)
-        e2e_t += time.perf_counter() - t0
-        e2e_steps += r["total_steps"]
-        d2h = r["arrivals"].nbytes + n * (4 + 4 + 8)
+    if not args.no_e2e:
+        for k, a in enumerate(atmos):
+            ig.fan_run(a, params[k], th_p, ph_p)   # size the handles' device buffers
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            out = [None] * len(atmos)
+
+            def work(k):
+                out[k] = ig.fan_run(atmos[k], params[k], th_p, ph_p)
+            ths = [threading.Thread(target=work, args=(k,)) for k in range(len(atmos))]
+            t0 = time.perf_counter()
+            for t_ in ths:
+                t_.start()
+            for t_ in ths:
+                t_.join()
+            e2e_t += time.perf_counter() - t0
+            e2e_steps += sum(r["total_steps"] for r in out)
+            d2h = sum(r["arrivals"].nbytes + n * (4 + 4 + 8) for r in out)
     if world > 1:
         t = torch.tensor([float(e2e_steps), e2e_t], dtype=torch.float64, device=dev)
         s = t.clone()
@@ -329,11 +353,11 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict({"parallelism": f"independent fans per GPU x{world}",
                                    "ray_steps_per_step": tot_steps / args.steps / world}),
-            "e2e": {"value": e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n,
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps,
+            "e2e": {"value": e2e_steps / e2e_t if e2e_t > 0 else None, "unit": UNIT,
+                    "h2d_bytes_per_step": 2 * 8 * n * len(atmos), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps * len(atmos),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak if peak else None, "traffic": None,
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (best of 5)",
                          "flops_per_step": FLOPS_PER_STEP},
             "clocks": clocks,
@@ -359,7 +383,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg")
+    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak measurement")
+    ap.add_argument("--az-step", type=float, default=FAN["az"][2],
+                    help="azimuth spacing in degrees (a larger value gives a smaller fan, for profiling)")
     args = ap.parse_args()
+    if args.az_step != FAN["az"][2]:
+        FAN["az"] = (FAN["az"][0], FAN["az"][1], args.az_step)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

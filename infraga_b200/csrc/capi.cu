@@ -19,6 +19,9 @@ struct iga_atmo_s {
     int device = 0;
     StratProfile prof;
     double* d_knots = nullptr;
+    // stream of the host-buffer entry points: one per handle, so calls on
+    // different atmospheres from different host threads overlap on the GPU
+    cudaStream_t stream = nullptr;
     // reusable device buffers of the host-buffer entry points
     std::mutex mu;
     void* d_buf = nullptr;
@@ -50,6 +53,7 @@ int upload(iga_atmo_s* h) {
     const size_t bytes = h->prof.table.size() * sizeof(double);
     IGA_CUDA(cudaMalloc(&h->d_knots, bytes), "cudaMalloc(knots)");
     IGA_CUDA(cudaMemcpy(h->d_knots, h->prof.table.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(knots)");
+    IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     return IGA_OK;
 }
 
@@ -198,6 +202,7 @@ int iga_atmo_destroy(iga_atmo_t h) {
     if (!h) return IGA_OK;
     if (h->d_knots) cudaFree(h->d_knots);
     if (h->d_buf) cudaFree(h->d_buf);
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return IGA_OK;
 }
@@ -273,7 +278,7 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
     int* d_stat = reinterpret_cast<int*>(base); base += b_n;
     long long* d_steps = reinterpret_cast<long long*>(base);
 
-    cudaStream_t st = 0;
+    cudaStream_t st = h->stream;
     IGA_CUDA(cudaMemcpyAsync(d_th, theta_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D theta");
     IGA_CUDA(cudaMemcpyAsync(d_ph, phi_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D phi");
     rc = run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_stat, d_ws, st);

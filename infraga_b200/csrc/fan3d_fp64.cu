@@ -23,6 +23,15 @@ namespace iga {
 
 namespace {
 
+#ifndef IGA_FAN_THREADS
+#define IGA_FAN_THREADS 128
+#endif
+#ifndef IGA_FAN_MINB
+#define IGA_FAN_MINB 3
+#endif
+constexpr int kThreads = IGA_FAN_THREADS;
+constexpr double kBlCutoffKm = 40.0;
+
 // Evolving state: 0 x, 1 y, 2 z, 3 nu_z, 4-6 X_th, 7 mu_th_z, 8-10 X_ph, 11 mu_ph_z.
 template <bool AMP> struct Dim { static constexpr int n = AMP ? 12 : 4; };
 
@@ -52,8 +61,13 @@ __device__ __forceinline__ void rhs(const double* __restrict__ tab, const Fan3DA
         cubic_f1(r0, q, 4, u0, u0z);
         cubic_f1(r0, q, 6, v0, v0z);
     }
-    // no-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-(z-zg)/bl)
-    const double Xb = exp(-(z - a.z0) * a.inv_bl);
+    // No-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-(z-zg)/bl).
+    // The reference evaluates X at every altitude; more than 40 km above the
+    // ground X < 1e-173, below half an ulp of every term it is added to
+    // (S rounds to 1, the X-terms of S' and S'' vanish against the spline
+    // derivatives), so X = 0 there gives the same doubles without the exp.
+    const double hz = z - a.z0;
+    const double Xb = hz < kBlCutoffKm ? exp(-hz * a.inv_bl) : 0.0;
     const double opX = 1.0 + Xb;
     const double iop = 1.0 / opX;
     const double sc0 = (1.0 - Xb) * iop;
@@ -202,11 +216,15 @@ __device__ __forceinline__ void ray_init(const Fan3DArgs& a, double theta, doubl
 }
 
 template <bool AMP, bool SMEM>
-__global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
+__global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = Dim<AMP>::n;
-    extern __shared__ double s_tab[];
+    // dynamic shared memory: [N][kThreads] row k-1 of each lane's ray, then
+    // (SMEM) the knot table
+    extern __shared__ double s_mem[];
+    double* s_prev = s_mem;
     const double* tab;
     if (SMEM) {
+        double* s_tab = s_mem + N * kThreads;
         const int tot = a.n_knots * kStride;
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
         __syncthreads();
@@ -214,6 +232,7 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
     } else {
         tab = a.knots;
     }
+    double* prev = s_prev + threadIdx.x;   // element i at prev[i * kThreads]
 
     const int nb = a.bounces + 1;
     const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
@@ -221,25 +240,22 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
     int ray = (int)atomicAdd(a.queue, 1u);
     if (ray >= a.n_rays) return;
 
-    double y[N], pm1[N];
+    double y[N];
     RayConst rc;
-    double theta, phi;
     int seg, bnc, kb, na;
     long long steps;
-    double s, tt, att, seg_tt, seg_att, pend_t, pend_a, zmax;
-    bool have_pend;
+    // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
+    // sums (bulk mode) or the pending last-segment increments (write_rays mode)
+    double s, tt, att, pt, pa, zmax;
 
     auto start_ray = [&](int r) {
-        theta = a.theta_deg[r] * kPi / 180.0;
-        phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
+        const double theta = a.theta_deg[r] * kPi / 180.0;
+        const double phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
         ray_init<AMP>(a, theta, phi, y, rc);
         seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
         bnc = 0; kb = 0; na = 0; steps = 0;
-        s = 0.0; tt = 0.0; att = 0.0; seg_tt = 0.0; seg_att = 0.0; pend_t = 0.0; pend_a = 0.0;
+        s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = a.z0;
-        have_pend = false;
-#pragma unroll
-        for (int i = 0; i < N; i++) pm1[i] = y[i];
     };
     start_ray(ray);
 
@@ -266,11 +282,10 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
 
         double dt, da;
         seg_increment(tab, a, seg, y, acc, rc, dt, da);
-        if (a.write_rays) {
-            if (have_pend) { tt += pend_t; att += pend_a; }
-            pend_t = dt; pend_a = da; have_pend = true;
-        } else {
-            seg_tt += dt; seg_att += da;
+        if (a.write_rays) {   // all segments but the bounce's last (main.infraga.3d.cpp:451-453)
+            tt += pt; att += pa; pt = dt; pa = da;
+        } else {              // per-bounce sum added at the end (main.infraga.3d.cpp:486-487)
+            pt += dt; pa += da;
         }
 
         // ---- stop checks (rk4solver.cpp:57-75, break/ground_check :438-453) ----
@@ -286,14 +301,15 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) { pm1[i] = y[i]; y[i] = acc[i]; }
+            for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
             continue;
         }
 
         // ---- end of a bounce segment (main.infraga.3d.cpp:436-538) ----
         const int K = capped ? a.length : kb;
         steps += K;
-        if (!a.write_rays) { tt += seg_tt; att += seg_att; }
+        if (!a.write_rays) { tt += pt; att += pa; }
+        pt = 0.0; pa = 0.0;
         int status = -1;
         if (zmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);
@@ -306,8 +322,9 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
             if (baz < -180.0) baz += 360.0;
             else if (baz > 180.0) baz -= 360.0;
             const double ex = acc[0] - a.src_x, ey = acc[1] - a.src_y;
-            out[0] = a.theta_deg[ray];
-            out[1] = a.phi_deg[ray];
+            const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
+            out[0] = th_deg;
+            out[1] = ph_deg;
             out[2] = (double)bnc;
             out[3] = acc[0];
             out[4] = acc[1];
@@ -316,16 +333,16 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
             out[7] = zmax;
             out[8] = incl;
             out[9] = baz;
-            out[10] = AMP ? amp_db(tab, a, seg, acc, rc, theta, phi) : 0.0;
+            out[10] = AMP ? amp_db(tab, a, seg, acc, rc, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0) : 0.0;
             out[11] = -2.0 * att;
             na++;
-            // reflection from rows k-2 (pm1) and k-1 (y): geoac::approx_intercept
+            // reflection from rows k-2 (prev) and k-1 (y): geoac::approx_intercept
             // and geoac::set_refl (geoac.eqset.3d.strat.cpp:110-209), flat ground
             const double dz_grnd = a.z0 - y[2];
-            const double dz_k = y[2] - pm1[2];
+            const double dz_k = y[2] - prev[2 * kThreads];
             double p[N];
 #pragma unroll
-            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - pm1[i]) / dz_k * dz_grnd;
+            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kThreads]) / dz_k * dz_grnd;
             y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
             if (AMP) {
                 y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
@@ -336,13 +353,11 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
                 y[7] = -p[7] + (-2.0 * dnuz_ds) * ds0_dth;
                 y[11] = -p[11] + (-2.0 * dnuz_ds) * ds0_dph;
             }
-#pragma unroll
-            for (int i = 0; i < N; i++) pm1[i] = y[i];
             bnc++;
             if (bnc > a.bounces) status = 0;
         }
         if (status < 0) {
-            s = 0.0; kb = 0; seg_tt = 0.0; seg_att = 0.0; have_pend = false;
+            s = 0.0; kb = 0;
             continue;
         }
         // ray finished: record and take the next one from the queue
@@ -358,23 +373,21 @@ __global__ void __launch_bounds__(128) fan3d_fp64_kernel(const __grid_constant__
 template <bool AMP, bool SMEM>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     auto kern = fan3d_fp64_kernel<AMP, SMEM>;
-    const size_t smem = SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0;
-    cudaError_t e;
-    if (SMEM) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
+    const size_t smem = (size_t)Dim<AMP>::n * kThreads * sizeof(double) +
+                        (SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    long long want = ((long long)a.n_rays + 127) / 128;
+    long long want = ((long long)a.n_rays + kThreads - 1) / kThreads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, 128, smem, stream>>>(a);
+    kern<<<(unsigned)grid, kThreads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -382,7 +395,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 
 cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
     const size_t smem = (size_t)a.n_knots * kStride * sizeof(double);
-    const bool fits = smem <= 96 * 1024;
+    const bool fits = smem <= 64 * 1024;
     if (calc_amp) return fits ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<true, false>(a, stream, grid_used);
     return fits ? launch_impl<false, true>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
 }
