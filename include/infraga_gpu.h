@@ -56,6 +56,18 @@ enum iga_precision { IGA_FP64 = 0, IGA_FP32C = 1 };
  * turning ht, arrival incl, back az, trans. coeff. [dB], absorption [dB]. */
 #define IGA_ARRIVAL_COLS 12
 
+/* Optional per-arrival diagnostics (arrival_aux), IGA_AUX_COLS doubles per
+ * arrival row, all from the ray's Jacobian auxiliaries (calc_amp = 1; zero
+ * otherwise):
+ *   0  |d(x,y)/d(inclination)| of the ground intercept [km/rad], formed as
+ *      find_eigenray forms its Newton derivatives (geoac.eigenray.3d.cpp:334-348)
+ *   1  |d(x,y)/d(azimuth)| of the ground intercept [km/rad]
+ *   2  ray-tube Jacobian D at the arrival row (geoac::jacobian); amplitude
+ *      is proportional to |D|^-1/2, so |D| -> 0 marks a caustic
+ *   3  caustics passed so far: sign changes of D between consecutive RK4 rows,
+ *      counted as the write_caustics output does (main.infraga.3d.cpp:448-480) */
+#define IGA_AUX_COLS 4
+
 typedef struct iga_atmo_s* iga_atmo_t;
 
 /* One stratified profile already in solver units (the values set_region
@@ -135,11 +147,13 @@ int iga_fan_params_default(iga_atmo_t atmo, iga_fan_params* params);
  * IGA_E_TRUNCATED is returned).  ray_index (nullable, cap ints) gets the ray
  * of each row; ray_steps (nullable, n_rays) the accepted RK4 steps of each
  * ray (the sum of prop_rk4's returned k); ray_status (nullable, n_rays) an
- * iga_ray_status; total_steps (nullable) the sum over all rays. */
+ * iga_ray_status; total_steps (nullable) the sum over all rays;
+ * arrival_aux (nullable, cap rows of IGA_AUX_COLS) the diagnostics above. */
 int iga_fan_run(iga_atmo_t atmo, const iga_fan_params* params,
                 const double* theta_deg, const double* phi_deg, int n_rays,
                 double* arrivals, int cap, int* n_out, int* ray_index,
-                long long* ray_steps, int* ray_status, long long* total_steps);
+                long long* ray_steps, int* ray_status, long long* total_steps,
+                double* arrival_aux);
 
 /* Bytes of device workspace iga_fan_run_device needs (ray queue counters). */
 size_t iga_fan_workspace_bytes(void);
@@ -153,12 +167,14 @@ size_t iga_fan_workspace_bytes(void);
  *   d_n_arr     [n_rays] ints, arrivals of each ray
  *   d_ray_steps [n_rays] long longs
  *   d_ray_status[n_rays] ints (nullable)
+ *   d_arrival_aux [n_rays * (bounces + 1) * IGA_AUX_COLS] doubles (nullable),
+ *               laid out like d_arrivals
  *   d_workspace iga_fan_workspace_bytes() bytes, 16-byte aligned; the call
  *               resets it on `stream` before the launch */
 int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
                        const double* d_theta_deg, const double* d_phi_deg, int n_rays,
                        double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
-                       int* d_ray_status, void* d_workspace, void* stream);
+                       int* d_ray_status, double* d_arrival_aux, void* d_workspace, void* stream);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libinfraga_gpu.so")
 ARRIVAL_COLS = 12
+AUX_COLS = 4
 
 IGA_OK, IGA_E_INVALID, IGA_E_IO, IGA_E_NOMEM, IGA_E_CUDA, IGA_E_NODEVICE, IGA_E_TRUNCATED, IGA_E_UNSUPPORTED = \
     0, -1, -2, -3, -4, -5, -6, -7
@@ -70,9 +71,10 @@ _SIGS = {
     "iga_atmo_limits": (_I, [_VP, _P(_D), _P(_D)]),
     "iga_atmo_destroy": (_I, [_VP]),
     "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
-    "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL)]),
+    "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL),
+                         _P(_D)]),
     "iga_fan_workspace_bytes": (ctypes.c_size_t, []),
-    "iga_fan_run_device": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "iga_fan_run_device": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 
@@ -173,10 +175,12 @@ class Atmosphere:
             pass
 
 
-def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg):
+def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, with_aux: bool = False):
     """Trace a ray fan (host buffers).  Returns a dict with ``arrivals``
     [n_rows, 12] in the reference's .arrivals.dat column order, ``ray_index``,
-    ``ray_steps``, ``ray_status`` and ``total_steps``."""
+    ``ray_steps``, ``ray_status``, ``total_steps`` and, with ``with_aux``,
+    ``aux`` [n_rows, 4]: |d(x,y)/d incl|, |d(x,y)/d az| [km/rad], the Jacobian
+    D and the caustic count of each arrival."""
     th = np.ascontiguousarray(theta_deg, dtype=np.float64)
     ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
     n = int(th.size)
@@ -185,15 +189,20 @@ def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg):
     ray_index = np.zeros(max(cap, 1), dtype=np.int32)
     steps = np.zeros(max(n, 1), dtype=np.int64)
     status = np.zeros(max(n, 1), dtype=np.int32)
+    aux = np.zeros((max(cap, 1), AUX_COLS), dtype=np.float64) if with_aux else None
     n_out = _I()
     tot = _LL()
     rc = lib().iga_fan_run(atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph), n, _dptr(arr), cap,
                            ctypes.byref(n_out), ray_index.ctypes.data_as(_P(_I)), steps.ctypes.data_as(_P(_LL)),
-                           status.ctypes.data_as(_P(_I)), ctypes.byref(tot))
+                           status.ctypes.data_as(_P(_I)), ctypes.byref(tot),
+                           _dptr(aux) if with_aux else None)
     _check(rc, "iga_fan_run")
     m = n_out.value
-    return {"arrivals": arr[:m], "ray_index": ray_index[:m], "ray_steps": steps[:n], "ray_status": status[:n],
-            "total_steps": int(tot.value)}
+    out = {"arrivals": arr[:m], "ray_index": ray_index[:m], "ray_steps": steps[:n], "ray_status": status[:n],
+           "total_steps": int(tot.value)}
+    if with_aux:
+        out["aux"] = aux[:m]
+    return out
 
 
 def fan_workspace_bytes() -> int:
@@ -201,9 +210,10 @@ def fan_workspace_bytes() -> int:
 
 
 def fan_run_device(atmo: Atmosphere, params: FanParams, d_theta: int, d_phi: int, n_rays: int, d_arrivals: int,
-                   d_n_arr: int, d_steps: int, d_status: int, d_workspace: int, stream: int = 0) -> None:
+                   d_n_arr: int, d_steps: int, d_status: int, d_workspace: int, stream: int = 0,
+                   d_aux: int = 0) -> None:
     """Device-pointer form (pointers as integers, e.g. ``tensor.data_ptr()``)."""
     rc = lib().iga_fan_run_device(atmo.handle, ctypes.byref(params), _VP(d_theta), _VP(d_phi), int(n_rays),
                                   _VP(d_arrivals), _VP(d_n_arr), _VP(d_steps), _VP(d_status) if d_status else None,
-                                  _VP(d_workspace), _VP(stream) if stream else None)
+                                  _VP(d_aux) if d_aux else None, _VP(d_workspace), _VP(stream) if stream else None)
     _check(rc, "iga_fan_run_device")

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -26,6 +27,11 @@ struct iga_atmo_s {
     std::mutex mu;
     void* d_buf = nullptr;
     size_t d_buf_bytes = 0;
+    // FP32-compensated path: FP32 knot table and alpha(z) tables per frequency
+    float* d_knots_f = nullptr;
+    std::mutex alpha_mu;
+    struct AlphaTab { float* d = nullptr; int n = 0; double z0 = 0.0, inv_h = 0.0; };
+    std::map<double, AlphaTab> alpha;   // kept until destroy (launches may still read them)
 };
 
 namespace {
@@ -54,6 +60,66 @@ int upload(iga_atmo_s* h) {
     IGA_CUDA(cudaMalloc(&h->d_knots, bytes), "cudaMalloc(knots)");
     IGA_CUDA(cudaMemcpy(h->d_knots, h->prof.table.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(knots)");
     IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // FP32 segment rows: z_k, 1/dz, then for c, u, v the power-basis
+    // coefficients of the Hermite cubic f = a0 + a1 X + a2 X^2 + a3 X^3
+    // (X = (z - z_k)/dz), formed in FP64.  With A = s0 dx - df and
+    // B = -s1 dx + df (interpolation.cpp:213-221): a1 = df + A = s0 dx,
+    // a2 = B - 2A, a3 = A - B.  Rounding these to FP32 keeps ~7 digits in the
+    // derivatives, where FP32 knot values would lose ~4 to cancellation.
+    const StratProfile& P = h->prof;
+    const size_t n = P.z.size();
+    std::vector<float> tf(n * iga::kStrideF, 0.0f);
+    const std::vector<double>* fv[3] = {&P.c, &P.u, &P.v};
+    const std::vector<double>* sv[3] = {&P.cs, &P.us, &P.vs};
+    for (size_t k = 0; k < n; k++) {
+        float* o = &tf[k * iga::kStrideF];
+        o[0] = (float)P.z[k];
+        if (k + 1 == n) break;
+        const double dx = P.z[k + 1] - P.z[k];
+        o[1] = (float)(1.0 / dx);
+        for (int f = 0; f < 3; f++) {
+            const double f0 = (*fv[f])[k], f1 = (*fv[f])[k + 1];
+            const double s0 = (*sv[f])[k], s1 = (*sv[f])[k + 1];
+            const double df = f1 - f0, A = s0 * dx - df, B = -s1 * dx + df;
+            o[2 + 4 * f] = (float)f0;
+            o[3 + 4 * f] = (float)(s0 * dx);
+            o[4 + 4 * f] = (float)(B - 2.0 * A);
+            o[5 + 4 * f] = (float)(A - B);
+        }
+    }
+    IGA_CUDA(cudaMalloc(&h->d_knots_f, tf.size() * sizeof(float)), "cudaMalloc(knots_f)");
+    IGA_CUDA(cudaMemcpy(h->d_knots_f, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(knots_f)");
+    return IGA_OK;
+}
+
+// Sutherland-Bass alpha(z) for one frequency on a 10 m grid spanning the
+// profile plus 2 km either side, evaluated in FP64 with the reference's model
+// (c and rho from the profile splines, clamped like atmo::c/rho; the gas
+// polynomials at the unclamped z) and stored as FP32 for the FP32C kernel.
+constexpr double kAlphaStepKm = 0.01;
+
+int ensure_alpha(iga_atmo_s* h, double freq, iga_atmo_s::AlphaTab& out) {
+    std::lock_guard<std::mutex> lock(h->alpha_mu);
+    auto it = h->alpha.find(freq);
+    if (it != h->alpha.end()) { out = it->second; return IGA_OK; }
+    const StratProfile& P = h->prof;
+    const double z0 = P.z.front() - 2.0, z1 = P.z.back() + 2.0;
+    const int n = (int)std::ceil((z1 - z0) / kAlphaStepKm) + 1;
+    iga::SBConst sb{std::pow(10.0, -0.67887), std::pow(10.0, -0.10744), std::pow(10.0, -3.3979)};
+    std::vector<float> tab(n);
+    for (int i = 0; i < n; i++) {
+        const double z = z0 + i * kAlphaStepKm;
+        double c, rho, d1, d2;
+        iga::spline_eval(P.z, P.c, P.cs, z, c, d1, d2);
+        iga::spline_eval(P.z, P.rho, P.rhos, z, rho, d1, d2);
+        tab[i] = (float)iga::sb_alpha_cart(c, rho, z, freq, 1.0, sb);
+    }
+    iga_atmo_s::AlphaTab t;
+    t.n = n; t.z0 = z0; t.inv_h = 1.0 / kAlphaStepKm;
+    IGA_CUDA(cudaMalloc(&t.d, n * sizeof(float)), "cudaMalloc(alpha)");
+    IGA_CUDA(cudaMemcpy(t.d, tab.data(), n * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(alpha)");
+    h->alpha[freq] = t;
+    out = t;
     return IGA_OK;
 }
 
@@ -120,16 +186,27 @@ int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
 }
 
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
-               double* d_arr, int* d_n, long long* d_steps, int* d_status, void* d_ws, cudaStream_t st) {
+               double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
+               cudaStream_t st) {
     iga::Fan3DArgs a;
     int rc = build_args(h, p, a);
     if (rc) return rc;
     a.theta_deg = d_th; a.phi_deg = d_ph; a.n_rays = n_rays;
-    a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status;
+    a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status; a.aux = d_aux;
     a.queue = static_cast<unsigned int*>(d_ws);
+    if (p->precision == IGA_FP32C) {
+        iga_atmo_s::AlphaTab t;
+        rc = ensure_alpha(h, p->freq, t);
+        if (rc) return rc;
+        a.knots_f = h->d_knots_f;
+        a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
+    }
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    IGA_CUDA(iga::launch_fan3d_fp64(a, p->calc_amp != 0, st, nullptr), "fan3d kernel launch");
+    if (p->precision == IGA_FP32C)
+        IGA_CUDA(iga::launch_fan3d_fp32c(a, p->calc_amp != 0, st, nullptr), "fan3d fp32c kernel launch");
+    else
+        IGA_CUDA(iga::launch_fan3d_fp64(a, p->calc_amp != 0, st, nullptr), "fan3d kernel launch");
     return IGA_OK;
 }
 
@@ -203,6 +280,8 @@ int iga_atmo_destroy(iga_atmo_t h) {
     if (h->d_knots) cudaFree(h->d_knots);
     if (h->d_buf) cudaFree(h->d_buf);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->d_knots_f) cudaFree(h->d_knots_f);
+    for (auto& kv : h->alpha) cudaFree(kv.second.d);
     delete h;
     return IGA_OK;
 }
@@ -227,27 +306,27 @@ int iga_fan_params_default(iga_atmo_t h, iga_fan_params* p) {
 size_t iga_fan_workspace_bytes(void) { return 256; }
 
 int iga_fan_run_device(iga_atmo_t h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
-                       double* d_arr, int* d_n, long long* d_steps, int* d_status, void* d_ws, void* stream) {
+                       double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
+                       void* stream) {
     if (!h) return IGA_E_INVALID;
     int rc = validate(p, n_rays);
     if (rc) return rc;
     if (n_rays > 0 && (!d_th || !d_ph || !d_arr || !d_n || !d_steps)) return IGA_E_INVALID;
     if (!d_ws || (reinterpret_cast<uintptr_t>(d_ws) & 15)) return IGA_E_INVALID;
-    if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
     IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
-    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_ws, static_cast<cudaStream_t>(stream));
+    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_aux, d_ws,
+                      static_cast<cudaStream_t>(stream));
 }
 
 int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, const double* phi_deg, int n_rays,
                 double* arrivals, int cap, int* n_out, int* ray_index, long long* ray_steps, int* ray_status,
-                long long* total_steps) {
+                long long* total_steps, double* arrival_aux) {
     if (!h || !n_out) return IGA_E_INVALID;
     *n_out = 0;
     int rc = validate(p, n_rays);
     if (rc) return rc;
     if (n_rays > 0 && (!theta_deg || !phi_deg)) return IGA_E_INVALID;
     if (cap > 0 && !arrivals) return IGA_E_INVALID;
-    if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
     IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
     if (total_steps) *total_steps = 0;
     if (n_rays == 0) return IGA_OK;
@@ -259,7 +338,8 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
     const size_t b_arr = align(sizeof(double) * 12 * (size_t)nb * n_rays);
     const size_t b_n = align(sizeof(int) * (size_t)n_rays);
     const size_t b_st = align(sizeof(long long) * (size_t)n_rays);
-    const size_t need = b_ws + 2 * b_ang + b_arr + 2 * b_n + b_st;
+    const size_t b_aux = arrival_aux ? align(sizeof(double) * 4 * (size_t)nb * n_rays) : 0;
+    const size_t need = b_ws + 2 * b_ang + b_arr + 2 * b_n + b_st + b_aux;
 
     std::lock_guard<std::mutex> lock(h->mu);
     if (h->d_buf_bytes < need) {
@@ -276,12 +356,13 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
     double* d_arr = reinterpret_cast<double*>(base); base += b_arr;
     int* d_n = reinterpret_cast<int*>(base); base += b_n;
     int* d_stat = reinterpret_cast<int*>(base); base += b_n;
-    long long* d_steps = reinterpret_cast<long long*>(base);
+    long long* d_steps = reinterpret_cast<long long*>(base); base += b_st;
+    double* d_aux = arrival_aux ? reinterpret_cast<double*>(base) : nullptr;
 
     cudaStream_t st = h->stream;
     IGA_CUDA(cudaMemcpyAsync(d_th, theta_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D theta");
     IGA_CUDA(cudaMemcpyAsync(d_ph, phi_deg, sizeof(double) * n_rays, cudaMemcpyHostToDevice, st), "H2D phi");
-    rc = run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_stat, d_ws, st);
+    rc = run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_stat, d_aux, d_ws, st);
     if (rc) return rc;
     std::vector<int> n_arr(n_rays), stat(n_rays);
     std::vector<long long> steps(n_rays);
@@ -290,6 +371,9 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
     IGA_CUDA(cudaMemcpyAsync(stat.data(), d_stat, sizeof(int) * n_rays, cudaMemcpyDeviceToHost, st), "D2H status");
     IGA_CUDA(cudaMemcpyAsync(steps.data(), d_steps, sizeof(long long) * n_rays, cudaMemcpyDeviceToHost, st), "D2H steps");
     IGA_CUDA(cudaMemcpyAsync(rows.data(), d_arr, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H arrivals");
+    std::vector<double> aux_rows(arrival_aux ? (size_t)4 * nb * n_rays : 0);
+    if (arrival_aux)
+        IGA_CUDA(cudaMemcpyAsync(aux_rows.data(), d_aux, aux_rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H aux");
     IGA_CUDA(cudaStreamSynchronize(st), "fan kernel");
 
     long long tot = 0;
@@ -302,6 +386,7 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
             if (w < cap) {
                 memcpy(arrivals + (size_t)w * 12, &rows[((size_t)i * nb + j) * 12], 12 * sizeof(double));
                 if (ray_index) ray_index[w] = i;
+                if (arrival_aux) memcpy(arrival_aux + (size_t)w * 4, &aux_rows[((size_t)i * nb + j) * 4], 4 * sizeof(double));
             }
         }
     }

@@ -85,13 +85,29 @@ struct SBConst {
     double x2;       // CO2 fraction
 };
 
+// exp10 and reciprocal cube root on either side of the compiler.
+__host__ __device__ __forceinline__ double iga_exp10(double x) {
+#ifdef __CUDA_ARCH__
+    return exp10(x);
+#else
+    return pow(10.0, x);
+#endif
+}
+__host__ __device__ __forceinline__ double iga_rcbrt(double x) {
+#ifdef __CUDA_ARCH__
+    return rcbrt(x);
+#else
+    return 1.0 / cbrt(x);
+#endif
+}
+
 // Sutherland & Bass (2004) absorption, Cartesian variant of the reference
 // (atmo_state.abs.cart.cpp:12-142), in dB/km times tweak_abs.  Inputs are the
 // sound speed [km/s] and density [g/cm^3] at the evaluation point and its
 // altitude z [km].  The reference's N-profile polynomial uses z^2 where z^4
 // is meant (line 78); that is reproduced.  The H2O branch for z > 100 km is
 // unreachable in the reference (it is nested under z <= 30) and so absent.
-__device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, double z, double freq,
+__host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, double z, double freq,
                                                 double tweak_abs, const SBConst& k) {
     const double mu_o = 18.192e-6, T_o = 293.15, P_o = 101325.0, S = 117.0;
     const double cs = c_kms * 1.0e3;
@@ -102,19 +118,19 @@ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, do
 
     const double z2 = z * z, z3 = z2 * z, z4 = z3 * z, z5 = z4 * z;
     double X0 = k.x0_low, X1 = k.x1_low;
-    if (z > 90.0) X0 = exp10(49.296 - (1.5524 * z) + (1.8714e-2 * z2) - (1.1069e-4 * z3) + (3.199e-7 * z4) - (3.6211e-10 * z5));
-    if (z > 76.0) X1 = exp10((1.3972e-1) - (5.6269e-3 * z) + (3.9407e-5 * z2) - (1.0737e-7 * z3));
+    if (z > 90.0) X0 = iga_exp10(49.296 - (1.5524 * z) + (1.8714e-2 * z2) - (1.1069e-4 * z3) + (3.199e-7 * z4) - (3.6211e-10 * z5));
+    if (z > 76.0) X1 = iga_exp10((1.3972e-1) - (5.6269e-3 * z) + (3.9407e-5 * z2) - (1.0737e-7 * z3));
     const double X2 = k.x2;
-    const double X3 = exp10(z > 80.0 ? (-4.234 - (3.0975e-2 * z))
+    const double X3 = iga_exp10(z > 80.0 ? (-4.234 - (3.0975e-2 * z))
                                      : (-19.027 + (1.3093 * z) - (4.6496e-2 * z2) + (7.8543e-4 * z3) - (6.5169e-6 * z4) + (2.1343e-8 * z5)));
-    const double X4 = exp10(z > 95.0 ? (-3.2456 + (4.6642e-2 * z) - (2.6894e-4 * z2) + (5.264e-7 * z3))
+    const double X4 = iga_exp10(z > 95.0 ? (-3.2456 + (4.6642e-2 * z) - (2.6894e-4 * z2) + (5.264e-7 * z3))
                                      : (-11.195 + (1.5408e-1 * z) - (1.4348e-3 * z2) + (1.0166e-5 * z3)));
-    const double X5 = exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * z2) + (4.2609e-10 * z5));
-    const double X6 = exp10(z > 30.0 ? (-4.2563 + (7.6245e-2 * z) - (2.1824e-3 * z2) - (2.3010e-6 * z3) + (2.4265e-7 * z4) - (1.2500e-9 * z5))
+    const double X5 = iga_exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * z2) + (4.2609e-10 * z5));
+    const double X6 = iga_exp10(z > 30.0 ? (-4.2563 + (7.6245e-2 * z) - (2.1824e-3 * z2) - (2.3010e-6 * z3) + (2.4265e-7 * z4) - (1.2500e-9 * z5))
                                      : (-1.7491 + (4.4986e-2 * z) - (6.8549e-2 * z2) + (5.4639e-3 * z3) - (1.5539e-4 * z4) + (1.5063e-6 * z5)));
     const double X_ON = (X0 + X1) / 0.9903;
 
-    const double Tm13 = rcbrt(T_z);
+    const double Tm13 = iga_rcbrt(T_z);
     const double Z_rot0 = 54.1 * exp(-17.3 * Tm13);
     const double Z_rot1 = 63.3 * exp(-16.7 * Tm13);
     const double Z_rot_ = 1.0 / ((X1 / Z_rot1) + (X0 / Z_rot0));
@@ -134,7 +150,7 @@ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, do
     const double a_cl = alpha_1 * beta_2;
     const double a_rot = alpha_2 * beta_1 * X_ON;
 
-    const double Tr = rcbrt(T_z / T_o) - 1.0;
+    const double Tr = iga_rcbrt(T_z / T_o) - 1.0;
     const double A1 = (X0 + X1) * 24.0 * exp(-9.16 * Tr);
     const double A2 = (X4 + X5) * 2400.0;
     const double B = 40400.0 * exp(10.0 * Tr);

@@ -25,6 +25,7 @@ struct Fan3DArgs {
     int* n_arr;
     long long* ray_steps;
     int* ray_status;         // nullable
+    double* aux;             // nullable: [n_rays][bounces+1][4] per-arrival diagnostics
     unsigned int* queue;     // [0] next ray (device ray queue)
     // geometry / limits
     double src_x, src_y, src_z;
@@ -43,7 +44,17 @@ struct Fan3DArgs {
     double dcz_g, duz_g, dvz_g;   // z-derivatives of c, u, v at the ground (set_refl)
     double c_ratio;          // c_gnd / c0 (arrival inclination)
     SBConst sb;
+    // FP32-compensated path only
+    const float* knots_f;    // [n_knots][kStrideF]: per segment z_k, 1/dz and the power-basis
+                             // cubic coefficients a0..a3 of c, u, v (last row: z only)
+    const float* alpha_tab;  // Sutherland-Bass alpha(z) [dB/km, tweak_abs = 1] on a uniform grid
+    int alpha_n;
+    double alpha_z0, alpha_inv_h;
 };
+
+constexpr int kStrideF = 14;  // floats per segment row of the FP32 table
+
+cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 
 cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 

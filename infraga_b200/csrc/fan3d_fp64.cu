@@ -18,6 +18,7 @@
 // The 1D spline table (altitude knots, interleaved c/u/v/rho values and
 // slopes) is staged in shared memory once per CTA.
 #include "fan3d.cuh"
+#include "fan3d_common.cuh"
 
 namespace iga {
 
@@ -35,10 +36,6 @@ constexpr double kBlCutoffKm = 40.0;
 // Evolving state: 0 x, 1 y, 2 z, 3 nu_z, 4-6 X_th, 7 mu_th_z, 8-10 X_ph, 11 mu_ph_z.
 template <bool AMP> struct Dim { static constexpr int n = AMP ? 12 : 4; };
 
-struct RayConst {
-    double nx, ny;             // nu_x, nu_y
-    double mtx, mty, mpx, mpy; // mu_th_{x,y}, mu_ph_{x,y}
-};
 
 // Right-hand side of the ray (and, with AMP, auxiliary) equations at state y:
 // update_refs (geoac.eqset.3d.strat.cpp:225-328) + eval_src_eq (:333-389)
@@ -124,15 +121,6 @@ __device__ __forceinline__ void rhs(const double* __restrict__ tab, const Fan3DA
     }
 }
 
-// Boundary-layer scaling of atmo::u/v (bndlyr_sc, atmo_state.3d.strat.cpp:85-92).
-__device__ __forceinline__ double bl_scale(const Fan3DArgs& a, double z) {
-    if (z < a.z_bl) {
-        const double X = exp(-(z - a.z0) * a.inv_bl);
-        return (1.0 - X) / (1.0 + X);
-    }
-    return 1.0;
-}
-
 // Travel-time and absorption increments of the segment y0 -> y1, evaluated at
 // the segment midpoint (travel_time :486-511, atten :688-699, SB_alpha).
 __device__ __forceinline__ void seg_increment(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
@@ -156,35 +144,6 @@ __device__ __forceinline__ void seg_increment(const double* __restrict__ tab, co
     const double cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
     dt = ds / sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
     da = sb_alpha_cart(c, rho, zm, a.freq, a.tweak_abs, a.sb) * ds;
-}
-
-// geoac::amp with geoac::jacobian at the below-ground row
-// (geoac.eqset.3d.strat.cpp:704-748).
-__device__ double amp_db(const double* __restrict__ tab, const Fan3DArgs& a, int& seg, const double* y,
-                         const RayConst& rc, double theta, double phi) {
-    const double zk = y[2];
-    const double ze = fmin(fmax(zk, a.z_lo), a.z_hi);
-    seg = seg_walk(tab, a.n_knots, ze, seg);
-    const double* r0 = tab + seg * kStride;
-    const Cubic q = cubic_at(r0, ze);
-    const double c = cubic_f(r0, q, 2);
-    const double sc = bl_scale(a, zk);
-    const double wx = cubic_f(r0, q, 4) * sc, wy = cubic_f(r0, q, 6) * sc;
-    const double rho = cubic_f(r0, q, 8);
-    const double nz = y[3];
-    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nz * nz);
-    const double num0 = 1.0 - (rc.nx * a.u0s + rc.ny * a.v0s) / a.c0;
-    const double cgx = c * rc.nx / num + wx, cgy = c * rc.ny / num + wy, cgz = c * nz / num;
-    const double ct = cos(theta), st = sin(theta);
-    const double g0x = a.c0 * ct * cos(phi) + a.u0s, g0y = a.c0 * ct * sin(phi) + a.v0s, g0z = a.c0 * st;
-    const double cgm = sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
-    const double cgm0 = sqrt(g0x * g0x + g0y * g0y + g0z * g0z);
-    const double ex = cgx / cgm, ey = cgy / cgm, ez = cgz / cgm;
-    const double Xt[3] = {y[4], y[5], y[6]}, Xp[3] = {y[8], y[9], y[10]};
-    const double jac = ex * (Xt[1] * Xp[2] - Xp[1] * Xt[2]) - Xt[0] * (ey * Xp[2] - ez * Xp[1]) + Xp[0] * (ey * Xt[2] - ez * Xt[1]);
-    const double numr = rho * num * (c * c * c) * cgm0 * ct;
-    const double den = a.rho0 * num0 * (a.c0 * a.c0 * a.c0) * cgm * jac;
-    return 20.0 * log10(sqrt(fabs(numr / den)));
 }
 
 // Launch state of a ray: geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105).
@@ -242,7 +201,8 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
 
     double y[N];
     RayConst rc;
-    int seg, bnc, kb, na;
+    int seg, bnc, kb, na, caustics;
+    double D_prev = 0.0;
     long long steps;
     // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
     // sums (bulk mode) or the pending last-segment increments (write_rays mode)
@@ -253,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         const double phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
         ray_init<AMP>(a, theta, phi, y, rc);
         seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-        bnc = 0; kb = 0; na = 0; steps = 0;
+        bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = a.z0;
     };
@@ -267,6 +227,11 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         s += ds;
         double acc[N], stg[N], f[N];
         rhs<AMP>(tab, a, seg, y, rc, f);
+        if (AMP && a.aux && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
+            const double D = ray_jacobian(f, y);
+            if (kb >= 2 && D * D_prev < 0.0) caustics++;
+            D_prev = D;
+        }
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
         rhs<AMP>(tab, a, seg, stg, rc, f);
@@ -333,8 +298,14 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
             out[7] = zmax;
             out[8] = incl;
             out[9] = baz;
-            out[10] = AMP ? amp_db(tab, a, seg, acc, rc, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0) : 0.0;
+            double jac = 0.0;
+            out[10] = AMP ? amp_db(tab, a, seg, acc, rc, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0, &jac) : 0.0;
             out[11] = -2.0 * att;
+            if (a.aux) {
+                double* ax = a.aux + ((size_t)ray * nb + na) * 4;
+                if (AMP) write_aux(ax, a, acc, rc, jac, caustics);
+                else ax[0] = ax[1] = ax[2] = ax[3] = 0.0;
+            }
             na++;
             // reflection from rows k-2 (prev) and k-1 (y): geoac::approx_intercept
             // and geoac::set_refl (geoac.eqset.3d.strat.cpp:110-209), flat ground

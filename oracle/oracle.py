@@ -66,8 +66,12 @@ def default_cfg(**kw) -> FanCfg:
     return c
 
 
-def fan_3d(met_path: str, theta_deg, phi_deg, fmt: str = "zTuvdp", **cfg_kw):
-    """Run the oracle 3D stratified fan.  Returns (arrivals [n_rows, 12], steps per ray)."""
+AUX_COLS = 4
+
+
+def fan_3d(met_path: str, theta_deg, phi_deg, fmt: str = "zTuvdp", with_aux: bool = False, **cfg_kw):
+    """Run the oracle 3D stratified fan.  Returns (arrivals [n_rows, 12], steps
+    per ray), plus the per-arrival diagnostics [n_rows, 4] when with_aux."""
     th = np.ascontiguousarray(theta_deg, dtype=np.float64)
     ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
     cfg = default_cfg(**cfg_kw)
@@ -76,14 +80,19 @@ def fan_3d(met_path: str, theta_deg, phi_deg, fmt: str = "zTuvdp", **cfg_kw):
     arr = np.zeros((n * nb, ARR_COLS), dtype=np.float64)
     n_arr = np.zeros(n, dtype=np.int32)
     steps = np.zeros(n, dtype=np.int64)
+    aux = np.zeros((n * nb, AUX_COLS), dtype=np.float64)
     P = ctypes.POINTER
     rc = lib().orc_fan_3d(met_path.encode(), fmt.encode(), ctypes.byref(cfg),
                           th.ctypes.data_as(P(ctypes.c_double)), ph.ctypes.data_as(P(ctypes.c_double)),
                           ctypes.c_int(n), arr.ctypes.data_as(P(ctypes.c_double)),
-                          n_arr.ctypes.data_as(P(ctypes.c_int)), steps.ctypes.data_as(P(ctypes.c_longlong)))
+                          n_arr.ctypes.data_as(P(ctypes.c_int)), steps.ctypes.data_as(P(ctypes.c_longlong)),
+                          aux.ctypes.data_as(P(ctypes.c_double)))
     if rc != 0:
         raise RuntimeError(f"oracle fan failed ({rc}) for {met_path}")
-    rows = np.concatenate([arr[i * nb:i * nb + n_arr[i]] for i in range(n)]) if n else arr[:0]
+    sel = np.concatenate([np.arange(i * nb, i * nb + n_arr[i]) for i in range(n)]).astype(np.int64) if n else []
+    rows = arr[sel]
+    if with_aux:
+        return rows, steps, aux[sel]
     return rows, steps
 
 

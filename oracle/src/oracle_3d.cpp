@@ -61,6 +61,7 @@ struct Ray {
     double theta, phi;
     Refs refs;
     int acc_c = 0, acc_u = 0, acc_v = 0, acc_rho = 0;
+    double D_prev = 0.0;
 };
 
 // ---- topography on flat ground (atmo_state.3d.strat.cpp:51-83) ----
@@ -606,7 +607,7 @@ static double amp(Ray& r, const double* s) {
 struct SegOut { int k; bool check; double zmax; };
 
 static SegOut prop_rk4(Ray& r, double rows[3][18], double zmax_in, double freq, bool per_step,
-                       double& tt, double& att) {
+                       double& tt, double& att, int* caustics) {
     const int eq = r.eq_cnt;
     const int length = int(r.cfg->s_max / r.cfg->ds_min);
     double s = 0.0, ds;
@@ -624,6 +625,14 @@ static SegOut prop_rk4(Ray& r, double rows[3][18], double zmax_in, double freq, 
     int k;
     for (k = 0; k < length - 1; k++) {
         o.zmax = std::max(o.zmax, cur[2]);
+        // Caustics as the write_caustics path counts them: sign changes of
+        // the Jacobian between consecutive rows 1..k-1 of a bounce
+        // (main.infraga.3d.cpp:448-480).
+        if (caustics && r.calc_amp && k >= 1) {
+            const double D = jacobian(r, cur);
+            if (k >= 2 && D * r.D_prev < 0.0) (*caustics)++;
+            r.D_prev = D;
+        }
         for (int i = 0; i < eq; i++) t0[i] = cur[i];
         update_refs(r, t0);
         ds = set_ds(r, t0);
@@ -670,7 +679,7 @@ using namespace orc::d3;
 
 extern "C" int orc_fan_3d(const char* met_path, const char* fmt, const orc_fan_cfg* cfg,
                           const double* theta_deg, const double* phi_deg, int n_rays,
-                          double* arrivals, int* n_arr, long long* steps) {
+                          double* arrivals, int* n_arr, long long* steps, double* aux) {
     static_assert(sizeof(orc_fan_cfg) > 0, "");
     Atmo A;
     if (!load_profile(met_path, fmt, cfg->reverse_winds != 0, A.P)) return -1;
@@ -693,10 +702,11 @@ extern "C" int orc_fan_3d(const char* met_path, const char* fmt, const orc_fan_c
         double z_src = std::max(cfg->src[2], topo_z(r, cfg->src[0], cfg->src[1]));
         set_initial(r, rows[1], cfg->src[0], cfg->src[1], z_src);
         double tt = 0.0, att = 0.0, zmax = A.z0;
+        int caustics = 0;
         long long st = 0;
         int na = 0;
         for (int bnc = 0; bnc <= cfg->bounces; bnc++) {
-            SegOut o = prop_rk4(r, rows, zmax, cfg->freq, cfg->write_rays != 0, tt, att);
+            SegOut o = prop_rk4(r, rows, zmax, cfg->freq, cfg->write_rays != 0, tt, att, &caustics);
             st += o.k;
             zmax = o.zmax;
             if (zmax < (A.z0 + cfg->turn_ht_min)) break;
@@ -713,6 +723,22 @@ extern "C" int orc_fan_3d(const char* met_path, const char* fmt, const orc_fan_c
             out[7] = zmax; out[8] = incl; out[9] = baz;
             out[10] = r.calc_amp ? 20.0 * log10(amp(r, sk)) : 0.0;
             out[11] = -2.0 * att;
+            if (aux) {
+                // Launch-angle sensitivity of the ground intercept, the
+                // expressions find_eigenray uses for its Newton step
+                // (geoac.eigenray.3d.cpp:334-348, flat ground).
+                double* ax = aux + ((size_t)ir * nb + na) * ORC_AUX_COLS;
+                double c_src = a_c(r, cfg->src[0], cfg->src[1], z_src);
+                double c_grnd = a_c(r, sk[0], sk[1], topo_z(r, sk[0], sk[1]));
+                double ds_dth = -c_src / c_grnd * sk[8] / sk[5];
+                double ds_dph = -c_src / c_grnd * sk[14] / sk[5];
+                double dx_dth = sk[6] + sk[3] * ds_dth, dy_dth = sk[7] + sk[4] * ds_dth;
+                double dx_dph = sk[12] + sk[3] * ds_dph, dy_dph = sk[13] + sk[4] * ds_dph;
+                ax[0] = r.calc_amp ? sqrt(dx_dth * dx_dth + dy_dth * dy_dth) : 0.0;
+                ax[1] = r.calc_amp ? sqrt(dx_dph * dx_dph + dy_dph * dy_dph) : 0.0;
+                ax[2] = r.calc_amp ? jacobian(r, sk) : 0.0;
+                ax[3] = caustics;
+            }
             na++;
             double nxt[18];
             set_refl(r, rows[0], rows[1], nxt);

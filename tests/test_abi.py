@@ -45,7 +45,7 @@ def test_status_strings():
 def test_invalid_arguments_rejected_without_device():
     L = ig.lib()
     n = ctypes.c_int()
-    assert L.iga_fan_run(None, None, None, None, 0, None, 0, ctypes.byref(n), None, None, None, None) == _lib.IGA_E_INVALID
+    assert L.iga_fan_run(None, None, None, None, 0, None, 0, ctypes.byref(n), None, None, None, None, None) == _lib.IGA_E_INVALID
     assert L.iga_atmo_load(None, b"zTuvdp", 0, None) == _lib.IGA_E_INVALID
 
 

@@ -1,0 +1,77 @@
+"""FP32-compensated fan (IGA_FP32C) against the FP64 reference: error bounds
+on arrivals whose FP64 values are stable at FP32 precision, counts of the
+arrivals outside that set, and of rays whose bounce / turning classification
+flips."""
+import numpy as np
+import pytest
+
+import infraga_b200 as ig
+from infraga_b200 import synth
+from tests._cases import (case_setup, fp32c_errors, fp64_stability, load_cases, match_arrivals, parse_golden,
+                          profile_path, worst_rows)
+
+pytestmark = pytest.mark.gpu
+
+CASES = {k: v for k, v in load_cases().items() if v["binary"] == "iga_ref_3d" and v["mode"] == "prop"}
+
+
+@pytest.fixture(scope="module")
+def dev():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    ig.lib()
+    return torch
+
+
+def ray_ids(rows, th, ph):
+    key = {(a, b): i for i, (a, b) in enumerate(zip(th, ph))}
+    return np.array([key[(r[0], r[1])] for r in rows], dtype=np.int64)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp32c_matches_reference_cases(dev, name):
+    """Against the reference's own FP64 output (golden fixtures)."""
+    c = CASES[name]
+    th, ph, p = case_setup(c["args"])
+    atmo = ig.Atmosphere.load(profile_path(c["seed"]))
+    base, stab = fp64_stability(ig, atmo, atmo.default_params(**p), th, ph)
+    ref, _ = parse_golden(name)
+    assert base["arrivals"].shape == ref.shape
+    r = ig.fan_run(atmo, atmo.default_params(**p, precision=ig.FP32C), th, ph)
+    a, b, st, flipped = match_arrivals(r["arrivals"], r["ray_index"].astype(np.int64), ref, ray_ids(ref, th, ph),
+                                       th.size, stab)
+    ok, err = fp32c_errors(a, b, st, calc_amp=p["calc_amp"])
+    print(name, "flips", flipped.size, err)
+    print("  worst range:", worst_rows(a, b, st, 3, 3))
+    print("  worst amp:", worst_rows(a, b, st, 10, 3))
+    assert flipped.size <= max(1, th.size // 100), f"classification flips on rays {flipped}"
+    assert ok, err
+    # over every matched arrival (stable or not), <= 1000 km and 5 bounces
+    assert err["range_km_p90"] <= 0.01 and err["time_s_p90"] <= 0.03, err
+
+
+def test_fp32c_full_fan_vs_fp64(dev):
+    """71,520-ray fan, 10 bounces, 2000 km: FP32C against FP64 on the GPU."""
+    th, ph = synth.fan_angles(0.5, 60.01, 0.1, 0, 357, 3)
+    atmo = ig.Atmosphere.load(profile_path(1))
+    kw = dict(bounces=10, rng_max=2000.0, write_rays=0)
+    r64, stab = fp64_stability(ig, atmo, atmo.default_params(**kw), th, ph)
+    r32 = ig.fan_run(atmo, atmo.default_params(**kw, precision=ig.FP32C), th, ph)
+    a, b, st, flipped = match_arrivals(r32["arrivals"], r32["ray_index"].astype(np.int64),
+                                       r64["arrivals"], r64["ray_index"].astype(np.int64), th.size, stab)
+    ok, err = fp32c_errors(a, b, st)
+    frac_flip = flipped.size / th.size
+    steps_rel = abs(r32["total_steps"] - r64["total_steps"]) / r64["total_steps"]
+    print("full fan fp32c vs fp64: flips", flipped.size, f"({100 * frac_flip:.3f}%)", err, "steps rel", steps_rel)
+    print("  worst range:", worst_rows(a, b, st, 3, 4))
+    print("  worst amp:", worst_rows(a, b, st, 10, 4))
+    assert frac_flip < 1e-3
+    assert steps_rel < 1e-4
+    # the one-sided perturbation check misses a few edge rays: at most 0.1%
+    # of the stable arrivals may fall outside the bounds
+    assert err["n_range_stable_violations"] <= 1e-3 * err["n_range_stable"], err
+    assert err["n_amp_stable_violations"] <= 1e-3 * err["n_amp_stable"], err
+    # distribution over every matched arrival of the 2000 km, 10-bounce fan
+    assert err["range_km_p50"] <= 0.005 and err["range_km_p90"] <= 0.015 and err["range_km_p99"] <= 0.05, err
+    assert err["time_s_p90"] <= 0.05 and err["amp_db_p90"] <= 0.1, err
