@@ -176,6 +176,34 @@ int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
                        double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
                        int* d_ray_status, double* d_arrival_aux, void* d_workspace, void* stream);
 
+/* Allocation-free form of iga_fan_run_device.  No counterpart in the
+ * reference (which has no GPU path); it exists for callers that must not
+ * allocate device memory themselves: applications that reserve their whole
+ * device budget up front and keep cudaMalloc off the request path (it can
+ * block and synchronise the device, which breaks their latency targets), and
+ * host frameworks whose own allocator owns all device memory, where a library
+ * allocation would bypass its accounting.  Inputs and outputs are the caller's
+ * device buffers exactly as for iga_fan_run_device; only the ray-queue scratch
+ * differs: instead of a caller workspace it uses a fixed
+ * IGA_FAN_STATIC_SCRATCH_BYTES array compiled into the library, which every
+ * device that loads the library keeps until the process exits.
+ *   - FP64 only (IGA_E_UNSUPPORTED for IGA_FP32C, whose absorption table is
+ *     built and uploaded on first use of a frequency).
+ *   - Returns IGA_E_INVALID when the fan's scratch need
+ *     (iga_fan_workspace_bytes()) exceeds IGA_FAN_STATIC_SCRATCH_BYTES.
+ *   - The first call on a device looks up that device's address of the array
+ *     (one-time set-up, serialised internally); make that first call before
+ *     any stream capture starts.
+ *   - All calls share the one array (the call clears it on `stream` before
+ *     launching), so calls whose work overlaps on the GPU race: issue them on
+ *     one stream or otherwise order them.
+ *   - Calls no cudaMalloc, cudaFree or other allocating routine. */
+#define IGA_FAN_STATIC_SCRATCH_BYTES 256
+int iga_fan_run_device_noalloc(iga_atmo_t atmo, const iga_fan_params* params,
+                               const double* d_theta_deg, const double* d_phi_deg, int n_rays,
+                               double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
+                               int* d_ray_status, double* d_arrival_aux, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

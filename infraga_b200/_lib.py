@@ -75,6 +75,7 @@ _SIGS = {
                          _P(_D)]),
     "iga_fan_workspace_bytes": (ctypes.c_size_t, []),
     "iga_fan_run_device": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "iga_fan_run_device_noalloc": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 

@@ -396,3 +396,49 @@ int iga_fan_run(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, 
 }
 
 }  // extern "C"
+
+// ---- allocation-free fan entry (iga_fan_run_device_noalloc) ----
+namespace {
+constexpr int kMaxStaticDevices = 64;
+// Ray-queue scratch for iga_fan_run_device_noalloc.  Host code must not use
+// this name as an address (on the host it only stands in for the symbol):
+// the per-device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_fan_static_scratch[IGA_FAN_STATIC_SCRATCH_BYTES];
+std::mutex g_static_mu;
+void* g_static_addr[kMaxStaticDevices] = {};
+}  // namespace
+
+extern "C" int iga_fan_run_device_noalloc(iga_atmo_t h, const iga_fan_params* p, const double* d_th,
+                                          const double* d_ph, int n_rays, double* d_arr, int* d_n,
+                                          long long* d_steps, int* d_status, double* d_aux, void* stream) {
+    if (!h) return IGA_E_INVALID;
+    int rc = validate(p, n_rays);
+    if (rc) return rc;
+    if (n_rays > 0 && (!d_th || !d_ph || !d_arr || !d_n || !d_steps)) return IGA_E_INVALID;
+    if (p->precision != IGA_FP64) {
+        g_cuda_err = "iga_fan_run_device_noalloc: FP64 only (FP32C builds its absorption table on first use)";
+        return IGA_E_UNSUPPORTED;
+    }
+    if (iga_fan_workspace_bytes() > IGA_FAN_STATIC_SCRATCH_BYTES) {
+        g_cuda_err = "iga_fan_run_device_noalloc: scratch need " + std::to_string(iga_fan_workspace_bytes()) +
+                     " bytes exceeds the static " + std::to_string(IGA_FAN_STATIC_SCRATCH_BYTES) + "-byte array";
+        return IGA_E_INVALID;
+    }
+    if (h->device < 0 || h->device >= kMaxStaticDevices) return IGA_E_UNSUPPORTED;
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    void* ws = nullptr;
+    {
+        // one-time, per device, with that device current
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_addr[h->device]) {
+            void* ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_fan_static_scratch);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fan_static_scratch)");
+            g_static_addr[h->device] = ptr;
+        }
+        ws = g_static_addr[h->device];
+    }
+    // run_device clears the queue counter on `stream` before the launch
+    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_aux, ws,
+                      static_cast<cudaStream_t>(stream));
+}
