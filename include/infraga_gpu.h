@@ -176,6 +176,49 @@ int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
                        double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
                        int* d_ray_status, double* d_arrival_aux, void* d_workspace, void* stream);
 
+/* ---- eigenray search ---- */
+
+/* One source-receiver pair of an eigenray search (km; receiver on the ground). */
+typedef struct iga_eig_pair {
+    double src[3];           /* source x, y, altitude */
+    double rcvr[2];          /* receiver x, y */
+} iga_eig_pair;
+
+/* Eigenray search settings: run_eig_search's locals and the geoac::eigenray
+ * globals (main.infraga.3d.cpp:779-791, geoac.eigenray.3d.cpp:21-28).
+ * fan carries the propagation settings (ds, s_max, limits, ground, frequency,
+ * absorption, precision); its bounces/calc_amp/write_rays/src are ignored. */
+typedef struct iga_eig_params {
+    iga_fan_params fan;
+    double incl_min, incl_max;   /* deg; search range (0.5, 45) */
+    double incl_step_min;        /* deg; geoac::dth_sml (0.001) */
+    double incl_step_max;        /* deg; geoac::dth_big (0.1) */
+    double damping;              /* geoac::damping (1e-3) */
+    double tolerance;            /* km; geoac::tolerance (0.1) */
+    double az_err_lim;           /* deg; az_dev_lim (2) */
+    int bnc_min, bnc_max;        /* bounce counts searched (0, 0) */
+    int iterations;              /* Newton iteration limit (25) */
+    int chunk;                   /* sweep inclinations traced per search per GPU round (0 = automatic) */
+} iga_eig_params;
+
+/* Defaults of run_eig_search after set_region (as iga_fan_params_default for fan). */
+int iga_eig_params_default(iga_atmo_t atmo, iga_eig_params* params);
+
+/* Replaces run_eig_search's search loop (src/main.infraga.3d.cpp:939-950):
+ * for every pair and every bounce count in [bnc_min, bnc_max], the inclination
+ * sweep with azimuth correction of geoac::est_eigenray
+ * (src/geoac/geoac.eigenray.3d.cpp:34-144) and the damped Newton refinement of
+ * geoac::find_eigenray (:146-371), all searches running together (every ray
+ * trace of a round is one GPU launch).  Output rows (IGA_ARRIVAL_COLS) are the
+ * reference's eigenray .arrivals.dat rows, ordered by pair, bounce count, then
+ * discovery; pair_index (nullable) gets each row's pair; total_steps
+ * (nullable) the RK4 steps of every trace.  Capacity/truncation as iga_fan_run.
+ * The reference's find_eigenray follows only the first reflection during its
+ * Newton iterations (an unconditional break, geoac.eigenray.3d.cpp:206) while
+ * its final trace and output use all bounces; that is reproduced. */
+int iga_eig_run(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_pair* pairs, int n_pairs,
+                double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps);
+
 /* Allocation-free form of iga_fan_run_device.  No counterpart in the
  * reference (which has no GPU path); it exists for callers that must not
  * allocate device memory themselves: applications that reserve their whole

@@ -47,6 +47,19 @@ class FanParams(ctypes.Structure):
     ]
 
 
+class EigParams(ctypes.Structure):
+    """Mirror of iga_eig_params."""
+    _fields_ = [("fan", FanParams), ("incl_min", ctypes.c_double), ("incl_max", ctypes.c_double),
+                ("incl_step_min", ctypes.c_double), ("incl_step_max", ctypes.c_double),
+                ("damping", ctypes.c_double), ("tolerance", ctypes.c_double), ("az_err_lim", ctypes.c_double),
+                ("bnc_min", ctypes.c_int), ("bnc_max", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("chunk", ctypes.c_int)]
+
+
+class EigPair(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_double * 3), ("rcvr", ctypes.c_double * 2)]
+
+
 class Profile(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("z", ctypes.POINTER(ctypes.c_double)), ("c", ctypes.POINTER(ctypes.c_double)),
                 ("u", ctypes.POINTER(ctypes.c_double)), ("v", ctypes.POINTER(ctypes.c_double)),
@@ -76,6 +89,8 @@ _SIGS = {
     "iga_fan_workspace_bytes": (ctypes.c_size_t, []),
     "iga_fan_run_device": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "iga_fan_run_device_noalloc": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "iga_eig_params_default": (_I, [_VP, _P(EigParams)]),
+    "iga_eig_run": (_I, [_VP, _P(EigParams), _P(EigPair), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL)]),
 }
 
 
@@ -204,6 +219,44 @@ def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, with_aux: b
     if with_aux:
         out["aux"] = aux[:m]
     return out
+
+
+def eig_params(atmo: Atmosphere, **overrides) -> EigParams:
+    """iga_eig_params with the run_eig_search defaults; keyword overrides go to
+    the eigen fields or, for propagation settings, to params.fan."""
+    p = EigParams()
+    _check(lib().iga_eig_params_default(atmo.handle, ctypes.byref(p)), "iga_eig_params_default")
+    eig_fields = {f for f, _ in EigParams._fields_}
+    for k, v in overrides.items():
+        if k in eig_fields:
+            setattr(p, k, v)
+        else:
+            setattr(p.fan, k, v)
+    return p
+
+
+def eig_run(atmo: Atmosphere, params: EigParams, pairs):
+    """Eigenray search for a list of ((sx, sy, sz), (rx, ry)) pairs.  Returns
+    a dict with ``eigenrays`` [n, 12] (the reference's eigenray arrival rows),
+    ``pair_index`` and ``total_steps``."""
+    arr = (EigPair * max(1, len(pairs)))()
+    for i, (src, rcv) in enumerate(pairs):
+        arr[i].src = (_D * 3)(*src)
+        arr[i].rcvr = (_D * 2)(*rcv)
+    cap = max(16, 64 * len(pairs) * (params.bnc_max - params.bnc_min + 1))
+    while True:
+        out = np.zeros((cap, ARRIVAL_COLS), dtype=np.float64)
+        idx = np.zeros(cap, dtype=np.int32)
+        n_out = _I()
+        tot = _LL()
+        rc = lib().iga_eig_run(atmo.handle, ctypes.byref(params), arr, len(pairs), _dptr(out), cap,
+                               ctypes.byref(n_out), idx.ctypes.data_as(_P(_I)), ctypes.byref(tot))
+        if rc == IGA_E_TRUNCATED:
+            cap = n_out.value
+            continue
+        _check(rc, "iga_eig_run")
+        m = n_out.value
+        return {"eigenrays": out[:m], "pair_index": idx[:m], "total_steps": int(tot.value)}
 
 
 def fan_workspace_bytes() -> int:

@@ -16,26 +16,9 @@
 
 using iga::StratProfile;
 
-struct iga_atmo_s {
-    int device = 0;
-    StratProfile prof;
-    double* d_knots = nullptr;
-    // stream of the host-buffer entry points: one per handle, so calls on
-    // different atmospheres from different host threads overlap on the GPU
-    cudaStream_t stream = nullptr;
-    // reusable device buffers of the host-buffer entry points
-    std::mutex mu;
-    void* d_buf = nullptr;
-    size_t d_buf_bytes = 0;
-    // FP32-compensated path: FP32 knot table and alpha(z) tables per frequency
-    float* d_knots_f = nullptr;
-    std::mutex alpha_mu;
-    struct AlphaTab { float* d = nullptr; int n = 0; double z0 = 0.0, inv_h = 0.0; };
-    std::map<double, AlphaTab> alpha;   // kept until destroy (launches may still read them)
-};
+#include "handle.h"
 
-namespace {
-
+namespace iga_internal {
 thread_local std::string g_cuda_err;
 thread_local std::string g_err;
 
@@ -45,12 +28,11 @@ int cuda_fail(cudaError_t e, const char* what) {
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return IGA_E_NODEVICE;
     return IGA_E_CUDA;
 }
+}  // namespace iga_internal
 
-#define IGA_CUDA(call, what)                         \
-    do {                                             \
-        cudaError_t e_ = (call);                     \
-        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
-    } while (0)
+using namespace iga_internal;
+
+namespace {
 
 int upload(iga_atmo_s* h) {
     int dev;
@@ -134,6 +116,10 @@ void bl_host(double z, double z0, double bl, double& sc, double& dsc_z) {
     }
 }
 
+}  // namespace
+
+namespace iga_internal {
+
 int validate(const iga_fan_params* p, int n_rays) {
     if (!p || n_rays < 0) return IGA_E_INVALID;
     if (p->geometry != IGA_GEOM_3D) return IGA_E_UNSUPPORTED;
@@ -184,6 +170,10 @@ int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     a.sb.x2 = std::pow(10.0, -3.3979);
     return IGA_OK;
 }
+
+}  // namespace iga_internal
+
+namespace {
 
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,

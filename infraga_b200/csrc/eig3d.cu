@@ -1,0 +1,499 @@
+// Eigenray search for the 3D stratified solver on flat ground.
+//
+// Every (source-receiver pair, bounce count) search is an independent chain
+// of ray traces whose control flow depends on each trace's result; the host
+// runs all chains as state machines that replay the reference's
+// est_eigenray / find_eigenray logic exactly (geoac.eigenray.3d.cpp:34-371),
+// and every round collects the traces all chains need next into one launch
+// of trace3d_fp64_kernel.  While a chain sweeps inclinations with a fixed
+// step, the angles it will try next are known in advance, so it submits a
+// chunk of them at once and keeps the results up to the first bracket.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fan3d_common.cuh"
+#include "handle.h"
+
+namespace iga {
+namespace {
+
+struct TraceReq {
+    double x0, y0;       // source position
+    double theta, phi;   // launch angles [rad] (geoac::theta, geoac::phi)
+    int n_seg;           // prop_rk4 segments to trace (bounces + 1)
+    int flags;
+};
+enum : int { kStopOnEscape = 1, kRecord = 2 };
+
+struct TraceRes {
+    double y[12];        // state at the last row (12-state layout)
+    double rc[6];        // nu_x, nu_y, mu_th_x, mu_th_y, mu_ph_x, mu_ph_y
+    double tt, att, zmax, amp_db, incl, baz;
+    long long steps;
+    int escaped;         // the last traced segment left the region
+    int pad;
+};
+
+constexpr int kTraceThreads = 128;
+
+// One request per thread: launch, integrate n_seg prop_rk4 segments with
+// flat-ground reflections between them, return the last row.  Record mode
+// accumulates travel time / absorption per step and the turning height over
+// rows 1..k-1 of each segment starting from 0, as find_eigenray's final trace
+// does (geoac.eigenray.3d.cpp:229-262).
+template <bool AMP>
+__global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __grid_constant__ Fan3DArgs a,
+                                                                    const TraceReq* __restrict__ reqs,
+                                                                    TraceRes* __restrict__ out, int n) {
+    constexpr int N = Dim<AMP>::n;
+    extern __shared__ double s_mem[];
+    double* s_prev = s_mem;
+    double* s_tab = s_mem + N * kTraceThreads;
+    const int tot = a.n_knots * kStride;
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
+    __syncthreads();
+    const double* tab = s_tab;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double* prev = s_prev + threadIdx.x;
+    const TraceReq q = reqs[r];
+    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+    const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
+
+    double y[N];
+    RayConst rc;
+    ray_init<AMP>(a, q.theta, q.phi, y, rc);
+    y[0] = q.x0;
+    y[1] = q.y0;
+    int seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+    double tt = 0.0, att = 0.0, zmax = 0.0;
+    long long steps = 0;
+    double acc[N];
+    bool esc = false;
+    for (int sg = 0; sg < q.n_seg; sg++) {
+        double s = 0.0, pt = 0.0, pa = 0.0;
+        int kb = 0;
+        bool capped = false;
+#pragma unroll
+        for (int i = 0; i < N; i++) prev[i * kTraceThreads] = y[i];
+        while (true) {
+            if (record && kb >= 1) zmax = fmax(zmax, y[2]);
+            double ds = a.ds_max;
+            if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - a.z0) / 0.2);
+            s += ds;
+            double stg[N], f[N];
+            rhs<AMP>(tab, a, seg, y, rc, f);
+#pragma unroll
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
+            rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
+            rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
+            rhs<AMP>(tab, a, seg, stg, rc, f);
+#pragma unroll
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+            kb++;
+            if (record) {
+                double dt, da;
+                seg_increment(tab, a, seg, y, acc, rc, dt, da);
+                tt += pt; att += pa; pt = dt; pa = da;
+            }
+            const double rx = acc[0] - q.x0, ry = acc[1] - q.y0;
+            esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) ||
+                  (acc[0] < a.x_min) || (acc[1] > a.y_max) || (acc[1] < a.y_min) || (acc[2] > a.alt_max);
+            const bool gnd = !esc && (acc[2] < a.z0);
+            if (!esc && !gnd) {
+                if (kb >= a.length - 1) { capped = true; esc = true; }
+                else if (!isfinite(acc[2]) || !isfinite(acc[3])) esc = true;
+            }
+            if (!esc && !gnd) {
+#pragma unroll
+                for (int i = 0; i < N; i++) { prev[i * kTraceThreads] = y[i]; y[i] = acc[i]; }
+                continue;
+            }
+            break;
+        }
+        steps += capped ? a.length : kb;
+        if (sg == q.n_seg - 1 || (esc && stop)) break;
+        // reflection from rows k-2 (prev) and k-1 (y), flat ground
+        const double dz_grnd = a.z0 - y[2];
+        const double dz_k = y[2] - prev[2 * kTraceThreads];
+        double p[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kTraceThreads]) / dz_k * dz_grnd;
+        y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
+        if (AMP) {
+            y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
+            y[8] = p[8]; y[9] = p[9]; y[10] = -p[10];
+            const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
+            const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
+            const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + rc.nx * a.duz_g + rc.ny * a.dvz_g);
+            y[7] = -p[7] + (-2.0 * dnuz_ds) * ds0_dth;
+            y[11] = -p[11] + (-2.0 * dnuz_ds) * ds0_dph;
+        }
+    }
+    TraceRes& o = out[r];
+#pragma unroll
+    for (int i = 0; i < 12; i++) o.y[i] = i < N ? acc[i] : 0.0;
+    o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
+    o.steps = steps;
+    o.escaped = esc ? 1 : 0;
+    if (record) {
+        o.tt = tt; o.att = att; o.zmax = zmax;
+        o.amp_db = AMP ? amp_db(tab, a, seg, acc, rc, q.theta, q.phi, nullptr) : 0.0;
+        // arrival inclination with c at the (clamped) below-ground altitude,
+        // as find_eigenray writes it (geoac.eigenray.3d.cpp:265)
+        const double ze = fmin(fmax(acc[2], a.z_lo), a.z_hi);
+        seg = seg_walk(tab, a.n_knots, ze, seg);
+        const double* r0 = tab + seg * kStride;
+        const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
+        o.incl = -asin(c_k / a.c0 * acc[3]) * (180.0 / kPi);
+        double baz = 90.0 - atan2(-rc.ny, -rc.nx) * (180.0 / kPi);
+        while (baz > 180.0) baz -= 360.0;
+        while (baz < -180.0) baz += 360.0;
+        o.baz = baz;
+    }
+}
+
+template <bool AMP>
+cudaError_t launch_trace(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    auto kern = trace3d_fp64_kernel<AMP>;
+    const size_t smem = (size_t)Dim<AMP>::n * kTraceThreads * sizeof(double) + (size_t)a.n_knots * kStride * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<(n + kTraceThreads - 1) / kTraceThreads, kTraceThreads, smem, st>>>(a, d_req, d_res, n);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- host side
+
+constexpr double kRad = kPi / 180.0;
+
+struct Chain {
+    int pair = 0, nb = 0;
+    double sx = 0, sy = 0, rx = 0, ry = 0, rcvr_rng = 0, rcvr_az = 0;
+    enum Phase { kEst, kNewton, kRecordTrace, kDone } phase = kEst;
+    double theta_start = 0;
+    // est_eigenray state
+    double th_min = 0, th_max = 0, dth = 0, dph = 0, r = 0, r_prev = 0, phi = 0, th = 0, th_next = 0;
+    int iterations = 0;
+    bool th_max_reached = false;
+    // find_eigenray state (dth/dph start at 0: the reference leaves them
+    // uninitialised until the first Newton update)
+    double theta = 0, phi_n = 0, dr_prev = 0, step_sc = 1, ndth = 0, ndph = 0;
+    int n = 0;
+    // requests of the current round
+    std::vector<double> sweep;   // inclinations submitted (est phase)
+    int req0 = 0;                // first request index in its batch
+    std::vector<std::vector<double>> rows;
+};
+
+struct Settings {
+    double theta_max, dth_big, dth_sml, damping, tolerance, az_err_lim, rng_max;
+    int iterations, chunk;
+};
+
+double mod_dth(const Settings& S, double dr, double dr_dtheta) {   // geoac::mod_dth (geoac.eigenray.3d.cpp:32)
+    return S.dth_big - (S.dth_big - S.dth_sml) * exp(-1.0 / 2.0 * pow(dr / dr_dtheta, 2));
+}
+
+void est_begin(Chain& c, const Settings& S, double theta_start) {
+    c.phase = Chain::kEst;
+    c.theta_start = theta_start;
+    c.th_min = theta_start;
+    c.th_max = S.theta_max;
+    c.iterations = 0;
+    c.dth = S.dth_big;
+    c.dph = 100.0;
+    c.phi = c.rcvr_az;
+    c.th_max_reached = false;
+    c.r = c.rcvr_rng;
+    c.r_prev = c.rcvr_rng;
+    c.th = c.th_min;
+}
+
+// After est_eigenray (and find_eigenray, if it ran): run_eig_search's
+// theta_start = theta_next and loop condition (main.infraga.3d.cpp:943-949).
+void search_continue(Chain& c, const Settings& S) {
+    const double ts = c.th_next;
+    if (ts < S.theta_max) est_begin(c, S, ts);
+    else c.phase = Chain::kDone;
+}
+
+void newton_begin(Chain& c, double th_est, double ph_est) {
+    c.phase = Chain::kNewton;
+    c.theta = th_est;
+    c.phi_n = ph_est;
+    c.dr_prev = 10000.0;
+    c.step_sc = 1.0;
+    c.ndth = 0.0;
+    c.ndph = 0.0;
+    c.n = 0;
+}
+
+// One body of est_eigenray's inclination loop for the trace at c.th.
+// Returns true when the chain leaves the sweep (later speculative results
+// are then discarded).
+bool est_step(Chain& c, const Settings& S, const TraceRes& res) {
+    if (c.th + c.dth >= c.th_max) c.th_max_reached = true;
+    const double theta = c.th;
+    c.r = sqrt(pow(res.y[0] - c.sx, 2) + pow(res.y[1] - c.sy, 2));
+    if (res.escaped) c.r = S.rng_max;
+    if (((c.r - c.rcvr_rng) * (c.r_prev - c.rcvr_rng) <= 0.0) && (c.r < S.rng_max) && (c.r_prev < S.rng_max) &&
+        (c.th > c.th_min)) {
+        if (c.iterations == 0) c.th_next = c.th;
+        c.dph = atan2(res.y[1] - c.sy, res.y[0] - c.sx) * (180.0 / kPi);
+        c.dph -= atan2(c.ry - c.sy, c.rx - c.sx) * (180.0 / kPi);
+        while (c.dph > 180.0) c.dph -= 360.0;
+        while (c.dph < -180.0) c.dph += 360.0;
+        if (fabs(c.dph) < S.az_err_lim) {
+            newton_begin(c, theta - c.dth, c.phi);
+            return true;
+        }
+        c.phi -= c.dph * (kPi / 180.0) * 0.9;
+        c.th_min = std::max(c.th - 5.0 * (kPi / 180.0), c.th_min);
+        c.iterations++;
+        // break out of the inclination loop
+        if (c.th_max_reached) { c.th_next = c.th_max; search_continue(c, S); return true; }
+        if (!(fabs(c.dph * (180.0 / kPi)) > S.az_err_lim && c.iterations < 5)) { search_continue(c, S); return true; }
+        c.r = c.rcvr_rng; c.r_prev = c.rcvr_rng; c.th = c.th_min;
+        return true;
+    }
+    if (c.iterations >= 2) c.dth = mod_dth(S, c.r - c.rcvr_rng, (c.r - c.r_prev) / (2.0 * c.dth));
+    c.r_prev = c.r;
+    c.th += c.dth;
+    if (!(c.th <= c.th_max)) {   // loop ran out (th_max_reached is set on its last pass)
+        if (c.th_max_reached) { c.th_next = c.th_max; search_continue(c, S); return true; }
+        if (!(fabs(c.dph * (180.0 / kPi)) > S.az_err_lim && c.iterations < 5)) { search_continue(c, S); return true; }
+        c.r = c.rcvr_rng; c.r_prev = c.rcvr_rng; c.th = c.th_min;
+        return true;
+    }
+    return false;
+}
+
+// One iteration of find_eigenray's Newton loop on the trace at (theta, phi).
+void newton_step(Chain& c, const Settings& S, const Fan3DArgs& a, const TraceRes& res) {
+    if (res.escaped) {
+        c.theta -= c.ndth * c.step_sc;
+        c.phi_n -= c.ndph * c.step_sc;
+        c.step_sc /= 2.0;
+    } else {
+        const double x = res.y[0], dx = c.rx - x;
+        const double y = res.y[1], dy = c.ry - y;
+        const double dr = sqrt(pow(dx, 2) + pow(dy, 2));
+        if (dr < S.tolerance) {
+            c.phase = Chain::kRecordTrace;
+            return;
+        } else if (c.n > 0 && dr > c.dr_prev) {
+            c.theta -= c.ndth * c.step_sc;
+            c.phi_n -= c.ndph * c.step_sc;
+            c.step_sc /= 2.0;
+        } else {
+            c.step_sc = std::min(1.0, c.step_sc * 1.25);
+            const double c_src = a.c0, c_grnd = a.c_gnd;
+            const double nx = res.rc[0], ny = res.rc[1], nz = res.y[3];
+            const double ds_dth = -c_src / c_grnd * res.y[6] / nz;
+            const double ds_dph = -c_src / c_grnd * res.y[10] / nz;
+            const double dx_dth = res.y[4] + nx * ds_dth, dy_dth = res.y[5] + ny * ds_dth;
+            const double dx_dph = res.y[8] + nx * ds_dph, dy_dph = res.y[9] + ny * ds_dph;
+            const double det = pow(1.0 + S.damping, 2) * (dx_dth * dy_dph - dx_dph * dy_dth);
+            c.ndth = ((1.0 + S.damping) * dy_dph * dx - dx_dph * dy) / det;
+            c.ndph = ((1.0 + S.damping) * dx_dth * dy - dy_dth * dx) / det;
+            c.theta += c.ndth * c.step_sc;
+            c.phi_n += c.ndph * c.step_sc;
+            c.dr_prev = dr;
+        }
+    }
+    if (sqrt(c.ndth * c.ndth + c.ndph * c.ndph) * c.step_sc < 1.0e-12) { search_continue(c, S); return; }
+    c.n++;
+}
+
+}  // namespace
+}  // namespace iga
+
+using namespace iga;
+using namespace iga_internal;
+
+extern "C" int iga_eig_params_default(iga_atmo_t h, iga_eig_params* p) {
+    if (!h || !p) return IGA_E_INVALID;
+    memset(p, 0, sizeof(*p));
+    int rc = iga_fan_params_default(h, &p->fan);
+    if (rc) return rc;
+    p->incl_min = 0.5; p->incl_max = 45.0;
+    p->incl_step_min = 0.001; p->incl_step_max = 0.1;
+    p->damping = 1.0e-3; p->tolerance = 0.1; p->az_err_lim = 2.0;
+    p->bnc_min = 0; p->bnc_max = 0;
+    p->iterations = 25;
+    p->chunk = 0;
+    return IGA_OK;
+}
+
+extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs,
+                           double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps) {
+    if (!h || !P || !n_out || n_pairs < 0 || (n_pairs > 0 && !pairs) || (cap > 0 && !eigenrays)) return IGA_E_INVALID;
+    *n_out = 0;
+    if (total_steps) *total_steps = 0;
+    iga_fan_params fp = P->fan;
+    fp.geometry = IGA_GEOM_3D;
+    fp.bounces = 0;
+    fp.calc_amp = 1;
+    fp.write_rays = 1;
+    int rc = validate(&fp, 1);
+    if (rc) return rc;
+    if (fp.precision != IGA_FP64) return IGA_E_UNSUPPORTED;
+    if (P->bnc_min < 0 || P->bnc_max < P->bnc_min || P->iterations < 0 || !(P->tolerance > 0.0) ||
+        !(P->incl_step_max > 0.0) || !(P->incl_step_min > 0.0) || !(P->incl_max > P->incl_min))
+        return IGA_E_INVALID;
+    if (n_pairs == 0) return IGA_OK;
+    for (int i = 1; i < n_pairs; i++)
+        if (pairs[i].src[2] != pairs[0].src[2]) {
+            g_cuda_err = "iga_eig_run: all pairs of one call must share the source altitude";
+            return IGA_E_UNSUPPORTED;
+        }
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    fp.src[0] = 0.0; fp.src[1] = 0.0; fp.src[2] = pairs[0].src[2];
+    Fan3DArgs a;
+    rc = build_args(h, &fp, a);
+    if (rc) return rc;
+
+    Settings S;
+    S.theta_max = P->incl_max * (kPi / 180.0);
+    S.dth_big = P->incl_step_max * (kPi / 180.0);
+    S.dth_sml = P->incl_step_min * (kPi / 180.0);
+    S.damping = P->damping; S.tolerance = P->tolerance; S.az_err_lim = P->az_err_lim;
+    S.rng_max = fp.rng_max; S.iterations = P->iterations; S.chunk = P->chunk;
+    const double theta_min = P->incl_min * (kPi / 180.0);
+
+    std::vector<Chain> chains;
+    for (int ip = 0; ip < n_pairs; ip++) {
+        for (int nb = P->bnc_min; nb <= P->bnc_max; nb++) {
+            Chain c;
+            c.pair = ip; c.nb = nb;
+            c.sx = pairs[ip].src[0]; c.sy = pairs[ip].src[1];
+            c.rx = pairs[ip].rcvr[0]; c.ry = pairs[ip].rcvr[1];
+            c.rcvr_rng = sqrt(pow(c.rx - c.sx, 2) + pow(c.ry - c.sy, 2));
+            c.rcvr_az = atan2(c.ry - c.sy, c.rx - c.sx);
+            if (theta_min < S.theta_max) est_begin(c, S, theta_min);
+            else c.phase = Chain::kDone;
+            chains.push_back(std::move(c));
+        }
+    }
+
+    cudaStream_t st = h->stream;
+    TraceReq* d_req = nullptr;
+    TraceRes* d_res = nullptr;
+    size_t cap_req = 0;
+    long long steps_tot = 0;
+    auto fail = [&](int code) { if (d_req) cudaFree(d_req); if (d_res) cudaFree(d_res); return code; };
+
+    std::vector<TraceReq> req6, req18;
+    std::vector<TraceRes> res6, res18;
+    while (true) {
+        req6.clear(); req18.clear();
+        int sweeping = 0;
+        for (auto& c : chains) if (c.phase == Chain::kEst && c.iterations < 2) sweeping++;
+        int chunk = S.chunk > 0 ? S.chunk : std::max(8, std::min(128, sweeping > 0 ? 262144 / sweeping : 128));
+        for (auto& c : chains) {
+            // find_eigenray gives up after `iterations` Newton steps
+            if (c.phase == Chain::kNewton && c.n >= S.iterations) search_continue(c, S);
+            c.sweep.clear();
+            if (c.phase == Chain::kEst) {
+                c.req0 = (int)req6.size();
+                // with a fixed step the next inclinations are known: submit a chunk
+                const int m = c.iterations < 2 ? chunk : 1;
+                double th = c.th;
+                for (int j = 0; j < m && th <= c.th_max; j++) {
+                    c.sweep.push_back(th);
+                    req6.push_back({c.sx, c.sy, th, c.phi, c.nb + 1, kStopOnEscape});
+                    th += c.dth;
+                }
+            } else if (c.phase == Chain::kNewton) {
+                c.req0 = (int)req18.size();
+                req18.push_back({c.sx, c.sy, c.theta, c.phi_n, 1 + std::min(c.nb, 1), kStopOnEscape});
+            } else if (c.phase == Chain::kRecordTrace) {
+                c.req0 = (int)req18.size();
+                req18.push_back({c.sx, c.sy, c.theta, c.phi_n, c.nb + 1, kRecord});
+            }
+        }
+        if (req6.empty() && req18.empty()) break;
+        const size_t need = std::max(req6.size(), req18.size());
+        if (need > cap_req) {
+            if (d_req) cudaFree(d_req);
+            if (d_res) cudaFree(d_res);
+            d_req = nullptr; d_res = nullptr;
+            cap_req = std::max(need, cap_req * 2);
+            cudaError_t e1 = cudaMalloc(&d_req, 2 * cap_req * sizeof(TraceReq));
+            cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc(&d_res, 2 * cap_req * sizeof(TraceRes)) : e1;
+            if (e2 != cudaSuccess) return fail(cuda_fail(e2, "cudaMalloc(eigen traces)"));
+        }
+        TraceReq* d_req18 = d_req + cap_req;
+        TraceRes* d_res18 = d_res + cap_req;
+        cudaError_t e = cudaSuccess;
+        if (!req6.empty()) {
+            e = cudaMemcpyAsync(d_req, req6.data(), req6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = launch_trace<false>(a, d_req, d_res, (int)req6.size(), st);
+        }
+        if (e == cudaSuccess && !req18.empty()) {
+            e = cudaMemcpyAsync(d_req18, req18.data(), req18.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = launch_trace<true>(a, d_req18, d_res18, (int)req18.size(), st);
+        }
+        res6.resize(req6.size());
+        res18.resize(req18.size());
+        if (e == cudaSuccess && !req6.empty())
+            e = cudaMemcpyAsync(res6.data(), d_res, res6.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && !req18.empty())
+            e = cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
+        for (auto& r : res6) steps_tot += r.steps;
+        for (auto& r : res18) steps_tot += r.steps;
+
+        for (auto& c : chains) {
+            if (c.phase == Chain::kEst && !c.sweep.empty()) {
+                for (size_t j = 0; j < c.sweep.size(); j++) {
+                    if (est_step(c, S, res6[c.req0 + j])) break;
+                }
+            } else if (c.phase == Chain::kNewton) {
+                newton_step(c, S, a, res18[c.req0]);
+            } else if (c.phase == Chain::kRecordTrace) {
+                const TraceRes& t = res18[c.req0];
+                std::vector<double> row(IGA_ARRIVAL_COLS);
+                row[0] = c.theta * (180.0 / kPi);
+                row[1] = 90.0 - c.phi_n * (180.0 / kPi);
+                row[2] = c.nb;
+                row[3] = t.y[0];
+                row[4] = t.y[1];
+                row[5] = t.tt;
+                row[6] = sqrt(pow(t.y[0] - c.sx, 2) + pow(t.y[1] - c.sy, 2)) / t.tt;
+                row[7] = t.zmax;
+                row[8] = t.incl;
+                row[9] = t.baz;
+                row[10] = t.amp_db;
+                row[11] = -2.0 * t.att;
+                c.rows.push_back(std::move(row));
+                search_continue(c, S);
+            }
+        }
+    }
+    if (d_req) cudaFree(d_req);
+    if (d_res) cudaFree(d_res);
+
+    int w = 0;
+    for (auto& c : chains) {
+        for (auto& row : c.rows) {
+            if (w < cap) {
+                memcpy(eigenrays + (size_t)w * IGA_ARRIVAL_COLS, row.data(), IGA_ARRIVAL_COLS * sizeof(double));
+                if (pair_index) pair_index[w] = c.pair;
+            }
+            w++;
+        }
+    }
+    *n_out = w;
+    if (total_steps) *total_steps = steps_tot;
+    return w > cap ? IGA_E_TRUNCATED : IGA_OK;
+}

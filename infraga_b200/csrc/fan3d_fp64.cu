@@ -31,148 +31,7 @@ namespace {
 #define IGA_FAN_MINB 3
 #endif
 constexpr int kThreads = IGA_FAN_THREADS;
-constexpr double kBlCutoffKm = 40.0;
 
-// Evolving state: 0 x, 1 y, 2 z, 3 nu_z, 4-6 X_th, 7 mu_th_z, 8-10 X_ph, 11 mu_ph_z.
-template <bool AMP> struct Dim { static constexpr int n = AMP ? 12 : 4; };
-
-
-// Right-hand side of the ray (and, with AMP, auxiliary) equations at state y:
-// update_refs (geoac.eqset.3d.strat.cpp:225-328) + eval_src_eq (:333-389)
-// with atmo::calc_uvw (atmo_state.3d.strat.cpp:462-734) on flat ground.
-template <bool AMP>
-__device__ __forceinline__ void rhs(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
-                                    const double* y, const RayConst& rc, double* f) {
-    const double z = y[2];
-    const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
-    seg = seg_walk(tab, a.n_knots, ze, seg);
-    const double* r0 = tab + seg * kStride;
-    const Cubic q = cubic_at(r0, ze);
-    double c, cz, czz = 0.0, u0, u0z, u0zz = 0.0, v0, v0z, v0zz = 0.0;
-    if (AMP) {
-        cubic_f2(r0, q, 2, c, cz, czz);
-        cubic_f2(r0, q, 4, u0, u0z, u0zz);
-        cubic_f2(r0, q, 6, v0, v0z, v0zz);
-    } else {
-        cubic_f1(r0, q, 2, c, cz);
-        cubic_f1(r0, q, 4, u0, u0z);
-        cubic_f1(r0, q, 6, v0, v0z);
-    }
-    // No-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-(z-zg)/bl).
-    // The reference evaluates X at every altitude; more than 40 km above the
-    // ground X < 1e-173, below half an ulp of every term it is added to
-    // (S rounds to 1, the X-terms of S' and S'' vanish against the spline
-    // derivatives), so X = 0 there gives the same doubles without the exp.
-    const double hz = z - a.z0;
-    const double Xb = hz < kBlCutoffKm ? exp(-hz * a.inv_bl) : 0.0;
-    const double opX = 1.0 + Xb;
-    const double iop = 1.0 / opX;
-    const double sc0 = (1.0 - Xb) * iop;
-    const double dX2 = -Xb * a.inv_bl;
-    const double dsc2 = -2.0 * dX2 * (iop * iop);
-    const double u = u0 * sc0, v = v0 * sc0;
-    const double uz = u0z * sc0 + u0 * dsc2;
-    const double vz = v0z * sc0 + v0 * dsc2;
-
-    const double nz = y[3];
-    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nz * nz);
-    const double inum = 1.0 / num;
-    const double cgx = c * rc.nx * inum + u;
-    const double cgy = c * rc.ny * inum + v;
-    const double cgz = c * nz * inum;
-    const double cgm = sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
-    const double icg = 1.0 / cgm;
-    f[0] = cgx * icg;
-    f[1] = cgy * icg;
-    f[2] = cgz * icg;
-    const double Kz = num * cz + rc.nx * uz + rc.ny * vz;
-    f[3] = -icg * Kz;
-    if (AMP) {
-        const double ddX22 = Xb * (a.inv_bl * a.inv_bl);
-        const double ddsc22 = -2.0 * (ddX22 * (iop * iop) - 2.0 * dX2 * dX2 * (iop * iop * iop));
-        const double uzz = u0zz * sc0 + 2.0 * u0z * dsc2 + u0 * ddsc22;
-        const double vzz = v0zz * sc0 + 2.0 * v0z * dsc2 + v0 * ddsc22;
-        const double Xtz = y[6], Xpz = y[10], mtz = y[7], mpz = y[11];
-        const double dc3 = Xtz * cz, dc4 = Xpz * cz;
-        const double du3 = Xtz * uz, du4 = Xpz * uz;
-        // The reference adds the azimuth variation of v into dv[3] and
-        // leaves dv[4] at zero (geoac.eqset.3d.strat.cpp:298).
-        const double dv3 = Xtz * vz + Xpz * vz;
-        const double dnu0 = (rc.nx * rc.mtx + rc.ny * rc.mty + nz * mtz) * inum;
-        const double dnu1 = (rc.nx * rc.mpx + rc.ny * rc.mpy + nz * mpz) * inum;
-        const double cin = c * inum, cin2 = cin * inum;
-        const double g0x = rc.nx * inum * dc3 + cin * rc.mtx - cin2 * rc.nx * dnu0 + du3;
-        const double g0y = rc.ny * inum * dc3 + cin * rc.mty - cin2 * rc.ny * dnu0 + dv3;
-        const double g0z = nz * inum * dc3 + cin * mtz - cin2 * nz * dnu0;
-        const double g1x = rc.nx * inum * dc4 + cin * rc.mpx - cin2 * rc.nx * dnu1 + du4;
-        const double g1y = rc.ny * inum * dc4 + cin * rc.mpy - cin2 * rc.ny * dnu1;
-        const double g1z = nz * inum * dc4 + cin * mpz - cin2 * nz * dnu1;
-        const double dm0 = (cgx * g0x + cgy * g0y + cgz * g0z) * icg;
-        const double dm1 = (cgx * g1x + cgy * g1y + cgz * g1z) * icg;
-        const double icg2 = icg * icg;
-        f[4] = g0x * icg - cgx * icg2 * dm0;
-        f[5] = g0y * icg - cgy * icg2 * dm0;
-        f[6] = g0z * icg - cgz * icg2 * dm0;
-        f[8] = g1x * icg - cgx * icg2 * dm1;
-        f[9] = g1y * icg - cgy * icg2 * dm1;
-        f[10] = g1z * icg - cgz * icg2 * dm1;
-        f[7] = dm0 * icg2 * Kz - icg * (dnu0 * cz + num * (Xtz * czz) + rc.mtx * uz + rc.mty * vz + rc.nx * (Xtz * uzz) + rc.ny * (Xtz * vzz));
-        f[11] = dm1 * icg2 * Kz - icg * (dnu1 * cz + num * (Xpz * czz) + rc.mpx * uz + rc.mpy * vz + rc.nx * (Xpz * uzz) + rc.ny * (Xpz * vzz));
-    }
-}
-
-// Travel-time and absorption increments of the segment y0 -> y1, evaluated at
-// the segment midpoint (travel_time :486-511, atten :688-699, SB_alpha).
-__device__ __forceinline__ void seg_increment(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
-                                              const double* y0, const double* y1, const RayConst& rc,
-                                              double& dt, double& da) {
-    const double dx = y1[0] - y0[0], dy = y1[1] - y0[1], dz = y1[2] - y0[2];
-    const double zm = y0[2] + dz * 0.5;
-    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
-    const double nzm = y0[3] + (y1[3] - y0[3]) * 0.5;
-    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
-    const double ze = fmin(fmax(zm, a.z_lo), a.z_hi);
-    seg = seg_walk(tab, a.n_knots, ze, seg);
-    const double* r0 = tab + seg * kStride;
-    const Cubic q = cubic_at(r0, ze);
-    const double c = cubic_f(r0, q, 2);
-    const double sc = bl_scale(a, zm);
-    const double u = cubic_f(r0, q, 4) * sc;
-    const double v = cubic_f(r0, q, 6) * sc;
-    const double rho = cubic_f(r0, q, 8);
-    const double inum = 1.0 / num;
-    const double cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
-    dt = ds / sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
-    da = sb_alpha_cart(c, rho, zm, a.freq, a.tweak_abs, a.sb) * ds;
-}
-
-// Launch state of a ray: geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105).
-template <bool AMP>
-__device__ __forceinline__ void ray_init(const Fan3DArgs& a, double theta, double phi, double* y, RayConst& rc) {
-    const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
-    const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
-    const double n0x = ct * cp, n0y = ct * sp, n0z = st;
-    const double ms = 1.0 + (n0x * mx + n0y * my + n0z * 0.0);
-    const double ims = 1.0 / ms, ims2 = ims * ims;
-    y[0] = a.src_x; y[1] = a.src_y; y[2] = a.src_z;
-    rc.nx = n0x * ims; rc.ny = n0y * ims; y[3] = n0z * ims;
-    if (AMP) {
-        const double tx = -st * cp, ty = -st * sp, tz = ct;
-        const double px = -ct * sp, py = ct * cp, pz = 0.0;
-        const double tm = tx * mx + ty * my + tz * 0.0;
-        const double pm = px * mx + py * my + pz * 0.0;
-        rc.mtx = tx * ims - n0x * ims2 * tm;
-        rc.mty = ty * ims - n0y * ims2 * tm;
-        y[7] = tz * ims - n0z * ims2 * tm;
-        rc.mpx = px * ims - n0x * ims2 * pm;
-        rc.mpy = py * ims - n0y * ims2 * pm;
-        y[11] = pz * ims - n0z * ims2 * pm;
-        y[4] = y[5] = y[6] = 0.0;
-        y[8] = y[9] = y[10] = 0.0;
-    } else {
-        rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0;
-    }
-}
 
 template <bool AMP, bool SMEM>
 __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(const __grid_constant__ Fan3DArgs a) {

@@ -1,0 +1,46 @@
+// Internal (not part of the C ABI): the atmosphere handle and helpers shared
+// by the C ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "../../include/infraga_gpu.h"
+#include "atmo_host.h"
+#include "fan3d.cuh"
+
+using iga::StratProfile;
+
+struct iga_atmo_s {
+    int device = 0;
+    StratProfile prof;
+    double* d_knots = nullptr;
+    // stream of the host-buffer entry points: one per handle, so calls on
+    // different atmospheres from different host threads overlap on the GPU
+    cudaStream_t stream = nullptr;
+    // reusable device buffers of the host-buffer entry points
+    std::mutex mu;
+    void* d_buf = nullptr;
+    size_t d_buf_bytes = 0;
+    // FP32-compensated path: FP32 knot table and alpha(z) tables per frequency
+    float* d_knots_f = nullptr;
+    std::mutex alpha_mu;
+    struct AlphaTab { float* d = nullptr; int n = 0; double z0 = 0.0, inv_h = 0.0; };
+    std::map<double, AlphaTab> alpha;   // kept until destroy (launches may still read them)
+};
+
+namespace iga_internal {
+extern thread_local std::string g_cuda_err;
+extern thread_local std::string g_err;
+int cuda_fail(cudaError_t e, const char* what);
+int validate(const iga_fan_params* p, int n_rays);
+int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a);
+}  // namespace iga_internal
+
+#define IGA_CUDA(call, what)                                                  \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return iga_internal::cuda_fail(e_, what);      \
+    } while (0)

@@ -45,6 +45,15 @@ CASES = {
                                            "max_rng=900", "write_rays=true"]),
 }
 
+# Eigenray searches (run_eig_search through the same driver; the reference
+# writes these rows with setprecision(8)).  name -> (profile seed, argv)
+EIG_CASES = {
+    "3d_eig_a": (0, ["rcvr_x=250", "rcvr_y=40", "bnc_min=0", "bnc_max=2"]),
+    "3d_eig_b": (4, ["rcvr_x=330", "rcvr_y=90", "bnc_min=0", "bnc_max=1"]),
+    "3d_eig_c": (3, ["rcvr_x=520", "rcvr_y=0", "bnc_min=1", "bnc_max=3"]),
+    "3d_eig_none": (2, ["rcvr_x=180", "rcvr_y=-30", "bnc_min=0", "bnc_max=1"]),
+}
+
 
 def profile_path(seed: int) -> str:
     return os.path.join(PROFILES, f"gen{seed}.met")
@@ -62,6 +71,15 @@ def main():
         with open(os.path.join(HERE, name + ".txt"), "w") as f:
             f.write(r.stdout)
         meta[name] = {"binary": binary, "mode": mode, "seed": seed, "args": args}
+        print(name, r.stdout.strip().splitlines()[-1])
+    for name, (seed, args) in EIG_CASES.items():
+        out = os.path.join(HERE, name + ".txt")
+        cmd = [os.path.join(REF, "iga_ref_3d"), "eig", profile_path(seed), *args, "out=" + out,
+               "out_id=" + os.path.join("/tmp", name)]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(out, "a") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": "iga_ref_3d", "mode": "eig", "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(meta, f, indent=1)

@@ -1,0 +1,70 @@
+"""GPU eigenray search (iga_eig_run) against the reference's own
+est_eigenray/find_eigenray output (tests/golden/3d_eig_*, written by the
+reference with 8 significant digits)."""
+import numpy as np
+import pytest
+
+import infraga_b200 as ig
+from tests._cases import load_cases, parse_golden, profile_path
+
+pytestmark = pytest.mark.gpu
+
+CASES = {k: v for k, v in load_cases().items() if v["mode"] == "eig"}
+
+# The search stops once the ray lands within tolerance (0.1 km) of the
+# receiver, so rounding differences can end it one Newton step apart; the
+# bounds below are set by that stopping rule, not by the integration.
+# Columns: incl, az [deg], n_b, x, y [km], time [s], cel [km/s], turning ht [km],
+# arrival incl, back az [deg], amplitude, absorption [dB].
+EIG_ATOL = np.array([2e-3, 2e-3, 0, 0.1, 0.1, 0.5, 2e-4, 0.05, 2e-3, 2e-3, 0.2, 0.05])
+
+
+def eig_setup(args):
+    kv = dict(a.split("=", 1) for a in args)
+    src = (float(kv.get("src_x", 0.0)), float(kv.get("src_y", 0.0)), float(kv.get("src_alt", 0.0)))
+    rcvr = (float(kv.get("rcvr_x", -250.0)), float(kv.get("rcvr_y", 0.0)))
+    over = dict(bnc_min=int(kv.get("bnc_min", 0)), bnc_max=int(kv.get("bnc_max", 0)))
+    return src, rcvr, over
+
+
+@pytest.fixture(scope="module")
+def dev():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    ig.lib()
+    return torch
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_eigenrays_match_reference(dev, name):
+    c = CASES[name]
+    src, rcvr, over = eig_setup(c["args"])
+    atmo = ig.Atmosphere.load(profile_path(c["seed"]))
+    params = ig.eig_params(atmo, **over)
+    r = ig.eig_run(atmo, params, [(src, rcvr)])
+    ref, _ = parse_golden(name)
+    got = r["eigenrays"]
+    print(name, "reference", ref.shape[0], "gpu", got.shape[0], "steps", r["total_steps"])
+    assert got.shape == ref.shape, (got[:, :3], ref[:, :3])
+    d = np.abs(got - ref)
+    print("  max |diff| per column:", np.array2string(d.max(axis=0, initial=0.0), precision=3))
+    np.testing.assert_array_equal(got[:, 2], ref[:, 2])
+    bad = d > EIG_ATOL[None, :] + 1e-7 * np.abs(ref)
+    assert not bad.any(), (np.argwhere(bad)[:5], got[bad], ref[bad])
+    # every eigenray lands within the search tolerance of the receiver for
+    # bounce counts the Newton iteration follows (the reference's Newton loop
+    # traces at most one reflection, so n_b >= 2 rows are not eigenrays)
+    one = got[:, 2] <= 1
+    assert np.all(np.hypot(got[one, 3] - rcvr[0], got[one, 4] - rcvr[1]) < params.tolerance + 1e-9)
+
+
+def test_eigen_batch_equals_single_pairs(dev):
+    """Searching several pairs in one call gives each pair's single-call result."""
+    atmo = ig.Atmosphere.load(profile_path(4))
+    params = ig.eig_params(atmo, bnc_min=0, bnc_max=1)
+    pairs = [((0.0, 0.0, 0.0), (330.0, 90.0)), ((0.0, 0.0, 0.0), (250.0, -40.0)), ((10.0, 5.0, 0.0), (300.0, 60.0))]
+    batch = ig.eig_run(atmo, params, pairs)
+    for i, p in enumerate(pairs):
+        single = ig.eig_run(atmo, params, [p])
+        np.testing.assert_array_equal(batch["eigenrays"][batch["pair_index"] == i], single["eigenrays"])
