@@ -42,7 +42,14 @@ FAN = dict(incl=(0.5, 60.01, 0.1), az=(0.0, 357.0, 3.0), bounces=10, rng_max=200
 # Sutherland-Bass evaluation), counting add/sub/mul as 1, FMA as 2,
 # div/sqrt/reciprocal as 4 and exp/exp10/log/cbrt as 20 FLOPs.
 FLOPS_PER_STEP = 2600.0
+# The FP32-compensated path runs the same equations but reads the absorption
+# from a tabulated alpha(z) (one lerp instead of the ~1,000-FLOP Sutherland-Bass
+# evaluation) and adds the hi/lo TwoSum updates: ~1,650 per ray-step.
+FLOPS_PER_STEP_FP32C = 1650.0
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per fan launch of the dominant kernel, from the ncu
+# captures summarised in profiles/ (None until captured).
+TRAFFIC = {"fp64": None, "fp32c": None}
 
 
 def config_dict(extra=None):
@@ -231,6 +238,27 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def fp32_peak_tflops(torch):
+    """Measured FP32 (non-tensor-core: TF32 off) SGEMM throughput, 8192^3, best of 5."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+            best = min(best, s.elapsed_time(e) * 1e-3)
+        del a, b
+        return 2.0 * n ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -249,7 +277,11 @@ def run_ours(args):
     atmos = [ig.Atmosphere.load(m) for m in mets]
     th, ph = fan_angles()
     n = th.size
-    params = [a.default_params(bounces=FAN["bounces"], rng_max=FAN["rng_max"], write_rays=0) for a in atmos]
+    precs = {"fp64": ig.FP64, "fp32c": ig.FP32C}
+    head = "fp32c" if args.precision in ("fp32c", "both") else "fp64"
+    legs = [p_ for p_ in ("fp32c", "fp64") if args.precision in (p_, "both")]
+    all_params = {k: [a.default_params(bounces=FAN["bounces"], rng_max=FAN["rng_max"], write_rays=0,
+                                       precision=precs[k]) for a in atmos] for k in legs}
     nb = FAN["bounces"] + 1
     d_th = torch.tensor(th, dtype=torch.float64, device=dev)
     d_ph = torch.tensor(ph, dtype=torch.float64, device=dev)
@@ -262,7 +294,7 @@ def run_ours(args):
     main = torch.cuda.current_stream()
     side = [torch.cuda.Stream(device=dev) for _ in atmos]
 
-    def step():
+    def step(params):
         # the four seed fans of the workload, concurrently on four streams
         for k, a in enumerate(atmos):
             side[k].wait_stream(main)
@@ -273,44 +305,54 @@ def run_ours(args):
         for k in range(len(atmos)):
             main.wait_stream(side[k])
 
-    peak = fp64_peak_tflops(torch) if not args.no_peak else None
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    peaks = {}
+    if not args.no_peak:
+        peaks = {"fp64": fp64_peak_tflops(torch), "fp32c": fp32_peak_tflops(torch)}
 
     props = torch.cuda.get_device_properties(dev)
     gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
-    sampler = ClockSampler(gpu_id)
-    sampler.start()
-    steps_acc = torch.zeros((), dtype=torch.int64, device=dev)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t_wall0 = time.perf_counter()
-    for i in range(args.steps):
-        flush.zero_()
-        evs[i][0].record(main)
-        step()
-        evs[i][1].record(main)
-        for b in bufs:
-            steps_acc += b["st"].sum()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    wall = time.perf_counter() - t_wall0
-    clocks = sampler.stop()
-    kern_s = sum(s.elapsed_time(e) for s, e in evs) * 1e-3
-    my_steps = int(steps_acc.item())
 
-    tot_steps, max_t = my_steps, kern_s
-    if world > 1:
-        t = torch.tensor([float(my_steps), kern_s], dtype=torch.float64, device=dev)
-        s = t.clone()
-        dist.all_reduce(s[:1], op=dist.ReduceOp.SUM)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
-        tot_steps, max_t = int(s[0].item()), float(t[1].item())
-    value = tot_steps / max_t
+    def measure(params):
+        for _ in range(args.warmup):
+            step(params)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(gpu_id)
+        sampler.start()
+        steps_acc = torch.zeros((), dtype=torch.int64, device=dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t_wall0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(main)
+            step(params)
+            evs[i][1].record(main)
+            for b in bufs:
+                steps_acc += b["st"].sum()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        wall = time.perf_counter() - t_wall0
+        clocks = sampler.stop()
+        kern_s = sum(s_.elapsed_time(e_) for s_, e_ in evs) * 1e-3
+        my_steps = int(steps_acc.item())
+        tot_steps, max_t = my_steps, kern_s
+        if world > 1:
+            t = torch.tensor([float(my_steps), kern_s], dtype=torch.float64, device=dev)
+            s2 = t.clone()
+            dist.all_reduce(s2[:1], op=dist.ReduceOp.SUM)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
+            tot_steps, max_t = int(s2[0].item()), float(t[1].item())
+        return {"value": tot_steps / max_t, "ms_per_step": 1e3 * max_t / args.steps, "my_steps": my_steps,
+                "kern_s": kern_s, "tot_steps": tot_steps, "wall": wall, "clocks": clocks}
+
+    res = {k: measure(all_params[k]) for k in legs}
+    params = all_params[head]
+    value = res[head]["value"]
+    tot_steps, max_t = res[head]["tot_steps"], res[head]["ms_per_step"] * args.steps * 1e-3
+    my_steps, kern_s, wall, clocks = res[head]["my_steps"], res[head]["kern_s"], res[head]["wall"], res[head]["clocks"]
 
     # e2e: the public host-buffer C ABI (iga_fan_run: H2D of the launch angles
     # from pinned memory, kernel, D2H of the arrival records), one host thread
@@ -346,23 +388,35 @@ def run_ours(args):
 
     result = None
     if rank == 0:
-        achieved = FLOPS_PER_STEP * my_steps / kern_s / 1e12
+        fps = FLOPS_PER_STEP_FP32C if head == "fp32c" else FLOPS_PER_STEP
+        achieved = fps * my_steps / kern_s / 1e12
+        peak = peaks.get(head)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * max_t / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict({"parallelism": f"independent fans per GPU x{world}",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32c (fp32 state/RHS, hi/lo positions, fp64 sums)" if head == "fp32c" else "f64",
+            "data": "synthetic",
+            "config": config_dict({"parallelism": f"independent fans per GPU x{world}", "precision": head,
                                    "ray_steps_per_step": tot_steps / args.steps / world}),
             "e2e": {"value": e2e_steps / e2e_t if e2e_t > 0 else None, "unit": UNIT,
                     "h2d_bytes_per_step": 2 * 8 * n * len(atmos), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": args.steps * len(atmos),
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
-                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (best of 5)",
-                         "flops_per_step": FLOPS_PER_STEP},
+            "roofline": {"bound": "fp32" if head == "fp32c" else "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": TRAFFIC.get(head),
+                         "peak_source": ("measured in this run: cuBLAS " +
+                                         ("SGEMM (TF32 off)" if head == "fp32c" else "DGEMM") +
+                                         " 8192^3 via torch.matmul, best of 5"),
+                         "flops_per_step": fps},
+            "legs": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "clocks": v["clocks"],
+                         "roofline_frac": ((FLOPS_PER_STEP_FP32C if k == "fp32c" else FLOPS_PER_STEP) *
+                                           v["my_steps"] / v["kern_s"] / 1e12 / peaks[k]) if k in peaks else None}
+                     for k, v in res.items()},
             "clocks": clocks,
             "wall_s_timed_region": wall,
         }
+        if "fp32c" in res and "fp64" in res:
+            line["fp32c_over_fp64"] = res["fp32c"]["value"] / res["fp64"]["value"]
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(mets[0])
         result = line
@@ -384,7 +438,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg")
-    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak measurement")
+    ap.add_argument("--no-peak", action="store_true", help="skip the GEMM peak measurements")
+    ap.add_argument("--precision", choices=["both", "fp32c", "fp64"], default="both",
+                    help="fan precision(s) to time; the headline is fp32c unless only fp64 is run")
     ap.add_argument("--az-step", type=float, default=FAN["az"][2],
                     help="azimuth spacing in degrees (a larger value gives a smaller fan, for profiling)")
     args = ap.parse_args()
