@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define IGA_ABI_VERSION 1
+#define IGA_ABI_VERSION 2
 
 /* ---- status codes ---- */
 enum iga_status {
@@ -44,7 +44,9 @@ enum iga_ray_status {
     IGA_RAY_LOW_TURN = 2,    /* turning height below turn_ht_min (main.infraga.3d.cpp:503) */
     IGA_RAY_SHORT = 3,       /* ground reached in < 2 steps (main.infraga.3d.cpp:507) */
     IGA_RAY_NONFINITE = 4,   /* state became NaN/Inf */
-    IGA_RAY_STEPCAP = 5      /* s_max/ds_min steps without a stop (prop_rk4 array bound) */
+    IGA_RAY_STEPCAP = 5,     /* s_max/ds_min steps without a stop (prop_rk4 array bound) */
+    IGA_RAY_TIME = 6         /* travel time above time_max (spherical run_prop,
+                                main.infraga.sph.cpp:515) */
 };
 
 /* geometry / precision selectors */
@@ -53,14 +55,18 @@ enum iga_precision { IGA_FP64 = 0, IGA_FP32C = 1 };
 
 /* Columns of an arrival row, in the reference's .arrivals.dat order
  * (main.infraga.3d.cpp:362-374): incl, az, n_b, x_0, y_0, time, cel,
- * turning ht, arrival incl, back az, trans. coeff. [dB], absorption [dB]. */
+ * turning ht, arrival incl, back az, trans. coeff. [dB], absorption [dB].
+ * For IGA_GEOM_SPH columns 3 and 4 are lat_0, lon_0 [deg] and the celerity
+ * uses the great-circle range (main.infraga.sph.cpp:379-391, 526-539). */
 #define IGA_ARRIVAL_COLS 12
 
 /* Optional per-arrival diagnostics (arrival_aux), IGA_AUX_COLS doubles per
  * arrival row, all from the ray's Jacobian auxiliaries (calc_amp = 1; zero
  * otherwise):
  *   0  |d(x,y)/d(inclination)| of the ground intercept [km/rad], formed as
- *      find_eigenray forms its Newton derivatives (geoac.eigenray.3d.cpp:334-348)
+ *      find_eigenray forms its Newton derivatives (geoac.eigenray.3d.cpp:334-348;
+ *      spherical: d(lat,lon) of geoac.eigenray.sph.cpp:351-359 scaled to
+ *      ground distance by r_grnd and r_grnd cos(lat))
  *   1  |d(x,y)/d(azimuth)| of the ground intercept [km/rad]
  *   2  ray-tube Jacobian D at the arrival row (geoac::jacobian); amplitude
  *      is proportional to |D|^-1/2, so |D| -> 0 marks a caustic
@@ -84,7 +90,7 @@ typedef struct iga_profile {
 /* Ray-fan parameters: the geoac globals (geoac.params.3d.cpp:27-41), the
  * topo::z0 ground height and the run_prop locals (main.infraga.3d.cpp:206-215). */
 typedef struct iga_fan_params {
-    int geometry;            /* IGA_GEOM_3D */
+    int geometry;            /* IGA_GEOM_3D or IGA_GEOM_SPH */
     int precision;           /* IGA_FP64 or IGA_FP32C */
     int bounces;             /* reflections to follow (>= 0) */
     int calc_amp;            /* 1: 18 equations with the Jacobian auxiliaries */
@@ -92,13 +98,18 @@ typedef struct iga_fan_params {
                                 write_rays=true path (all segments but the last of
                                 each bounce, main.infraga.3d.cpp:451-453) */
     int reserved;
-    double src[3];           /* source x, y [km], altitude [km] */
+    double src[3];           /* 3D: source x, y [km], altitude [km];
+                                SPH: source latitude, longitude [deg], altitude [km] */
     double ds_min, ds_max, s_max;
     double alt_max, rng_max, x_min, x_max, y_min, y_max;
     double z_grnd;           /* topo::z0 */
     double freq;             /* Hz */
     double tweak_abs;        /* atmo::tweak_abs (abs_coeff=) */
     double turn_ht_min;      /* km */
+    /* IGA_GEOM_SPH only: break_check region (geoac.params.sph.cpp:33-37, in
+       degrees here) and run_prop's travel-time cap [hours] */
+    double lat_min, lat_max, lon_min, lon_max;
+    double time_max;
 } iga_fan_params;
 
 /* ---- library / device ---- */
@@ -132,6 +143,13 @@ int iga_atmo_destroy(iga_atmo_t atmo);
  * ds 0.001..0.05, s_max 1000, alt_max = z_top, rng_max 2000, x/y +-2000,
  * z_grnd = z_ground, freq 0.1, tweak_abs 1, turn_ht_min 0.2. */
 int iga_fan_params_default(iga_atmo_t atmo, iga_fan_params* params);
+
+/* Defaults for either geometry.  IGA_GEOM_3D: as iga_fan_params_default.
+ * IGA_GEOM_SPH: run_prop of infraga-sph (main.infraga.sph.cpp:207-222,
+ * geoac.params.sph.cpp:23-37, atmo_io.sph.strat.cpp:27-39): source at
+ * latitude 30, longitude 0, altitude 0; rng_max 1000; latitude +-90,
+ * longitude +-180; time_max 10 h; the other fields as for 3D. */
+int iga_fan_params_init(iga_atmo_t atmo, int geometry, iga_fan_params* params);
 
 /* ---- ray fans ---- */
 

@@ -19,7 +19,7 @@ IGA_OK, IGA_E_INVALID, IGA_E_IO, IGA_E_NOMEM, IGA_E_CUDA, IGA_E_NODEVICE, IGA_E_
     0, -1, -2, -3, -4, -5, -6, -7
 GEOM_3D, GEOM_SPH = 0, 1
 FP64, FP32C = 0, 1
-RAY_STATUS = {0: "bounces", 1: "escaped", 2: "low_turn", 3: "short", 4: "nonfinite", 5: "stepcap"}
+RAY_STATUS = {0: "bounces", 1: "escaped", 2: "low_turn", 3: "short", 4: "nonfinite", 5: "stepcap", 6: "time_max"}
 
 
 class NativeLibraryError(RuntimeError):
@@ -44,6 +44,9 @@ class FanParams(ctypes.Structure):
         ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
         ("z_grnd", ctypes.c_double), ("freq", ctypes.c_double), ("tweak_abs", ctypes.c_double),
         ("turn_ht_min", ctypes.c_double),
+        ("lat_min", ctypes.c_double), ("lat_max", ctypes.c_double),
+        ("lon_min", ctypes.c_double), ("lon_max", ctypes.c_double),
+        ("time_max", ctypes.c_double),
     ]
 
 
@@ -84,6 +87,7 @@ _SIGS = {
     "iga_atmo_limits": (_I, [_VP, _P(_D), _P(_D)]),
     "iga_atmo_destroy": (_I, [_VP]),
     "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
+    "iga_fan_params_init": (_I, [_VP, _I, _P(FanParams)]),
     "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL),
                          _P(_D)]),
     "iga_fan_workspace_bytes": (ctypes.c_size_t, []),
@@ -169,9 +173,11 @@ class Atmosphere:
         _check(lib().iga_atmo_limits(self._h, ctypes.byref(lo), ctypes.byref(hi)), "iga_atmo_limits")
         return lo.value, hi.value
 
-    def default_params(self, **overrides) -> FanParams:
+    def default_params(self, geometry: int = GEOM_3D, **overrides) -> FanParams:
+        """run_prop defaults for ``geometry`` (GEOM_3D or GEOM_SPH) with
+        keyword overrides of any iga_fan_params field."""
         p = FanParams()
-        _check(lib().iga_fan_params_default(self._h, ctypes.byref(p)), "iga_fan_params_default")
+        _check(lib().iga_fan_params_init(self._h, int(geometry), ctypes.byref(p)), "iga_fan_params_init")
         for k, v in overrides.items():
             if k == "src":
                 p.src = (_D * 3)(*v)

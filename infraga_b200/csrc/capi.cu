@@ -122,12 +122,77 @@ namespace iga_internal {
 
 int validate(const iga_fan_params* p, int n_rays) {
     if (!p || n_rays < 0) return IGA_E_INVALID;
-    if (p->geometry != IGA_GEOM_3D) return IGA_E_UNSUPPORTED;
+    if (p->geometry != IGA_GEOM_3D && p->geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
     if (p->precision != IGA_FP64 && p->precision != IGA_FP32C) return IGA_E_INVALID;
+    if (p->geometry == IGA_GEOM_SPH) {
+        if (p->precision != IGA_FP64) {
+            g_cuda_err = "spherical geometry: FP64 only";
+            return IGA_E_UNSUPPORTED;
+        }
+        if (!(std::fabs(p->src[0]) < 90.0) || !std::isfinite(p->src[1])) return IGA_E_INVALID;
+        if (!(p->time_max > 0.0)) return IGA_E_INVALID;
+    }
     if (p->bounces < 0 || !(p->ds_min > 0.0) || !(p->ds_max >= p->ds_min) || !(p->s_max > 0.0)) return IGA_E_INVALID;
     if (!std::isfinite(p->s_max / p->ds_min) || p->s_max / p->ds_min > 2.0e9) return IGA_E_INVALID;
     if (!(p->freq > 0.0) || !(p->tweak_abs >= 0.0)) return IGA_E_INVALID;
     for (int i = 0; i < 3; i++) if (!std::isfinite(p->src[i])) return IGA_E_INVALID;
+    return IGA_OK;
+}
+
+// Spherical launch constants (set_initial, set_refl, break_check and the
+// atmo:: accessors of atmo_state.sph.strat.cpp evaluated at the source and the
+// ground point with the reference's own r -> z arithmetic).
+int build_args_sph(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const StratProfile& P = h->prof;
+    const double d2r = iga::kPi / 180.0;
+    a.r_earth = iga::kEarthRadiusKm;
+    a.z0 = p->z_grnd;
+    a.r_grnd = a.r_earth + a.z0;
+    // main.infraga.sph.cpp:318-320: angles to radians, z_src = max(z_src, topo::z - r0)
+    a.src_x = p->src[0] * d2r;
+    a.src_y = p->src[1] * d2r;
+    a.src_z = std::max(p->src[2], a.r_grnd - a.r_earth);
+    a.cos_lat_src = std::cos(a.src_x);
+    a.lat_min = p->lat_min * d2r; a.lat_max = p->lat_max * d2r;
+    a.lon_min = p->lon_min * d2r; a.lon_max = p->lon_max * d2r;
+    a.time_max_h = p->time_max;
+    const double half_ang = p->rng_max / (2.0 * a.r_earth);
+    if (half_ang > 0.0 && half_ang < 0.5 * iga::kPi - 1e-6) {
+        const double sh = std::sin(half_ang);
+        a.hav_rng = sh * sh;
+        a.rng_exact_only = 0;
+    } else {
+        a.hav_rng = 0.0;
+        a.rng_exact_only = 1;
+    }
+    // values at the source radius r0 + z_src and the ground radius r_grnd
+    const double r_src = a.r_earth + a.src_z;
+    const double zs = r_src - a.r_earth, zg = a.r_grnd - a.r_earth;
+    auto bl_sc = [&](double r, double& sc, double& dsc) {   // bndlyr_sc / bndlyr_dsc(n = 0)
+        sc = 1.0; dsc = 0.0;
+        if (r - a.r_earth < a.z0 + 2.0) {
+            const double X = std::exp(-(r - a.r_grnd) / 0.1);
+            sc = (1.0 - X) / (1.0 + X);
+            dsc = -2.0 * (-X / 0.1) / std::pow(1.0 + X, 2);
+        }
+    };
+    double f, d1, d2, sc, dsc;
+    iga::spline_eval(P.z, P.c, P.cs, zs, f, d1, d2); a.c0 = f;
+    bl_sc(r_src, sc, dsc);
+    iga::spline_eval(P.z, P.u, P.us, zs, f, d1, d2); a.u0s = f * sc;
+    iga::spline_eval(P.z, P.v, P.vs, zs, f, d1, d2); a.v0s = f * sc;
+    iga::spline_eval(P.z, P.rho, P.rhos, zs, f, d1, d2); a.rho0 = f;
+    double dcg;
+    iga::spline_eval(P.z, P.c, P.cs, zg, f, d1, d2); a.c_gnd = f; dcg = d1; a.dcz_g = d1;
+    bl_sc(a.r_grnd, sc, dsc);
+    iga::spline_eval(P.z, P.u, P.us, zg, f, d1, d2); a.duz_g = f * dsc + d1 * sc;
+    iga::spline_eval(P.z, P.v, P.vs, zg, f, d1, d2); a.dvz_g = f * dsc + d1 * sc;
+    a.c_ratio = a.c_gnd / a.c0;
+    // set_refl (geoac.eqset.sph.strat.cpp:184-194) factors of dnu_r/ds and ds0
+    a.refl_k1 = a.c0 / a.c_gnd * dcg;
+    a.refl_k2 = std::pow(a.c_gnd, 2) / a.c0 * 1.0 / a.r_grnd;
+    a.refl_k3 = -1.0 / a.c_gnd;
+    a.refl_mcr = -a.c0 / a.c_gnd;
     return IGA_OK;
 }
 
@@ -168,6 +233,7 @@ int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     a.sb.x0_low = std::pow(10.0, -0.67887);
     a.sb.x1_low = std::pow(10.0, -0.10744);
     a.sb.x2 = std::pow(10.0, -3.3979);
+    if (p->geometry == IGA_GEOM_SPH) return build_args_sph(h, p, a);
     return IGA_OK;
 }
 
@@ -193,7 +259,9 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     }
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    if (p->precision == IGA_FP32C)
+    if (p->geometry == IGA_GEOM_SPH)
+        IGA_CUDA(iga::launch_fansph_fp64(a, p->calc_amp != 0, st, nullptr), "fansph kernel launch");
+    else if (p->precision == IGA_FP32C)
         IGA_CUDA(iga::launch_fan3d_fp32c(a, p->calc_amp != 0, st, nullptr), "fan3d fp32c kernel launch");
     else
         IGA_CUDA(iga::launch_fan3d_fp64(a, p->calc_amp != 0, st, nullptr), "fan3d kernel launch");
@@ -290,6 +358,20 @@ int iga_fan_params_default(iga_atmo_t h, iga_fan_params* p) {
     p->x_min = -2000.0; p->x_max = 2000.0; p->y_min = -2000.0; p->y_max = 2000.0;
     p->z_grnd = h->prof.z.front();
     p->freq = 0.1; p->tweak_abs = 1.0; p->turn_ht_min = 0.2;
+    p->lat_min = -90.0; p->lat_max = 90.0; p->lon_min = -180.0; p->lon_max = 180.0;
+    p->time_max = 10.0;
+    return IGA_OK;
+}
+
+int iga_fan_params_init(iga_atmo_t h, int geometry, iga_fan_params* p) {
+    if (geometry != IGA_GEOM_3D && geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
+    int rc = iga_fan_params_default(h, p);
+    if (rc) return rc;
+    if (geometry == IGA_GEOM_SPH) {
+        p->geometry = IGA_GEOM_SPH;
+        p->src[0] = 30.0; p->src[1] = 0.0; p->src[2] = 0.0;
+        p->rng_max = 1000.0;
+    }
     return IGA_OK;
 }
 

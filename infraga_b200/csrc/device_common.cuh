@@ -101,14 +101,23 @@ __host__ __device__ __forceinline__ double iga_rcbrt(double x) {
 #endif
 }
 
-// Sutherland & Bass (2004) absorption, Cartesian variant of the reference
-// (atmo_state.abs.cart.cpp:12-142), in dB/km times tweak_abs.  Inputs are the
-// sound speed [km/s] and density [g/cm^3] at the evaluation point and its
-// altitude z [km].  The reference's N-profile polynomial uses z^2 where z^4
-// is meant (line 78); that is reproduced.  The H2O branch for z > 100 km is
-// unreachable in the reference (it is nested under z <= 30) and so absent.
-__host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, double z, double freq,
-                                                double tweak_abs, const SBConst& k) {
+// Sutherland & Bass (2004) absorption in dB/km times tweak_abs.  Inputs are
+// the sound speed [km/s] and density [g/cm^3] at the evaluation point and its
+// altitude z [km].  SPH selects the spherical variant of the reference
+// (atmo_state.abs.sph.cpp:11-147) over the Cartesian one
+// (atmo_state.abs.cart.cpp:12-142); they differ in two places:
+//  - the Cartesian N-profile polynomial uses z^2 where z^4 is meant (cart
+//    line 78); the spherical one has z^4.  Both are reproduced.
+//  - the rotational loss: Cartesian a_rot = alpha_2 beta_1 X_ON with
+//    alpha_2 carrying 1/sqrt((1+cchi^2)(1+(sigma cchi)^2)); the spherical
+//    a_rot has only 1/sqrt(1+cchi^2) under its root.
+// The classical term a_cl (x 1.003 with the diffusion term) is the same
+// expression in both, written in each file's own grouping.  The H2O branch
+// for z > 100 km is unreachable in the reference (nested under z <= 30) and
+// so absent.
+template <bool SPH>
+__host__ __device__ __forceinline__ double sb_alpha(double c_kms, double rho_gcc, double z, double freq,
+                                                    double tweak_abs, const SBConst& k) {
     const double mu_o = 18.192e-6, T_o = 293.15, P_o = 101325.0, S = 117.0;
     const double cs = c_kms * 1.0e3;
     const double T_z = cs * cs / (kRgas * kGamma);
@@ -125,7 +134,7 @@ __host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rh
                                      : (-19.027 + (1.3093 * z) - (4.6496e-2 * z2) + (7.8543e-4 * z3) - (6.5169e-6 * z4) + (2.1343e-8 * z5)));
     const double X4 = iga_exp10(z > 95.0 ? (-3.2456 + (4.6642e-2 * z) - (2.6894e-4 * z2) + (5.264e-7 * z3))
                                      : (-11.195 + (1.5408e-1 * z) - (1.4348e-3 * z2) + (1.0166e-5 * z3)));
-    const double X5 = iga_exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * z2) + (4.2609e-10 * z5));
+    const double X5 = iga_exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * (SPH ? z4 : z2)) + (4.2609e-10 * z5));
     const double X6 = iga_exp10(z > 30.0 ? (-4.2563 + (7.6245e-2 * z) - (2.1824e-3 * z2) - (2.3010e-6 * z3) + (2.4265e-7 * z4) - (1.2500e-9 * z5))
                                      : (-1.7491 + (4.4986e-2 * z) - (6.8549e-2 * z2) + (5.4639e-3 * z3) - (1.5539e-4 * z4) + (1.5063e-6 * z5)));
     const double X_ON = (X0 + X1) / 0.9903;
@@ -142,13 +151,20 @@ __host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rh
 
     const double beta_0 = 2.0 * kPi * freq / cs;
     const double nu2 = nu * nu, sq = sqrt(1.0 + nu2);
-    const double beta_1 = sqrt(0.5 * (sq + 1.0) / (1.0 + nu2));
     const double cc2 = cchi * cchi, sc2 = (sigma * cchi) * (sigma * cchi);
-    const double beta_2 = sqrt((1.0 + cc2) / (1.0 + sc2));
-    const double alpha_1 = beta_0 * sqrt(0.5 * (sq - 1.0) / (1.0 + nu2));
-    const double alpha_2 = beta_0 * (((sigma / 2.0 - 1.0 / (2.0 * sigma)) * chi) / (sqrt((1.0 + cc2) * (1.0 + sc2))));
-    const double a_cl = alpha_1 * beta_2;
-    const double a_rot = alpha_2 * beta_1 * X_ON;
+    double a_cl, a_rot;
+    if (SPH) {
+        a_cl = beta_0 * sqrt(0.5 * (sq - 1.0) * (1.0 + cc2) / ((1.0 + nu2) * (1.0 + sc2)));
+        a_rot = beta_0 * X_ON * ((sigma * sigma - 1.0) * chi / (2.0 * sigma)) *
+                sqrt(0.5 * (sq + 1.0) / ((1.0 + nu2) * (1.0 + cc2)));
+    } else {
+        const double beta_1 = sqrt(0.5 * (sq + 1.0) / (1.0 + nu2));
+        const double beta_2 = sqrt((1.0 + cc2) / (1.0 + sc2));
+        const double alpha_1 = beta_0 * sqrt(0.5 * (sq - 1.0) / (1.0 + nu2));
+        const double alpha_2 = beta_0 * (((sigma / 2.0 - 1.0 / (2.0 * sigma)) * chi) / (sqrt((1.0 + cc2) * (1.0 + sc2))));
+        a_cl = alpha_1 * beta_2;
+        a_rot = alpha_2 * beta_1 * X_ON;
+    }
 
     const double Tr = iga_rcbrt(T_z / T_o) - 1.0;
     const double A1 = (X0 + X1) * 24.0 * exp(-9.16 * Tr);
@@ -183,7 +199,13 @@ __host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rh
         const double q = freq / fv[m];
         a_vib += (A_max / cs) * ((2.0 * f2 / fv[m]) / (1.0 + q * q));
     }
+    if (SPH) return (a_cl + a_rot + 0.003 * a_cl + a_vib) * tweak_abs * 8.685889e3;
     return (a_cl * 1.003 + a_rot + a_vib) * tweak_abs * 8.685889e3;
+}
+
+__host__ __device__ __forceinline__ double sb_alpha_cart(double c_kms, double rho_gcc, double z, double freq,
+                                                         double tweak_abs, const SBConst& k) {
+    return sb_alpha<false>(c_kms, rho_gcc, z, freq, tweak_abs, k);
 }
 
 }  // namespace iga

@@ -44,6 +44,19 @@ struct Fan3DArgs {
     double dcz_g, duz_g, dvz_g;   // z-derivatives of c, u, v at the ground (set_refl)
     double c_ratio;          // c_gnd / c0 (arrival inclination)
     SBConst sb;
+    // spherical geometry only (src_x/src_y hold the source latitude and
+    // longitude in radians; z-like quantities above are altitudes)
+    double r_earth;          // globe::r0
+    double r_grnd;           // topo::z = r_earth + z0 (flat ground radius)
+    double cos_lat_src;
+    double lat_min, lat_max, lon_min, lon_max;   // radians (break_check)
+    double time_max_h;       // run_prop's travel-time cap [hours]
+    double hav_rng;          // sin^2(rng_max / (2 r_earth)): haversine range threshold
+    int rng_exact_only;      // 1: rng_max >= pi r_earth or the threshold is unusable
+    double refl_k1;          // c0 / c_grnd * dc/dr at the ground (set_refl dnu_r_ds)
+    double refl_k2;          // c_grnd^2 / c0 / r_grnd
+    double refl_k3;          // -1 / c_grnd
+    double refl_mcr;         // -c0 / c_grnd
     // FP32-compensated path only
     const float* knots_f;    // [n_knots][kStrideF]: per segment z_k, 1/dz and the power-basis
                              // cubic coefficients a0..a3 of c, u, v (last row: z only)
@@ -57,5 +70,10 @@ constexpr int kStrideF = 14;  // floats per segment row of the FP32 table
 cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 
 cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
+// Spherical (global) stratified fan, FP64 (fansph_fp64.cu).
+cudaError_t launch_fansph_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
+constexpr double kEarthRadiusKm = 6370.0;   // globe::r0 (util/globe.cpp:10)
 
 }  // namespace iga

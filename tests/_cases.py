@@ -82,6 +82,41 @@ def case_setup(args, z_ground: float = 0.0, z_top: float = 150.0):
     return th, ph, p
 
 
+# Spherical fans: columns 3/4 are latitude/longitude in degrees (1e-6 deg is
+# about 0.1 m on the ground); the rest as for 3D.
+SPH_ATOL = FP64_ATOL.copy()
+SPH_ATOL[3] = SPH_ATOL[4] = 1e-6
+
+
+def case_setup_sph(args, z_ground: float = 0.0, z_top: float = 150.0):
+    """Angles and iga_fan_params fields for an infraga-sph run_prop argument
+    list (main.infraga.sph.cpp:207-320), with that CLI's defaults."""
+    kv = dict(a.split("=", 1) for a in args)
+    shared = [a for a in args if a.split("=", 1)[0] not in ("src_lat", "src_lon", "src_alt", "max_rng")]
+    _, _, p = case_setup(shared, z_ground, z_top)
+    src = (float(kv.get("src_lat", 30.0)), float(kv.get("src_lon", 0.0)), float(kv.get("src_alt", 0.0)))
+    z_src = max(src[2], p["z_grnd"])
+    th, ph = synth.fan_angles(*_fan_args(kv), src_above_ground=(z_src - p["z_grnd"]) >= 0.01)
+    for k in ("x_min", "x_max", "y_min", "y_max"):
+        del p[k]
+    p.update(geometry=1, src=src, rng_max=float(kv.get("max_rng", 1000.0)),
+             lat_min=float(kv.get("min_lat", -90.0)), lat_max=float(kv.get("max_lat", 90.0)),
+             lon_min=float(kv.get("min_lon", -180.0)), lon_max=float(kv.get("max_lon", 180.0)),
+             time_max=float(kv.get("max_time", 10.0)))
+    return th, ph, p
+
+
+def _fan_args(kv):
+    th_min, th_max, th_step = 0.5, 45.0, 0.5
+    az_min, az_max, az_step = -90.0, -90.0, 1.0
+    if "inclination" in kv:
+        th_min = th_max = float(kv["inclination"]); th_step = 1.0
+    if "azimuth" in kv:
+        az_min = az_max = float(kv["azimuth"]); az_step = 1.0
+    return (float(kv.get("incl_min", th_min)), float(kv.get("incl_max", th_max)), float(kv.get("incl_step", th_step)),
+            float(kv.get("az_min", az_min)), float(kv.get("az_max", az_max)), float(kv.get("az_step", az_step)))
+
+
 def compare_arrivals(got: np.ndarray, ref: np.ndarray, atol=FP64_ATOL, rtol=FP64_RTOL, amp_skip_db: float = 60.0):
     """Column-wise comparison; returns (ok, report).  Amplitude is compared
     only where the reference value is above -amp_skip_db (near-caustic
@@ -96,7 +131,7 @@ def compare_arrivals(got: np.ndarray, ref: np.ndarray, atol=FP64_ATOL, rtol=FP64
     if bad.any():
         i, j = np.argwhere(bad)[0]
         return False, f"{bad.sum()} values out of tolerance; first row {i} col {j}: got {got[i, j]!r} ref {ref[i, j]!r}"
-    return True, f"max abs diff per column {d.max(axis=0)}"
+    return True, f"max abs diff per column {d.max(axis=0, initial=0.0)}"
 
 
 # FP32-compensated path vs the FP64 reference.

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in this directory from the reference solver
 itself (oracle/_ref, compiled from the reference sources by oracle/Makefile).
 
-    python tests/golden/make_golden.py        # needs the reference sources (make -C oracle ref)
+    python tests/golden/make_golden.py           # all cases; needs make -C oracle ref
+    python tests/golden/make_golden.py NAME...   # only these cases (cases.json is merged)
 
 Each fixture is the full-precision output of the reference's own solver
 functions driven by oracle/harness/*.cpp: one line per arrival
@@ -45,6 +46,33 @@ CASES = {
                                            "max_rng=900", "write_rays=true"]),
 }
 
+# Spherical (global) fans through oracle/harness/harness_sph.cpp; angles in
+# degrees as on the infraga-sph command line.
+SPH_CASES = {
+    "sph_c0_bulk": ("iga_ref_sph", "prop", 0, ["incl_min=1", "incl_max=45", "incl_step=2", "azimuth=90", "bounces=3",
+                                               "src_lat=30", "src_lon=10", "write_rays=false"]),
+    "sph_rays": ("iga_ref_sph", "prop", 1, ["incl_min=2", "incl_max=38", "incl_step=4", "az_min=0", "az_max=300",
+                                            "az_step=60", "bounces=2", "src_lat=-45", "src_lon=-60", "max_rng=800",
+                                            "write_rays=true"]),
+    "sph_noamp": ("iga_ref_sph", "prop", 2, ["incl_min=3", "incl_max=33", "incl_step=6", "az_min=-90", "az_max=90",
+                                             "az_step=90", "bounces=2", "src_lat=10", "src_lon=100", "calc_amp=false",
+                                             "write_rays=false"]),
+    "sph_elevated": ("iga_ref_sph", "prop", 3, ["incl_min=-30", "incl_max=30", "incl_step=6", "azimuth=45",
+                                                "bounces=2", "src_alt=10", "src_lat=0", "src_lon=0", "max_rng=800",
+                                                "write_rays=false"]),
+    "sph_dateline": ("iga_ref_sph", "prop", 4, ["incl_min=5", "incl_max=35", "incl_step=5", "azimuth=80", "bounces=3",
+                                                "src_lat=-20", "src_lon=177", "z_grnd=0.5", "freq=0.5",
+                                                "abs_coeff=0.3", "turn_ht_min=10", "max_rng=1500",
+                                                "write_rays=true"]),
+    "sph_pole": ("iga_ref_sph", "prop", 0, ["incl_min=4", "incl_max=36", "incl_step=8", "az_min=-10", "az_max=10",
+                                            "az_step=10", "bounces=6", "src_lat=84", "src_lon=45", "max_rng=3000",
+                                            "write_rays=false"]),
+    "sph_limits": ("iga_ref_sph", "prop", 1, ["incl_min=5", "incl_max=40", "incl_step=7", "az_min=45", "az_max=135",
+                                              "az_step=45", "bounces=4", "src_lat=40", "src_lon=-100",
+                                              "max_lat=43", "min_lon=-104", "max_lon=-95", "max_time=0.3",
+                                              "write_rays=false"]),
+}
+
 # Eigenray searches (run_eig_search through the same driver; the reference
 # writes these rows with setprecision(8)).  name -> (profile seed, argv)
 EIG_CASES = {
@@ -60,11 +88,19 @@ def profile_path(seed: int) -> str:
 
 
 def main():
+    only = set(sys.argv[1:])
+    want = lambda name: not only or name in only  # noqa: E731
     os.makedirs(PROFILES, exist_ok=True)
     for seed in range(5):
         synth.write_met(profile_path(seed), seed)
     meta = {}
+    meta_path = os.path.join(HERE, "cases.json")
+    if only and os.path.exists(meta_path):
+        with open(meta_path) as f:
+            meta = json.load(f)
     for name, (binary, mode, seed, args) in CASES.items():
+        if not want(name):
+            continue
         exe = os.path.join(REF, binary)
         cmd = [exe, mode, profile_path(seed), *args]
         r = subprocess.run(cmd, capture_output=True, text=True, check=True)
@@ -72,7 +108,18 @@ def main():
             f.write(r.stdout)
         meta[name] = {"binary": binary, "mode": mode, "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
+    for name, (binary, mode, seed, args) in SPH_CASES.items():
+        if not want(name):
+            continue
+        cmd = [os.path.join(REF, binary), mode, profile_path(seed), *args]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(os.path.join(HERE, name + ".txt"), "w") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": binary, "mode": mode, "seed": seed, "args": args}
+        print(name, r.stdout.strip().splitlines()[-1])
     for name, (seed, args) in EIG_CASES.items():
+        if not want(name):
+            continue
         out = os.path.join(HERE, name + ".txt")
         cmd = [os.path.join(REF, "iga_ref_3d"), "eig", profile_path(seed), *args, "out=" + out,
                "out_id=" + os.path.join("/tmp", name)]
@@ -81,7 +128,7 @@ def main():
             f.write(r.stdout)
         meta[name] = {"binary": "iga_ref_3d", "mode": "eig", "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
-    with open(os.path.join(HERE, "cases.json"), "w") as f:
+    with open(meta_path, "w") as f:
         json.dump(meta, f, indent=1)
 
 
