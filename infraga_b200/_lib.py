@@ -86,6 +86,9 @@ _SIGS = {
     "iga_atmo_create": (_I, [_P(Profile), _P(_VP)]),
     "iga_atmo_limits": (_I, [_VP, _P(_D), _P(_D)]),
     "iga_atmo_destroy": (_I, [_VP]),
+    "iga_atmo_load_rngdep": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                  _I, _P(_VP)]),
+    "iga_atmo_region": (_I, [_VP, _P(_D), _P(_D), _P(_D), _P(_D)]),
     "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
     "iga_fan_params_init": (_I, [_VP, _I, _P(FanParams)]),
     "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL),
@@ -155,6 +158,24 @@ class Atmosphere:
         _check(lib().iga_atmo_load(str(met_path).encode(), fmt.encode(), int(reverse_winds), ctypes.byref(h)),
                f"iga_atmo_load({met_path})")
         return cls(h)
+
+    @classmethod
+    def load_rngdep(cls, prefix: str, lat_file: str, lon_file: str, topo_file: str | None = None,
+                    fmt: str = "zTuvdp", reverse_winds: bool = False) -> "Atmosphere":
+        """Range-dependent grid ({prefix}{n}.met node profiles on the lat/lon
+        node lists) with optional terrain (the range-dependent set_region,
+        atmo_io.sph.rngdep.cpp:61-311)."""
+        h = _VP()
+        _check(lib().iga_atmo_load_rngdep(str(prefix).encode(), str(lat_file).encode(), str(lon_file).encode(),
+                                          str(topo_file).encode() if topo_file else None, fmt.encode(),
+                                          int(reverse_winds), ctypes.byref(h)), f"iga_atmo_load_rngdep({prefix})")
+        return cls(h)
+
+    def region(self):
+        """(lat_min, lat_max, lon_min, lon_max) [deg] of geoac::set_limits."""
+        v = [_D() for _ in range(4)]
+        _check(lib().iga_atmo_region(self._h, *[ctypes.byref(x) for x in v]), "iga_atmo_region")
+        return tuple(x.value for x in v)
 
     @classmethod
     def from_arrays(cls, z, c, u, v, rho) -> "Atmosphere":

@@ -74,6 +74,30 @@ int upload(iga_atmo_s* h) {
     return IGA_OK;
 }
 
+int upload_rngdep(iga_atmo_s* h) {
+    int dev;
+    IGA_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    h->device = dev;
+    const iga::RngdepGrid& g = h->grid;
+    h->prof.z = g.z;   // knot altitudes (limits and defaults)
+    std::vector<double> buf(g.table);
+    buf.insert(buf.end(), g.x.begin(), g.x.end());
+    buf.insert(buf.end(), g.y.begin(), g.y.end());
+    buf.insert(buf.end(), g.z.begin(), g.z.end());
+    IGA_CUDA(cudaMalloc(&h->d_hyb, buf.size() * sizeof(double)), "cudaMalloc(hybrid tables)");
+    IGA_CUDA(cudaMemcpy(h->d_hyb, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(hybrid)");
+    if (h->has_topo) {
+        const iga::Terrain& t = h->topo;
+        std::vector<double> tb(t.table);
+        tb.insert(tb.end(), t.x.begin(), t.x.end());
+        tb.insert(tb.end(), t.y.begin(), t.y.end());
+        IGA_CUDA(cudaMalloc(&h->d_topo, tb.size() * sizeof(double)), "cudaMalloc(terrain)");
+        IGA_CUDA(cudaMemcpy(h->d_topo, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(terrain)");
+    }
+    IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    return IGA_OK;
+}
+
 // Sutherland-Bass alpha(z) for one frequency on a 10 m grid spanning the
 // profile plus 2 km either side, evaluated in FP64 with the reference's model
 // (c and rho from the profile splines, clamped like atmo::c/rho; the gas
@@ -196,9 +220,89 @@ int build_args_sph(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     return IGA_OK;
 }
 
+// Range-dependent spherical launch constants (run_prop of infraga-sph-rngdep,
+// main.infraga.sph.rngdep.cpp:310-320; set_initial; topo::set_bndlyr
+// atmo_state.sph.rngdep.cpp:22-33).
+int build_args_sphr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const iga::RngdepGrid& g = h->grid;
+    const double d2r = iga::kPi / 180.0;
+    a.r_earth = iga::kEarthRadiusKm;
+    a.src_x = p->src[0] * d2r;
+    a.src_y = p->src[1] * d2r;
+    a.cos_lat_src = std::cos(a.src_x);
+    a.lat_min = p->lat_min * d2r; a.lat_max = p->lat_max * d2r;
+    a.lon_min = p->lon_min * d2r; a.lon_max = p->lon_max * d2r;
+    a.time_max_h = p->time_max;
+    const double half_ang = p->rng_max / (2.0 * a.r_earth);
+    a.rng_exact_only = (half_ang > 0.0 && half_ang < 0.5 * iga::kPi - 1e-6) ? 0 : 1;
+    a.hav_rng = a.rng_exact_only ? 0.0 : std::pow(std::sin(half_ang), 2);
+    // ground: terrain (z_max = max(0, terrain) + 0.01, z_bndlyr = max + 2) or flat z0
+    a.z0 = p->z_grnd;
+    a.r_grnd = a.r_earth + a.z0;
+    auto topo_r = [&](double lat, double lon) {
+        if (!h->has_topo) return a.r_grnd;
+        double z, dz[2];
+        iga::terrain_eval1(h->topo, lat, lon, z, dz);
+        return a.r_earth + z;
+    };
+    if (h->has_topo) {
+        a.topo_zmax = h->topo.z_max + 0.01;
+        a.z_bl = h->topo.z_max + 2.0;
+        a.x_cut = h->topo.z_max + 40.0;
+    } else {
+        a.topo_zmax = a.z0;
+        a.z_bl = a.z0 + 2.0;
+        a.x_cut = a.z0 + 40.0;
+    }
+    a.src_z = std::max(p->src[2], topo_r(a.src_x, a.src_y) - a.r_earth);
+    const double r_src = a.r_earth + a.src_z;
+    double sc = 1.0;
+    if (r_src - a.r_earth < a.z_bl) {
+        const double X = std::exp(-(r_src - topo_r(a.src_x, a.src_y)) / 0.1);
+        sc = (1.0 - X) / (1.0 + X);
+    }
+    double f, df[3];
+    const double zs = r_src - a.r_earth;
+    iga::hybrid_eval1(g, 0, a.src_x, a.src_y, zs, f, df); a.c0 = f;
+    iga::hybrid_eval1(g, 1, a.src_x, a.src_y, zs, f, df); a.u0s = f * sc;
+    iga::hybrid_eval1(g, 2, a.src_x, a.src_y, zs, f, df); a.v0s = f * sc;
+    iga::hybrid_eval1(g, 3, a.src_x, a.src_y, zs, f, df); a.rho0 = f;
+    a.refl_mcr = 0.0;   // position dependent here: formed in the kernel
+    a.hyb_tab = h->d_hyb;
+    const size_t n_rec = (size_t)g.nx * g.ny * g.nz * iga::kHybRec;
+    a.hyb_x = h->d_hyb + n_rec;
+    a.hyb_y = a.hyb_x + g.nx;
+    a.hyb_z = a.hyb_y + g.ny;
+    a.hyb_nx = g.nx; a.hyb_ny = g.ny; a.hyb_nz = g.nz;
+    if (h->has_topo) {
+        const iga::Terrain& t = h->topo;
+        a.topo_tab = h->d_topo;
+        a.topo_x = h->d_topo + (size_t)t.nx * t.ny * 4;
+        a.topo_y = a.topo_x + t.nx;
+        a.topo_nx = t.nx; a.topo_ny = t.ny;
+    } else {
+        a.topo_tab = nullptr; a.topo_x = a.topo_y = nullptr; a.topo_nx = a.topo_ny = 0;
+    }
+    return IGA_OK;
+}
+
 int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     const StratProfile& P = h->prof;
     memset(&a, 0, sizeof(a));
+    if (h->kind == 1) {
+        a.bounces = p->bounces;
+        a.write_rays = p->write_rays ? 1 : 0;
+        a.length = (int)(p->s_max / p->ds_min);
+        a.ds_min = p->ds_min; a.ds_max = p->ds_max; a.s_max = p->s_max;
+        a.alt_max = p->alt_max; a.rng_max = p->rng_max;
+        a.bl = 0.1;
+        a.inv_bl = 1.0 / a.bl;
+        a.freq = p->freq; a.tweak_abs = p->tweak_abs; a.turn_ht_min = p->turn_ht_min;
+        a.sb.x0_low = std::pow(10.0, -0.67887);
+        a.sb.x1_low = std::pow(10.0, -0.10744);
+        a.sb.x2 = std::pow(10.0, -3.3979);
+        return build_args_sphr(h, p, a);
+    }
     a.knots = h->d_knots;
     a.n_knots = (int)P.z.size();
     a.uniform = P.uniform ? 1 : 0;
@@ -244,6 +348,10 @@ namespace {
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st) {
+    if (h->kind == 1 && (p->geometry != IGA_GEOM_SPH || p->precision != IGA_FP64)) {
+        g_cuda_err = "range-dependent atmosphere: spherical geometry, FP64 only";
+        return IGA_E_UNSUPPORTED;
+    }
     iga::Fan3DArgs a;
     int rc = build_args(h, p, a);
     if (rc) return rc;
@@ -259,7 +367,9 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     }
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    if (p->geometry == IGA_GEOM_SPH)
+    if (h->kind == 1)
+        IGA_CUDA(iga::launch_fansphr_fp64(a, p->calc_amp != 0, st, nullptr), "fansphr kernel launch");
+    else if (p->geometry == IGA_GEOM_SPH)
         IGA_CUDA(iga::launch_fansph_fp64(a, p->calc_amp != 0, st, nullptr), "fansph kernel launch");
     else if (p->precision == IGA_FP32C)
         IGA_CUDA(iga::launch_fan3d_fp32c(a, p->calc_amp != 0, st, nullptr), "fan3d fp32c kernel launch");
@@ -309,6 +419,46 @@ int iga_atmo_load(const char* met_path, const char* format, int reverse_winds, i
     return IGA_OK;
 }
 
+int iga_atmo_load_rngdep(const char* prefix, const char* lat_file, const char* lon_file, const char* topo_file,
+                         const char* format, int reverse_winds, iga_atmo_t* out) {
+    if (!prefix || !lat_file || !lon_file || !out) return IGA_E_INVALID;
+    *out = nullptr;
+    iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
+    if (!h) return IGA_E_NOMEM;
+    h->kind = 1;
+    int rc = iga::load_rngdep(prefix, lat_file, lon_file, format ? format : "zTuvdp", reverse_winds != 0, h->grid, g_err);
+    if (rc == IGA_OK && topo_file && topo_file[0]) {
+        rc = iga::load_terrain(topo_file, h->topo, g_err);
+        h->has_topo = (rc == IGA_OK);
+    }
+    if (rc == IGA_OK) rc = upload_rngdep(h);
+    if (rc != IGA_OK) { iga_atmo_destroy(h); return rc; }
+    *out = h;
+    return IGA_OK;
+}
+
+int iga_atmo_region(iga_atmo_t h, double* lat_min, double* lat_max, double* lon_min, double* lon_max) {
+    if (!h) return IGA_E_INVALID;
+    double r[4] = {-90.0, 90.0, -180.0, 180.0};
+    if (h->kind == 1) {
+        // geoac::set_limits (atmo_io.sph.rngdep.cpp:27-43): grid (and terrain) extent less 1e-3 deg
+        const double buf = 1.0e-3 * (iga::kPi / 180.0);
+        double a0 = h->grid.x.front() + buf, a1 = h->grid.x.back() - buf;
+        double b0 = h->grid.y.front() + buf, b1 = h->grid.y.back() - buf;
+        if (h->has_topo) {
+            a0 = std::max(a0, h->topo.x.front() + buf); a1 = std::min(a1, h->topo.x.back() - buf);
+            b0 = std::max(b0, h->topo.y.front() + buf); b1 = std::min(b1, h->topo.y.back() - buf);
+        }
+        const double r2d = 180.0 / iga::kPi;
+        r[0] = a0 * r2d; r[1] = a1 * r2d; r[2] = b0 * r2d; r[3] = b1 * r2d;
+    }
+    if (lat_min) *lat_min = r[0];
+    if (lat_max) *lat_max = r[1];
+    if (lon_min) *lon_min = r[2];
+    if (lon_max) *lon_max = r[3];
+    return IGA_OK;
+}
+
 int iga_atmo_create(const iga_profile* pr, iga_atmo_t* out) {
     if (!pr || !out || pr->n < 3 || !pr->z || !pr->c || !pr->u || !pr->v || !pr->rho) return IGA_E_INVALID;
     *out = nullptr;
@@ -339,6 +489,8 @@ int iga_atmo_destroy(iga_atmo_t h) {
     if (h->d_buf) cudaFree(h->d_buf);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->d_knots_f) cudaFree(h->d_knots_f);
+    if (h->d_hyb) cudaFree(h->d_hyb);
+    if (h->d_topo) cudaFree(h->d_topo);
     for (auto& kv : h->alpha) cudaFree(kv.second.d);
     delete h;
     return IGA_OK;
@@ -371,6 +523,15 @@ int iga_fan_params_init(iga_atmo_t h, int geometry, iga_fan_params* p) {
         p->geometry = IGA_GEOM_SPH;
         p->src[0] = 30.0; p->src[1] = 0.0; p->src[2] = 0.0;
         p->rng_max = 1000.0;
+        if (h->kind == 1) {
+            // run_prop of infraga-sph-rngdep (main.infraga.sph.rngdep.cpp:209, 238-239):
+            // 2 bounces, source at the centre of the set_limits region
+            iga_atmo_region(h, &p->lat_min, &p->lat_max, &p->lon_min, &p->lon_max);
+            const double d2r = iga::kPi / 180.0, r2d = 180.0 / iga::kPi;
+            p->src[0] = (p->lat_max * d2r + p->lat_min * d2r) / 2.0 * r2d;
+            p->src[1] = (p->lon_max * d2r + p->lon_min * d2r) / 2.0 * r2d;
+            p->bounces = 2;
+        }
     }
     return IGA_OK;
 }

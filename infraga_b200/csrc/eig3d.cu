@@ -346,6 +346,10 @@ extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_
     int rc = validate(&fp, 1);
     if (rc) return rc;
     if (fp.precision != IGA_FP64) return IGA_E_UNSUPPORTED;
+    if (h->kind != 0) {
+        g_cuda_err = "eigenray search: stratified atmospheres only";
+        return IGA_E_UNSUPPORTED;
+    }
     if (P->bnc_min < 0 || P->bnc_max < P->bnc_min || P->iterations < 0 || !(P->tolerance > 0.0) ||
         !(P->incl_step_max > 0.0) || !(P->incl_step_min > 0.0) || !(P->incl_max > P->incl_min))
         return IGA_E_INVALID;

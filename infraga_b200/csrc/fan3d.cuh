@@ -57,6 +57,18 @@ struct Fan3DArgs {
     double refl_k2;          // c_grnd^2 / c0 / r_grnd
     double refl_k3;          // -1 / c_grnd
     double refl_mcr;         // -c0 / c_grnd
+    // range-dependent atmosphere and terrain (spherical range-dependent kernel)
+    const double* hyb_tab;   // [nx][ny][nz][64] node records (atmo_rngdep.h)
+    const double* hyb_x;     // node latitudes [rad]
+    const double* hyb_y;     // node longitudes [rad]
+    const double* hyb_z;     // knot altitudes [km]
+    int hyb_nx, hyb_ny, hyb_nz;
+    const double* topo_tab;  // [nx][ny][4] terrain f, f_lat, f_lon, f_lat,lon (null: flat ground at z0)
+    const double* topo_x;
+    const double* topo_y;
+    int topo_nx, topo_ny;
+    double topo_zmax;        // topo::z_max of ground_check (max terrain + 0.01, or z0)
+    double x_cut;            // r - r_earth above which exp(-(r - z_g)/bl) < 1e-173 everywhere
     // FP32-compensated path only
     const float* knots_f;    // [n_knots][kStrideF]: per segment z_k, 1/dz and the power-basis
                              // cubic coefficients a0..a3 of c, u, v (last row: z only)
@@ -73,6 +85,9 @@ cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t st
 
 // Spherical (global) stratified fan, FP64 (fansph_fp64.cu).
 cudaError_t launch_fansph_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
+// Spherical range-dependent fan with optional terrain, FP64 (fansphr_fp64.cu).
+cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 
 constexpr double kEarthRadiusKm = 6370.0;   // globe::r0 (util/globe.cpp:10)
 

@@ -9,13 +9,21 @@
 
 #include "../../include/infraga_gpu.h"
 #include "atmo_host.h"
+#include "atmo_rngdep.h"
 #include "fan3d.cuh"
 
 using iga::StratProfile;
 
 struct iga_atmo_s {
     int device = 0;
-    StratProfile prof;
+    // 0: stratified profile (prof); 1: range-dependent grid (grid, optional topo)
+    int kind = 0;
+    StratProfile prof;        // range-dependent: z only (knot altitudes)
+    iga::RngdepGrid grid;
+    iga::Terrain topo;
+    bool has_topo = false;
+    double* d_hyb = nullptr;  // hybrid node records, then node lat, lon, z
+    double* d_topo = nullptr; // terrain node records, then node lat, lon
     double* d_knots = nullptr;
     // stream of the host-buffer entry points: one per handle, so calls on
     // different atmospheres from different host threads overlap on the GPU

@@ -86,3 +86,82 @@ def fan_angles(incl_min: float, incl_max: float, incl_step: float,
             th += incl_step
         phi += az_step
     return np.asarray(th_out, dtype=np.float64), np.asarray(ph_out, dtype=np.float64)
+
+
+def write_rngdep_grid(out_dir: str, seed: int, n_lat: int = 21, n_lon: int = 21, lat0: float = 30.0,
+                      lon0: float = -110.0, dlat: float = 1.0, dlon: float = 1.0, prefix: str = "node",
+                      z_top: float = 150.0, dz: float = 0.2, node_rms: float = 1.0):
+    """Range-dependent grid in the layout set_region reads for the range-
+    dependent solvers (atmo_io.sph.rngdep.cpp:61-131): a latitude list, a
+    longitude list (degrees, one per line) and one ``zTuvdp`` profile per node
+    named ``{prefix}{n}.met`` with n = i_lat * n_lon + i_lon.
+
+    Each node is the single-profile generator above with jet amplitudes that
+    vary smoothly across the grid (seeded phases, +-30 %), the same 20 gravity
+    waves everywhere (so horizontal differences stay smooth) and a small
+    node-specific perturbation (``node_rms`` m/s rms, 8 waves).
+    Returns (prefix_path, lat_file, lon_file).
+    """
+    os.makedirs(out_dir, exist_ok=True)
+    g = np.random.default_rng(seed)
+    ph = g.uniform(0.0, 2 * np.pi, 4)
+    lats = lat0 + dlat * np.arange(n_lat)
+    lons = lon0 + dlon * np.arange(n_lon)
+    lat_file = os.path.join(out_dir, f"{prefix}_lat.dat")
+    lon_file = os.path.join(out_dir, f"{prefix}_lon.dat")
+    with open(lat_file, "w") as f:
+        f.write("".join(f"{x:.6f}\n" for x in lats))
+    with open(lon_file, "w") as f:
+        f.write("".join(f"{x:.6f}\n" for x in lons))
+    for i in range(n_lat):
+        for j in range(n_lon):
+            a = i / max(n_lat - 1, 1)
+            b = j / max(n_lon - 1, 1)
+            js = (1.0 + 0.3 * np.sin(2 * np.pi * a + ph[0]) * np.cos(np.pi * b + ph[1]),
+                  1.0 + 0.3 * np.cos(np.pi * a + ph[2]) * np.sin(2 * np.pi * b + ph[3]))
+            z, T, u, v, rho, p = profile_columns(seed, z_top=z_top, dz=dz, jet_scale=js,
+                                                 rng=np.random.default_rng(seed))
+            if node_rms > 0.0:
+                gn = np.random.default_rng([seed, i, j])
+                amp = node_rms / np.sqrt(8 / 2.0)
+                for comp in (u, v):
+                    lam = gn.uniform(2.0, 20.0, 8)
+                    phs = gn.uniform(0.0, 2 * np.pi, 8)
+                    comp += amp * np.sin(2 * np.pi * z[:, None] / lam[None, :] + phs[None, :]).sum(axis=1)
+            path = os.path.join(out_dir, f"{prefix}{i * n_lon + j}.met")
+            with open(path, "w") as f:
+                f.write(f"# synthetic infraga-b200 range-dependent node ({i}, {j}), seed {seed}\n")
+                for row in zip(z, T, u, v, rho, p):
+                    f.write("\t".join(f"{x:.10e}" for x in row) + "\n")
+    return os.path.join(out_dir, prefix), lat_file, lon_file
+
+
+def fractal_terrain(seed: int, n_lat: int, n_lon: int, z_max: float = 3.0, slope: float = -2.0):
+    """Seeded fractal terrain: white noise shaped to a power spectrum
+    proportional to k^slope, rescaled to [0, z_max] km."""
+    g = np.random.default_rng(seed)
+    w = g.standard_normal((n_lat, n_lon))
+    ky = np.fft.fftfreq(n_lat)[:, None]
+    kx = np.fft.fftfreq(n_lon)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amp = k ** (slope / 2.0)
+    amp[0, 0] = 0.0
+    z = np.real(np.fft.ifft2(np.fft.fft2(w) * amp))
+    z -= z.min()
+    z *= z_max / max(z.max(), 1e-30)
+    return z
+
+
+def write_terrain(path: str, seed: int, lat0: float, lat1: float, lon0: float, lon1: float, step: float,
+                  z_max: float = 3.0):
+    """Terrain file for topo_file= (atmo_io.sph.rngdep.cpp:213-225): rows
+    ``lat lon z`` [deg, deg, km], latitude-major, longitude increasing fastest."""
+    lats = np.round(np.arange(lat0, lat1 + step * 0.5, step), 8)
+    lons = np.round(np.arange(lon0, lon1 + step * 0.5, step), 8)
+    z = fractal_terrain(seed, lats.size, lons.size, z_max)
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        for i, la in enumerate(lats):
+            f.write("".join(f"{la:.8f}\t{lo:.8f}\t{z[i, j]:.8e}\n" for j, lo in enumerate(lons)))
+    return path

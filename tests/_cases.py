@@ -106,6 +106,27 @@ def case_setup_sph(args, z_ground: float = 0.0, z_top: float = 150.0):
     return th, ph, p
 
 
+def golden_src(name: str):
+    """Source (lat, lon, alt) a range-dependent fixture ran with (its
+    ``# src`` line: run_prop puts the default source at the region centre)."""
+    with open(os.path.join(GOLDEN, name + ".txt")) as f:
+        for line in f:
+            if line.startswith("# src "):
+                return tuple(float(x) for x in line.split()[2:5])
+    raise ValueError(f"{name}: no source line")
+
+
+def golden_angles(name: str):
+    """(theta, phi) of every ray of a fixture, from its ``R`` lines."""
+    th, ph = [], []
+    with open(os.path.join(GOLDEN, name + ".txt")) as f:
+        for line in f:
+            if line.startswith("R\t"):
+                _, t, p, _ = line.split("\t")
+                th.append(float(t)); ph.append(float(p))
+    return np.array(th), np.array(ph)
+
+
 def _fan_args(kv):
     th_min, th_max, th_step = 0.5, 45.0, 0.5
     az_min, az_max, az_step = -90.0, -90.0, 1.0

@@ -73,6 +73,29 @@ SPH_CASES = {
                                               "write_rays=false"]),
 }
 
+# Spherical range-dependent fans through oracle/harness/harness_sphr.cpp over
+# a seeded 5 x 5 node grid (1.5 deg spacing, 151 levels) and a seeded fractal
+# terrain on a 0.2 deg grid (files under rngdep/).  "TOPO" stands for the
+# terrain file.
+RNGDEP_DIR = os.path.join(HERE, "rngdep")
+RNGDEP_CASES = {
+    "sphr_flat": ["incl_min=2", "incl_max=30", "incl_step=4", "az_min=45", "az_max=225", "az_step=180",
+                  "bounces=3", "write_rays=false"],
+    "sphr_topo": ["topo_file=TOPO", "incl_min=2", "incl_max=30", "incl_step=4", "az_min=90", "az_max=270",
+                  "az_step=180", "bounces=3", "write_rays=true"],
+    "sphr_topo_noamp": ["topo_file=TOPO", "calc_amp=false", "incl_min=5", "incl_max=25", "incl_step=10",
+                        "az_min=0", "az_max=270", "az_step=90", "bounces=2"],
+    "sphr_topo_elevated": ["topo_file=TOPO", "src_alt=5", "incl_min=-30", "incl_max=10", "incl_step=10",
+                           "az_min=0", "az_max=270", "az_step=90", "bounces=2"],
+}
+
+
+def rngdep_files():
+    """(prefix, lat_file, lon_file, topo_file) of the committed range-dependent fixtures."""
+    return (os.path.join(RNGDEP_DIR, "node"), os.path.join(RNGDEP_DIR, "node_lat.dat"),
+            os.path.join(RNGDEP_DIR, "node_lon.dat"), os.path.join(RNGDEP_DIR, "topo.dat"))
+
+
 # Eigenray searches (run_eig_search through the same driver; the reference
 # writes these rows with setprecision(8)).  name -> (profile seed, argv)
 EIG_CASES = {
@@ -117,6 +140,21 @@ def main():
             f.write(r.stdout)
         meta[name] = {"binary": binary, "mode": mode, "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
+    if not only or any(n in only for n in RNGDEP_CASES):
+        synth.write_rngdep_grid(RNGDEP_DIR, 5, n_lat=5, n_lon=5, lat0=30.0, lon0=-110.0, dlat=1.5, dlon=1.5,
+                                dz=1.0, prefix="node")
+        synth.write_terrain(os.path.join(RNGDEP_DIR, "topo.dat"), 5, 30.0, 36.0, -110.0, -104.0, 0.2, 2.0)
+    prefix, lat_f, lon_f, topo_f = rngdep_files()
+    for name, args in RNGDEP_CASES.items():
+        if not want(name):
+            continue
+        argv = [a.replace("TOPO", topo_f) for a in args]
+        cmd = [os.path.join(REF, "iga_ref_sphr"), "prop", prefix, lat_f, lon_f, *argv]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(os.path.join(HERE, name + ".txt"), "w") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": "iga_ref_sphr", "mode": "prop", "seed": 5, "args": args}
+        print(name, r.stdout.strip().splitlines()[-2])
     for name, (seed, args) in EIG_CASES.items():
         if not want(name):
             continue
