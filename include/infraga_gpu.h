@@ -127,21 +127,24 @@ int iga_device_count(int* count);
  * and uploads the tables to the current CUDA device. */
 int iga_atmo_load(const char* met_path, const char* format, int reverse_winds, iga_atmo_t* out);
 
-/* Replaces set_region(prefix, lat_file, lon_file[, topo_file], format,
- * invert_winds) of the range-dependent spherical solver
- * (src/atmo/atmo_io.sph.rngdep.cpp:61-188, 191-311): latitude and longitude
- * node lists [deg], node profiles {prefix}{n}.met with n = i_lat * n_lon +
- * i_lon, and optionally a terrain file of "lat lon z" rows [deg, deg, km].
- * Builds the hybrid-spline node tables (interp::set for hybrid_spline_3D,
- * src/util/interpolation.cpp:910-1045) and the terrain spline tables in
- * FP64 on the host and uploads them.  topo_file may be NULL (flat ground at
- * z_grnd).  Such a handle runs spherical FP64 fans (IGA_GEOM_SPH). */
-int iga_atmo_load_rngdep(const char* prefix, const char* lat_file, const char* lon_file, const char* topo_file,
-                         const char* format, int reverse_winds, iga_atmo_t* out);
+/* Replaces set_region(prefix, x_file, y_file[, topo_file], format,
+ * invert_winds) of the range-dependent solvers
+ * (src/atmo/atmo_io.sph.rngdep.cpp:61-311, src/atmo/atmo_io.3d.rngdep.cpp:58-330).
+ * geometry = IGA_GEOM_SPH: latitude and longitude node lists [deg] and terrain
+ * rows "lat lon z" [deg, deg, km]; IGA_GEOM_3D: x and y node lists [km] and
+ * terrain rows "x y z" [km].  Node profiles are {prefix}{n}.met with
+ * n = i_x * n_y + i_y.  Builds the hybrid-spline node tables (interp::set for
+ * hybrid_spline_3D, src/util/interpolation.cpp:910-1045) and the terrain
+ * spline tables in FP64 on the host and uploads them.  topo_file may be NULL
+ * (flat ground).  Such a handle runs FP64 fans of the geometry it was loaded
+ * for. */
+int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_file, const char* topo_file,
+                         const char* format, int reverse_winds, int geometry, iga_atmo_t* out);
 
-/* Horizontal propagation region of an atmosphere [deg] (geoac::set_limits):
- * for a range-dependent grid its node extent, intersected with the terrain
- * extent, less 1e-3 deg on each side; the whole globe for a 1D profile. */
+/* Horizontal propagation region of an atmosphere (geoac::set_limits): for a
+ * range-dependent grid its node extent, intersected with the terrain extent,
+ * less 1e-3 deg (spherical, degrees) or 0.001 km (3D, km) on each side; the
+ * whole globe in degrees for a 1D profile. */
 int iga_atmo_region(iga_atmo_t atmo, double* lat_min, double* lat_max, double* lon_min, double* lon_max);
 
 /* Same as iga_atmo_load from arrays already in solver units. */
@@ -168,7 +171,9 @@ int iga_fan_params_default(iga_atmo_t atmo, iga_fan_params* params);
  * longitude +-180; time_max 10 h; the other fields as for 3D.  On a
  * range-dependent handle (run_prop of infraga-sph-rngdep,
  * main.infraga.sph.rngdep.cpp:207-239): 2 bounces, the iga_atmo_region
- * limits, and the source at the centre of that region. */
+ * limits, and the source at the centre of that region.  IGA_GEOM_3D on a
+ * 3D range-dependent handle (main.infraga.3d.rngdep.cpp:210-242): x/y limits
+ * from iga_atmo_region, source at its centre, rng_max 1000. */
 int iga_fan_params_init(iga_atmo_t atmo, int geometry, iga_fan_params* params);
 
 /* ---- ray fans ---- */

@@ -87,7 +87,7 @@ _SIGS = {
     "iga_atmo_limits": (_I, [_VP, _P(_D), _P(_D)]),
     "iga_atmo_destroy": (_I, [_VP]),
     "iga_atmo_load_rngdep": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
-                                  _I, _P(_VP)]),
+                                  _I, _I, _P(_VP)]),
     "iga_atmo_region": (_I, [_VP, _P(_D), _P(_D), _P(_D), _P(_D)]),
     "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
     "iga_fan_params_init": (_I, [_VP, _I, _P(FanParams)]),
@@ -160,15 +160,17 @@ class Atmosphere:
         return cls(h)
 
     @classmethod
-    def load_rngdep(cls, prefix: str, lat_file: str, lon_file: str, topo_file: str | None = None,
-                    fmt: str = "zTuvdp", reverse_winds: bool = False) -> "Atmosphere":
-        """Range-dependent grid ({prefix}{n}.met node profiles on the lat/lon
-        node lists) with optional terrain (the range-dependent set_region,
-        atmo_io.sph.rngdep.cpp:61-311)."""
+    def load_rngdep(cls, prefix: str, x_file: str, y_file: str, topo_file: str | None = None,
+                    fmt: str = "zTuvdp", reverse_winds: bool = False, geometry: int = GEOM_SPH) -> "Atmosphere":
+        """Range-dependent grid ({prefix}{n}.met node profiles on the node
+        lists: lat/lon in degrees for GEOM_SPH, x/y in km for GEOM_3D) with
+        optional terrain (the range-dependent set_region,
+        atmo_io.sph.rngdep.cpp:61-311 and atmo_io.3d.rngdep.cpp:58-330)."""
         h = _VP()
-        _check(lib().iga_atmo_load_rngdep(str(prefix).encode(), str(lat_file).encode(), str(lon_file).encode(),
+        _check(lib().iga_atmo_load_rngdep(str(prefix).encode(), str(x_file).encode(), str(y_file).encode(),
                                           str(topo_file).encode() if topo_file else None, fmt.encode(),
-                                          int(reverse_winds), ctypes.byref(h)), f"iga_atmo_load_rngdep({prefix})")
+                                          int(reverse_winds), int(geometry), ctypes.byref(h)),
+               f"iga_atmo_load_rngdep({prefix})")
         return cls(h)
 
     def region(self):

@@ -31,13 +31,13 @@ int file_length(const char* path) {
     return n - 1;
 }
 
-int read_list(const char* path, int n, std::vector<double>& out, std::string& err) {
+int read_list(const char* path, int n, bool degrees, std::vector<double>& out, std::string& err) {
     std::ifstream in(path);
     if (!in.is_open()) { err = std::string("cannot open '") + path + "'"; return IGA_E_IO; }
     out.resize(n);
     for (int i = 0; i < n; i++) {
         if (!(in >> out[i])) { err = std::string("'") + path + "': expected " + std::to_string(n) + " values"; return IGA_E_IO; }
-        out[i] *= kPi / 180.0;
+        if (degrees) out[i] *= kPi / 180.0;
     }
     for (int i = 0; i + 1 < n; i++)
         if (!(out[i + 1] > out[i])) { err = std::string("'") + path + "': node coordinates must increase"; return IGA_E_IO; }
@@ -52,13 +52,13 @@ inline int dn(int i) { return i > 0 ? i - 1 : 0; }
 }  // namespace
 
 int load_rngdep(const char* prefix, const char* lat_file, const char* lon_file, const char* format,
-                bool reverse_winds, RngdepGrid& g, std::string& err) {
+                bool reverse_winds, bool degrees, RngdepGrid& g, std::string& err) {
     const int nx = file_length(lat_file), ny = file_length(lon_file);
     if (nx < 2 || ny < 2) { err = "latitude/longitude node lists need at least 2 entries each"; return IGA_E_IO; }
     g = RngdepGrid();
-    int rc = read_list(lat_file, nx, g.x, err);
+    int rc = read_list(lat_file, nx, degrees, g.x, err);
     if (rc) return rc;
-    if ((rc = read_list(lon_file, ny, g.y, err))) return rc;
+    if ((rc = read_list(lon_file, ny, degrees, g.y, err))) return rc;
     g.nx = nx; g.ny = ny;
     for (int ix = 0; ix < nx; ix++) {
         for (int iy = 0; iy < ny; iy++) {
@@ -150,7 +150,7 @@ void build_hybrid_table(RngdepGrid& g) {
     }
 }
 
-int load_terrain(const char* path, Terrain& t, std::string& err) {
+int load_terrain(const char* path, bool degrees, Terrain& t, std::string& err) {
     // file_2d_dims: N rows; n_lon = index of the first row whose lon decreases
     const int N = file_length(path);
     std::ifstream in(path);
@@ -174,8 +174,8 @@ int load_terrain(const char* path, Terrain& t, std::string& err) {
     for (int ix = 0; ix < nx; ix++)
         for (int iy = 0; iy < ny; iy++) {
             const double* r = &a[3 * ((size_t)ix * ny + iy)];
-            t.x[ix] = r[0] * (kPi / 180.0);
-            t.y[iy] = r[1] * (kPi / 180.0);
+            t.x[ix] = degrees ? r[0] * (kPi / 180.0) : r[0];
+            t.y[iy] = degrees ? r[1] * (kPi / 180.0) : r[1];
             t.f[(size_t)ix * ny + iy] = r[2];
         }
     for (int i = 0; i + 1 < nx; i++) if (!(t.x[i + 1] > t.x[i])) { err = "terrain latitudes must increase"; return IGA_E_IO; }

@@ -41,28 +41,30 @@ constexpr int kHybXOff = 4 * kHybP;      // first extra block (c), then u, v
 
 struct RngdepGrid {
     int nx = 0, ny = 0, nz = 0;                 // latitude, longitude, altitude counts
-    std::vector<double> x, y, z;                // lat [rad], lon [rad], z [km]
+    std::vector<double> x, y, z;                // lat, lon [rad] (or x, y [km]), z [km]
     std::vector<double> f[4];                   // c, u, v, rho at [(ix * ny + iy) * nz + iz]
     std::vector<double> table;                  // nx * ny * nz * kHybRec
 };
 
 struct Terrain {
     int nx = 0, ny = 0;
-    std::vector<double> x, y;                   // lat, lon [rad]
+    std::vector<double> x, y;                   // lat, lon [rad] (or x, y [km])
     std::vector<double> f;                      // [ix * ny + iy] km
     std::vector<double> table;                  // nx * ny * 4: f, f_x, f_y, f_xy
     double z_max = 0.0;                         // max node height
 };
 
-// set_region for the range-dependent solvers (atmo_io.sph.rngdep.cpp:61-188):
-// latitude and longitude lists in degrees, node profiles {prefix}{n}.met with
-// n = i_lat * n_lon + i_lon, same columns and conversions as the 1D loader.
+// set_region for the range-dependent solvers (atmo_io.sph.rngdep.cpp:61-188,
+// atmo_io.3d.rngdep.cpp:58-190): node coordinate lists (latitude/longitude in
+// degrees when `degrees`, else x/y in km), node profiles {prefix}{n}.met with
+// n = i_x * n_y + i_y, same columns and conversions as the 1D loader.
 int load_rngdep(const char* prefix, const char* lat_file, const char* lon_file, const char* format,
-                bool reverse_winds, RngdepGrid& g, std::string& err);
+                bool reverse_winds, bool degrees, RngdepGrid& g, std::string& err);
 
-// Terrain file of rows "lat lon z" (deg, deg, km), latitude-major
-// (atmo_io.sph.rngdep.cpp:205-225 with file_2d_dims, fileIO.cpp:64-85).
-int load_terrain(const char* path, Terrain& t, std::string& err);
+// Terrain file of rows "lat lon z" (deg, deg, km; or "x y z" in km when not
+// `degrees`), first coordinate major (atmo_io.sph.rngdep.cpp:205-225,
+// atmo_io.3d.rngdep.cpp:205-223, file_2d_dims fileIO.cpp:64-85).
+int load_terrain(const char* path, bool degrees, Terrain& t, std::string& err);
 
 void build_hybrid_table(RngdepGrid& g);
 void build_terrain_table(Terrain& t);

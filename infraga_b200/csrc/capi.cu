@@ -286,10 +286,62 @@ int build_args_sphr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     return IGA_OK;
 }
 
+// 3D range-dependent launch constants (run_prop of infraga-3d-rngdep,
+// main.infraga.3d.rngdep.cpp:235-309; set_initial; topo::set_bndlyr).
+// Without terrain topo::z is 0 in this solver (atmo_state.3d.rngdep.cpp:45-51).
+int build_args_3dr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const iga::RngdepGrid& g = h->grid;
+    a.src_x = p->src[0]; a.src_y = p->src[1];
+    a.x_min = p->x_min; a.x_max = p->x_max; a.y_min = p->y_min; a.y_max = p->y_max;
+    a.z0 = p->z_grnd;
+    auto topo_z = [&](double x, double y) {
+        if (!h->has_topo) return 0.0;
+        double z, dz[2];
+        iga::terrain_eval1(h->topo, x, y, z, dz);
+        return z;
+    };
+    if (h->has_topo) {
+        a.topo_zmax = h->topo.z_max + 0.01;
+        a.z_bl = h->topo.z_max + 2.0;
+        a.x_cut = h->topo.z_max + 40.0;
+    } else {
+        a.topo_zmax = a.z0;
+        a.z_bl = a.z0 + 2.0;
+        a.x_cut = 40.0;
+    }
+    a.src_z = std::max(p->src[2], topo_z(a.src_x, a.src_y));
+    double sc = 1.0;
+    if (a.src_z < a.z_bl) {
+        const double X = std::exp(-(a.src_z - topo_z(a.src_x, a.src_y)) / 0.1);
+        sc = (1.0 - X) / (1.0 + X);
+    }
+    double f, df[3];
+    iga::hybrid_eval1(g, 0, a.src_x, a.src_y, a.src_z, f, df); a.c0 = f;
+    iga::hybrid_eval1(g, 1, a.src_x, a.src_y, a.src_z, f, df); a.u0s = f * sc;
+    iga::hybrid_eval1(g, 2, a.src_x, a.src_y, a.src_z, f, df); a.v0s = f * sc;
+    iga::hybrid_eval1(g, 3, a.src_x, a.src_y, a.src_z, f, df); a.rho0 = f;
+    a.hyb_tab = h->d_hyb;
+    const size_t n_rec = (size_t)g.nx * g.ny * g.nz * iga::kHybRec;
+    a.hyb_x = h->d_hyb + n_rec;
+    a.hyb_y = a.hyb_x + g.nx;
+    a.hyb_z = a.hyb_y + g.ny;
+    a.hyb_nx = g.nx; a.hyb_ny = g.ny; a.hyb_nz = g.nz;
+    if (h->has_topo) {
+        const iga::Terrain& t = h->topo;
+        a.topo_tab = h->d_topo;
+        a.topo_x = h->d_topo + (size_t)t.nx * t.ny * 4;
+        a.topo_y = a.topo_x + t.nx;
+        a.topo_nx = t.nx; a.topo_ny = t.ny;
+    } else {
+        a.topo_tab = nullptr; a.topo_x = a.topo_y = nullptr; a.topo_nx = a.topo_ny = 0;
+    }
+    return IGA_OK;
+}
+
 int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     const StratProfile& P = h->prof;
     memset(&a, 0, sizeof(a));
-    if (h->kind == 1) {
+    if (h->kind != 0) {
         a.bounces = p->bounces;
         a.write_rays = p->write_rays ? 1 : 0;
         a.length = (int)(p->s_max / p->ds_min);
@@ -301,7 +353,7 @@ int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
         a.sb.x0_low = std::pow(10.0, -0.67887);
         a.sb.x1_low = std::pow(10.0, -0.10744);
         a.sb.x2 = std::pow(10.0, -3.3979);
-        return build_args_sphr(h, p, a);
+        return h->kind == 1 ? build_args_sphr(h, p, a) : build_args_3dr(h, p, a);
     }
     a.knots = h->d_knots;
     a.n_knots = (int)P.z.size();
@@ -348,8 +400,8 @@ namespace {
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st) {
-    if (h->kind == 1 && (p->geometry != IGA_GEOM_SPH || p->precision != IGA_FP64)) {
-        g_cuda_err = "range-dependent atmosphere: spherical geometry, FP64 only";
+    if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) || p->precision != IGA_FP64)) {
+        g_cuda_err = "range-dependent atmosphere: FP64, with the geometry it was loaded for";
         return IGA_E_UNSUPPORTED;
     }
     iga::Fan3DArgs a;
@@ -369,6 +421,8 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     if (n_rays == 0) return IGA_OK;
     if (h->kind == 1)
         IGA_CUDA(iga::launch_fansphr_fp64(a, p->calc_amp != 0, st, nullptr), "fansphr kernel launch");
+    else if (h->kind == 2)
+        IGA_CUDA(iga::launch_fan3dr_fp64(a, p->calc_amp != 0, st, nullptr), "fan3dr kernel launch");
     else if (p->geometry == IGA_GEOM_SPH)
         IGA_CUDA(iga::launch_fansph_fp64(a, p->calc_amp != 0, st, nullptr), "fansph kernel launch");
     else if (p->precision == IGA_FP32C)
@@ -419,16 +473,18 @@ int iga_atmo_load(const char* met_path, const char* format, int reverse_winds, i
     return IGA_OK;
 }
 
-int iga_atmo_load_rngdep(const char* prefix, const char* lat_file, const char* lon_file, const char* topo_file,
-                         const char* format, int reverse_winds, iga_atmo_t* out) {
-    if (!prefix || !lat_file || !lon_file || !out) return IGA_E_INVALID;
+int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_file, const char* topo_file,
+                         const char* format, int reverse_winds, int geometry, iga_atmo_t* out) {
+    if (!prefix || !x_file || !y_file || !out) return IGA_E_INVALID;
+    if (geometry != IGA_GEOM_3D && geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
     *out = nullptr;
     iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
     if (!h) return IGA_E_NOMEM;
-    h->kind = 1;
-    int rc = iga::load_rngdep(prefix, lat_file, lon_file, format ? format : "zTuvdp", reverse_winds != 0, h->grid, g_err);
+    const bool sph = geometry == IGA_GEOM_SPH;
+    h->kind = sph ? 1 : 2;
+    int rc = iga::load_rngdep(prefix, x_file, y_file, format ? format : "zTuvdp", reverse_winds != 0, sph, h->grid, g_err);
     if (rc == IGA_OK && topo_file && topo_file[0]) {
-        rc = iga::load_terrain(topo_file, h->topo, g_err);
+        rc = iga::load_terrain(topo_file, sph, h->topo, g_err);
         h->has_topo = (rc == IGA_OK);
     }
     if (rc == IGA_OK) rc = upload_rngdep(h);
@@ -440,7 +496,17 @@ int iga_atmo_load_rngdep(const char* prefix, const char* lat_file, const char* l
 int iga_atmo_region(iga_atmo_t h, double* lat_min, double* lat_max, double* lon_min, double* lon_max) {
     if (!h) return IGA_E_INVALID;
     double r[4] = {-90.0, 90.0, -180.0, 180.0};
-    if (h->kind == 1) {
+    if (h->kind == 2) {
+        // geoac::set_limits (atmo_io.3d.rngdep.cpp:25-40): grid (and terrain) extent less 0.001 km
+        const double buf = 0.001;
+        double a0 = h->grid.x.front() + buf, a1 = h->grid.x.back() - buf;
+        double b0 = h->grid.y.front() + buf, b1 = h->grid.y.back() - buf;
+        if (h->has_topo) {
+            a0 = std::max(a0, h->topo.x.front() + buf); a1 = std::min(a1, h->topo.x.back() - buf);
+            b0 = std::max(b0, h->topo.y.front() + buf); b1 = std::min(b1, h->topo.y.back() - buf);
+        }
+        r[0] = a0; r[1] = a1; r[2] = b0; r[3] = b1;
+    } else if (h->kind == 1) {
         // geoac::set_limits (atmo_io.sph.rngdep.cpp:27-43): grid (and terrain) extent less 1e-3 deg
         const double buf = 1.0e-3 * (iga::kPi / 180.0);
         double a0 = h->grid.x.front() + buf, a1 = h->grid.x.back() - buf;
@@ -519,6 +585,15 @@ int iga_fan_params_init(iga_atmo_t h, int geometry, iga_fan_params* p) {
     if (geometry != IGA_GEOM_3D && geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
     int rc = iga_fan_params_default(h, p);
     if (rc) return rc;
+    if (h->kind == 2 && geometry == IGA_GEOM_3D) {
+        // run_prop of infraga-3d-rngdep (main.infraga.3d.rngdep.cpp:210-242): the
+        // set_limits region and the source at its centre; rng_max keeps the
+        // 1000 km of geoac.params.3d.cpp (set_limits here does not reset it)
+        iga_atmo_region(h, &p->x_min, &p->x_max, &p->y_min, &p->y_max);
+        p->src[0] = (p->x_max + p->x_min) / 2.0;
+        p->src[1] = (p->y_max + p->y_min) / 2.0;
+        p->rng_max = 1000.0;
+    }
     if (geometry == IGA_GEOM_SPH) {
         p->geometry = IGA_GEOM_SPH;
         p->src[0] = 30.0; p->src[1] = 0.0; p->src[2] = 0.0;

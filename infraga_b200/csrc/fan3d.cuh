@@ -86,6 +86,9 @@ cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t st
 // Spherical (global) stratified fan, FP64 (fansph_fp64.cu).
 cudaError_t launch_fansph_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 
+// 3D Cartesian range-dependent fan with optional terrain, FP64 (fan3dr_fp64.cu).
+cudaError_t launch_fan3dr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
 // Spherical range-dependent fan with optional terrain, FP64 (fansphr_fp64.cu).
 cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 

@@ -90,11 +90,13 @@ def fan_angles(incl_min: float, incl_max: float, incl_step: float,
 
 def write_rngdep_grid(out_dir: str, seed: int, n_lat: int = 21, n_lon: int = 21, lat0: float = 30.0,
                       lon0: float = -110.0, dlat: float = 1.0, dlon: float = 1.0, prefix: str = "node",
-                      z_top: float = 150.0, dz: float = 0.2, node_rms: float = 1.0):
+                      z_top: float = 150.0, dz: float = 0.2, node_rms: float = 1.0, axes=("lat", "lon")):
     """Range-dependent grid in the layout set_region reads for the range-
     dependent solvers (atmo_io.sph.rngdep.cpp:61-131): a latitude list, a
     longitude list (degrees, one per line) and one ``zTuvdp`` profile per node
-    named ``{prefix}{n}.met`` with n = i_lat * n_lon + i_lon.
+    named ``{prefix}{n}.met`` with n = i_lat * n_lon + i_lon.  For the 3D
+    Cartesian solver the same layout holds with x/y node lists in km
+    (``axes=("x", "y")``, atmo_io.3d.rngdep.cpp:86-110).
 
     Each node is the single-profile generator above with jet amplitudes that
     vary smoothly across the grid (seeded phases, +-30 %), the same 20 gravity
@@ -107,8 +109,8 @@ def write_rngdep_grid(out_dir: str, seed: int, n_lat: int = 21, n_lon: int = 21,
     ph = g.uniform(0.0, 2 * np.pi, 4)
     lats = lat0 + dlat * np.arange(n_lat)
     lons = lon0 + dlon * np.arange(n_lon)
-    lat_file = os.path.join(out_dir, f"{prefix}_lat.dat")
-    lon_file = os.path.join(out_dir, f"{prefix}_lon.dat")
+    lat_file = os.path.join(out_dir, f"{prefix}_{axes[0]}.dat")
+    lon_file = os.path.join(out_dir, f"{prefix}_{axes[1]}.dat")
     with open(lat_file, "w") as f:
         f.write("".join(f"{x:.6f}\n" for x in lats))
     with open(lon_file, "w") as f:
@@ -156,7 +158,8 @@ def fractal_terrain(seed: int, n_lat: int, n_lon: int, z_max: float = 3.0, slope
 def write_terrain(path: str, seed: int, lat0: float, lat1: float, lon0: float, lon1: float, step: float,
                   z_max: float = 3.0):
     """Terrain file for topo_file= (atmo_io.sph.rngdep.cpp:213-225): rows
-    ``lat lon z`` [deg, deg, km], latitude-major, longitude increasing fastest."""
+    ``lat lon z`` [deg, deg, km], latitude-major, longitude increasing fastest
+    (for the 3D solvers ``x y z`` in km, atmo_io.3d.rngdep.cpp:209-223)."""
     lats = np.round(np.arange(lat0, lat1 + step * 0.5, step), 8)
     lons = np.round(np.arange(lon0, lon1 + step * 0.5, step), 8)
     z = fractal_terrain(seed, lats.size, lons.size, z_max)

@@ -90,6 +90,27 @@ RNGDEP_CASES = {
 }
 
 
+# 3D Cartesian range-dependent fans through oracle/harness/harness_3dr.cpp:
+# 5 x 5 nodes at 150 km spacing over [-300, 300] km, terrain on a 20 km grid
+# (files under rngdep3d/).
+RNGDEP3D_DIR = os.path.join(HERE, "rngdep3d")
+RNGDEP3D_CASES = {
+    "3dr_flat": ["incl_min=2", "incl_max=30", "incl_step=4", "az_min=45", "az_max=225", "az_step=180",
+                 "bounces=3", "write_rays=false"],
+    "3dr_topo": ["topo_file=TOPO", "incl_min=2", "incl_max=30", "incl_step=4", "az_min=90", "az_max=270",
+                 "az_step=180", "bounces=3", "write_rays=true"],
+    "3dr_topo_noamp": ["topo_file=TOPO", "calc_amp=false", "incl_min=5", "incl_max=25", "incl_step=10",
+                       "az_min=0", "az_max=270", "az_step=90", "bounces=2"],
+    "3dr_topo_elevated": ["topo_file=TOPO", "src_alt=5", "incl_min=-30", "incl_max=10", "incl_step=10",
+                          "az_min=0", "az_max=270", "az_step=90", "bounces=2"],
+}
+
+
+def rngdep3d_files():
+    return (os.path.join(RNGDEP3D_DIR, "node"), os.path.join(RNGDEP3D_DIR, "node_x.dat"),
+            os.path.join(RNGDEP3D_DIR, "node_y.dat"), os.path.join(RNGDEP3D_DIR, "topo.dat"))
+
+
 def rngdep_files():
     """(prefix, lat_file, lon_file, topo_file) of the committed range-dependent fixtures."""
     return (os.path.join(RNGDEP_DIR, "node"), os.path.join(RNGDEP_DIR, "node_lat.dat"),
@@ -154,6 +175,21 @@ def main():
         with open(os.path.join(HERE, name + ".txt"), "w") as f:
             f.write(r.stdout)
         meta[name] = {"binary": "iga_ref_sphr", "mode": "prop", "seed": 5, "args": args}
+        print(name, r.stdout.strip().splitlines()[-2])
+    if not only or any(n in only for n in RNGDEP3D_CASES):
+        synth.write_rngdep_grid(RNGDEP3D_DIR, 9, n_lat=5, n_lon=5, lat0=-300.0, lon0=-300.0, dlat=150.0,
+                                dlon=150.0, dz=1.0, prefix="node", axes=("x", "y"))
+        synth.write_terrain(os.path.join(RNGDEP3D_DIR, "topo.dat"), 9, -300.0, 300.0, -300.0, 300.0, 20.0, 2.0)
+    prefix, x_f, y_f, topo_f = rngdep3d_files()
+    for name, args in RNGDEP3D_CASES.items():
+        if not want(name):
+            continue
+        argv = [a.replace("TOPO", topo_f) for a in args]
+        cmd = [os.path.join(REF, "iga_ref_3dr"), "prop", prefix, x_f, y_f, *argv]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(os.path.join(HERE, name + ".txt"), "w") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": "iga_ref_3dr", "mode": "prop", "seed": 9, "args": args}
         print(name, r.stdout.strip().splitlines()[-2])
     for name, (seed, args) in EIG_CASES.items():
         if not want(name):
