@@ -290,6 +290,52 @@ int iga_fan_run_device_noalloc(iga_atmo_t atmo, const iga_fan_params* params,
                                double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
                                int* d_ray_status, double* d_arrival_aux, void* stream);
 
+/* ---- request server (continuous batching on one GPU) ----
+ * No counterpart in the reference (its CLI runs one job per process).  A
+ * server keeps the callers' atmosphere handles resident, queues fan and
+ * eigenray requests, admits them as slots (CUDA streams) and device memory
+ * (hbm_budget) free up, and runs admitted requests concurrently on the GPU.
+ * A request's results are those of iga_fan_run / iga_eig_run for the same
+ * inputs, alone or in any mix. */
+typedef struct iga_server_s* iga_server_t;
+
+typedef struct iga_server_config {
+    int device;              /* CUDA device of the server and of the atmospheres it serves */
+    int max_inflight;        /* concurrent fan requests (streams); default 8 */
+    int eig_workers;         /* concurrent eigenray requests; default 2 */
+    int small_rays;          /* fans up to this size use high-priority streams and no CTA cap; 4096 */
+    double big_fan_sm_frac;  /* larger fans use at most this fraction of the resident CTA slots; 0.75 */
+    size_t hbm_budget;       /* device bytes all admitted requests may hold; default 8 GiB */
+} iga_server_config;
+
+typedef struct iga_server_stats {
+    long long completed, pending;
+    double p50_s, p99_s;             /* submit -> results on the host, all completed requests */
+    double fan_p50_s, fan_p99_s, eig_p50_s, eig_p99_s;
+    long long ray_steps, rays, eigenrays;
+    double wall_s;                   /* first submit -> last completion */
+    size_t bytes_in_use;
+} iga_server_stats;
+
+int iga_server_config_default(iga_server_config* config);
+int iga_server_create(const iga_server_config* config, iga_server_t* out);
+/* Queue a fan (inputs copied; returns at once).  id identifies the request. */
+int iga_server_submit_fan(iga_server_t server, iga_atmo_t atmo, const iga_fan_params* params,
+                          const double* theta_deg, const double* phi_deg, int n_rays, long long* id);
+int iga_server_submit_eig(iga_server_t server, iga_atmo_t atmo, const iga_eig_params* params,
+                          const iga_eig_pair* pairs, int n_pairs, long long* id);
+/* done = 1 once the request's results are on the host.  timeout_s: 0 polls,
+ * < 0 waits without limit. */
+int iga_server_wait(iga_server_t server, long long id, double timeout_s, int* done);
+/* Copy a finished request's rows (IGA_ARRIVAL_COLS each; fan: ray by ray,
+ * index = ray; eigen: as iga_eig_run, index = pair) and release it.  With
+ * cap < n_out it returns IGA_E_TRUNCATED and keeps the request. */
+int iga_server_fetch(iga_server_t server, long long id, double* rows, int cap, int* n_out, int* index,
+                     long long* total_steps, double* latency_s);
+int iga_server_get_stats(iga_server_t server, iga_server_stats* stats);
+/* Finishes the requests on the GPU, drops the queued ones, frees the server. */
+int iga_server_destroy(iga_server_t server);
+
 #ifdef __cplusplus
 }
 #endif

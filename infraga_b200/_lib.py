@@ -63,6 +63,22 @@ class EigPair(ctypes.Structure):
     _fields_ = [("src", ctypes.c_double * 3), ("rcvr", ctypes.c_double * 2)]
 
 
+class ServerConfig(ctypes.Structure):
+    """Mirror of iga_server_config."""
+    _fields_ = [("device", ctypes.c_int), ("max_inflight", ctypes.c_int), ("eig_workers", ctypes.c_int),
+                ("small_rays", ctypes.c_int), ("big_fan_sm_frac", ctypes.c_double), ("hbm_budget", ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    """Mirror of iga_server_stats."""
+    _fields_ = [("completed", ctypes.c_longlong), ("pending", ctypes.c_longlong),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double),
+                ("fan_p50_s", ctypes.c_double), ("fan_p99_s", ctypes.c_double),
+                ("eig_p50_s", ctypes.c_double), ("eig_p99_s", ctypes.c_double),
+                ("ray_steps", ctypes.c_longlong), ("rays", ctypes.c_longlong), ("eigenrays", ctypes.c_longlong),
+                ("wall_s", ctypes.c_double), ("bytes_in_use", ctypes.c_size_t)]
+
+
 class Profile(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("z", ctypes.POINTER(ctypes.c_double)), ("c", ctypes.POINTER(ctypes.c_double)),
                 ("u", ctypes.POINTER(ctypes.c_double)), ("v", ctypes.POINTER(ctypes.c_double)),
@@ -89,6 +105,14 @@ _SIGS = {
     "iga_atmo_load_rngdep": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                   _I, _I, _P(_VP)]),
     "iga_atmo_region": (_I, [_VP, _P(_D), _P(_D), _P(_D), _P(_D)]),
+    "iga_server_config_default": (_I, [_P(ServerConfig)]),
+    "iga_server_create": (_I, [_P(ServerConfig), _P(_VP)]),
+    "iga_server_submit_fan": (_I, [_VP, _VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_LL)]),
+    "iga_server_submit_eig": (_I, [_VP, _VP, _P(EigParams), _P(EigPair), _I, _P(_LL)]),
+    "iga_server_wait": (_I, [_VP, _LL, _D, _P(_I)]),
+    "iga_server_fetch": (_I, [_VP, _LL, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_D)]),
+    "iga_server_get_stats": (_I, [_VP, _P(ServerStats)]),
+    "iga_server_destroy": (_I, [_VP]),
     "iga_fan_params_default": (_I, [_VP, _P(FanParams)]),
     "iga_fan_params_init": (_I, [_VP, _I, _P(FanParams)]),
     "iga_fan_run": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL), _P(_I), _P(_LL),
@@ -300,3 +324,82 @@ def fan_run_device(atmo: Atmosphere, params: FanParams, d_theta: int, d_phi: int
                                   _VP(d_arrivals), _VP(d_n_arr), _VP(d_steps), _VP(d_status) if d_status else None,
                                   _VP(d_aux) if d_aux else None, _VP(d_workspace), _VP(stream) if stream else None)
     _check(rc, "iga_fan_run_device")
+
+
+class Server:
+    """Continuous-batching request server (iga_server_*): submit fan and
+    eigenray requests from any thread, wait for and fetch their results."""
+
+    def __init__(self, **config):
+        cfg = ServerConfig()
+        _check(lib().iga_server_config_default(ctypes.byref(cfg)), "iga_server_config_default")
+        for k, v in config.items():
+            setattr(cfg, k, v)
+        self._h = _VP()
+        _check(lib().iga_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "iga_server_create")
+        self._kind = {}
+
+    def submit_fan(self, atmo: Atmosphere, params: FanParams, theta_deg, phi_deg) -> int:
+        th = np.ascontiguousarray(theta_deg, dtype=np.float64)
+        ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
+        rid = _LL()
+        _check(lib().iga_server_submit_fan(self._h, atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph),
+                                           int(th.size), ctypes.byref(rid)), "iga_server_submit_fan")
+        self._kind[rid.value] = ("fan", int(th.size) * (params.bounces + 1))
+        return rid.value
+
+    def submit_eig(self, atmo: Atmosphere, params: EigParams, pairs) -> int:
+        arr = (EigPair * max(len(pairs), 1))()
+        for i, (src, rcvr) in enumerate(pairs):
+            arr[i].src = (_D * 3)(*src)
+            arr[i].rcvr = (_D * 2)(*rcvr)
+        rid = _LL()
+        _check(lib().iga_server_submit_eig(self._h, atmo.handle, ctypes.byref(params), arr, len(pairs),
+                                           ctypes.byref(rid)), "iga_server_submit_eig")
+        self._kind[rid.value] = ("eig", 0)
+        return rid.value
+
+    def wait(self, rid: int, timeout_s: float = -1.0) -> bool:
+        done = _I()
+        _check(lib().iga_server_wait(self._h, rid, float(timeout_s), ctypes.byref(done)), "iga_server_wait")
+        return bool(done.value)
+
+    def fetch(self, rid: int):
+        """Results of a finished request: dict with rows [n, 12], index,
+        total_steps and latency_s (submit -> results on the host)."""
+        cap = max(self._kind.get(rid, ("", 0))[1], 64)
+        while True:
+            rows = np.zeros((cap, ARRIVAL_COLS), dtype=np.float64)
+            idx = np.zeros(cap, dtype=np.int32)
+            n, steps, lat = _I(), _LL(), _D()
+            rc = lib().iga_server_fetch(self._h, rid, _dptr(rows), cap, ctypes.byref(n), idx.ctypes.data_as(_P(_I)),
+                                        ctypes.byref(steps), ctypes.byref(lat))
+            if rc == -6:   # IGA_E_TRUNCATED: request kept, retry with the count it reported
+                cap = n.value
+                continue
+            _check(rc, "iga_server_fetch")
+            self._kind.pop(rid, None)
+            m = n.value
+            return {"rows": rows[:m], "index": idx[:m], "total_steps": int(steps.value), "latency_s": lat.value}
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().iga_server_get_stats(self._h, ctypes.byref(st)), "iga_server_get_stats")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._h:
+            lib().iga_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -399,7 +399,7 @@ namespace {
 
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
-               cudaStream_t st) {
+               cudaStream_t st, int grid_cap = 0) {
     if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) || p->precision != IGA_FP64)) {
         g_cuda_err = "range-dependent atmosphere: FP64, with the geometry it was loaded for";
         return IGA_E_UNSUPPORTED;
@@ -410,6 +410,7 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     a.theta_deg = d_th; a.phi_deg = d_ph; a.n_rays = n_rays;
     a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status; a.aux = d_aux;
     a.queue = static_cast<unsigned int*>(d_ws);
+    a.grid_cap = grid_cap;
     if (p->precision == IGA_FP32C) {
         iga_atmo_s::AlphaTab t;
         rc = ensure_alpha(h, p->freq, t);
@@ -433,6 +434,17 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
 }
 
 }  // namespace
+
+namespace iga_internal {
+int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
+               double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
+               cudaStream_t st, int grid_cap) {
+    int rc = validate(p, n_rays);
+    if (rc) return rc;
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_aux, d_ws, st, grid_cap);
+}
+}  // namespace iga_internal
 
 extern "C" {
 

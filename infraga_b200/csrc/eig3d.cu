@@ -333,11 +333,15 @@ extern "C" int iga_eig_params_default(iga_atmo_t h, iga_eig_params* p) {
     return IGA_OK;
 }
 
-extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs,
-                           double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps) {
-    if (!h || !P || !n_out || n_pairs < 0 || (n_pairs > 0 && !pairs) || (cap > 0 && !eigenrays)) return IGA_E_INVALID;
-    *n_out = 0;
-    if (total_steps) *total_steps = 0;
+namespace iga_internal {
+
+// The whole search on one stream, results in host vectors (iga_eig_run and
+// the request server).  Device scratch is stream-ordered (cudaMallocAsync /
+// cudaFreeAsync), so searches on different streams overlap on the GPU.
+int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, cudaStream_t st,
+               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out) {
+    out_rows.clear(); out_pair.clear(); steps_out = 0;
+    if (!h || !P || n_pairs < 0 || (n_pairs > 0 && !pairs)) return IGA_E_INVALID;
     iga_fan_params fp = P->fan;
     fp.geometry = IGA_GEOM_3D;
     fp.bounces = 0;
@@ -388,12 +392,16 @@ extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_
         }
     }
 
-    cudaStream_t st = h->stream;
     TraceReq* d_req = nullptr;
     TraceRes* d_res = nullptr;
     size_t cap_req = 0;
     long long steps_tot = 0;
-    auto fail = [&](int code) { if (d_req) cudaFree(d_req); if (d_res) cudaFree(d_res); return code; };
+    auto release = [&]() {
+        if (d_req) cudaFreeAsync(d_req, st);
+        if (d_res) cudaFreeAsync(d_res, st);
+        d_req = nullptr; d_res = nullptr;
+    };
+    auto fail = [&](int code) { release(); return code; };
 
     std::vector<TraceReq> req6, req18;
     std::vector<TraceRes> res6, res18;
@@ -427,13 +435,11 @@ extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_
         if (req6.empty() && req18.empty()) break;
         const size_t need = std::max(req6.size(), req18.size());
         if (need > cap_req) {
-            if (d_req) cudaFree(d_req);
-            if (d_res) cudaFree(d_res);
-            d_req = nullptr; d_res = nullptr;
+            release();
             cap_req = std::max(need, cap_req * 2);
-            cudaError_t e1 = cudaMalloc(&d_req, 2 * cap_req * sizeof(TraceReq));
-            cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc(&d_res, 2 * cap_req * sizeof(TraceRes)) : e1;
-            if (e2 != cudaSuccess) return fail(cuda_fail(e2, "cudaMalloc(eigen traces)"));
+            cudaError_t e1 = cudaMallocAsync(&d_req, 2 * cap_req * sizeof(TraceReq), st);
+            cudaError_t e2 = e1 == cudaSuccess ? cudaMallocAsync(&d_res, 2 * cap_req * sizeof(TraceRes), st) : e1;
+            if (e2 != cudaSuccess) return fail(cuda_fail(e2, "cudaMallocAsync(eigen traces)"));
         }
         TraceReq* d_req18 = d_req + cap_req;
         TraceRes* d_res18 = d_res + cap_req;
@@ -484,20 +490,35 @@ extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_
             }
         }
     }
-    if (d_req) cudaFree(d_req);
-    if (d_res) cudaFree(d_res);
-
-    int w = 0;
+    release();
     for (auto& c : chains) {
         for (auto& row : c.rows) {
-            if (w < cap) {
-                memcpy(eigenrays + (size_t)w * IGA_ARRIVAL_COLS, row.data(), IGA_ARRIVAL_COLS * sizeof(double));
-                if (pair_index) pair_index[w] = c.pair;
-            }
-            w++;
+            out_rows.insert(out_rows.end(), row.begin(), row.end());
+            out_pair.push_back(c.pair);
         }
     }
+    steps_out = steps_tot;
+    return IGA_OK;
+}
+
+}  // namespace iga_internal
+
+extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs,
+                           double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps) {
+    if (!h || !P || !n_out || n_pairs < 0 || (n_pairs > 0 && !pairs) || (cap > 0 && !eigenrays)) return IGA_E_INVALID;
+    *n_out = 0;
+    if (total_steps) *total_steps = 0;
+    std::vector<double> rows;
+    std::vector<int> pidx;
+    long long steps = 0;
+    int rc = eig_search(h, P, pairs, n_pairs, h->stream, rows, pidx, steps);
+    if (rc) return rc;
+    const int w = (int)pidx.size();
+    for (int i = 0; i < w && i < cap; i++) {
+        memcpy(eigenrays + (size_t)i * IGA_ARRIVAL_COLS, &rows[(size_t)i * IGA_ARRIVAL_COLS], IGA_ARRIVAL_COLS * sizeof(double));
+        if (pair_index) pair_index[i] = pidx[i];
+    }
     *n_out = w;
-    if (total_steps) *total_steps = steps_tot;
+    if (total_steps) *total_steps = steps;
     return w > cap ? IGA_E_TRUNCATED : IGA_OK;
 }

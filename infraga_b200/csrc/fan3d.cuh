@@ -27,6 +27,7 @@ struct Fan3DArgs {
     int* ray_status;         // nullable
     double* aux;             // nullable: [n_rays][bounces+1][4] per-arrival diagnostics
     unsigned int* queue;     // [0] next ray (device ray queue)
+    int grid_cap;            // > 0: at most this many CTAs (the request server shares the GPU)
     // geometry / limits
     double src_x, src_y, src_z;
     double ds_min, ds_max, s_max;

@@ -405,6 +405,7 @@ cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     long long want = ((long long)a.n_rays + kThreadsC - 1) / kThreadsC;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
+    if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
     kern<<<(unsigned)grid, kThreadsC, smem, stream>>>(a);

@@ -6,6 +6,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/infraga_gpu.h"
 #include "atmo_host.h"
@@ -45,6 +46,13 @@ extern thread_local std::string g_err;
 int cuda_fail(cudaError_t e, const char* what);
 int validate(const iga_fan_params* p, int n_rays);
 int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a);
+// iga_fan_run_device with an optional CTA cap (0 = none), for the request server
+int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
+               double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
+               cudaStream_t st, int grid_cap);
+// the eigenray search on one stream (eig3d.cu)
+int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, cudaStream_t st,
+               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out);
 }  // namespace iga_internal
 
 #define IGA_CUDA(call, what)                                                  \
