@@ -430,6 +430,127 @@ def run_ours(args):
     return 0 if result is not None or rank != 0 else 1
 
 
+# ---------------------------------------------------------------- serving
+SERVE = dict(rate=200.0, requests=200, fan_rays=(100, 100_000), eig_pairs=(1, 64), eig_frac=0.25,
+             n_strat=56, n_rngdep=8, seed=11)
+
+
+def serving_workload(tmp, args):
+    """Config-4 request stream: Poisson arrivals (rate/s) of ray-fan requests
+    (log-uniform 100..100,000 rays) and eigenray requests (1..64 pairs) over
+    64 resident synthetic atmospheres (56 stratified, 8 spherical 11x11
+    range-dependent grids)."""
+    from infraga_b200 import synth
+    g = np.random.default_rng(SERVE["seed"])
+    strat = [synth.write_met(os.path.join(tmp, f"s{i}.met"), 100 + i) for i in range(SERVE["n_strat"])]
+    grids = []
+    for i in range(SERVE["n_rngdep"]):
+        d = os.path.join(tmp, f"g{i}")
+        grids.append(synth.write_rngdep_grid(d, 200 + i, n_lat=11, n_lon=11, lat0=30.0 + i, lon0=-110.0 + 2 * i,
+                                             dlat=1.0, dlon=1.0, prefix="node"))
+    th_all, ph_all = synth.fan_angles(0.5, 60.01, 0.1, 0.0, 357.0, 3.0)
+    t = 0.0
+    reqs = []
+    for _ in range(args.serve_requests):
+        t += g.exponential(1.0 / args.serve_rate)
+        if g.random() < SERVE["eig_frac"]:
+            n = int(g.integers(SERVE["eig_pairs"][0], SERVE["eig_pairs"][1] + 1))
+            rng_km = g.uniform(50.0, 500.0, n)
+            az = g.uniform(0.0, 2 * np.pi, n)
+            pairs = [((0.0, 0.0, 0.0), (float(r * np.cos(a)), float(r * np.sin(a)))) for r, a in zip(rng_km, az)]
+            reqs.append(dict(t=t, kind="eig", atmo=int(g.integers(0, SERVE["n_strat"])), pairs=pairs))
+        else:
+            n = int(np.exp(g.uniform(np.log(SERVE["fan_rays"][0]), np.log(SERVE["fan_rays"][1]))))
+            pick = np.sort(g.choice(th_all.size, size=min(n, th_all.size), replace=False))
+            a = int(g.integers(0, SERVE["n_strat"] + SERVE["n_rngdep"]))
+            reqs.append(dict(t=t, kind="fan", atmo=a, th=th_all[pick], ph=ph_all[pick]))
+    return strat, grids, reqs
+
+
+def run_serving(args):
+    """p50/p99 request latency and throughput of the request server under the
+    config-4 stream, beside the one-request-at-a-time FP64 path."""
+    import torch
+    import infraga_b200 as ig
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp(prefix="iga_serve_")
+    strat_files, grid_files, reqs = serving_workload(tmp, args)
+    strat = [ig.Atmosphere.load(m) for m in strat_files]
+    grids = [ig.Atmosphere.load_rngdep(*g_) for g_ in grid_files]
+    eigp = ig.eig_params(strat[0], bnc_min=0, bnc_max=1)
+
+    def params_for(r, precision):
+        if r["atmo"] < len(strat):
+            a = strat[r["atmo"]]
+            return a, a.default_params(bounces=5, rng_max=1000.0, write_rays=0, precision=precision)
+        a = grids[r["atmo"] - len(strat)]
+        return a, a.default_params(geometry=ig.GEOM_SPH, bounces=2, write_rays=0)
+
+    # warm the kernels and the absorption tables once
+    for r in reqs[:8]:
+        if r["kind"] == "fan":
+            a, p = params_for(r, ig.FP32C)
+            ig.fan_run(a, p, r["th"][:64], r["ph"][:64])
+    torch.cuda.synchronize()
+    sampler = ClockSampler("0")
+    sampler.start()
+    with ig.Server(max_inflight=8, eig_workers=2, hbm_budget=64 << 30) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for r in reqs:
+            dt = r["t"] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            if r["kind"] == "fan":
+                a, p = params_for(r, ig.FP32C)
+                ids.append(srv.submit_fan(a, p, r["th"], r["ph"]))
+            else:
+                ids.append(srv.submit_eig(strat[r["atmo"]], eigp, r["pairs"]))
+        for i in ids:
+            srv.wait(i, -1.0)
+            srv.fetch(i)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    clocks = sampler.stop()
+
+    # comparator: the same stream served one request at a time, FP64
+    lat, steps64 = [], 0
+    t_start = time.perf_counter()
+    for r in reqs:
+        now = time.perf_counter() - t_start
+        if now < r["t"]:
+            time.sleep(r["t"] - now)
+        if r["kind"] == "fan":
+            a, p = params_for(r, ig.FP64)
+            steps64 += ig.fan_run(a, p, r["th"], r["ph"])["total_steps"]
+        else:
+            steps64 += ig.eig_run(strat[r["atmo"]], eigp, r["pairs"])["total_steps"]
+        lat.append(time.perf_counter() - t_start - r["t"])
+    serial_wall = time.perf_counter() - t_start
+    n_fan = sum(r["kind"] == "fan" for r in reqs)
+    line = {"metric": "serving latency p50/p99 [s] and ray-steps/s", "value": st["ray_steps"] / st["wall_s"],
+            "unit": "ray-steps/s", "impl": "ours-serving", "n_gpus": 1, "higher_is_better": True,
+            "scaling": "none", "vs_baseline": None,
+            "dtype": "f32c fans (3D stratified), f64 range-dependent fans and eigen",
+            "data": "synthetic",
+            "config": {"workload": f"poisson {args.serve_rate:g}/s, {len(reqs)} requests ({n_fan} fans of "
+                                   f"100..100000 rays log-uniform, {len(reqs) - n_fan} eigen of 1..64 pairs), "
+                                   f"{len(strat)} stratified + {len(grids)} 11x11 range-dependent atmospheres",
+                       "fan_settings": "3D stratified: 5 bounces, 1000 km, FP32C; sph range-dependent: 2 bounces, FP64",
+                       "eigen_settings": "bnc 0..1, FP64"},
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "fan_p50_s": st["fan_p50_s"], "fan_p99_s": st["fan_p99_s"],
+            "eig_p50_s": st["eig_p50_s"], "eig_p99_s": st["eig_p99_s"], "completed": st["completed"],
+            "rays": st["rays"], "eigenrays": st["eigenrays"], "wall_s": wall,
+            "one_at_a_time_fp64": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                                   "ray_steps_per_s": steps64 / serial_wall, "wall_s": serial_wall},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    for a in strat + grids:
+        a.close()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,7 +564,13 @@ def main():
                     help="fan precision(s) to time; the headline is fp32c unless only fp64 is run")
     ap.add_argument("--az-step", type=float, default=FAN["az"][2],
                     help="azimuth spacing in degrees (a larger value gives a smaller fan, for profiling)")
+    ap.add_argument("--serving", action="store_true",
+                    help="run the request-server benchmark (Poisson stream of fan and eigen requests) instead")
+    ap.add_argument("--serve-rate", type=float, default=SERVE["rate"], help="request arrival rate [1/s]")
+    ap.add_argument("--serve-requests", type=int, default=SERVE["requests"], help="requests in the stream")
     args = ap.parse_args()
+    if args.serving:
+        return run_serving(args)
     if args.az_step != FAN["az"][2]:
         FAN["az"] = (FAN["az"][0], FAN["az"][1], args.az_step)
     if args.impl == "reference":
