@@ -431,7 +431,7 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------- serving
-SERVE = dict(rate=200.0, requests=200, fan_rays=(100, 100_000), eig_pairs=(1, 64), eig_frac=0.25,
+SERVE = dict(rate=200.0, requests=60, fan_rays=(100, 100_000), eig_pairs=(1, 64), eig_frac=0.25,
              n_strat=56, n_rngdep=8, seed=11)
 
 
@@ -506,9 +506,10 @@ def run_serving(args):
                 ids.append(srv.submit_fan(a, p, r["th"], r["ph"]))
             else:
                 ids.append(srv.submit_eig(strat[r["atmo"]], eigp, r["pairs"]))
-        for i in ids:
+        for k, i in enumerate(ids):
             srv.wait(i, -1.0)
             srv.fetch(i)
+            print(f"serving: request {k} done at {time.perf_counter() - t0:.2f} s", file=sys.stderr, flush=True)
         wall = time.perf_counter() - t0
         st = srv.stats()
     clocks = sampler.stop()
@@ -526,6 +527,7 @@ def run_serving(args):
         else:
             steps64 += ig.eig_run(strat[r["atmo"]], eigp, r["pairs"])["total_steps"]
         lat.append(time.perf_counter() - t_start - r["t"])
+        print(f"one-at-a-time: {r['kind']} done at {time.perf_counter() - t_start:.2f} s", file=sys.stderr, flush=True)
     serial_wall = time.perf_counter() - t_start
     n_fan = sum(r["kind"] == "fan" for r in reqs)
     line = {"metric": "serving latency p50/p99 [s] and ray-steps/s", "value": st["ray_steps"] / st["wall_s"],
