@@ -258,7 +258,11 @@ int iga_eig_params_default(iga_atmo_t atmo, iga_eig_params* params);
  * (nullable) the RK4 steps of every trace.  Capacity/truncation as iga_fan_run.
  * The reference's find_eigenray follows only the first reflection during its
  * Newton iterations (an unconditional break, geoac.eigenray.3d.cpp:206) while
- * its final trace and output use all bounces; that is reproduced. */
+ * its final trace and output use all bounces; that is reproduced.
+ * fan.precision = IGA_FP32C traces the rays in FP32-compensated form (the
+ * fan kernel's arithmetic) while the bracket and Newton updates stay in FP64;
+ * the eigenrays found then agree with the FP64 search to within the search
+ * tolerance (0.1 km at the receiver) rather than to rounding. */
 int iga_eig_run(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_pair* pairs, int n_pairs,
                 double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps);
 

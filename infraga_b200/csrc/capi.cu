@@ -436,6 +436,15 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
 }  // namespace
 
 namespace iga_internal {
+int fp32c_setup(iga_atmo_s* h, double freq, iga::Fan3DArgs& a) {
+    iga_atmo_s::AlphaTab t;
+    int rc = ensure_alpha(h, freq, t);
+    if (rc) return rc;
+    a.knots_f = h->d_knots_f;
+    a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
+    return IGA_OK;
+}
+
 int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st, int grid_cap) {

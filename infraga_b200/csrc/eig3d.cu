@@ -9,32 +9,21 @@
 // step, the angles it will try next are known in advance, so it submits a
 // chunk of them at once and keeps the results up to the first bracket.
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <vector>
 
+#include "eig3d.cuh"
 #include "fan3d_common.cuh"
 #include "handle.h"
 
 namespace iga {
 namespace {
-
-struct TraceReq {
-    double x0, y0;       // source position
-    double theta, phi;   // launch angles [rad] (geoac::theta, geoac::phi)
-    int n_seg;           // prop_rk4 segments to trace (bounces + 1)
-    int flags;
-};
-enum : int { kStopOnEscape = 1, kRecord = 2 };
-
-struct TraceRes {
-    double y[12];        // state at the last row (12-state layout)
-    double rc[6];        // nu_x, nu_y, mu_th_x, mu_th_y, mu_ph_x, mu_ph_y
-    double tt, att, zmax, amp_db, incl, baz;
-    long long steps;
-    int escaped;         // the last traced segment left the region
-    int pad;
-};
 
 constexpr int kTraceThreads = 128;
 
@@ -46,7 +35,8 @@ constexpr int kTraceThreads = 128;
 template <bool AMP>
 __global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                     const TraceReq* __restrict__ reqs,
-                                                                    TraceRes* __restrict__ out, int n) {
+                                                                    TraceRes* __restrict__ out, int n,
+                                                                    SegRes* __restrict__ seg_out, int seg_stride) {
     constexpr int N = Dim<AMP>::n;
     extern __shared__ double s_mem[];
     double* s_prev = s_mem;
@@ -118,6 +108,10 @@ __global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __gri
             break;
         }
         steps += capped ? a.length : kb;
+        if (seg_out) {
+            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+            g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
+        }
         if (sg == q.n_seg - 1 || (esc && stop)) break;
         // reflection from rows k-2 (prev) and k-1 (y), flat ground
         const double dz_grnd = a.z0 - y[2];
@@ -160,13 +154,14 @@ __global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __gri
 }
 
 template <bool AMP>
-cudaError_t launch_trace(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st) {
+cudaError_t launch_trace(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st,
+                         SegRes* seg_out = nullptr, int seg_stride = 0) {
     if (n <= 0) return cudaSuccess;
     auto kern = trace3d_fp64_kernel<AMP>;
     const size_t smem = (size_t)Dim<AMP>::n * kTraceThreads * sizeof(double) + (size_t)a.n_knots * kStride * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(n + kTraceThreads - 1) / kTraceThreads, kTraceThreads, smem, st>>>(a, d_req, d_res, n);
+    kern<<<(n + kTraceThreads - 1) / kTraceThreads, kTraceThreads, smem, st>>>(a, d_req, d_res, n, seg_out, seg_stride);
     return cudaGetLastError();
 }
 
@@ -189,6 +184,7 @@ struct Chain {
     int n = 0;
     // requests of the current round
     std::vector<double> sweep;   // inclinations submitted (est phase)
+    std::vector<int> sweep_req;  // their (shared) sweep requests
     int req0 = 0;                // first request index in its batch
     std::vector<std::vector<double>> rows;
 };
@@ -349,7 +345,6 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     fp.write_rays = 1;
     int rc = validate(&fp, 1);
     if (rc) return rc;
-    if (fp.precision != IGA_FP64) return IGA_E_UNSUPPORTED;
     if (h->kind != 0) {
         g_cuda_err = "eigenray search: stratified atmospheres only";
         return IGA_E_UNSUPPORTED;
@@ -368,6 +363,8 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     Fan3DArgs a;
     rc = build_args(h, &fp, a);
     if (rc) return rc;
+    const bool f32 = fp.precision == IGA_FP32C;
+    if (f32 && (rc = fp32c_setup(h, fp.freq, a))) return rc;
 
     Settings S;
     S.theta_max = P->incl_max * (kPi / 180.0);
@@ -394,19 +391,32 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
 
     TraceReq* d_req = nullptr;
     TraceRes* d_res = nullptr;
+    SegRes* d_seg = nullptr;
     size_t cap_req = 0;
     long long steps_tot = 0;
+    const int max_seg = P->bnc_max + 1;
     auto release = [&]() {
         if (d_req) cudaFreeAsync(d_req, st);
         if (d_res) cudaFreeAsync(d_res, st);
-        d_req = nullptr; d_res = nullptr;
+        if (d_seg) cudaFreeAsync(d_seg, st);
+        d_req = nullptr; d_res = nullptr; d_seg = nullptr;
     };
     auto fail = [&](int code) { release(); return code; };
 
     std::vector<TraceReq> req6, req18;
-    std::vector<TraceRes> res6, res18;
+    std::vector<TraceRes> res18;
+    std::vector<SegRes> seg6;
+    // searches of one pair for different bounce counts sweep the same launch
+    // angles until their first bracket: one trace serves them all
+    std::map<std::array<double, 4>, int> uniq;
+    // IGA_EIG_VERBOSE=1: per-call work summary on stderr (diagnostics only)
+    const char* vb = getenv("IGA_EIG_VERBOSE");
+    const bool verbose = vb != nullptr;
+    const bool per_round = vb && vb[0] == '2';
+    long long n_rounds = 0, n6 = 0, n18 = 0, st6 = 0, st18 = 0;
+    const auto t_begin = std::chrono::steady_clock::now();
     while (true) {
-        req6.clear(); req18.clear();
+        req6.clear(); req18.clear(); uniq.clear();
         int sweeping = 0;
         for (auto& c : chains) if (c.phase == Chain::kEst && c.iterations < 2) sweeping++;
         int chunk = S.chunk > 0 ? S.chunk : std::max(8, std::min(128, sweeping > 0 ? 262144 / sweeping : 128));
@@ -414,14 +424,23 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             // find_eigenray gives up after `iterations` Newton steps
             if (c.phase == Chain::kNewton && c.n >= S.iterations) search_continue(c, S);
             c.sweep.clear();
+            c.sweep_req.clear();
             if (c.phase == Chain::kEst) {
-                c.req0 = (int)req6.size();
                 // with a fixed step the next inclinations are known: submit a chunk
                 const int m = c.iterations < 2 ? chunk : 1;
                 double th = c.th;
                 for (int j = 0; j < m && th <= c.th_max; j++) {
                     c.sweep.push_back(th);
-                    req6.push_back({c.sx, c.sy, th, c.phi, c.nb + 1, kStopOnEscape});
+                    const std::array<double, 4> key{c.sx, c.sy, th, c.phi};
+                    auto it = uniq.find(key);
+                    if (it == uniq.end()) {
+                        uniq.emplace(key, (int)req6.size());
+                        c.sweep_req.push_back((int)req6.size());
+                        req6.push_back({c.sx, c.sy, th, c.phi, c.nb + 1, kStopOnEscape});
+                    } else {
+                        c.sweep_req.push_back(it->second);
+                        req6[it->second].n_seg = std::max(req6[it->second].n_seg, c.nb + 1);
+                    }
                     th += c.dth;
                 }
             } else if (c.phase == Chain::kNewton) {
@@ -433,40 +452,80 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             }
         }
         if (req6.empty() && req18.empty()) break;
+        const auto t_round = std::chrono::steady_clock::now();
         const size_t need = std::max(req6.size(), req18.size());
         if (need > cap_req) {
             release();
             cap_req = std::max(need, cap_req * 2);
             cudaError_t e1 = cudaMallocAsync(&d_req, 2 * cap_req * sizeof(TraceReq), st);
             cudaError_t e2 = e1 == cudaSuccess ? cudaMallocAsync(&d_res, 2 * cap_req * sizeof(TraceRes), st) : e1;
-            if (e2 != cudaSuccess) return fail(cuda_fail(e2, "cudaMallocAsync(eigen traces)"));
+            cudaError_t e3 = e2 == cudaSuccess ? cudaMallocAsync(&d_seg, cap_req * max_seg * sizeof(SegRes), st) : e2;
+            if (e3 != cudaSuccess) return fail(cuda_fail(e3, "cudaMallocAsync(eigen traces)"));
         }
         TraceReq* d_req18 = d_req + cap_req;
         TraceRes* d_res18 = d_res + cap_req;
         cudaError_t e = cudaSuccess;
         if (!req6.empty()) {
             e = cudaMemcpyAsync(d_req, req6.data(), req6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = launch_trace<false>(a, d_req, d_res, (int)req6.size(), st);
+            if (e == cudaSuccess)
+                e = f32 ? launch_trace_fp32c(a, d_req, d_res, (int)req6.size(), false, st, d_seg, max_seg)
+                        : launch_trace<false>(a, d_req, d_res, (int)req6.size(), st, d_seg, max_seg);
         }
         if (e == cudaSuccess && !req18.empty()) {
             e = cudaMemcpyAsync(d_req18, req18.data(), req18.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = launch_trace<true>(a, d_req18, d_res18, (int)req18.size(), st);
+            if (e == cudaSuccess)
+                e = f32 ? launch_trace_fp32c(a, d_req18, d_res18, (int)req18.size(), true, st)
+                        : launch_trace<true>(a, d_req18, d_res18, (int)req18.size(), st);
         }
-        res6.resize(req6.size());
+        seg6.resize(req6.size() * max_seg);
         res18.resize(req18.size());
         if (e == cudaSuccess && !req6.empty())
-            e = cudaMemcpyAsync(res6.data(), d_res, res6.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(seg6.data(), d_seg, seg6.size() * sizeof(SegRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && !req18.empty())
             e = cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
-        for (auto& r : res6) steps_tot += r.steps;
-        for (auto& r : res18) steps_tot += r.steps;
+        // each search's view of its sweep traces: the entry of its own
+        // segment count, or the earlier entry where the trace escaped
+        auto sweep_view = [&](int idx, int m, TraceRes& t) {
+            const SegRes* g = &seg6[(size_t)idx * max_seg];
+            int j = 0;
+            while (j < m - 1 && !g[j].escaped) j++;
+            t.y[0] = g[j].x; t.y[1] = g[j].y; t.escaped = g[j].escaped; t.steps = g[j].steps;
+        };
+        long long m6 = 0;
+        for (auto& c : chains) {
+            if (c.phase != Chain::kEst) continue;
+            for (size_t j = 0; j < c.sweep_req.size(); j++) {
+                TraceRes t;
+                sweep_view(c.sweep_req[j], c.nb + 1, t);
+                steps_tot += t.steps; st6 += t.steps;
+                m6 = std::max(m6, t.steps);
+            }
+        }
+        for (auto& r : res18) { steps_tot += r.steps; st18 += r.steps; }
+        n_rounds++; n6 += (long long)req6.size(); n18 += (long long)res18.size();
+        if (per_round) {
+            long long m18 = 0;
+            for (auto& r : res18) m18 = std::max(m18, r.steps);
+            int n_est = 0, n_newt = 0, n_rec = 0;
+            for (auto& c : chains) {
+                n_est += c.phase == Chain::kEst;
+                n_newt += c.phase == Chain::kNewton;
+                n_rec += c.phase == Chain::kRecordTrace;
+            }
+            fprintf(stderr, "round %lld: sweep %zu (max %lld steps) newton/record %zu (max %lld) chains est %d newton %d "
+                            "record %d chunk %d %.4f s\n",
+                    n_rounds, req6.size(), m6, res18.size(), m18, n_est, n_newt, n_rec, chunk,
+                    std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count());
+        }
 
         for (auto& c : chains) {
             if (c.phase == Chain::kEst && !c.sweep.empty()) {
                 for (size_t j = 0; j < c.sweep.size(); j++) {
-                    if (est_step(c, S, res6[c.req0 + j])) break;
+                    TraceRes t;
+                    sweep_view(c.sweep_req[j], c.nb + 1, t);
+                    if (est_step(c, S, t)) break;
                 }
             } else if (c.phase == Chain::kNewton) {
                 newton_step(c, S, a, res18[c.req0]);
@@ -491,6 +550,12 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         }
     }
     release();
+    if (verbose) {
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();
+        fprintf(stderr, "eig_search: %zu chains, %lld rounds, sweep traces %lld (%lld steps), "
+                        "newton/record traces %lld (%lld steps), %.3f s\n",
+                chains.size(), n_rounds, n6, st6, n18, st18, secs);
+    }
     for (auto& c : chains) {
         for (auto& row : c.rows) {
             out_rows.insert(out_rows.end(), row.begin(), row.end());

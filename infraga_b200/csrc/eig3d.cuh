@@ -1,0 +1,43 @@
+// Ray-trace requests of the eigenray search (eig3d.cu) and the trace kernels
+// that serve them: FP64 (eig3d.cu) and FP32-compensated (fan3d_fp32c.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "fan3d.cuh"
+
+namespace iga {
+
+struct TraceReq {
+    double x0, y0;       // source position
+    double theta, phi;   // launch angles [rad] (geoac::theta, geoac::phi)
+    int n_seg;           // prop_rk4 segments to trace (bounces + 1)
+    int flags;
+};
+enum : int { kStopOnEscape = 1, kRecord = 2 };
+
+struct TraceRes {
+    double y[12];        // state at the last row (12-state layout)
+    double rc[6];        // nu_x, nu_y, mu_th_x, mu_th_y, mu_ph_x, mu_ph_y
+    double tt, att, zmax, amp_db, incl, baz;
+    long long steps;
+    int escaped;         // the last traced segment left the region
+    int pad;
+};
+
+// Per-segment result of a sweep trace: the last row of segment j (or the
+// row where the trace escaped), the steps so far and whether it escaped.
+// Sweep requests of several searches that share a launch (same source and
+// launch angles, different bounce counts) are traced once with the largest
+// segment count; each search reads the entry of its own count.
+struct SegRes {
+    double x, y;
+    long long steps;
+    int escaped;
+    int pad;
+};
+
+// FP32-compensated traces (same contract as the FP64 trace kernel).  With
+// seg_out != null, segment j of request r also writes seg_out[r * seg_stride + j].
+cudaError_t launch_trace_fp32c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, bool amp,
+                               cudaStream_t st, SegRes* seg_out = nullptr, int seg_stride = 0);
+
+}  // namespace iga

@@ -50,6 +50,8 @@ int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a);
 int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st, int grid_cap);
+// FP32 knot table and alpha(z) table of `freq` into the launch arguments
+int fp32c_setup(iga_atmo_s* h, double freq, iga::Fan3DArgs& a);
 // the eigenray search on one stream (eig3d.cu)
 int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, cudaStream_t st,
                std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out);

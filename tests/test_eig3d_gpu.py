@@ -68,3 +68,33 @@ def test_eigen_batch_equals_single_pairs(dev):
     for i, p in enumerate(pairs):
         single = ig.eig_run(atmo, params, [p])
         np.testing.assert_array_equal(batch["eigenrays"][batch["pair_index"] == i], single["eigenrays"])
+
+
+# FP32-compensated ray integration with FP64 bracket/Newton updates: the same
+# eigenrays within the search tolerance.  A trace's FP32 rounding moves its
+# landing point by metres, so the Newton iteration stops at a slightly
+# different launch angle (still within 0.1 km of the receiver); near
+# caustics the amplitude differs more.  Bounds for the matched rows:
+FP32C_EIG_TOL = {"incl": 0.05, "az": 0.05, "time": 0.5, "amp_db": 1.0}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp32c_eigenrays_match_reference(dev, name):
+    c = CASES[name]
+    src, rcvr, over = eig_setup(c["args"])
+    atmo = ig.Atmosphere.load(profile_path(c["seed"]))
+    params = ig.eig_params(atmo, **over)
+    params.fan.precision = ig.FP32C
+    r = ig.eig_run(atmo, params, [(src, rcvr)])
+    ref, _ = parse_golden(name)
+    got = r["eigenrays"]
+    print(name, "reference", ref.shape[0], "fp32c", got.shape[0])
+    for row in ref[ref[:, 2] <= 1]:
+        cand = got[got[:, 2] == row[2]]
+        assert cand.shape[0] > 0, row[:3]
+        j = np.argmin(np.abs(cand[:, 0] - row[0]) + np.abs(cand[:, 1] - row[1]))
+        m = cand[j]
+        assert abs(m[0] - row[0]) < FP32C_EIG_TOL["incl"] and abs(m[1] - row[1]) < FP32C_EIG_TOL["az"], (m[:3], row[:3])
+        assert abs(m[5] - row[5]) < FP32C_EIG_TOL["time"]
+        assert abs(m[10] - row[10]) < FP32C_EIG_TOL["amp_db"]
+        assert np.hypot(m[3] - rcvr[0], m[4] - rcvr[1]) < params.tolerance + 1e-3
