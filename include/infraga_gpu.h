@@ -147,6 +147,14 @@ int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_f
  * whole globe in degrees for a 1D profile. */
 int iga_atmo_region(iga_atmo_t atmo, double* lat_min, double* lat_max, double* lon_min, double* lon_max);
 
+/* Terrain height and gradient at a horizontal point of a range-dependent
+ * handle loaded with a terrain file: topo::z and topo::dz
+ * (src/atmo/atmo_state.sph.rngdep.cpp:58-97, atmo_state.3d.rngdep.cpp:45-80),
+ * with the point clamped into the terrain grid.  Spherical: x, y = latitude,
+ * longitude in RADIANS, z = height above r_earth [km], gradient per radian;
+ * 3D: x, y [km], gradient per km.  IGA_E_UNSUPPORTED without terrain. */
+int iga_atmo_terrain(iga_atmo_t atmo, double x, double y, double* z, double* dz_dx, double* dz_dy);
+
 /* Same as iga_atmo_load from arrays already in solver units. */
 int iga_atmo_create(const iga_profile* profile, iga_atmo_t* out);
 
@@ -219,6 +227,51 @@ int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
                        double* d_arrivals, int* d_n_arr, long long* d_ray_steps,
                        int* d_ray_status, double* d_arrival_aux, void* d_workspace, void* stream);
 
+/* ---- sampled ray paths, terrain samples and caustics ---- */
+
+/* Path row: the reference's .raypaths.dat columns (main.infraga.3d.cpp:381-388;
+ * spherical: lat, lon [deg] instead of x, y) and the bounce of the row:
+ *   x|lat, y|lon, z [km], trans. coeff. [dB] (0 without calc_amp),
+ *   absorption [dB] (-2 x the running sum), time [s], bounce.
+ * In IGA_PATH_TERRAIN mode column 2 is the ground height under the row
+ * (.terrain.dat, main.infraga.3d.cpp:481-486) and column 3 is 0. */
+#define IGA_PATH_COLS 7
+/* Caustic row: x|lat, y|lon, z [km], time [s], bounce (.caustics-N.dat,
+ * main.infraga.3d.cpp:470-475; the 3D range-dependent CLI also writes a
+ * 0.0 column before the time, main.infraga.3d.rngdep.cpp:467-471). */
+#define IGA_CAUSTIC_COLS 5
+enum iga_path_mode {
+    IGA_PATH_RAYS = 0,       /* rows m == 1 and m % 15 == 0 of every bounce (write_rays) */
+    IGA_PATH_TERRAIN = 1     /* rows m % 10 == 1 (write_topo) */
+};
+
+/* Replaces the write_rays / write_topo / write_caustics branches of run_prop's
+ * per-ray loop (src/main.infraga.3d.cpp:443-497, main.infraga.sph.cpp:455-510,
+ * main.infraga.3d.rngdep.cpp:440-488, main.infraga.sph.rngdep.cpp:450-503):
+ * for every ray of the fan, the RK4 rows m (1 <= m < k of each bounce
+ * segment) that the reference samples, with time and absorption summed per
+ * step as the reference does whenever it writes paths (params->write_rays is
+ * taken as 1), and the caustic points (sign changes of the ray-tube Jacobian
+ * between consecutive rows; needs calc_amp = 1).  FP64 only.
+ *   ray_steps   nullable: the per-ray step counts an iga_fan_run of the same
+ *               fan returned; without it the call first counts them itself
+ *   path_rows   nullable: path_cap rows of IGA_PATH_COLS; *n_path (needed
+ *               when path_rows is given) = rows produced; path_start
+ *               (nullable, n_rays + 1) = first row of each ray and the total.
+ *               The rows of ray i number at most
+ *               (bounces + 1) + ray_steps[i] / 15 (IGA_PATH_RAYS; / 10 for
+ *               IGA_PATH_TERRAIN) + 1.
+ *   caustic_rows nullable: caustic_cap rows of IGA_CAUSTIC_COLS, ray by ray
+ *               in step order; *n_caustic = rows produced; caustic_ray
+ *               (nullable, caustic_cap) the ray of each row.
+ * Returns IGA_E_TRUNCATED when either output had too little room (the counts
+ * then give the room needed). */
+int iga_fan_paths(iga_atmo_t atmo, const iga_fan_params* params,
+                  const double* theta_deg, const double* phi_deg, int n_rays, int path_mode,
+                  const long long* ray_steps,
+                  double* path_rows, long long path_cap, long long* n_path, long long* path_start,
+                  double* caustic_rows, long long caustic_cap, long long* n_caustic, int* caustic_ray);
+
 /* ---- eigenray search ---- */
 
 /* One source-receiver pair of an eigenray search (km; receiver on the ground). */
@@ -265,6 +318,16 @@ int iga_eig_params_default(iga_atmo_t atmo, iga_eig_params* params);
  * tolerance (0.1 km at the receiver) rather than to rounding. */
 int iga_eig_run(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_pair* pairs, int n_pairs,
                 double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps);
+
+/* Replaces run_eig_direct's call of geoac::find_eigenray
+ * (src/main.infraga.3d.cpp:1079-1080, src/geoac/geoac.eigenray.3d.cpp:146-371):
+ * the damped Newton refinement alone, from the launch estimate incl_est
+ * [deg] and az_est [deg clockwise from north] for `bounces` reflections, with
+ * params' damping, tolerance and iteration limit.  *found = 1 and eigenray
+ * (IGA_ARRIVAL_COLS doubles, the row iga_eig_run would give) are set when the
+ * arrival came within tolerance of the receiver; *found = 0 otherwise. */
+int iga_eig_direct(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_pair* pair, double incl_est,
+                   double az_est, int bounces, double* eigenray, int* found, long long* total_steps);
 
 /* Allocation-free form of iga_fan_run_device.  No counterpart in the
  * reference (which has no GPU path); it exists for callers that must not

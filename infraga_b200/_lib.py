@@ -122,6 +122,10 @@ _SIGS = {
     "iga_fan_run_device_noalloc": (_I, [_VP, _P(FanParams), _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
     "iga_eig_params_default": (_I, [_VP, _P(EigParams)]),
     "iga_eig_run": (_I, [_VP, _P(EigParams), _P(EigPair), _I, _P(_D), _I, _P(_I), _P(_I), _P(_LL)]),
+    "iga_eig_direct": (_I, [_VP, _P(EigParams), _P(EigPair), _D, _D, _I, _P(_D), _P(_I), _P(_LL)]),
+    "iga_fan_paths": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _I, _P(_LL), _P(_D), _LL, _P(_LL), _P(_LL),
+                           _P(_D), _LL, _P(_LL), _P(_I)]),
+    "iga_atmo_terrain": (_I, [_VP, _D, _D, _P(_D), _P(_D), _P(_D)]),
 }
 
 
@@ -310,6 +314,62 @@ def eig_run(atmo: Atmosphere, params: EigParams, pairs):
         _check(rc, "iga_eig_run")
         m = n_out.value
         return {"eigenrays": out[:m], "pair_index": idx[:m], "total_steps": int(tot.value)}
+
+
+def eig_direct(atmo: Atmosphere, params: EigParams, src, rcvr, incl_est: float, az_est: float, bounces: int):
+    """find_eigenray alone from a launch estimate (degrees).  Returns the
+    eigenray row [12] or None when the refinement did not converge."""
+    pair = EigPair()
+    pair.src = (_D * 3)(*src)
+    pair.rcvr = (_D * 2)(*rcvr)
+    row = np.zeros(ARRIVAL_COLS, dtype=np.float64)
+    found = _I()
+    tot = _LL()
+    _check(lib().iga_eig_direct(atmo.handle, ctypes.byref(params), ctypes.byref(pair), float(incl_est), float(az_est),
+                                int(bounces), _dptr(row), ctypes.byref(found), ctypes.byref(tot)), "iga_eig_direct")
+    return row if found.value else None
+
+
+PATH_RAYS, PATH_TERRAIN = 0, 1
+PATH_COLS, CAUSTIC_COLS = 7, 5
+
+
+def fan_paths(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, mode: int = PATH_RAYS,
+              caustics: bool = False, ray_steps=None):
+    """Sampled ray-path rows (run_prop's write_rays / write_topo rows) and,
+    with ``caustics``, caustic points of a fan.  Returns a dict with
+    ``paths`` [n, 7], ``path_start`` [n_rays + 1] and, with caustics,
+    ``caustics`` [m, 5] and ``caustic_ray`` [m]."""
+    th = np.ascontiguousarray(theta_deg, dtype=np.float64)
+    ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
+    n = th.size
+    if ray_steps is None:
+        ray_steps = fan_run(atmo, params, th, ph)["ray_steps"]
+    steps = np.ascontiguousarray(ray_steps, dtype=np.int64)
+    div = 15 if mode == PATH_RAYS else 10
+    cap = int(np.sum(params.bounces + 1 + steps // div + 1))
+    rows = np.zeros((max(cap, 1), PATH_COLS), dtype=np.float64)
+    start = np.zeros(n + 1, dtype=np.int64)
+    n_path = _LL()
+    ccap = 4096 if caustics else 0
+    while True:
+        crow = np.zeros((max(ccap, 1), CAUSTIC_COLS), dtype=np.float64)
+        cray = np.zeros(max(ccap, 1), dtype=np.int32)
+        n_caus = _LL()
+        rc = lib().iga_fan_paths(atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph), n, int(mode),
+                                 steps.ctypes.data_as(_P(_LL)), _dptr(rows), cap, ctypes.byref(n_path),
+                                 start.ctypes.data_as(_P(_LL)), _dptr(crow) if caustics else None, ccap,
+                                 ctypes.byref(n_caus) if caustics else None,
+                                 cray.ctypes.data_as(_P(_I)) if caustics else None)
+        if rc == IGA_E_TRUNCATED and caustics and n_caus.value > ccap:
+            ccap = n_caus.value
+            continue
+        _check(rc, "iga_fan_paths")
+        out = {"paths": rows[:n_path.value], "path_start": start}
+        if caustics:
+            out["caustics"] = crow[:n_caus.value]
+            out["caustic_ray"] = cray[:n_caus.value]
+        return out
 
 
 def fan_workspace_bytes() -> int:

@@ -399,7 +399,7 @@ namespace {
 
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
-               cudaStream_t st, int grid_cap = 0) {
+               cudaStream_t st, int grid_cap = 0, const PathSpec* ps = nullptr) {
     if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) || p->precision != IGA_FP64)) {
         g_cuda_err = "range-dependent atmosphere: FP64, with the geometry it was loaded for";
         return IGA_E_UNSUPPORTED;
@@ -411,6 +411,14 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status; a.aux = d_aux;
     a.queue = static_cast<unsigned int*>(d_ws);
     a.grid_cap = grid_cap;
+    if (ps) {
+        if (p->precision != IGA_FP64) {
+            g_cuda_err = "sampled ray paths: FP64 only";
+            return IGA_E_UNSUPPORTED;
+        }
+        a.path_rows = ps->rows; a.path_off = ps->off; a.path_n = ps->n; a.path_mode = ps->mode;
+        a.caus_rows = ps->caus; a.caus_count = ps->caus_count; a.caus_cap = ps->caus_cap;
+    }
     if (p->precision == IGA_FP32C) {
         iga_atmo_s::AlphaTab t;
         rc = ensure_alpha(h, p->freq, t);
@@ -447,11 +455,11 @@ int fp32c_setup(iga_atmo_s* h, double freq, iga::Fan3DArgs& a) {
 
 int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
-               cudaStream_t st, int grid_cap) {
+               cudaStream_t st, int grid_cap, const PathSpec* paths) {
     int rc = validate(p, n_rays);
     if (rc) return rc;
     IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
-    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_aux, d_ws, st, grid_cap);
+    return run_device(h, p, d_th, d_ph, n_rays, d_arr, d_n, d_steps, d_status, d_aux, d_ws, st, grid_cap, paths);
 }
 }  // namespace iga_internal
 
@@ -511,6 +519,17 @@ int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_f
     if (rc == IGA_OK) rc = upload_rngdep(h);
     if (rc != IGA_OK) { iga_atmo_destroy(h); return rc; }
     *out = h;
+    return IGA_OK;
+}
+
+int iga_atmo_terrain(iga_atmo_t h, double x, double y, double* z, double* dz_dx, double* dz_dy) {
+    if (!h) return IGA_E_INVALID;
+    if (!h->has_topo) return IGA_E_UNSUPPORTED;
+    double zz = 0.0, d[2] = {0.0, 0.0};
+    iga::terrain_eval1(h->topo, x, y, zz, d);
+    if (z) *z = zz;
+    if (dz_dx) *dz_dx = d[0];
+    if (dz_dy) *dz_dy = d[1];
     return IGA_OK;
 }
 

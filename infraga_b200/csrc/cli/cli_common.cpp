@@ -1,0 +1,835 @@
+// Drop-in command-line front ends over libinfraga_gpu.so (see cli_common.h).
+//
+// Output formats follow the reference mains line for line, because files
+// written by these binaries are read by the same downstream tools
+// (infraga/run_infraga.py, plotting scripts): header text and column order
+// of run_prop (src/main.infraga.3d.cpp:348-402, main.infraga.sph.cpp:357-411,
+// main.infraga.3d.rngdep.cpp:141-197, main.infraga.sph.rngdep.cpp:149-205)
+// and of run_eig_search / find_eigenray (main.infraga.3d.cpp:893-936,
+// src/geoac/geoac.eigenray.3d.cpp:220-318), written through std::ofstream
+// with the same precision manipulators so numbers print identically
+// (spherical rows switch their stream to 8 significant digits at the first
+// latitude and keep it, as the reference streams do).
+#include "cli_common.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <strings.h>
+
+#include <algorithm>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "infraga_gpu.h"
+
+namespace cli {
+namespace {
+
+constexpr double Pi = 3.141592653589793238462643;   // geoac.params.3d.cpp:9
+constexpr double kR0 = 6370.0;                       // globe::r0 (util/globe.cpp:10)
+
+// strncmp(arg, key, n) == 0, value at arg + off (the reference's matching,
+// including its few keys whose compare length or value offset is off by some
+// characters).
+bool match(const char* a, const char* k, size_t n, size_t off, const char** v) {
+    if (strncmp(a, k, n) != 0) return false;
+    *v = a + off;
+    return true;
+}
+bool key(const char* a, const char* k, const char** v) { return match(a, k, strlen(k), strlen(k), v); }
+bool key2(const char* a, const char* k1, const char* k2, const char** v) { return key(a, k1, v) || key(a, k2, v); }
+
+// util/fileIO.cpp:87-90
+bool str2bool(const char* s) { return s[0] != '\0' && (strcasecmp(s, "true") == 0 || atoi(s) != 0); }
+
+bool confirm_unknown(const char* arg, bool leading_newline) {
+    if (leading_newline) std::cout << '\n';
+    std::cout << "***WARNING*** Unrecognized parameter entry: " << arg << '\n';
+    std::cout << "Continue? (y/n):";
+    char c = 0;
+    std::cin >> c;
+    return c == 'y' || c == 'Y';
+}
+
+// The reference cuts the profile argument at its last '.' in place, so the
+// ".arrivals.dat" header's "profile:" line shows the shortened text too.
+void strip_extension(char* s) {
+    for (int m = (int)strlen(s); m >= 0; m--)
+        if (s[m] == '.') {
+            s[m] = '\0';
+            break;
+        }
+}
+
+const char* variant_name(Variant v) {
+    switch (v) {
+        case Variant::k3D: return "infraga-3d";
+        case Variant::kSph: return "infraga-sph";
+        case Variant::k3DRngdep: return "infraga-3d-rngdep";
+        default: return "infraga-sph-rngdep";
+    }
+}
+
+bool is_sph(Variant v) { return v == Variant::kSph || v == Variant::kSphRngdep; }
+bool is_rngdep(Variant v) { return v == Variant::k3DRngdep || v == Variant::kSphRngdep; }
+
+int fail(const char* what, int rc) {
+    std::cout << '\t' << "ERROR: " << what << ": " << iga_strerror(rc);
+    const char* ce = iga_last_cuda_error();
+    if (ce && ce[0]) std::cout << " (" << ce << ")";
+    std::cout << '\n';
+    return 0;   // the reference exits 0 after its error messages
+}
+
+void banner(Variant v, const char* mode) {
+    const std::string name = std::string("Running ") + variant_name(v);
+    const int w = (int)std::max(name.size(), strlen(mode)) + 10;
+    auto line = [&](const std::string& t) {
+        const int pad = w - 8 - (int)t.size();
+        std::cout << '\t' << "####" << std::string(pad / 2, ' ') << t << std::string(pad - pad / 2, ' ') << "####" << '\n';
+    };
+    std::cout << '\n' << '\t' << std::string(w, '#') << '\n';
+    line(name);
+    line(mode);
+    std::cout << '\t' << std::string(w, '#') << '\n' << '\n';
+}
+
+void usage(Variant v) {
+    const char* n = variant_name(v);
+    const bool sph = is_sph(v), rd = is_rngdep(v);
+    std::cout << '\n' << "Usage: " << n << " [option] " << (rd ? "prefix x_or_lat_file y_or_lon_file" : "profile.met")
+              << " [parameters]" << '\n';
+    std::cout << '\t' << "GPU (B200) ray tracing through "
+              << (rd ? "a range-dependent" : "a stratified") << ", moving medium"
+              << (sph ? " on the globe" : " (3D Cartesian)") << "; output files match the reference " << n << ".\n\n";
+    std::cout << "Options:" << '\n';
+    std::cout << '\t' << "-prop        ray fan over inclination/azimuth ranges (incl_min, incl_max, incl_step, az_min, az_max,"
+              << '\n' << '\t' << "             az_step, inclination, azimuth, bounces, " << (sph ? "src_lat, src_lon" : "src_x, src_y")
+              << ", src_alt, turn_ht_min, write_rays, write_caustics, write_topo)" << '\n';
+    if (v == Variant::k3D) {
+        std::cout << '\t' << "-eig_search  eigenrays from (src_x, src_y, src_alt) to (rcvr_x, rcvr_y) (incl_min, incl_max, bnc_min,"
+                  << '\n' << '\t' << "             bnc_max, bounces, verbose, iterations, damping, tolerance, az_dev_lim, incl_step_min,"
+                  << '\n' << '\t' << "             incl_step_max)" << '\n';
+        std::cout << '\t' << "-eig_direct  one eigenray near (incl_est, az_est) with a given bounce count" << '\n';
+    }
+    std::cout << '\t' << "Common: freq, abs_coeff, z_grnd, prof_format, reverse_winds, output_id, calc_amp, max_alt, max_rng,"
+              << '\n' << '\t' << "        " << (sph ? "min_lat, max_lat, min_lon, max_lon, max_time" : "min_x, max_x, min_y, max_y")
+              << ", min_ds, max_ds, max_s" << (rd ? ", topo_file" : "") << '\n';
+    std::cout << '\t' << "-back_proj, -wnl_wvfrm and the reference's MPI builds are not provided by the GPU front end." << '\n'
+              << '\n';
+}
+
+void version() {
+    std::cout << '\n' << '\t' << "infraga-gpu: B200 ray-fan and eigenray solver with the infraga 1.0.3 command-line interface"
+              << '\n' << '\t' << "C ABI version " << iga_version() << '\n' << '\n';
+}
+
+// ------------------------------------------------------------------------
+// -prop
+// ------------------------------------------------------------------------
+
+struct PropOpts {
+    double theta_min = 0.5, theta_max = 45.0, theta_step = 0.5;
+    double phi_min = -90.0, phi_max = -90.0, phi_step = 1.0;
+    bool write_atmo = false, write_rays = true, write_caustics = false, write_topo = false;
+    bool print_resid = false, use_blw = false;
+    const char* output_id = nullptr;
+    const char* topo_file = nullptr;
+};
+
+// Loads the atmosphere of argv (first pass: prof_format, reverse_winds,
+// topo_file; z_grnd there is overwritten by set_limits) and prints set_region's
+// messages.  Returns null on failure (messages printed).
+iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_out) {
+    const int first = is_rngdep(v) ? 5 : 3;
+    const char* fmt = "zTuvdp";
+    const char* topo = nullptr;
+    bool rev = false;
+    const char* val;
+    for (int i = first; i < argc; i++) {
+        if (key(argv[i], "prof_format=", &val)) fmt = val;
+        else if (key(argv[i], "z_grnd=", &val)) {}
+        else if (key(argv[i], "reverse_winds=", &val)) rev = str2bool(val);
+        else if (key(argv[i], "topo_file=", &val)) topo = val;
+    }
+    *topo_out = topo;
+    iga_atmo_t a = nullptr;
+    int rc;
+    if (!is_rngdep(v)) {
+        std::cout << "Interpolating atmosphere data in '" << argv[2] << "' using format '" << fmt << "'..." << '\n';
+        if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
+        if (topo) {
+            std::cout << '\t' << "ERROR: terrain (topo_file) with a stratified profile is not provided by the GPU front end;"
+                      << " use " << (is_sph(v) ? "infraga-sph-rngdep" : "infraga-3d-rngdep") << '\n' << '\n';
+            return nullptr;
+        }
+        rc = iga_atmo_load(argv[2], fmt, rev ? 1 : 0, &a);
+        if (rc == IGA_E_IO) {
+            std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\n';
+            return nullptr;
+        }
+    } else {
+        if (topo)
+            std::cout << "Interpolating atmosphere data in '" << argv[2] << "*' and topography data in '" << topo << "'..."
+                      << '\n';
+        else
+            std::cout << "Interpolating atmosphere data in '" << argv[2] << "'* using format '" << fmt << "'..." << '\n';
+        if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
+        rc = iga_atmo_load_rngdep(argv[2], argv[3], argv[4], topo, fmt, rev ? 1 : 0,
+                                  is_sph(v) ? IGA_GEOM_SPH : IGA_GEOM_3D, &a);
+        if (rc == IGA_E_IO) {
+            std::cout << '\t' << "ERROR: Invalid grid, profile or terrain files (" << argv[2] << "*, " << argv[3] << ", "
+                      << argv[4] << (topo ? ", " : "") << (topo ? topo : "") << ")" << '\n' << '\n';
+            return nullptr;
+        }
+    }
+    if (rc) {
+        fail("loading the atmosphere", rc);
+        return nullptr;
+    }
+    return a;
+}
+
+void print_region(Variant v, const iga_fan_params& p) {
+    std::cout << '\t' << "Propagation region limits:" << '\n';
+    if (is_sph(v)) {
+        std::cout << '\t' << '\t' << "latitude = " << p.lat_min << ", " << p.lat_max << '\n';
+        std::cout << '\t' << '\t' << "longitude = " << p.lon_min << ", " << p.lon_max << '\n';
+        std::cout << '\t' << '\t' << "altitude = " << p.z_grnd << ", " << p.alt_max << '\n' << '\n';
+    } else {
+        std::cout << '\t' << '\t' << "x = " << p.x_min << ", " << p.x_max << '\n';
+        std::cout << '\t' << '\t' << "y = " << p.y_min << ", " << p.y_max << '\n';
+        std::cout << '\t' << '\t' << "z = " << p.z_grnd << ", " << p.alt_max << '\n';
+    }
+}
+
+// Keys shared by every mode's second pass (propagation limits, absorption,
+// output naming).  Returns true when `a` was one of them.
+bool common_key(Variant v, const char* a, iga_fan_params& p, PropOpts& o, bool has_topo, double& freq) {
+    const char* val;
+    const bool sph = is_sph(v);
+    if (key(a, "freq=", &val)) freq = atof(val);
+    else if (key(a, "abs_coeff=", &val)) p.tweak_abs = std::max(0.0, atof(val));
+    else if (key2(a, "max_alt=", "alt_max=", &val)) {
+        p.alt_max = atof(val);
+        std::cout << '\t' << "User selected altitude maximum = " << p.alt_max << '\n';
+    } else if (key2(a, "max_rng=", "rng_max=", &val)) {
+        p.rng_max = atof(val);
+        std::cout << '\t' << "User selected range maximum = " << p.rng_max << '\n';
+    } else if (sph && key2(a, "max_time=", "time_max=", &val)) {
+        p.time_max = atof(val);
+        std::cout << '\t' << "User selected propagation time maximum = " << p.time_max << '\n';
+    } else if (sph && key2(a, "min_lat=", "lat_min=", &val)) {
+        p.lat_min = atof(val);
+        std::cout << '\t' << "User selected latitude minimum = " << p.lat_min * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    } else if (sph && key2(a, "max_lat=", "lat_max=", &val)) {
+        p.lat_max = atof(val);
+        std::cout << '\t' << "User selected latitude maximum = " << p.lat_max * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    } else if (sph && key2(a, "min_lon=", "lon_min=", &val)) {
+        p.lon_min = atof(val);
+        std::cout << '\t' << "User selected longitude minimum = " << p.lon_min * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    } else if (sph && key2(a, "max_lon=", "lon_max=", &val)) {
+        p.lon_max = atof(val);
+        std::cout << '\t' << "User selected longitude maximum = " << p.lon_max * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    } else if (!sph && key2(a, "min_x=", "x_min=", &val)) {
+        p.x_min = atof(val);
+        std::cout << '\t' << "User selected x minimum = " << p.x_min << '\n';
+    } else if (!sph && key2(a, "max_x=", "x_max=", &val)) {
+        p.x_max = atof(val);
+        std::cout << '\t' << "User selected x maximum = " << p.x_max << '\n';
+    } else if (!sph && key2(a, "min_y=", "y_min=", &val)) {
+        p.y_min = atof(val);
+        std::cout << '\t' << "User selected y minimum = " << p.y_min << '\n';
+    } else if (!sph && key2(a, "max_y=", "y_max=", &val)) {
+        p.y_max = atof(val);
+        std::cout << '\t' << "User selected y maximum = " << p.y_max << '\n';
+    } else if (key2(a, "min_ds=", "ds_min=", &val)) {
+        p.ds_min = atof(val);
+        std::cout << '\t' << "User selected ds minimum = " << p.ds_min << '\n';
+    } else if (key2(a, "max_ds=", "ds_max=", &val)) {
+        p.ds_max = atof(val);
+        std::cout << '\t' << "User selected ds maximum = " << p.ds_max << '\n';
+    } else if (key2(a, "max_s=", "s_max=", &val)) {
+        p.s_max = atof(val);
+        std::cout << '\t' << "User selected s maximum (path length between reflections) = " << p.s_max << '\n';
+    } else if (key(a, "write_atmo=", &val)) o.write_atmo = str2bool(val);
+    else if (key(a, "prof_format=", &val) || key(a, "reverse_winds=", &val) || key(a, "topo_file=", &val)) {}
+    else if (key(a, "output_id=", &val)) o.output_id = val;
+    else if (key(a, "z_grnd=", &val)) {
+        if (!has_topo) p.z_grnd = atof(val);
+        else std::cout << '\t' << "Note: cannot adjust ground elevation with topography." << '\n';
+    } else if (key(a, "topo_use_BLw=", &val)) o.use_blw = str2bool(val);
+    else return false;
+    return true;
+}
+
+// The source height raised to the ground (run_prop: z_src = max(z_src, topo::z(src)))
+// and the ground launch limit theta_grnd of one azimuth (main.infraga.3d.cpp:411-419,
+// main.infraga.sph.cpp:420-433, 3d.rngdep :205-214, sph.rngdep :212-225).
+struct Ground {
+    Variant v;
+    iga_atmo_t atmo;
+    bool topo;
+    double z0;
+    double z(double x, double y) const {   // topo::z, as an altitude [km]
+        if (topo) {
+            double zz = 0.0;
+            iga_atmo_terrain(atmo, x, y, &zz, nullptr, nullptr);
+            return zz;
+        }
+        return v == Variant::k3DRngdep ? 0.0 : z0;   // 3D range-dependent topo::z is 0 without terrain
+    }
+    double theta_grnd(double xs, double ys, double zs, double phi_deg) const {
+        if (zs - z(xs, ys) < 0.01) {
+            if (!topo) return 0.1;
+            double zz, d0, d1;
+            iga_atmo_terrain(atmo, xs, ys, &zz, &d0, &d1);
+            if (is_sph(v)) {
+                const double dzgdx = 1.0 / (kR0 * cos(xs)) * d1;
+                const double dzgdy = 1.0 / kR0 * d0;
+                return atan(dzgdx * sin(phi_deg * Pi / 180.0) + dzgdy * cos(phi_deg * Pi / 180.0)) * (180.0 / Pi) + 0.1;
+            }
+            return atan(d0 * sin(phi_deg * Pi / 180.0) + d1 * cos(phi_deg * Pi / 180.0)) * (180.0 / Pi) + 0.1;
+        }
+        return -89.9;
+    }
+};
+
+// Rows of one ray of a fan as the library returned them.
+struct FanChunk {
+    std::vector<double> arr;     // arrivals
+    std::vector<int> arr_ray;
+    std::vector<long long> steps;
+    std::vector<double> path;
+    std::vector<long long> path_start;
+    std::vector<double> caus;
+    std::vector<int> caus_ray;
+};
+
+int run_prop(int argc, char** argv, Variant v) {
+    banner(v, "Propagation");
+    const bool sph = is_sph(v), rd = is_rngdep(v);
+    const char* topo = nullptr;
+    iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo);
+    if (!atmo) return 0;
+    const bool has_topo = topo != nullptr;
+
+    iga_fan_params p;
+    int rc = iga_fan_params_init(atmo, sph ? IGA_GEOM_SPH : IGA_GEOM_3D, &p);
+    if (rc) return fail("parameters", rc);
+    print_region(v, p);
+    PropOpts o;
+    int bounces = p.bounces;
+    double xs = p.src[0], ys = p.src[1], zs = 0.0;
+    double freq = p.freq, turn_ht_min = p.turn_ht_min;
+    bool calc_amp = true;
+    const char* val;
+    for (int i = rd ? 5 : 3; i < argc; i++) {
+        const char* a = argv[i];
+        if (key2(a, "incl_min=", "min_incl=", &val)) o.theta_min = atof(val);
+        else if (key2(a, "incl_max=", "max_incl=", &val)) o.theta_max = atof(val);
+        else if (key2(a, "az_min=", "min_az=", &val)) o.phi_min = atof(val);
+        else if (key2(a, "az_max=", "max_az=", &val)) o.phi_max = atof(val);
+        else if (key(a, "incl_step=", &val)) o.theta_step = atof(val);
+        else if (key(a, "az_step=", &val)) o.phi_step = atof(val);
+        else if (key(a, "inclination=", &val)) { o.theta_min = o.theta_max = atof(val); o.theta_step = 1.0; }
+        else if (key(a, "azimuth=", &val)) { o.phi_min = o.phi_max = atof(val); o.phi_step = 1.0; }
+        else if (key(a, "bounces=", &val)) bounces = atoi(val);
+        else if (!sph && key2(a, "src_x=", "x_src=", &val)) xs = atof(val);
+        else if (!sph && key2(a, "src_y=", "y_src=", &val)) ys = atof(val);
+        else if (sph && key2(a, "src_lat=", "lat_src=", &val)) xs = atof(val);
+        else if (sph && key2(a, "src_lon=", "lon_src=", &val)) ys = atof(val);
+        else if (key(a, "src_alt=", &val) || match(a, "alt_src=", sph ? 8 : 6, 8, &val)) zs = atof(val);
+        else if (key(a, "turn_ht_min=", &val)) turn_ht_min = atof(val);
+        else if (key(a, "write_rays=", &val)) o.write_rays = str2bool(val);
+        else if (key(a, "write_caustics=", &val)) o.write_caustics = str2bool(val);
+        // infraga-3d-rngdep compares 8 characters and reads the value from the
+        // '=' on (main.infraga.3d.rngdep.cpp:269), so any calc_amp= turns it off
+        else if (v == Variant::k3DRngdep && match(a, "calc_amp=", 8, 8, &val)) calc_amp = str2bool(val);
+        else if (v != Variant::k3DRngdep && key(a, "calc_amp=", &val)) calc_amp = str2bool(val);
+        else if (key(a, "write_topo=", &val)) o.write_topo = str2bool(val);
+        else if (key(a, "print_resid=", &val)) o.print_resid = str2bool(val);
+        else if (common_key(v, a, p, o, has_topo, freq)) {}
+        else if (!confirm_unknown(a, v == Variant::k3DRngdep)) return 0;
+    }
+    if (o.use_blw) {
+        std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
+        return 0;
+    }
+    if (o.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
+    if (o.print_resid) std::cout << '\t' << "Note: print_resid is not provided by the GPU front end" << '\n';
+
+    // source: degrees on the command line, radians inside (spherical)
+    const double lat_r = xs * (Pi / 180.0), lon_r = ys * (Pi / 180.0);
+    Ground g{v, atmo, has_topo, p.z_grnd};
+    zs = sph ? std::max(zs, g.z(lat_r, lon_r)) : std::max(zs, g.z(xs, ys));
+    if (o.write_caustics) calc_amp = true;
+
+    const char* sum_src = sph ? "source location (lat, lon, alt): " : "source location: ";
+    const double sx = sph ? lat_r * (180.0 / Pi) : xs, sy = sph ? lon_r * (180.0 / Pi) : ys;
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "inclination: " << o.theta_min << ", " << o.theta_max << ", " << o.theta_step << '\n';
+    std::cout << '\t' << "azimuth: " << o.phi_min << ", " << o.phi_max << ", " << o.phi_step << '\n';
+    std::cout << '\t' << "bounces: " << bounces << '\n';
+    std::cout << '\t' << sum_src << sx << ", " << sy << ", " << zs << '\n';
+    if (!has_topo) std::cout << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    if (v == Variant::kSph) std::cout << '\t' << "turn_ht_min: " << turn_ht_min << '\n';
+    std::cout << '\t' << "frequency: " << freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << p.tweak_abs << (sph ? "\n" : "\n\n");
+    std::cout << '\t' << "write_atmo: " << (o.write_atmo ? "true" : "false") << '\n';
+    std::cout << '\t' << "write_rays: " << (o.write_rays ? "true" : "false") << '\n';
+    std::cout << '\t' << "write_topo: " << (o.write_topo ? "true" : "false") << '\n';
+    std::cout << '\t' << "write_caustics: " << (o.write_caustics ? "true" : "false") << '\n';
+    std::cout << '\t' << "calc_amp: " << (calc_amp ? "true" : "false") << '\n' << '\n';
+
+    if (!o.output_id) {
+        strip_extension(argv[2]);
+        o.output_id = argv[2];
+    }
+    const std::string id = o.output_id;
+
+    // launch angles: the reference's FP64-accumulated loops
+    if (!(o.theta_step > 0.0) || !(o.phi_step > 0.0)) {
+        std::cout << '\t' << "ERROR: incl_step and az_step must be positive" << '\n';
+        return 0;
+    }
+    std::vector<double> th, ph;
+    std::vector<size_t> az_end;
+    std::vector<char> topo_first;
+    const double src_x = sph ? lat_r : xs, src_y = sph ? lon_r : ys;
+    for (double phi = o.phi_min; phi <= o.phi_max; phi += o.phi_step) {
+        const double tg = g.theta_grnd(src_x, src_y, zs, phi);
+        const double t0 = std::max(o.theta_min, tg), t1 = std::max(o.theta_max, tg);
+        for (double theta = t0; theta <= t1; theta += o.theta_step) {
+            th.push_back(theta);
+            ph.push_back(phi);
+            topo_first.push_back(fabs(theta - t0) < o.theta_step);
+            if (th.size() > (size_t)200000000) {
+                std::cout << '\t' << "ERROR: more than 2e8 rays requested" << '\n';
+                return 0;
+            }
+        }
+        az_end.push_back(th.size());
+    }
+
+    p.bounces = bounces;
+    p.calc_amp = calc_amp ? 1 : 0;
+    p.write_rays = (o.write_rays || o.write_caustics) ? 1 : 0;
+    p.src[0] = xs; p.src[1] = ys; p.src[2] = zs;
+    p.freq = freq;
+    p.turn_ht_min = turn_ht_min;
+    p.precision = IGA_FP64;
+
+    std::ofstream results((id + ".arrivals.dat").c_str());
+    results << "# " << variant_name(v) << " -prop summary:" << '\n';
+    if (v == Variant::k3DRngdep) {
+        results << "#" << '\t' << "profile prefix: " << argv[2] << '\n';
+        results << "#" << '\t' << "profile grid files: " << argv[3] << ", " << argv[4] << '\n';
+    } else {
+        results << "#" << '\t' << "profile: " << argv[2] << '\n';
+    }
+    results << "#" << '\t' << "inclination: " << o.theta_min << ", " << o.theta_max << ", " << o.theta_step << '\n';
+    results << "#" << '\t' << "azimuth: " << o.phi_min << ", " << o.phi_max << ", " << o.phi_step << '\n';
+    results << "#" << '\t' << "bounces: " << bounces << '\n';
+    results << "#" << '\t' << sum_src << sx << ", " << sy << ", " << zs << '\n';
+    if (!has_topo) results << "#" << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    else results << "#" << '\t' << "topo file:" << topo << '\n';
+    if (v == Variant::kSph) results << "#" << '\t' << "turn_ht_min: " << turn_ht_min << '\n';
+    results << "#" << '\t' << "frequency: " << freq << '\n';
+    results << "#" << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n' << '\n';
+    const char* cols_3d[] = {"x_0 [km]", "y_0 [km]", "arrival incl [deg]", "back az [deg]"};
+    const char* cols_sph[] = {"lat_0 [deg]", "lon_0 [deg]", "inclination [deg]", "back azimuth [deg]"};
+    const char** cn = sph ? cols_sph : cols_3d;
+    results << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << cn[0] << '\t' << cn[1] << '\t' << "time [s]"
+            << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << cn[2] << '\t' << cn[3] << '\t'
+            << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
+
+    const char* pos_hdr = sph ? "# lat [deg]\tlon [deg]\tz [km]" : "# x [km]\ty [km]\tz [km]";
+    std::ofstream raypath;
+    if (o.write_rays) {
+        raypath.open((id + ".raypaths.dat").c_str());
+        raypath << pos_hdr << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\t' << "time [s]" << '\n';
+    }
+    std::vector<std::ofstream> caustics;
+    if (o.write_caustics) {
+        caustics.resize(bounces + 1);
+        for (int b = 0; b <= bounces; b++) {
+            caustics[b].open((id + ".caustics-" + std::to_string(b) + ".dat").c_str());
+            caustics[b] << pos_hdr << '\t' << "time [s]" << '\n';
+        }
+    }
+
+    // trace in chunks of rays (host and device memory stay bounded), write in ray order
+    const size_t n = th.size();
+    const size_t kChunk = 1u << 20;
+    const long long kPathRowsMax = 1LL << 25;
+    size_t az = 0;
+    bool first_result = true;
+    const int nb = bounces + 1;
+    for (size_t r0 = 0; r0 < n; r0 += kChunk) {
+        const size_t r1 = std::min(n, r0 + kChunk), m = r1 - r0;
+        FanChunk c;
+        c.arr.resize(m * nb * IGA_ARRIVAL_COLS);
+        c.arr_ray.resize(m * nb);
+        c.steps.resize(m);
+        int n_out = 0;
+        long long tot = 0;
+        rc = iga_fan_run(atmo, &p, &th[r0], &ph[r0], (int)m, c.arr.data(), (int)(m * nb), &n_out, c.arr_ray.data(),
+                         c.steps.data(), nullptr, &tot, nullptr);
+        if (rc) return fail("ray fan", rc);
+        // sampled paths and caustics, in sub-chunks whose path rows fit kPathRowsMax
+        std::vector<std::vector<double>> path_rows(m);
+        std::vector<std::vector<double>> caus_rows(m);
+        if (o.write_rays || o.write_caustics) {
+            size_t s0 = 0;
+            while (s0 < m) {
+                size_t s1 = s0;
+                long long bound = 0;
+                while (s1 < m) {
+                    const long long b = (long long)nb + c.steps[s1] / 15 + 1;
+                    if (s1 > s0 && bound + b > kPathRowsMax) break;
+                    bound += b;
+                    s1++;
+                }
+                const int k = (int)(s1 - s0);
+                std::vector<double> prow(o.write_rays ? (size_t)bound * IGA_PATH_COLS : 0);
+                std::vector<long long> pstart(k + 1);
+                long long n_path = 0, n_caus = 0;
+                std::vector<double> crow;
+                std::vector<int> cray;
+                long long ccap = o.write_caustics ? 4096 : 0;
+                for (int attempt = 0; attempt < 2; attempt++) {
+                    crow.assign((size_t)ccap * IGA_CAUSTIC_COLS, 0.0);
+                    cray.assign((size_t)ccap, 0);
+                    rc = iga_fan_paths(atmo, &p, &th[r0 + s0], &ph[r0 + s0], k, IGA_PATH_RAYS, &c.steps[s0],
+                                       o.write_rays ? prow.data() : nullptr, o.write_rays ? bound : 0,
+                                       o.write_rays ? &n_path : nullptr, o.write_rays ? pstart.data() : nullptr,
+                                       o.write_caustics ? crow.data() : nullptr, ccap,
+                                       o.write_caustics ? &n_caus : nullptr, o.write_caustics ? cray.data() : nullptr);
+                    if (rc == IGA_E_TRUNCATED && o.write_caustics && n_caus > ccap && n_path <= bound) {
+                        ccap = n_caus;
+                        continue;
+                    }
+                    break;
+                }
+                if (rc) return fail("ray paths", rc);
+                for (int i = 0; i < k && o.write_rays; i++)
+                    path_rows[s0 + i].assign(prow.begin() + pstart[i] * IGA_PATH_COLS,
+                                             prow.begin() + pstart[i + 1] * IGA_PATH_COLS);
+                for (long long j = 0; j < n_caus; j++) {
+                    auto& dst = caus_rows[s0 + cray[j]];
+                    dst.insert(dst.end(), crow.begin() + j * IGA_CAUSTIC_COLS, crow.begin() + (j + 1) * IGA_CAUSTIC_COLS);
+                }
+                s0 = s1;
+            }
+        }
+        size_t w = 0;   // next arrival row
+        for (size_t i = 0; i < m; i++) {
+            const size_t r = r0 + i;
+            std::cout << "Calculating ray path: " << th[r] << " degrees inclination, " << ph[r] << " degrees azimuth." << '\n';
+            for (const double* q = path_rows[i].data(); q < path_rows[i].data() + path_rows[i].size(); q += IGA_PATH_COLS) {
+                if (sph) raypath << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1];
+                else raypath << q[0] << '\t' << q[1];
+                raypath << '\t' << q[2] << '\t' << q[3] << '\t' << q[4] << '\t' << q[5] << '\n';
+            }
+            for (const double* q = caus_rows[i].data(); q < caus_rows[i].data() + caus_rows[i].size(); q += IGA_CAUSTIC_COLS) {
+                std::ofstream& cs = caustics[(int)q[4]];
+                if (sph) cs << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1];
+                else cs << q[0] << '\t' << q[1];
+                cs << '\t' << q[2];
+                if (v == Variant::k3DRngdep) cs << '\t' << 0.0;
+                cs << '\t' << q[3] << '\n';
+            }
+            for (; w < (size_t)n_out && c.arr_ray[w] == (int)i; w++) {
+                const double* q = &c.arr[w * IGA_ARRIVAL_COLS];
+                results << q[0] << '\t' << q[1] << '\t' << (int)q[2];
+                if (sph) results << '\t' << std::setprecision(8) << q[3] << '\t' << std::setprecision(8) << q[4];
+                else results << '\t' << q[3] << '\t' << q[4];
+                for (int col = 5; col < IGA_ARRIVAL_COLS; col++) results << '\t' << q[col];
+                results << '\n';
+                first_result = false;
+            }
+            if (o.write_rays) raypath << '\n';
+            while (az < az_end.size() && az_end[az] == r + 1) {
+                results << '\n';
+                az++;
+            }
+        }
+    }
+    while (az < az_end.size()) {   // azimuths without rays
+        results << '\n';
+        az++;
+    }
+    (void)first_result;
+
+    // terrain under the last ray that opened the terrain file (the first
+    // inclination of each azimuth by the reference's test; each reopening
+    // truncates the file)
+    if (o.write_topo) {
+        long long last = -1;
+        for (size_t r = 0; r < n; r++)
+            if (topo_first[r]) last = (long long)r;
+        std::ofstream tf;
+        if (last >= 0) {
+            tf.open((id + ".terrain.dat").c_str());
+            std::vector<long long> st(1);
+            int n_out = 0;
+            std::vector<double> arr((size_t)nb * IGA_ARRIVAL_COLS);
+            rc = iga_fan_run(atmo, &p, &th[last], &ph[last], 1, arr.data(), nb, &n_out, nullptr, st.data(), nullptr,
+                             nullptr, nullptr);
+            if (rc) return fail("terrain samples", rc);
+            const long long cap = (long long)nb + st[0] / 10 + 1;
+            std::vector<double> rows((size_t)cap * IGA_PATH_COLS);
+            long long np = 0;
+            rc = iga_fan_paths(atmo, &p, &th[last], &ph[last], 1, IGA_PATH_TERRAIN, st.data(), rows.data(), cap, &np,
+                               nullptr, nullptr, 0, nullptr, nullptr);
+            if (rc) return fail("terrain samples", rc);
+            for (long long j = 0; j < np; j++) {
+                const double* q = &rows[(size_t)j * IGA_PATH_COLS];
+                if (sph) tf << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1];
+                else tf << q[0] << '\t' << q[1];
+                tf << '\t' << q[2] << '\n';
+            }
+        }
+    }
+    iga_atmo_destroy(atmo);
+    return 0;
+}
+
+// ------------------------------------------------------------------------
+// -eig_search / -eig_direct (3D stratified)
+// ------------------------------------------------------------------------
+
+struct EigOpts {
+    double src[3] = {0.0, 0.0, 0.0};
+    double rcvr[2] = {-250.0, 0.0};
+    bool verbose = false;
+    const char* output_id = nullptr;
+};
+
+// Sampled path of one eigenray for {id}.eigenray-N.dat (find_eigenray's
+// final trace, geoac.eigenray.3d.cpp:220-279): rows of the first segment
+// as run_prop writes them, later segments with the raw altitude and the
+// absorption sum itself instead of -2 x it.
+int write_eigenray_file(const std::string& path, iga_atmo_t atmo, const iga_fan_params& base, const double* src,
+                        double theta, double az, int n_b) {
+    iga_fan_params q = base;
+    q.bounces = n_b;
+    q.calc_amp = 1;
+    q.write_rays = 1;
+    q.turn_ht_min = -1.0e30;   // the final trace never stops at a low turning height
+    q.src[0] = src[0]; q.src[1] = src[1]; q.src[2] = src[2];
+    long long st = 0;
+    int n_out = 0;
+    std::vector<double> arr((size_t)(n_b + 1) * IGA_ARRIVAL_COLS);
+    int rc = iga_fan_run(atmo, &q, &theta, &az, 1, arr.data(), n_b + 1, &n_out, nullptr, &st, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    const long long cap = (long long)n_b + 1 + st / 15 + 1;
+    std::vector<double> rows((size_t)cap * IGA_PATH_COLS);
+    long long np = 0;
+    rc = iga_fan_paths(atmo, &q, &theta, &az, 1, IGA_PATH_RAYS, &st, rows.data(), cap, &np, nullptr, nullptr, 0, nullptr,
+                       nullptr);
+    if (rc) return rc;
+    std::ofstream f(path.c_str());
+    f << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]"
+      << '\t' << "time [s]" << '\n';
+    for (long long j = 0; j < np; j++) {
+        const double* r = &rows[(size_t)j * IGA_PATH_COLS];
+        const double absorb = r[6] >= 1.0 ? -r[4] / 2.0 : r[4];
+        f << r[0] << '\t' << r[1] << '\t' << r[2] << '\t' << r[3] << '\t' << absorb << '\t' << r[5] << '\n';
+    }
+    return IGA_OK;
+}
+
+void print_eigenray(const double* q, const double* src, bool verbose) {
+    if (verbose) {
+        std::cout << '\t' << '\t' << "Eigenray Identified:" << '\n';
+        std::cout << '\t' << '\t' << '\t' << "inclination [deg] = " << std::setprecision(8) << q[0] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "azimuth [deg] = " << std::setprecision(8) << q[1] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "bounces [-] = " << (int)q[2] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "x [km E-W] = " << q[3] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "y [km N-S] = " << q[4] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "time [s] = " << q[5] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "celerity [km/s] = " << q[6] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "turning height [km] = " << q[7] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "arrival inclination [deg] = " << q[8] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "back azimuth = " << q[9] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "attenuation (geometric) [dB] = " << q[10] << '\n';
+        std::cout << '\t' << '\t' << '\t' << "absorption [dB] = " << q[11] << '\n' << '\n';
+    } else {
+        std::cout << '\t' << "Eigenray identified:" << '\t' << "theta, phi = " << std::setprecision(8) << q[0] << ", " << q[1]
+                  << " degrees." << '\n';
+    }
+    (void)src;
+}
+
+// Second pass of the eigenray modes.  direct = run_eig_direct's key set.
+bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep, EigOpts& o, bool has_topo,
+               double& incl_est, double& az_est_deg, bool& az_est_given, int& bounces) {
+    PropOpts po;
+    double freq = ep.fan.freq;
+    const char* val;
+    for (int i = 3; i < argc; i++) {
+        const char* a = argv[i];
+        if (!direct && key2(a, "incl_min=", "min_incl=", &val)) ep.incl_min = atof(val);
+        else if (!direct && key2(a, "incl_max=", "max_incl=", &val)) ep.incl_max = atof(val);
+        else if (!direct && key2(a, "bnc_min=", "min_bnc=", &val)) ep.bnc_min = atoi(val);
+        else if (!direct && key2(a, "bnc_max=", "max_bnc=", &val)) ep.bnc_max = atoi(val);
+        else if (!direct && key(a, "bounces=", &val)) ep.bnc_min = ep.bnc_max = atoi(val);
+        else if (direct && key(a, "incl_est=", &val)) incl_est = atof(val);
+        else if (direct && key(a, "az_est=", &val)) { az_est_deg = atof(val); az_est_given = true; }
+        else if (direct && key(a, "bounces=", &val)) bounces = atoi(val);
+        else if (key2(a, "src_x=", "x_src=", &val)) o.src[0] = atof(val);
+        else if (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val)) o.src[1] = atof(val);
+        else if (key2(a, "src_alt=", "alt_src=", &val)) o.src[2] = atof(val);
+        else if (key2(a, "rcvr_x=", "x_rcvr=", &val)) o.rcvr[0] = atof(val);
+        else if (key2(a, "rcvr_y=", "y_rcvr=", &val)) o.rcvr[1] = atof(val);
+        else if (key(a, "verbose=", &val)) o.verbose = str2bool(val);
+        else if (key(a, "iterations=", &val)) ep.iterations = (int)atof(val);
+        else if (key(a, "damping=", &val)) ep.damping = atof(val);
+        else if (key(a, "tolerance=", &val)) ep.tolerance = atof(val);
+        else if (!direct && key(a, "az_dev_lim=", &val)) ep.az_err_lim = atof(val);
+        else if (!direct && key2(a, "incl_step_min=", "min_incl_step=", &val)) ep.incl_step_min = atof(val);
+        else if (!direct && key2(a, "incl_step_max=", "max_incl_step=", &val)) ep.incl_step_max = atof(val);
+        else if (common_key(v, a, ep.fan, po, has_topo, freq)) {}
+        else if (!confirm_unknown(a, false)) return false;
+    }
+    ep.fan.freq = freq;
+    o.output_id = po.output_id;
+    if (po.use_blw) {
+        std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
+        return false;
+    }
+    if (po.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
+    return true;
+}
+
+int run_eig(int argc, char** argv, Variant v, bool direct) {
+    banner(v, direct ? "Eigenray Direct" : "Eigenray Search");
+    const char* topo = nullptr;
+    iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo);
+    if (!atmo) return 0;
+    iga_eig_params ep;
+    int rc = iga_eig_params_default(atmo, &ep);
+    if (rc) return fail("parameters", rc);
+    print_region(v, ep.fan);
+    EigOpts o;
+    o.verbose = direct;
+    double incl_est = 10.0, az_est = 0.0;
+    bool az_given = false;
+    int bounces = 0;
+    if (!parse_eig(argc, argv, v, direct, ep, o, false, incl_est, az_est, az_given, bounces)) return 0;
+    o.src[2] = std::max(ep.fan.z_grnd, o.src[2]);
+    const double z_rcvr = ep.fan.z_grnd;
+    if (!o.output_id) {
+        strip_extension(argv[2]);
+        o.output_id = argv[2];
+    }
+    const std::string id = o.output_id;
+    iga_eig_pair pair;
+    pair.src[0] = o.src[0]; pair.src[1] = o.src[1]; pair.src[2] = o.src[2];
+    pair.rcvr[0] = o.rcvr[0]; pair.rcvr[1] = o.rcvr[1];
+
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "source location: " << o.src[0] << ", " << o.src[1] << ", " << o.src[2] << '\n';
+    std::cout << '\t' << "receiver location: " << o.rcvr[0] << ", " << o.rcvr[1] << ", " << z_rcvr << '\n';
+    if (direct) {
+        const double phi_est = az_given ? Pi / 2.0 - az_est * (Pi / 180.0) : atan2(o.rcvr[1] - o.src[1], o.rcvr[0] - o.src[0]);
+        az_est = 90.0 - phi_est * 180.0 / Pi;
+        std::cout << '\t' << "inclination estimate: " << incl_est << '\n';
+        std::cout << '\t' << "azimuth estimate: " << az_est << '\n';
+        std::cout << '\t' << "bounces: " << bounces << '\n';
+    } else {
+        std::cout << '\t' << "inclination range: " << ep.incl_min << ", " << ep.incl_max << '\n';
+        std::cout << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
+    }
+    std::cout << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+    std::cout << '\t' << "damping:" << ep.damping << '\n';
+    std::cout << '\t' << "frequency: " << ep.fan.freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << '\n';
+
+    std::vector<double> rows;
+    int n_out = 0;
+    if (direct) {
+        rows.resize(IGA_ARRIVAL_COLS);
+        rc = iga_eig_direct(atmo, &ep, &pair, incl_est, az_est, bounces, rows.data(), &n_out, nullptr);
+        if (rc) return fail("eigenray search", rc);
+    } else {
+        std::ofstream res((id + ".arrivals.dat").c_str());
+        res << "# " << variant_name(v) << " -eig_search summary:" << '\n';
+        res << "# " << '\t' << "profile: " << argv[2] << '\n';
+        res << "# " << '\t' << "source location: " << o.src[0] << ", " << o.src[1] << ", " << o.src[2] << '\n';
+        res << "# " << '\t' << "receiver location: " << o.rcvr[0] << ", " << o.rcvr[1] << ", " << z_rcvr << '\n';
+        res << "# " << '\t' << "inclination range: " << ep.incl_min * (Pi / 180.0) * (180.0 / Pi) << ", "
+            << ep.incl_max * (Pi / 180.0) * (180.0 / Pi) << '\n';
+        res << "# " << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
+        res << "#" << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+        res << "# " << '\t' << "damping: " << ep.damping << '\n';
+        res << "# " << '\t' << "frequency: " << ep.fan.freq << '\n';
+        res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << '\n';
+        res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << "x_0 [km]" << '\t' << "y_0 [km]" << '\t'
+            << "time [s]" << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << "arrival incl [deg]" << '\t'
+            << "back az [deg]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
+        for (int nbc = ep.bnc_min; nbc <= ep.bnc_max; nbc++)
+            std::cout << "Searching for " << nbc << " bounce eigenray(s) with inclination between " << ep.incl_min
+                      << " and " << ep.incl_max << "." << '\n';
+        const int cap0 = 256;
+        rows.resize((size_t)cap0 * IGA_ARRIVAL_COLS);
+        long long steps = 0;
+        rc = iga_eig_run(atmo, &ep, &pair, 1, rows.data(), cap0, &n_out, nullptr, &steps);
+        if (rc == IGA_E_TRUNCATED) {
+            rows.resize((size_t)n_out * IGA_ARRIVAL_COLS);
+            rc = iga_eig_run(atmo, &ep, &pair, 1, rows.data(), n_out, &n_out, nullptr, &steps);
+        }
+        if (rc) return fail("eigenray search", rc);
+        for (int j = 0; j < n_out; j++) {
+            const double* q = &rows[(size_t)j * IGA_ARRIVAL_COLS];
+            res << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1] << '\t' << (int)q[2];
+            for (int col = 3; col < IGA_ARRIVAL_COLS; col++) res << '\t' << q[col];
+            res << '\n';
+        }
+    }
+    for (int j = 0; j < n_out; j++) {
+        const double* q = &rows[(size_t)j * IGA_ARRIVAL_COLS];
+        print_eigenray(q, o.src, o.verbose);
+        rc = write_eigenray_file(id + ".eigenray-" + std::to_string(j) + ".dat", atmo, ep.fan, o.src, q[0], q[1], (int)q[2]);
+        if (rc) return fail("eigenray path", rc);
+    }
+    if (!direct) std::cout << '\t' << "Identified " << n_out << " eigenray(s)." << '\n';
+    iga_atmo_destroy(atmo);
+    return 0;
+}
+
+}  // namespace
+
+int run(int argc, char** argv, Variant v) {
+    const int min_args = is_rngdep(v) ? 5 : 3;
+    if (argc < min_args) {
+        usage(v);
+        return 0;
+    }
+    const char* o = argv[1];
+    if (strncmp(o, "-version", 8) == 0 || strncmp(o, "-v", 2) == 0) version();
+    else if (strncmp(o, "-usage", 6) == 0 || strncmp(o, "-u", 2) == 0) usage(v);
+    else if (strncmp(o, "-prop", 5) == 0 || strncmp(o, "-p", 2) == 0) return run_prop(argc, argv, v);
+    else if (strncmp(o, "-back_proj", 10) == 0 || strncmp(o, "-b", 2) == 0)
+        std::cout << "-back_proj is not provided by the GPU front end." << '\n';
+    else if (strncmp(o, "-eig_search", 11) == 0 || strncmp(o, "-s", 2) == 0) {
+        if (v == Variant::k3D) return run_eig(argc, argv, v, false);
+        std::cout << "-eig_search is provided for infraga-3d only by the GPU front end." << '\n';
+    } else if (strncmp(o, "-eig_direct", 11) == 0 || strncmp(o, "-d", 2) == 0) {
+        if (v == Variant::k3D) return run_eig(argc, argv, v, true);
+        std::cout << "-eig_direct is provided for infraga-3d only by the GPU front end." << '\n';
+    } else if (strncmp(o, "-wnl_wvfrm", 10) == 0 || strncmp(o, "-w", 2) == 0)
+        std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
+    else
+        std::cout << "Unrecognized option." << '\n';
+    return 0;
+}
+
+}  // namespace cli

@@ -173,6 +173,7 @@ struct Chain {
     int pair = 0, nb = 0;
     double sx = 0, sy = 0, rx = 0, ry = 0, rcvr_rng = 0, rcvr_az = 0;
     enum Phase { kEst, kNewton, kRecordTrace, kDone } phase = kEst;
+    bool direct = false;         // find_eigenray alone (run_eig_direct): no sweep before or after
     double theta_start = 0;
     // est_eigenray state
     double th_min = 0, th_max = 0, dth = 0, dph = 0, r = 0, r_prev = 0, phi = 0, th = 0, th_next = 0;
@@ -216,6 +217,7 @@ void est_begin(Chain& c, const Settings& S, double theta_start) {
 // After est_eigenray (and find_eigenray, if it ran): run_eig_search's
 // theta_start = theta_next and loop condition (main.infraga.3d.cpp:943-949).
 void search_continue(Chain& c, const Settings& S) {
+    if (c.direct) { c.phase = Chain::kDone; return; }
     const double ts = c.th_next;
     if (ts < S.theta_max) est_begin(c, S, ts);
     else c.phase = Chain::kDone;
@@ -335,7 +337,8 @@ namespace iga_internal {
 // the request server).  Device scratch is stream-ordered (cudaMallocAsync /
 // cudaFreeAsync), so searches on different streams overlap on the GPU.
 int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, cudaStream_t st,
-               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out) {
+               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out,
+               const EigDirect* direct) {
     out_rows.clear(); out_pair.clear(); steps_out = 0;
     if (!h || !P || n_pairs < 0 || (n_pairs > 0 && !pairs)) return IGA_E_INVALID;
     iga_fan_params fp = P->fan;
@@ -383,8 +386,14 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             c.rx = pairs[ip].rcvr[0]; c.ry = pairs[ip].rcvr[1];
             c.rcvr_rng = sqrt(pow(c.rx - c.sx, 2) + pow(c.ry - c.sy, 2));
             c.rcvr_az = atan2(c.ry - c.sy, c.rx - c.sx);
-            if (theta_min < S.theta_max) est_begin(c, S, theta_min);
-            else c.phase = Chain::kDone;
+            if (direct) {
+                c.direct = true;
+                newton_begin(c, direct[ip].theta, direct[ip].phi);
+            } else if (theta_min < S.theta_max) {
+                est_begin(c, S, theta_min);
+            } else {
+                c.phase = Chain::kDone;
+            }
             chains.push_back(std::move(c));
         }
     }
@@ -567,6 +576,27 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
 }
 
 }  // namespace iga_internal
+
+extern "C" int iga_eig_direct(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pair, double incl_est,
+                              double az_est, int bounces, double* eigenray, int* found, long long* total_steps) {
+    if (!h || !P || !pair || !found || bounces < 0) return IGA_E_INVALID;
+    *found = 0;
+    if (total_steps) *total_steps = 0;
+    iga_eig_params q = *P;
+    q.bnc_min = q.bnc_max = bounces;
+    EigDirect d{incl_est * (kPi / 180.0), kPi / 2.0 - az_est * (kPi / 180.0)};
+    std::vector<double> rows;
+    std::vector<int> pidx;
+    long long steps = 0;
+    int rc = eig_search(h, &q, pair, 1, h->stream, rows, pidx, steps, &d);
+    if (rc) return rc;
+    if (!pidx.empty()) {
+        *found = 1;
+        if (eigenray) memcpy(eigenray, rows.data(), IGA_ARRIVAL_COLS * sizeof(double));
+    }
+    if (total_steps) *total_steps = steps;
+    return IGA_OK;
+}
 
 extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs,
                            double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps) {

@@ -28,6 +28,15 @@ struct Fan3DArgs {
     double* aux;             // nullable: [n_rays][bounces+1][4] per-arrival diagnostics
     unsigned int* queue;     // [0] next ray (device ray queue)
     int grid_cap;            // > 0: at most this many CTAs (the request server shares the GPU)
+    // sampled per-step output (run_prop's write_rays / write_topo / write_caustics);
+    // all null on the plain fan path
+    double* path_rows;       // [path_off[n_rays]][kPathCols]
+    const long long* path_off;   // [n_rays + 1]: row range of each ray
+    long long* path_n;       // [n_rays]: rows the ray produced (may exceed its range: dropped)
+    int path_mode;           // kPathRays or kPathTerrain
+    double* caus_rows;       // [caus_cap][kCausCols], appended in any order
+    unsigned long long* caus_count;
+    long long caus_cap;
     // geometry / limits
     double src_x, src_y, src_z;
     double ds_min, ds_max, s_max;
@@ -79,6 +88,26 @@ struct Fan3DArgs {
 };
 
 constexpr int kStrideF = 14;  // floats per segment row of the FP32 table
+
+// Sampled output rows.  Path rows: horizontal position (x, y [km] or lat, lon
+// [deg]), altitude [km] (terrain mode: the ground height there), amplitude
+// [dB] (0 without calc_amp or in terrain mode), absorption [dB] (-2 x the
+// running sum), travel time [s], bounce.  Caustic rows: position (3), time,
+// bounce, ray, and the ray's step index of the row (for ordering).
+constexpr int kPathCols = 7;
+constexpr int kCausCols = 7;
+constexpr int kPathRays = 0;      // rows m == 1 and m % 15 == 0 of each bounce (raypaths)
+constexpr int kPathTerrain = 1;   // rows m % 10 == 1 (terrain under the ray)
+
+__host__ __device__ inline bool path_sampled(int mode, int m) {
+    return mode == kPathRays ? (m == 1 || m % 15 == 0) : (m % 10 == 1);
+}
+
+// Upper bound on the path rows of a ray that took `steps` RK4 steps over at
+// most `segments` bounce segments: each segment of K rows samples m in 1..K-1.
+inline long long path_rows_bound(int mode, long long steps, int segments) {
+    return (long long)segments + steps / (mode == kPathRays ? 15 : 10) + 1;
+}
 
 cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 

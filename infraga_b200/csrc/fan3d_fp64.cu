@@ -33,7 +33,10 @@ namespace {
 constexpr int kThreads = IGA_FAN_THREADS;
 
 
-template <bool AMP, bool SMEM>
+// PATHS: also write the sampled per-step rows (raypaths / terrain samples)
+// and caustic points of run_prop's write_rays / write_topo / write_caustics
+// output (main.infraga.3d.cpp:443-497); the fan results are unchanged.
+template <bool AMP, bool SMEM, bool PATHS>
 __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = Dim<AMP>::n;
     // dynamic shared memory: [N][kThreads] row k-1 of each lane's ray, then
@@ -66,6 +69,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
     // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
     // sums (bulk mode) or the pending last-segment increments (write_rays mode)
     double s, tt, att, pt, pa, zmax;
+    long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
@@ -75,6 +79,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = a.z0;
+        if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
 
@@ -86,9 +91,19 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         s += ds;
         double acc[N], stg[N], f[N];
         rhs<AMP>(tab, a, seg, y, rc, f);
-        if (AMP && a.aux && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
+        if (AMP && (a.aux || (PATHS && a.caus_rows)) && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
             const double D = ray_jacobian(f, y);
-            if (kb >= 2 && D * D_prev < 0.0) caustics++;
+            if (kb >= 2 && D * D_prev < 0.0) {
+                caustics++;
+                if (PATHS && a.caus_rows) {   // row kb; time through segment (kb-1, kb)
+                    const unsigned long long w = atomicAdd(a.caus_count, 1ull);
+                    if ((long long)w < a.caus_cap) {
+                        double* o = a.caus_rows + w * kCausCols;
+                        o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; o[3] = tt + pt;
+                        o[4] = (double)bnc; o[5] = (double)ray; o[6] = (double)(steps + kb);
+                    }
+                }
+            }
             D_prev = D;
         }
 #pragma unroll
@@ -126,6 +141,21 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         if (!esc && !gnd) {
 #pragma unroll
             for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
+                // row m = kb of the bounce, above the ground: z = max(z, z_g) = z
+                if (p_n < p_cap) {
+                    double* o = a.path_rows + (p_base + p_n) * kPathCols;
+                    o[0] = y[0]; o[1] = y[1];
+                    o[2] = a.path_mode == kPathRays ? y[2] : a.z0;
+                    int sg = seg;
+                    o[3] = (AMP && a.path_mode == kPathRays)
+                               ? amp_db(tab, a, sg, y, rc, a.theta_deg[ray] * kPi / 180.0,
+                                        kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0, nullptr)
+                               : 0.0;
+                    o[4] = -2.0 * (att + pa); o[5] = tt + pt; o[6] = (double)bnc;
+                }
+                p_n++;
+            }
             continue;
         }
 
@@ -194,15 +224,16 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
         if (a.ray_status) a.ray_status[ray] = status;
+        if (PATHS && a.path_rows) a.path_n[ray] = p_n;
         ray = (int)atomicAdd(a.queue, 1u);
         if (ray >= a.n_rays) break;
         start_ray(ray);
     }
 }
 
-template <bool AMP, bool SMEM>
+template <bool AMP, bool SMEM, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
-    auto kern = fan3d_fp64_kernel<AMP, SMEM>;
+    auto kern = fan3d_fp64_kernel<AMP, SMEM, PATHS>;
     const size_t smem = (size_t)Dim<AMP>::n * kThreads * sizeof(double) +
                         (SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -227,8 +258,12 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 cudaError_t launch_fan3d_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
     const size_t smem = (size_t)a.n_knots * kStride * sizeof(double);
     const bool fits = smem <= 64 * 1024;
-    if (calc_amp) return fits ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<true, false>(a, stream, grid_used);
-    return fits ? launch_impl<false, true>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
+    if (a.path_rows || a.caus_rows) {
+        if (calc_amp) return fits ? launch_impl<true, true, true>(a, stream, grid_used) : launch_impl<true, false, true>(a, stream, grid_used);
+        return fits ? launch_impl<false, true, true>(a, stream, grid_used) : launch_impl<false, false, true>(a, stream, grid_used);
+    }
+    if (calc_amp) return fits ? launch_impl<true, true, false>(a, stream, grid_used) : launch_impl<true, false, false>(a, stream, grid_used);
+    return fits ? launch_impl<false, true, false>(a, stream, grid_used) : launch_impl<false, false, false>(a, stream, grid_used);
 }
 
 }  // namespace iga

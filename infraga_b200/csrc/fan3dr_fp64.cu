@@ -355,7 +355,10 @@ __device__ __forceinline__ void ray_init_3dr(const Fan3DArgs& a, double theta, d
     }
 }
 
-template <bool AMP>
+// PATHS: also write the sampled per-step rows and caustic points of
+// run_prop's write_rays / write_topo / write_caustics output
+// (main.infraga.3d.rngdep.cpp:440-488); the fan results are unchanged.
+template <bool AMP, bool PATHS>
 __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = Dim3r<AMP>::n;
     extern __shared__ double s_mem[];
@@ -389,6 +392,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
     double D_prev = 0.0;
     long long steps;
     double s, tt, att, pt, pa, zmax;
+    long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
@@ -397,6 +401,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = 0.0;
+        if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
 
@@ -407,12 +412,22 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         s += ds;
         double acc[N], stg[N], f[N];
         rhs_3dr<AMP>(a, vw, cl, y, f);
-        if (AMP && a.aux && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
+        if (AMP && (a.aux || (PATHS && a.caus_rows)) && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
             const double* Xt = y + 6;
             const double* Xp = y + 12;
             const double D = f[0] * (Xt[1] * Xp[2] - Xp[1] * Xt[2]) - Xt[0] * (f[1] * Xp[2] - f[2] * Xp[1]) +
                              Xp[0] * (f[1] * Xt[2] - f[2] * Xt[1]);
-            if (kb >= 2 && D * D_prev < 0.0) caustics++;
+            if (kb >= 2 && D * D_prev < 0.0) {
+                caustics++;
+                if (PATHS && a.caus_rows) {   // row kb (raw altitude); time through segment (kb-1, kb)
+                    const unsigned long long w = atomicAdd(a.caus_count, 1ull);
+                    if ((long long)w < a.caus_cap) {
+                        double* o = a.caus_rows + w * kCausCols;
+                        o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; o[3] = tt + pt;
+                        o[4] = (double)bnc; o[5] = (double)ray; o[6] = (double)(steps + kb);
+                    }
+                }
+            }
             D_prev = D;
         }
 #pragma unroll
@@ -447,6 +462,21 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         if (!esc && !gnd) {
 #pragma unroll
             for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
+                if (p_n < p_cap) {
+                    double* o = a.path_rows + (p_base + p_n) * kPathCols;
+                    Cells c2 = cl;
+                    const double zg = topo_z(vw, c2, y[0], y[1]);
+                    o[0] = y[0]; o[1] = y[1];
+                    o[2] = a.path_mode == kPathRays ? fmax(y[2], zg) : zg;
+                    o[3] = (AMP && a.path_mode == kPathRays)
+                               ? amp_db_3dr(a, vw, c2, y, a.theta_deg[ray] * kPi / 180.0,
+                                            kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0, nullptr)
+                               : 0.0;
+                    o[4] = -2.0 * (att + pa); o[5] = tt + pt; o[6] = (double)bnc;
+                }
+                p_n++;
+            }
             continue;
         }
 
@@ -517,15 +547,16 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
         if (a.ray_status) a.ray_status[ray] = status;
+        if (PATHS && a.path_rows) a.path_n[ray] = p_n;
         ray = (int)atomicAdd(a.queue, 1u);
         if (ray >= a.n_rays) break;
         start_ray(ray);
     }
 }
 
-template <bool AMP>
+template <bool AMP, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
-    auto kern = fan3dr_fp64_kernel<AMP>;
+    auto kern = fan3dr_fp64_kernel<AMP, PATHS>;
     const size_t smem = ((size_t)Dim3r<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -548,7 +579,9 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 }  // namespace
 
 cudaError_t launch_fan3dr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
-    return calc_amp ? launch_impl<true>(a, stream, grid_used) : launch_impl<false>(a, stream, grid_used);
+    if (a.path_rows || a.caus_rows)
+        return calc_amp ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<false, true>(a, stream, grid_used);
+    return calc_amp ? launch_impl<true, false>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
 }
 
 }  // namespace iga

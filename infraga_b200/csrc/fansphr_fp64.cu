@@ -392,7 +392,10 @@ __device__ __noinline__ void reflect_sphr(const Fan3DArgs& a, const Views& vw, C
     for (int i = 0; i < N; i++) y[i] = q[i];
 }
 
-template <bool AMP>
+// PATHS: also write the sampled per-step rows and caustic points of
+// run_prop's write_rays / write_topo / write_caustics output
+// (main.infraga.sph.rngdep.cpp:450-503); the fan results are unchanged.
+template <bool AMP, bool PATHS>
 __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = DimSph<AMP>::n;
     extern __shared__ double s_mem[];
@@ -427,6 +430,8 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
     double D_prev = 0.0;
     long long steps;
     double s, tt, att, pt, pa, rmax;
+    long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
+    const double rad2deg = 180.0 / kPi;
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * (kPi / 180.0);
@@ -435,6 +440,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         rmax = 0.0;
+        if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
 
@@ -446,9 +452,19 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         s += ds;
         double acc[N], stg[N], f[N];
         rhs_sphr<AMP>(a, vw, cl, y, f);
-        if (AMP && a.aux && kb >= 1) {
+        if (AMP && (a.aux || (PATHS && a.caus_rows)) && kb >= 1) {
             const double D = ray_det_sph(f, y);
-            if (kb >= 2 && D * D_prev < 0.0) caustics++;
+            if (kb >= 2 && D * D_prev < 0.0) {
+                caustics++;
+                if (PATHS && a.caus_rows) {   // row kb; time through segment (kb-1, kb)
+                    const unsigned long long w = atomicAdd(a.caus_count, 1ull);
+                    if ((long long)w < a.caus_cap) {
+                        double* o = a.caus_rows + w * kCausCols;
+                        o[0] = y[1] * rad2deg; o[1] = y[2] * rad2deg; o[2] = y[0] - a.r_earth; o[3] = tt + pt;
+                        o[4] = (double)bnc; o[5] = (double)ray; o[6] = (double)(steps + kb);
+                    }
+                }
+            }
             D_prev = D;
         }
 #pragma unroll
@@ -488,6 +504,20 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         if (!esc && !gnd) {
 #pragma unroll
             for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
+                if (p_n < p_cap) {
+                    double* o = a.path_rows + (p_base + p_n) * kPathCols;
+                    Cells c2 = cl;
+                    o[0] = y[1] * rad2deg; o[1] = y[2] * rad2deg;
+                    o[2] = a.path_mode == kPathRays ? y[0] - a.r_earth : topo_r(a, vw, c2, y[1], y[2]) - a.r_earth;
+                    o[3] = (AMP && a.path_mode == kPathRays)
+                               ? amp_db_sphr(a, vw, c2, y, a.theta_deg[ray] * (kPi / 180.0),
+                                             kPi / 2.0 - a.phi_deg[ray] * (kPi / 180.0), nullptr)
+                               : 0.0;
+                    o[4] = -2.0 * (att + pa); o[5] = tt + pt; o[6] = (double)bnc;
+                }
+                p_n++;
+            }
             continue;
         }
 
@@ -541,15 +571,16 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
         if (a.ray_status) a.ray_status[ray] = status;
+        if (PATHS && a.path_rows) a.path_n[ray] = p_n;
         ray = (int)atomicAdd(a.queue, 1u);
         if (ray >= a.n_rays) break;
         start_ray(ray);
     }
 }
 
-template <bool AMP>
+template <bool AMP, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
-    auto kern = fansphr_fp64_kernel<AMP>;
+    auto kern = fansphr_fp64_kernel<AMP, PATHS>;
     const size_t smem = ((size_t)DimSph<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -572,7 +603,9 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 }  // namespace
 
 cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
-    return calc_amp ? launch_impl<true>(a, stream, grid_used) : launch_impl<false>(a, stream, grid_used);
+    if (a.path_rows || a.caus_rows)
+        return calc_amp ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<false, true>(a, stream, grid_used);
+    return calc_amp ? launch_impl<true, false>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
 }
 
 }  // namespace iga

@@ -46,15 +46,33 @@ extern thread_local std::string g_err;
 int cuda_fail(cudaError_t e, const char* what);
 int validate(const iga_fan_params* p, int n_rays);
 int build_args(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a);
-// iga_fan_run_device with an optional CTA cap (0 = none), for the request server
+// Device buffers of the sampled per-step output (Fan3DArgs path_* / caus_*).
+struct PathSpec {
+    double* rows = nullptr;
+    const long long* off = nullptr;
+    long long* n = nullptr;
+    int mode = 0;
+    double* caus = nullptr;
+    unsigned long long* caus_count = nullptr;
+    long long caus_cap = 0;
+};
+// iga_fan_run_device with an optional CTA cap (0 = none), for the request
+// server, and optional sampled per-step output (paths.cu)
 int fan_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
-               cudaStream_t st, int grid_cap);
+               cudaStream_t st, int grid_cap, const PathSpec* paths = nullptr);
 // FP32 knot table and alpha(z) table of `freq` into the launch arguments
 int fp32c_setup(iga_atmo_s* h, double freq, iga::Fan3DArgs& a);
-// the eigenray search on one stream (eig3d.cu)
+// Launch estimate of find_eigenray alone (run_eig_direct): radians, the
+// reference's internal azimuth convention (phi = pi/2 - azimuth).
+struct EigDirect {
+    double theta, phi;
+};
+// the eigenray search on one stream (eig3d.cu); with `direct` (one entry per
+// pair) only the Newton refinement runs, for bounce count P->bnc_min
 int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, cudaStream_t st,
-               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out);
+               std::vector<double>& out_rows, std::vector<int>& out_pair, long long& steps_out,
+               const EigDirect* direct = nullptr);
 }  // namespace iga_internal
 
 #define IGA_CUDA(call, what)                                                  \

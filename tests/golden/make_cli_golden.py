@@ -1,0 +1,124 @@
+"""Regenerates the command-line fixtures under cli/ from the reference's own,
+unmodified command-line binaries (oracle/_ref/infraga-*, built from the
+reference sources by ``make -C oracle ref``).
+
+    python tests/golden/make_cli_golden.py           # all cases
+    python tests/golden/make_cli_golden.py NAME...   # only these cases
+
+Each case runs one binary in a scratch directory laid out by ``stage()``
+(the same layout the GPU front-end test uses, so header lines that echo
+file names match) and keeps every output file it wrote under cli/NAME/,
+with the argument list in cli/cases.json.  Atmospheres are the seeded
+synthetic fixtures already in this directory.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.path.join(ROOT, "oracle", "_ref")
+OUT = os.path.join(HERE, "cli")
+
+# name -> (binary, atmosphere kind, seed of the 1D profile, argv after the binary)
+# kinds: "1d" = profiles/gen{seed}.met staged as atmo.met;
+#        "sphr" / "3dr" = the rngdep/ or rngdep3d/ grid staged as grid/node*, grid/x.dat, grid/y.dat, topo.dat
+CASES = {
+    "3d_prop": ("infraga-3d", "1d", 0,
+                ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=90",
+                 "az_step=90", "bounces=2", "max_rng=600", "max_ds=0.25", "write_caustics=true", "write_topo=true"]),
+    "3d_prop_noamp": ("infraga-3d", "1d", 1,
+                      ["-p", "atmo.met", "incl_min=10", "incl_max=30.5", "incl_step=0.5", "azimuth=-60", "bounces=1",
+                       "max_rng=300", "calc_amp=false", "write_rays=false", "z_grnd=0.25", "freq=0.3"]),
+    "3d_eig": ("infraga-3d", "1d", 0,
+               ["-eig_search", "atmo.met", "rcvr_x=240", "rcvr_y=30", "bnc_min=0", "bnc_max=1", "incl_min=10",
+                "incl_max=17"]),
+    "3d_direct": ("infraga-3d", "1d", 0,
+                  ["-eig_direct", "atmo.met", "rcvr_x=240", "rcvr_y=30", "incl_est=8", "bounces=0",
+                   "output_id=direct"]),
+    "sph_prop": ("infraga-sph", "1d", 1,
+                 ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=180",
+                  "az_step=180", "bounces=1", "src_lat=20", "src_lon=-40", "max_rng=700", "max_ds=0.25", "write_caustics=true",
+                  "write_topo=true"]),
+    "3dr_prop": ("infraga-3d-rngdep", "3dr", 0,
+                 ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "incl_min=6",
+                  "incl_max=26", "incl_step=10", "az_min=90", "az_max=270", "az_step=180", "bounces=1",
+                  "max_rng=400", "max_ds=0.25", "write_caustics=true", "write_topo=true"]),
+    "3dr_calc_amp": ("infraga-3d-rngdep", "3dr", 0,
+                     ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "inclination=12", "azimuth=100",
+                      "bounces=1", "calc_amp=true", "write_rays=false", "output_id=amp"]),
+    "sphr_prop": ("infraga-sph-rngdep", "sphr", 0,
+                  ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "incl_min=6",
+                   "incl_max=26", "incl_step=10", "az_min=90", "az_max=270", "az_step=180", "bounces=1",
+                   "max_rng=400", "max_ds=0.25", "write_caustics=true", "write_topo=true"]),
+}
+
+
+def stage(work: str, kind: str, seed: int) -> None:
+    """Input files of a case in `work` under fixed relative names."""
+    if kind == "1d":
+        shutil.copy(os.path.join(HERE, "profiles", f"gen{seed}.met"), os.path.join(work, "atmo.met"))
+        return
+    src = os.path.join(HERE, "rngdep" if kind == "sphr" else "rngdep3d")
+    ax = ("node_lat.dat", "node_lon.dat") if kind == "sphr" else ("node_x.dat", "node_y.dat")
+    os.makedirs(os.path.join(work, "grid"), exist_ok=True)
+    for f in os.listdir(src):
+        if f.startswith("node") and f.endswith(".met"):
+            shutil.copy(os.path.join(src, f), os.path.join(work, "grid", f))
+    shutil.copy(os.path.join(src, ax[0]), os.path.join(work, "grid", "x.dat"))
+    shutil.copy(os.path.join(src, ax[1]), os.path.join(work, "grid", "y.dat"))
+    shutil.copy(os.path.join(src, "topo.dat"), os.path.join(work, "topo.dat"))
+
+
+def inputs(work: str) -> set[str]:
+    out = set()
+    for d, _, files in os.walk(work):
+        for f in files:
+            out.add(os.path.relpath(os.path.join(d, f), work))
+    return out
+
+
+def run_case(binary_dir: str, name: str, spec, keep_dir: str | None = None) -> dict[str, str]:
+    """Runs one case in a scratch directory; returns {relative path: text} of
+    every file the run wrote."""
+    binary, kind, seed, argv = spec
+    with tempfile.TemporaryDirectory() as work:
+        stage(work, kind, seed)
+        before = inputs(work)
+        subprocess.run([os.path.join(binary_dir, binary), *argv], cwd=work, stdin=subprocess.DEVNULL,
+                       stdout=subprocess.DEVNULL, check=True, timeout=600)
+        files = {}
+        for rel in sorted(inputs(work) - before):
+            with open(os.path.join(work, rel)) as f:
+                files[rel] = f.read()
+        return files
+
+
+def main(names: list[str]) -> None:
+    todo = {k: v for k, v in CASES.items() if not names or k in names}
+    meta_path = os.path.join(OUT, "cases.json")
+    meta = json.load(open(meta_path)) if os.path.exists(meta_path) else {}
+    for name, spec in todo.items():
+        files = run_case(REF, name, spec)
+        d = os.path.join(OUT, name)
+        if os.path.isdir(d):
+            shutil.rmtree(d)
+        for rel, text in files.items():
+            path = os.path.join(d, rel)
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            with open(path, "w") as f:
+                f.write(text)
+        meta[name] = {"binary": spec[0], "kind": spec[1], "seed": spec[2], "argv": spec[3], "files": sorted(files)}
+        print(name, sorted(files), sum(len(t) for t in files.values()), "bytes")
+    os.makedirs(OUT, exist_ok=True)
+    with open(meta_path, "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
