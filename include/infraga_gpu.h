@@ -274,10 +274,12 @@ int iga_fan_paths(iga_atmo_t atmo, const iga_fan_params* params,
 
 /* ---- eigenray search ---- */
 
-/* One source-receiver pair of an eigenray search (km; receiver on the ground). */
+/* One source-receiver pair of an eigenray search (receiver on the ground).
+ * 3D: x, y [km]; IGA_GEOM_SPH (params->fan.geometry): latitude, longitude
+ * [deg], as on infraga-sph's command line; altitude [km]. */
 typedef struct iga_eig_pair {
-    double src[3];           /* source x, y, altitude */
-    double rcvr[2];          /* receiver x, y */
+    double src[3];           /* source x|lat, y|lon, altitude */
+    double rcvr[2];          /* receiver x|lat, y|lon */
 } iga_eig_pair;
 
 /* Eigenray search settings: run_eig_search's locals and the geoac::eigenray
@@ -315,7 +317,13 @@ int iga_eig_params_default(iga_atmo_t atmo, iga_eig_params* params);
  * fan.precision = IGA_FP32C traces the rays in FP32-compensated form (the
  * fan kernel's arithmetic) while the bracket and Newton updates stay in FP64;
  * the eigenrays found then agree with the FP64 search to within the search
- * tolerance (0.1 km at the receiver) rather than to rounding. */
+ * tolerance (0.1 km at the receiver) rather than to rounding.
+ * fan.geometry = IGA_GEOM_SPH (fan from iga_fan_params_init(atmo,
+ * IGA_GEOM_SPH, ...)) runs infraga-sph's search instead
+ * (src/geoac/geoac.eigenray.sph.cpp:42-380, main.infraga.sph.cpp:965-990):
+ * great-circle ranges and bearings, the fixed sweep step until 3 azimuth
+ * corrections, Newton iterations through every bounce, rows with latitude /
+ * longitude in columns 3-4 (FP64 only; stratified profiles). */
 int iga_eig_run(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_pair* pairs, int n_pairs,
                 double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps);
 

@@ -278,11 +278,15 @@ def fan_run(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, with_aux: b
     return out
 
 
-def eig_params(atmo: Atmosphere, **overrides) -> EigParams:
+def eig_params(atmo: Atmosphere, geometry: int = GEOM_3D, **overrides) -> EigParams:
     """iga_eig_params with the run_eig_search defaults; keyword overrides go to
-    the eigen fields or, for propagation settings, to params.fan."""
+    the eigen fields or, for propagation settings, to params.fan.  For a
+    spherical search (geometry=GEOM_SPH) params.fan takes infraga-sph's
+    propagation defaults and pairs are given in degrees."""
     p = EigParams()
     _check(lib().iga_eig_params_default(atmo.handle, ctypes.byref(p)), "iga_eig_params_default")
+    if geometry != GEOM_3D:
+        _check(lib().iga_fan_params_init(atmo.handle, int(geometry), ctypes.byref(p.fan)), "iga_fan_params_init")
     eig_fields = {f for f, _ in EigParams._fields_}
     for k, v in overrides.items():
         if k in eig_fields:

@@ -111,8 +111,10 @@ void usage(Variant v) {
     std::cout << '\t' << "-prop        ray fan over inclination/azimuth ranges (incl_min, incl_max, incl_step, az_min, az_max,"
               << '\n' << '\t' << "             az_step, inclination, azimuth, bounces, " << (sph ? "src_lat, src_lon" : "src_x, src_y")
               << ", src_alt, turn_ht_min, write_rays, write_caustics, write_topo)" << '\n';
-    if (v == Variant::k3D) {
-        std::cout << '\t' << "-eig_search  eigenrays from (src_x, src_y, src_alt) to (rcvr_x, rcvr_y) (incl_min, incl_max, bnc_min,"
+    if (!rd) {
+        std::cout << '\t' << "-eig_search  eigenrays from " << (sph ? "(src_lat, src_lon, src_alt) to (rcvr_lat, rcvr_lon)"
+                                                                       : "(src_x, src_y, src_alt) to (rcvr_x, rcvr_y)")
+                  << " (incl_min, incl_max, bnc_min,"
                   << '\n' << '\t' << "             bnc_max, bounces, verbose, iterations, damping, tolerance, az_dev_lim, incl_step_min,"
                   << '\n' << '\t' << "             incl_step_max)" << '\n';
         std::cout << '\t' << "-eig_direct  one eigenray near (incl_est, az_est) with a given bounce count" << '\n';
@@ -602,9 +604,11 @@ int run_prop(int argc, char** argv, Variant v) {
 }
 
 // ------------------------------------------------------------------------
-// -eig_search / -eig_direct (3D stratified)
+// -eig_search / -eig_direct (3D and spherical stratified)
 // ------------------------------------------------------------------------
 
+// src / rcvr in the library's order: 3D (x, y, alt) / (x, y) [km];
+// spherical (lat, lon [deg], alt [km]) / (lat, lon)
 struct EigOpts {
     double src[3] = {0.0, 0.0, 0.0};
     double rcvr[2] = {-250.0, 0.0};
@@ -613,16 +617,19 @@ struct EigOpts {
 };
 
 // Sampled path of one eigenray for {id}.eigenray-N.dat (find_eigenray's
-// final trace, geoac.eigenray.3d.cpp:220-279): rows of the first segment
-// as run_prop writes them, later segments with the raw altitude and the
-// absorption sum itself instead of -2 x it.
+// final trace, geoac.eigenray.3d.cpp:220-279, geoac.eigenray.sph.cpp:230-268):
+// 3D rows of the first segment as run_prop writes them, later segments with
+// the raw altitude and the absorption sum itself instead of -2 x it; the
+// spherical file writes every segment alike, latitude and longitude with
+// 8 significant digits.
 int write_eigenray_file(const std::string& path, iga_atmo_t atmo, const iga_fan_params& base, const double* src,
-                        double theta, double az, int n_b) {
+                        double theta, double az, int n_b, bool sph) {
     iga_fan_params q = base;
     q.bounces = n_b;
     q.calc_amp = 1;
     q.write_rays = 1;
     q.turn_ht_min = -1.0e30;   // the final trace never stops at a low turning height
+    q.time_max = 1.0e30;       // nor at run_prop's travel-time cap
     q.src[0] = src[0]; q.src[1] = src[1]; q.src[2] = src[2];
     long long st = 0;
     int n_out = 0;
@@ -636,12 +643,17 @@ int write_eigenray_file(const std::string& path, iga_atmo_t atmo, const iga_fan_
                        nullptr);
     if (rc) return rc;
     std::ofstream f(path.c_str());
-    f << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]"
-      << '\t' << "time [s]" << '\n';
+    f << (sph ? "# lat [deg]\tlon [deg]\tz [km]" : "# x [km]\ty [km]\tz [km]") << '\t' << "trans. coeff. [dB]" << '\t'
+      << "absorption [dB]" << '\t' << "time [s]" << '\n';
     for (long long j = 0; j < np; j++) {
         const double* r = &rows[(size_t)j * IGA_PATH_COLS];
-        const double absorb = r[6] >= 1.0 ? -r[4] / 2.0 : r[4];
-        f << r[0] << '\t' << r[1] << '\t' << r[2] << '\t' << r[3] << '\t' << absorb << '\t' << r[5] << '\n';
+        if (sph) {
+            f << std::setprecision(8) << r[0] << '\t' << std::setprecision(8) << r[1] << '\t' << r[2] << '\t' << r[3] << '\t'
+              << r[4] << '\t' << r[5] << '\n';
+        } else {
+            const double absorb = r[6] >= 1.0 ? -r[4] / 2.0 : r[4];
+            f << r[0] << '\t' << r[1] << '\t' << r[2] << '\t' << r[3] << '\t' << absorb << '\t' << r[5] << '\n';
+        }
     }
     return IGA_OK;
 }
@@ -671,6 +683,7 @@ void print_eigenray(const double* q, const double* src, bool verbose) {
 // Second pass of the eigenray modes.  direct = run_eig_direct's key set.
 bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep, EigOpts& o, bool has_topo,
                double& incl_est, double& az_est_deg, bool& az_est_given, int& bounces) {
+    const bool sph = is_sph(v);
     PropOpts po;
     double freq = ep.fan.freq;
     const char* val;
@@ -681,14 +694,18 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
         else if (!direct && key2(a, "bnc_min=", "min_bnc=", &val)) ep.bnc_min = atoi(val);
         else if (!direct && key2(a, "bnc_max=", "max_bnc=", &val)) ep.bnc_max = atoi(val);
         else if (!direct && key(a, "bounces=", &val)) ep.bnc_min = ep.bnc_max = atoi(val);
-        else if (direct && key(a, "incl_est=", &val)) incl_est = atof(val);
-        else if (direct && key(a, "az_est=", &val)) { az_est_deg = atof(val); az_est_given = true; }
+        else if (direct && (key(a, "incl_est=", &val) || (sph && key(a, "est_incl=", &val)))) incl_est = atof(val);
+        else if (direct && key2(a, "az_est=", "est_az=", &val)) { az_est_deg = atof(val); az_est_given = true; }
         else if (direct && key(a, "bounces=", &val)) bounces = atoi(val);
-        else if (key2(a, "src_x=", "x_src=", &val)) o.src[0] = atof(val);
-        else if (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val)) o.src[1] = atof(val);
+        else if (!sph && key2(a, "src_x=", "x_src=", &val)) o.src[0] = atof(val);
+        else if (!sph && (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val))) o.src[1] = atof(val);
+        else if (sph && key2(a, "src_lat=", "lat_src=", &val)) o.src[0] = atof(val);
+        else if (sph && key2(a, "src_lon=", "lon_src=", &val)) o.src[1] = atof(val);
         else if (key2(a, "src_alt=", "alt_src=", &val)) o.src[2] = atof(val);
-        else if (key2(a, "rcvr_x=", "x_rcvr=", &val)) o.rcvr[0] = atof(val);
-        else if (key2(a, "rcvr_y=", "y_rcvr=", &val)) o.rcvr[1] = atof(val);
+        else if (!sph && key2(a, "rcvr_x=", "x_rcvr=", &val)) o.rcvr[0] = atof(val);
+        else if (!sph && key2(a, "rcvr_y=", "y_rcvr=", &val)) o.rcvr[1] = atof(val);
+        else if (sph && key2(a, "rcvr_lat=", "lat_rcvr=", &val)) o.rcvr[0] = atof(val);
+        else if (sph && key2(a, "rcvr_lon=", "lon_rcvr=", &val)) o.rcvr[1] = atof(val);
         else if (key(a, "verbose=", &val)) o.verbose = str2bool(val);
         else if (key(a, "iterations=", &val)) ep.iterations = (int)atof(val);
         else if (key(a, "damping=", &val)) ep.damping = atof(val);
@@ -714,12 +731,18 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     const char* topo = nullptr;
     iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo);
     if (!atmo) return 0;
+    const bool sph = is_sph(v);
     iga_eig_params ep;
     int rc = iga_eig_params_default(atmo, &ep);
+    if (!rc && sph) rc = iga_fan_params_init(atmo, IGA_GEOM_SPH, &ep.fan);
     if (rc) return fail("parameters", rc);
     print_region(v, ep.fan);
     EigOpts o;
-    o.verbose = direct;
+    o.verbose = direct && !sph;   // infraga-sph's -eig_direct is quiet by default
+    if (sph) {   // main.infraga.sph.cpp:788-789
+        o.src[0] = 30.0; o.src[1] = 0.0; o.src[2] = 0.0;
+        o.rcvr[0] = 30.0; o.rcvr[1] = -2.5;
+    }
     double incl_est = 10.0, az_est = 0.0;
     bool az_given = false;
     int bounces = 0;
@@ -735,11 +758,25 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     pair.src[0] = o.src[0]; pair.src[1] = o.src[1]; pair.src[2] = o.src[2];
     pair.rcvr[0] = o.rcvr[0]; pair.rcvr[1] = o.rcvr[1];
 
+    // locations as the reference echoes them (spherical: degrees -> radians -> degrees)
+    const double d2r = Pi / 180.0, r2d = 180.0 / Pi;
+    const double es[3] = {sph ? o.src[0] * d2r * r2d : o.src[0], sph ? o.src[1] * d2r * r2d : o.src[1], o.src[2]};
+    const double er[2] = {sph ? o.rcvr[0] * d2r * r2d : o.rcvr[0], sph ? o.rcvr[1] * d2r * r2d : o.rcvr[1]};
+    const char* loc_s = sph ? "source location (lat, lon, alt): " : "source location: ";
+    const char* loc_r = sph ? "receiver location (lat, lon, alt): " : "receiver location: ";
     std::cout << '\n' << "Parameter summary:" << '\n';
-    std::cout << '\t' << "source location: " << o.src[0] << ", " << o.src[1] << ", " << o.src[2] << '\n';
-    std::cout << '\t' << "receiver location: " << o.rcvr[0] << ", " << o.rcvr[1] << ", " << z_rcvr << '\n';
+    std::cout << '\t' << loc_s << es[0] << ", " << es[1] << ", " << es[2] << '\n';
+    std::cout << '\t' << loc_r << er[0] << ", " << er[1] << ", " << z_rcvr << '\n';
     if (direct) {
-        const double phi_est = az_given ? Pi / 2.0 - az_est * (Pi / 180.0) : atan2(o.rcvr[1] - o.src[1], o.rcvr[0] - o.src[0]);
+        double phi_est;
+        if (az_given) {
+            phi_est = Pi / 2.0 - az_est * (Pi / 180.0);
+        } else if (sph) {   // Pi/2 - globe::bearing(src, rcvr)
+            const double la1 = o.src[0] * d2r, lo1 = o.src[1] * d2r, la2 = o.rcvr[0] * d2r, lo2 = o.rcvr[1] * d2r;
+            phi_est = Pi / 2.0 - atan2(sin(lo2 - lo1), cos(la1) * tan(la2) - sin(la1) * cos(lo2 - lo1));
+        } else {
+            phi_est = atan2(o.rcvr[1] - o.src[1], o.rcvr[0] - o.src[0]);
+        }
         az_est = 90.0 - phi_est * 180.0 / Pi;
         std::cout << '\t' << "inclination estimate: " << incl_est << '\n';
         std::cout << '\t' << "azimuth estimate: " << az_est << '\n';
@@ -763,21 +800,29 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
         std::ofstream res((id + ".arrivals.dat").c_str());
         res << "# " << variant_name(v) << " -eig_search summary:" << '\n';
         res << "# " << '\t' << "profile: " << argv[2] << '\n';
-        res << "# " << '\t' << "source location: " << o.src[0] << ", " << o.src[1] << ", " << o.src[2] << '\n';
-        res << "# " << '\t' << "receiver location: " << o.rcvr[0] << ", " << o.rcvr[1] << ", " << z_rcvr << '\n';
+        res << "# " << '\t' << loc_s << es[0] << ", " << es[1] << ", " << es[2] << '\n';
+        res << "# " << '\t' << loc_r << er[0] << ", " << er[1] << ", " << z_rcvr << '\n';
         res << "# " << '\t' << "inclination range: " << ep.incl_min * (Pi / 180.0) * (180.0 / Pi) << ", "
             << ep.incl_max * (Pi / 180.0) * (180.0 / Pi) << '\n';
         res << "# " << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
         res << "#" << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
         res << "# " << '\t' << "damping: " << ep.damping << '\n';
         res << "# " << '\t' << "frequency: " << ep.fan.freq << '\n';
-        res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << '\n';
-        res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << "x_0 [km]" << '\t' << "y_0 [km]" << '\t'
-            << "time [s]" << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << "arrival incl [deg]" << '\t'
-            << "back az [deg]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
-        for (int nbc = ep.bnc_min; nbc <= ep.bnc_max; nbc++)
-            std::cout << "Searching for " << nbc << " bounce eigenray(s) with inclination between " << ep.incl_min
-                      << " and " << ep.incl_max << "." << '\n';
+        // infraga-sph writes no blank line after the summary (main.infraga.sph.cpp:944)
+        res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << (sph ? "" : "\n");
+        if (sph)
+            res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << "lat_0 [deg]" << '\t' << "lon_0 [deg]"
+                << '\t' << "time [s]" << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << "inclination [deg]"
+                << '\t' << "back azimuth [deg]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
+        else
+            res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << "x_0 [km]" << '\t' << "y_0 [km]" << '\t'
+                << "time [s]" << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << "arrival incl [deg]" << '\t'
+                << "back az [deg]" << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
+        for (int nbc = ep.bnc_min; nbc <= ep.bnc_max; nbc++) {
+            if (sph) std::cout << "Searching for " << nbc << " bounce eigenrays." << '\n';
+            else std::cout << "Searching for " << nbc << " bounce eigenray(s) with inclination between " << ep.incl_min
+                           << " and " << ep.incl_max << "." << '\n';
+        }
         const int cap0 = 256;
         rows.resize((size_t)cap0 * IGA_ARRIVAL_COLS);
         long long steps = 0;
@@ -797,7 +842,8 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     for (int j = 0; j < n_out; j++) {
         const double* q = &rows[(size_t)j * IGA_ARRIVAL_COLS];
         print_eigenray(q, o.src, o.verbose);
-        rc = write_eigenray_file(id + ".eigenray-" + std::to_string(j) + ".dat", atmo, ep.fan, o.src, q[0], q[1], (int)q[2]);
+        rc = write_eigenray_file(id + ".eigenray-" + std::to_string(j) + ".dat", atmo, ep.fan, o.src, q[0], q[1], (int)q[2],
+                                 sph);
         if (rc) return fail("eigenray path", rc);
     }
     if (!direct) std::cout << '\t' << "Identified " << n_out << " eigenray(s)." << '\n';
@@ -820,11 +866,11 @@ int run(int argc, char** argv, Variant v) {
     else if (strncmp(o, "-back_proj", 10) == 0 || strncmp(o, "-b", 2) == 0)
         std::cout << "-back_proj is not provided by the GPU front end." << '\n';
     else if (strncmp(o, "-eig_search", 11) == 0 || strncmp(o, "-s", 2) == 0) {
-        if (v == Variant::k3D) return run_eig(argc, argv, v, false);
-        std::cout << "-eig_search is provided for infraga-3d only by the GPU front end." << '\n';
+        if (!is_rngdep(v)) return run_eig(argc, argv, v, false);
+        std::cout << "-eig_search is provided for infraga-3d and infraga-sph only by the GPU front end." << '\n';
     } else if (strncmp(o, "-eig_direct", 11) == 0 || strncmp(o, "-d", 2) == 0) {
-        if (v == Variant::k3D) return run_eig(argc, argv, v, true);
-        std::cout << "-eig_direct is provided for infraga-3d only by the GPU front end." << '\n';
+        if (!is_rngdep(v)) return run_eig(argc, argv, v, true);
+        std::cout << "-eig_direct is provided for infraga-3d and infraga-sph only by the GPU front end." << '\n';
     } else if (strncmp(o, "-wnl_wvfrm", 10) == 0 || strncmp(o, "-w", 2) == 0)
         std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
     else

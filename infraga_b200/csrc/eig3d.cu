@@ -1,11 +1,12 @@
-// Eigenray search for the 3D stratified solver on flat ground.
+// Eigenray search for the 3D and spherical stratified solvers on flat ground.
 //
 // Every (source-receiver pair, bounce count) search is an independent chain
 // of ray traces whose control flow depends on each trace's result; the host
 // runs all chains as state machines that replay the reference's
-// est_eigenray / find_eigenray logic exactly (geoac.eigenray.3d.cpp:34-371),
-// and every round collects the traces all chains need next into one launch
-// of trace3d_fp64_kernel.  While a chain sweeps inclinations with a fixed
+// est_eigenray / find_eigenray logic exactly (geoac.eigenray.3d.cpp:34-371,
+// geoac.eigenray.sph.cpp:42-380), and every round collects the traces all
+// chains need next into one launch of trace3d_fp64_kernel (or the spherical
+// tracesph_fp64_kernel, eigsph.cu).  While a chain sweeps inclinations with a fixed
 // step, the angles it will try next are known in advance, so it submits a
 // chunk of them at once and keeps the results up to the first bracket.
 #include <algorithm>
@@ -171,7 +172,9 @@ constexpr double kRad = kPi / 180.0;
 
 struct Chain {
     int pair = 0, nb = 0;
+    // 3D: source / receiver x, y [km]; spherical: latitude, longitude [rad]
     double sx = 0, sy = 0, rx = 0, ry = 0, rcvr_rng = 0, rcvr_az = 0;
+    double phi0 = 0;             // first launch azimuth of a sweep (geoac::phi convention)
     enum Phase { kEst, kNewton, kRecordTrace, kDone } phase = kEst;
     bool direct = false;         // find_eigenray alone (run_eig_direct): no sweep before or after
     double theta_start = 0;
@@ -193,7 +196,27 @@ struct Chain {
 struct Settings {
     double theta_max, dth_big, dth_sml, damping, tolerance, az_err_lim, rng_max;
     int iterations, chunk;
+    // spherical search (geoac.eigenray.sph.cpp): great-circle ranges and
+    // bearings, strict upper inclination bound, mod_dth after 3 corrections,
+    // Newton traces through every bounce; flat-ground radius and the sound
+    // speeds of its Newton derivatives
+    bool sph = false;
+    double r_grnd = 0, c_src = 0, c_grnd = 0;
+    int fixed_step_iters() const { return sph ? 3 : 2; }
+    bool in_sweep(double th, double th_max) const { return sph ? th < th_max : th <= th_max; }
 };
+
+// globe::gc_dist and globe::bearing (util/globe.cpp:16-28), host side
+double gc_dist_h(double lat1, double lon1, double lat2, double lon2) {
+    const double t1 = pow(sin((lat2 - lat1) / 2.0), 2);
+    const double t2 = cos(lat1) * cos(lat2) * pow(sin((lon2 - lon1) / 2.0), 2);
+    return 2.0 * kEarthRadiusKm * asin(sqrt(t1 + t2));
+}
+double bearing_h(double lat1, double lon1, double lat2, double lon2) {
+    const double t1 = sin(lon2 - lon1);
+    const double t2 = cos(lat1) * tan(lat2) - sin(lat1) * cos(lon2 - lon1);
+    return atan2(t1, t2);
+}
 
 double mod_dth(const Settings& S, double dr, double dr_dtheta) {   // geoac::mod_dth (geoac.eigenray.3d.cpp:32)
     return S.dth_big - (S.dth_big - S.dth_sml) * exp(-1.0 / 2.0 * pow(dr / dr_dtheta, 2));
@@ -207,7 +230,7 @@ void est_begin(Chain& c, const Settings& S, double theta_start) {
     c.iterations = 0;
     c.dth = S.dth_big;
     c.dph = 100.0;
-    c.phi = c.rcvr_az;
+    c.phi = c.phi0;
     c.th_max_reached = false;
     c.r = c.rcvr_rng;
     c.r_prev = c.rcvr_rng;
@@ -240,13 +263,18 @@ void newton_begin(Chain& c, double th_est, double ph_est) {
 bool est_step(Chain& c, const Settings& S, const TraceRes& res) {
     if (c.th + c.dth >= c.th_max) c.th_max_reached = true;
     const double theta = c.th;
-    c.r = sqrt(pow(res.y[0] - c.sx, 2) + pow(res.y[1] - c.sy, 2));
+    c.r = S.sph ? gc_dist_h(c.sx, c.sy, res.y[0], res.y[1]) : sqrt(pow(res.y[0] - c.sx, 2) + pow(res.y[1] - c.sy, 2));
     if (res.escaped) c.r = S.rng_max;
     if (((c.r - c.rcvr_rng) * (c.r_prev - c.rcvr_rng) <= 0.0) && (c.r < S.rng_max) && (c.r_prev < S.rng_max) &&
         (c.th > c.th_min)) {
         if (c.iterations == 0) c.th_next = c.th;
-        c.dph = atan2(res.y[1] - c.sy, res.y[0] - c.sx) * (180.0 / kPi);
-        c.dph -= atan2(c.ry - c.sy, c.rx - c.sx) * (180.0 / kPi);
+        if (S.sph) {
+            c.dph = bearing_h(c.sx, c.sy, c.rx, c.ry) * (180.0 / kPi);
+            c.dph -= bearing_h(c.sx, c.sy, res.y[0], res.y[1]) * (180.0 / kPi);
+        } else {
+            c.dph = atan2(res.y[1] - c.sy, res.y[0] - c.sx) * (180.0 / kPi);
+            c.dph -= atan2(c.ry - c.sy, c.rx - c.sx) * (180.0 / kPi);
+        }
         while (c.dph > 180.0) c.dph -= 360.0;
         while (c.dph < -180.0) c.dph += 360.0;
         if (fabs(c.dph) < S.az_err_lim) {
@@ -262,10 +290,10 @@ bool est_step(Chain& c, const Settings& S, const TraceRes& res) {
         c.r = c.rcvr_rng; c.r_prev = c.rcvr_rng; c.th = c.th_min;
         return true;
     }
-    if (c.iterations >= 2) c.dth = mod_dth(S, c.r - c.rcvr_rng, (c.r - c.r_prev) / (2.0 * c.dth));
+    if (c.iterations >= S.fixed_step_iters()) c.dth = mod_dth(S, c.r - c.rcvr_rng, (c.r - c.r_prev) / (2.0 * c.dth));
     c.r_prev = c.r;
     c.th += c.dth;
-    if (!(c.th <= c.th_max)) {   // loop ran out (th_max_reached is set on its last pass)
+    if (!S.in_sweep(c.th, c.th_max)) {   // loop ran out (th_max_reached is set on its last pass)
         if (c.th_max_reached) { c.th_next = c.th_max; search_continue(c, S); return true; }
         if (!(fabs(c.dph * (180.0 / kPi)) > S.az_err_lim && c.iterations < 5)) { search_continue(c, S); return true; }
         c.r = c.rcvr_rng; c.r_prev = c.rcvr_rng; c.th = c.th_min;
@@ -311,6 +339,46 @@ void newton_step(Chain& c, const Settings& S, const Fan3DArgs& a, const TraceRes
     c.n++;
 }
 
+// One iteration of the spherical find_eigenray Newton loop
+// (geoac.eigenray.sph.cpp:176-371) on flat ground, where the terrain slope
+// terms vanish.  The reference's long double block is done in double.
+void newton_step_sph(Chain& c, const Settings& S, const TraceResSph& res) {
+    if (res.escaped) {
+        c.theta -= c.ndth * c.step_sc;
+        c.phi_n -= c.ndph * c.step_sc;
+        c.step_sc /= 2.0;
+    } else {
+        const double* s = res.y;
+        const double dr = gc_dist_h(s[1], s[2], c.rx, c.ry);
+        if (dr < S.tolerance) {
+            c.phase = Chain::kRecordTrace;
+            return;
+        } else if (c.n > 0 && dr > c.dr_prev) {
+            c.theta -= c.ndth * c.step_sc;
+            c.phi_n -= c.ndph * c.step_sc;
+            c.step_sc /= 2.0;
+        } else {
+            c.step_sc = std::min(1.0, c.step_sc * 1.25);
+            const double dlat = c.rx - s[1], dlon = c.ry - s[2];
+            const double r_grnd = S.r_grnd, c_grnd = S.c_grnd, c_src = S.c_src;
+            const double rc = r_grnd * cos(s[1]);
+            const double ds_dth = -c_src / c_grnd * s[6] / s[3];
+            const double ds_dph = -c_src / c_grnd * s[12] / s[3];
+            const double dlat_dth = s[7] + s[4] / r_grnd * ds_dth, dlon_dth = s[8] + s[5] / rc * ds_dth;
+            const double dlat_dph = s[13] + s[4] / r_grnd * ds_dph, dlon_dph = s[14] + s[5] / rc * ds_dph;
+            // (1 + damping)^2 multiplies the first product only, as written in the reference
+            const double det = pow(1.0 + S.damping, 2) * dlat_dth * dlon_dph - dlat_dph * dlon_dth;
+            c.ndth = ((1.0 + S.damping) * dlon_dph * dlat - dlat_dph * dlon) / det;
+            c.ndph = ((1.0 + S.damping) * dlat_dth * dlon - dlon_dth * dlat) / det;
+            c.theta += c.ndth * c.step_sc;
+            c.phi_n += c.ndph * c.step_sc;
+            c.dr_prev = dr;
+        }
+    }
+    if (sqrt(c.ndth * c.ndth + c.ndph * c.ndph) * c.step_sc < 1.0e-12) { search_continue(c, S); return; }
+    c.n++;
+}
+
 }  // namespace
 }  // namespace iga
 
@@ -342,7 +410,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     out_rows.clear(); out_pair.clear(); steps_out = 0;
     if (!h || !P || n_pairs < 0 || (n_pairs > 0 && !pairs)) return IGA_E_INVALID;
     iga_fan_params fp = P->fan;
-    fp.geometry = IGA_GEOM_3D;
+    const bool sph = fp.geometry == IGA_GEOM_SPH;
     fp.bounces = 0;
     fp.calc_amp = 1;
     fp.write_rays = 1;
@@ -350,6 +418,10 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     if (rc) return rc;
     if (h->kind != 0) {
         g_cuda_err = "eigenray search: stratified atmospheres only";
+        return IGA_E_UNSUPPORTED;
+    }
+    if (sph && fp.precision != IGA_FP64) {
+        g_cuda_err = "spherical eigenray search: FP64 only";
         return IGA_E_UNSUPPORTED;
     }
     if (P->bnc_min < 0 || P->bnc_max < P->bnc_min || P->iterations < 0 || !(P->tolerance > 0.0) ||
@@ -362,10 +434,18 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             return IGA_E_UNSUPPORTED;
         }
     IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
-    fp.src[0] = 0.0; fp.src[1] = 0.0; fp.src[2] = pairs[0].src[2];
+    // the launch arguments carry the source altitude; each trace request
+    // carries its own source x, y (latitude, longitude)
+    fp.src[0] = sph ? pairs[0].src[0] : 0.0; fp.src[1] = sph ? pairs[0].src[1] : 0.0; fp.src[2] = pairs[0].src[2];
     Fan3DArgs a;
     rc = build_args(h, &fp, a);
     if (rc) return rc;
+    double c_incl_src = 0.0;   // spherical find_eigenray: c at radius = source altitude, i.e. the lowest knot
+    if (sph) {
+        double f, d1, d2;
+        iga::spline_eval(h->prof.z, h->prof.c, h->prof.cs, h->prof.z.front(), f, d1, d2);
+        c_incl_src = f;
+    }
     const bool f32 = fp.precision == IGA_FP32C;
     if (f32 && (rc = fp32c_setup(h, fp.freq, a))) return rc;
 
@@ -375,7 +455,13 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     S.dth_sml = P->incl_step_min * (kPi / 180.0);
     S.damping = P->damping; S.tolerance = P->tolerance; S.az_err_lim = P->az_err_lim;
     S.rng_max = fp.rng_max; S.iterations = P->iterations; S.chunk = P->chunk;
-    const double theta_min = P->incl_min * (kPi / 180.0);
+    S.sph = sph;
+    S.r_grnd = a.r_grnd; S.c_src = a.c0; S.c_grnd = a.c_gnd;
+    double theta_min = P->incl_min * (kPi / 180.0);
+    if (sph) {   // run_eig_search's theta_grnd for flat ground (main.infraga.sph.cpp:965-981)
+        const double theta_grnd = pairs[0].src[2] - fp.z_grnd < 0.01 ? 0.1 * (kPi / 180.0) : -89.9 * (kPi / 180.0);
+        theta_min = std::max(theta_min, theta_grnd);
+    }
 
     std::vector<Chain> chains;
     for (int ip = 0; ip < n_pairs; ip++) {
@@ -384,8 +470,17 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             c.pair = ip; c.nb = nb;
             c.sx = pairs[ip].src[0]; c.sy = pairs[ip].src[1];
             c.rx = pairs[ip].rcvr[0]; c.ry = pairs[ip].rcvr[1];
-            c.rcvr_rng = sqrt(pow(c.rx - c.sx, 2) + pow(c.ry - c.sy, 2));
-            c.rcvr_az = atan2(c.ry - c.sy, c.rx - c.sx);
+            if (sph) {   // run_eig_search converts degrees (main.infraga.sph.cpp:889-890)
+                c.sx *= (kPi / 180.0); c.sy *= (kPi / 180.0);
+                c.rx *= (kPi / 180.0); c.ry *= (kPi / 180.0);
+                c.rcvr_rng = gc_dist_h(c.sx, c.sy, c.rx, c.ry);
+                c.rcvr_az = bearing_h(c.sx, c.sy, c.rx, c.ry);
+                c.phi0 = kPi / 2.0 - c.rcvr_az;
+            } else {
+                c.rcvr_rng = sqrt(pow(c.rx - c.sx, 2) + pow(c.ry - c.sy, 2));
+                c.rcvr_az = atan2(c.ry - c.sy, c.rx - c.sx);
+                c.phi0 = c.rcvr_az;
+            }
             if (direct) {
                 c.direct = true;
                 newton_begin(c, direct[ip].theta, direct[ip].phi);
@@ -399,7 +494,8 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     }
 
     TraceReq* d_req = nullptr;
-    TraceRes* d_res = nullptr;
+    unsigned char* d_res = nullptr;   // TraceRes or TraceResSph records
+    const size_t res_bytes = sph ? sizeof(TraceResSph) : sizeof(TraceRes);
     SegRes* d_seg = nullptr;
     size_t cap_req = 0;
     long long steps_tot = 0;
@@ -414,6 +510,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
 
     std::vector<TraceReq> req6, req18;
     std::vector<TraceRes> res18;
+    std::vector<TraceResSph> res18s;
     std::vector<SegRes> seg6;
     // searches of one pair for different bounce counts sweep the same launch
     // angles until their first bracket: one trace serves them all
@@ -427,7 +524,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     while (true) {
         req6.clear(); req18.clear(); uniq.clear();
         int sweeping = 0;
-        for (auto& c : chains) if (c.phase == Chain::kEst && c.iterations < 2) sweeping++;
+        for (auto& c : chains) if (c.phase == Chain::kEst && c.iterations < S.fixed_step_iters()) sweeping++;
         int chunk = S.chunk > 0 ? S.chunk : std::max(8, std::min(128, sweeping > 0 ? 262144 / sweeping : 128));
         for (auto& c : chains) {
             // find_eigenray gives up after `iterations` Newton steps
@@ -436,9 +533,9 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             c.sweep_req.clear();
             if (c.phase == Chain::kEst) {
                 // with a fixed step the next inclinations are known: submit a chunk
-                const int m = c.iterations < 2 ? chunk : 1;
+                const int m = c.iterations < S.fixed_step_iters() ? chunk : 1;
                 double th = c.th;
-                for (int j = 0; j < m && th <= c.th_max; j++) {
+                for (int j = 0; j < m && S.in_sweep(th, c.th_max); j++) {
                     c.sweep.push_back(th);
                     const std::array<double, 4> key{c.sx, c.sy, th, c.phi};
                     auto it = uniq.find(key);
@@ -454,7 +551,9 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
                 }
             } else if (c.phase == Chain::kNewton) {
                 c.req0 = (int)req18.size();
-                req18.push_back({c.sx, c.sy, c.theta, c.phi_n, 1 + std::min(c.nb, 1), kStopOnEscape});
+                // the 3D find_eigenray follows one reflection at most while iterating
+                // (geoac.eigenray.3d.cpp:206); the spherical one all of them
+                req18.push_back({c.sx, c.sy, c.theta, c.phi_n, sph ? c.nb + 1 : 1 + std::min(c.nb, 1), kStopOnEscape});
             } else if (c.phase == Chain::kRecordTrace) {
                 c.req0 = (int)req18.size();
                 req18.push_back({c.sx, c.sy, c.theta, c.phi_n, c.nb + 1, kRecord});
@@ -467,31 +566,39 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             release();
             cap_req = std::max(need, cap_req * 2);
             cudaError_t e1 = cudaMallocAsync(&d_req, 2 * cap_req * sizeof(TraceReq), st);
-            cudaError_t e2 = e1 == cudaSuccess ? cudaMallocAsync(&d_res, 2 * cap_req * sizeof(TraceRes), st) : e1;
+            cudaError_t e2 = e1 == cudaSuccess ? cudaMallocAsync(&d_res, 2 * cap_req * res_bytes, st) : e1;
             cudaError_t e3 = e2 == cudaSuccess ? cudaMallocAsync(&d_seg, cap_req * max_seg * sizeof(SegRes), st) : e2;
             if (e3 != cudaSuccess) return fail(cuda_fail(e3, "cudaMallocAsync(eigen traces)"));
         }
         TraceReq* d_req18 = d_req + cap_req;
-        TraceRes* d_res18 = d_res + cap_req;
+        unsigned char* d_res18 = d_res + cap_req * res_bytes;
         cudaError_t e = cudaSuccess;
         if (!req6.empty()) {
             e = cudaMemcpyAsync(d_req, req6.data(), req6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
-                e = f32 ? launch_trace_fp32c(a, d_req, d_res, (int)req6.size(), false, st, d_seg, max_seg)
-                        : launch_trace<false>(a, d_req, d_res, (int)req6.size(), st, d_seg, max_seg);
+                e = sph ? launch_trace_sph(a, d_req, reinterpret_cast<TraceResSph*>(d_res), (int)req6.size(), false, st,
+                                           d_seg, max_seg, c_incl_src)
+                    : f32 ? launch_trace_fp32c(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), false, st,
+                                               d_seg, max_seg)
+                          : launch_trace<false>(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), st, d_seg,
+                                                max_seg);
         }
         if (e == cudaSuccess && !req18.empty()) {
             e = cudaMemcpyAsync(d_req18, req18.data(), req18.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
-                e = f32 ? launch_trace_fp32c(a, d_req18, d_res18, (int)req18.size(), true, st)
-                        : launch_trace<true>(a, d_req18, d_res18, (int)req18.size(), st);
+                e = sph ? launch_trace_sph(a, d_req18, reinterpret_cast<TraceResSph*>(d_res18), (int)req18.size(), true,
+                                           st, nullptr, 0, c_incl_src)
+                    : f32 ? launch_trace_fp32c(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), true, st)
+                          : launch_trace<true>(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), st);
         }
         seg6.resize(req6.size() * max_seg);
-        res18.resize(req18.size());
+        res18.resize(sph ? 0 : req18.size());
+        res18s.resize(sph ? req18.size() : 0);
         if (e == cudaSuccess && !req6.empty())
             e = cudaMemcpyAsync(seg6.data(), d_seg, seg6.size() * sizeof(SegRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && !req18.empty())
-            e = cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
+            e = sph ? cudaMemcpyAsync(res18s.data(), d_res18, res18s.size() * sizeof(TraceResSph), cudaMemcpyDeviceToHost, st)
+                    : cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
         // each search's view of its sweep traces: the entry of its own
@@ -513,10 +620,12 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             }
         }
         for (auto& r : res18) { steps_tot += r.steps; st18 += r.steps; }
-        n_rounds++; n6 += (long long)req6.size(); n18 += (long long)res18.size();
+        for (auto& r : res18s) { steps_tot += r.steps; st18 += r.steps; }
+        n_rounds++; n6 += (long long)req6.size(); n18 += (long long)req18.size();
         if (per_round) {
             long long m18 = 0;
             for (auto& r : res18) m18 = std::max(m18, r.steps);
+            for (auto& r : res18s) m18 = std::max(m18, r.steps);
             int n_est = 0, n_newt = 0, n_rec = 0;
             for (auto& c : chains) {
                 n_est += c.phase == Chain::kEst;
@@ -525,7 +634,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             }
             fprintf(stderr, "round %lld: sweep %zu (max %lld steps) newton/record %zu (max %lld) chains est %d newton %d "
                             "record %d chunk %d %.4f s\n",
-                    n_rounds, req6.size(), m6, res18.size(), m18, n_est, n_newt, n_rec, chunk,
+                    n_rounds, req6.size(), m6, req18.size(), m18, n_est, n_newt, n_rec, chunk,
                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count());
         }
 
@@ -537,7 +646,26 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
                     if (est_step(c, S, t)) break;
                 }
             } else if (c.phase == Chain::kNewton) {
-                newton_step(c, S, a, res18[c.req0]);
+                if (sph) newton_step_sph(c, S, res18s[c.req0]);
+                else newton_step(c, S, a, res18[c.req0]);
+            } else if (c.phase == Chain::kRecordTrace && sph) {
+                // eig_results row of geoac.eigenray.sph.cpp:303-315
+                const TraceResSph& t = res18s[c.req0];
+                std::vector<double> row(IGA_ARRIVAL_COLS);
+                row[0] = c.theta * (180.0 / kPi);
+                row[1] = 90.0 - c.phi_n * (180.0 / kPi);
+                row[2] = c.nb;
+                row[3] = t.y[1] * 180.0 / kPi;
+                row[4] = t.y[2] * 180.0 / kPi;
+                row[5] = t.tt;
+                row[6] = gc_dist_h(t.y[1], t.y[2], c.sx, c.sy) / t.tt;
+                row[7] = t.rmax;
+                row[8] = t.incl;
+                row[9] = t.baz;
+                row[10] = t.amp_db;
+                row[11] = -2.0 * t.att;
+                c.rows.push_back(std::move(row));
+                search_continue(c, S);
             } else if (c.phase == Chain::kRecordTrace) {
                 const TraceRes& t = res18[c.req0];
                 std::vector<double> row(IGA_ARRIVAL_COLS);

@@ -35,6 +35,23 @@ struct SegRes {
     int pad;
 };
 
+// Result of a spherical trace (eigsph.cu): the last row in the 18-state
+// spherical layout (r, lat, lon, nu, X_th, mu_th, X_ph, mu_ph), and in record
+// mode the arrival columns find_eigenray forms on the device.
+struct TraceResSph {
+    double y[18];
+    double tt, att, rmax, amp_db, incl, baz;
+    long long steps;
+    int escaped;
+    int pad;
+};
+
+// Spherical stratified traces; source latitude/longitude per request (x0, y0,
+// radians), altitude from the launch arguments.  c_incl_src is the sound
+// speed find_eigenray divides by in its arrival inclination.
+cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceResSph* d_res, int n, bool amp,
+                             cudaStream_t st, SegRes* seg_out, int seg_stride, double c_incl_src);
+
 // FP32-compensated traces (same contract as the FP64 trace kernel).  With
 // seg_out != null, segment j of request r also writes seg_out[r * seg_stride + j].
 cudaError_t launch_trace_fp32c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, bool amp,

@@ -45,6 +45,12 @@ CASES = {
                  ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=180",
                   "az_step=180", "bounces=1", "src_lat=20", "src_lon=-40", "max_rng=700", "max_ds=0.25", "write_caustics=true",
                   "write_topo=true"]),
+    "sph_eig": ("infraga-sph", "1d", 0,
+                ["-eig_search", "atmo.met", "src_lat=30", "src_lon=0", "rcvr_lat=30.5", "rcvr_lon=2.5", "bnc_min=0",
+                 "bnc_max=0", "incl_min=10", "incl_max=15"]),
+    "sph_direct": ("infraga-sph", "1d", 0,
+                   ["-eig_direct", "atmo.met", "src_lat=30", "src_lon=0", "rcvr_lat=30.5", "rcvr_lon=2.5",
+                    "incl_est=12", "bounces=0", "output_id=direct"]),
     "3dr_prop": ("infraga-3d-rngdep", "3dr", 0,
                  ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "incl_min=6",
                   "incl_max=26", "incl_step=10", "az_min=90", "az_max=270", "az_step=180", "bounces=1",

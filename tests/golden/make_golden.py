@@ -126,6 +126,16 @@ EIG_CASES = {
     "3d_eig_none": (2, ["rcvr_x=180", "rcvr_y=-30", "bnc_min=0", "bnc_max=1"]),
 }
 
+# Spherical eigenray searches through oracle/harness/harness_sph.cpp (degrees
+# as on the infraga-sph command line).  name -> (profile seed, argv)
+SPH_EIG_CASES = {
+    "sph_eig_a": (0, ["src_lat=30", "src_lon=0", "rcvr_lat=30.5", "rcvr_lon=2.5", "bnc_min=0", "bnc_max=1"]),
+    "sph_eig_b": (4, ["src_lat=10", "src_lon=100", "rcvr_lat=12", "rcvr_lon=103", "bnc_min=0", "bnc_max=2"]),
+    "sph_eig_c": (0, ["src_lat=30", "src_lon=0", "rcvr_lat=31", "rcvr_lon=5", "bnc_min=1", "bnc_max=1",
+                      "incl_min=5", "incl_max=30"]),
+    "sph_eig_none": (2, ["src_lat=60", "src_lon=170", "rcvr_lat=60", "rcvr_lon=175", "bnc_min=0", "bnc_max=0"]),
+}
+
 
 def profile_path(seed: int) -> str:
     return os.path.join(PROFILES, f"gen{seed}.met")
@@ -201,6 +211,17 @@ def main():
         with open(out, "a") as f:
             f.write(r.stdout)
         meta[name] = {"binary": "iga_ref_3d", "mode": "eig", "seed": seed, "args": args}
+        print(name, r.stdout.strip().splitlines()[-1])
+    for name, (seed, args) in SPH_EIG_CASES.items():
+        if not want(name):
+            continue
+        out = os.path.join(HERE, name + ".txt")
+        cmd = [os.path.join(REF, "iga_ref_sph"), "eig", profile_path(seed), *args, "out=" + out,
+               "out_id=" + os.path.join("/tmp", name)]
+        r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+        with open(out, "a") as f:
+            f.write(r.stdout)
+        meta[name] = {"binary": "iga_ref_sph", "mode": "eig", "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
     with open(meta_path, "w") as f:
         json.dump(meta, f, indent=1)

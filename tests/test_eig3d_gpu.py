@@ -9,7 +9,7 @@ from tests._cases import load_cases, parse_golden, profile_path
 
 pytestmark = pytest.mark.gpu
 
-CASES = {k: v for k, v in load_cases().items() if v["mode"] == "eig"}
+CASES = {k: v for k, v in load_cases().items() if v["mode"] == "eig" and v["binary"] == "iga_ref_3d"}
 
 # The search stops once the ray lands within tolerance (0.1 km) of the
 # receiver, so rounding differences can end it one Newton step apart; the
