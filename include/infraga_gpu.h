@@ -299,7 +299,8 @@ typedef struct iga_eig_params {
     int chunk;                   /* sweep inclinations traced per search per GPU round (0 = automatic) */
 } iga_eig_params;
 
-/* Defaults of run_eig_search after set_region (as iga_fan_params_default for fan). */
+/* Defaults of run_eig_search after set_region (fan as iga_fan_params_default;
+ * on a range-dependent handle as iga_fan_params_init for its geometry). */
 int iga_eig_params_default(iga_atmo_t atmo, iga_eig_params* params);
 
 /* Replaces run_eig_search's search loop (src/main.infraga.3d.cpp:939-950):

@@ -111,14 +111,12 @@ void usage(Variant v) {
     std::cout << '\t' << "-prop        ray fan over inclination/azimuth ranges (incl_min, incl_max, incl_step, az_min, az_max,"
               << '\n' << '\t' << "             az_step, inclination, azimuth, bounces, " << (sph ? "src_lat, src_lon" : "src_x, src_y")
               << ", src_alt, turn_ht_min, write_rays, write_caustics, write_topo)" << '\n';
-    if (!rd) {
-        std::cout << '\t' << "-eig_search  eigenrays from " << (sph ? "(src_lat, src_lon, src_alt) to (rcvr_lat, rcvr_lon)"
-                                                                       : "(src_x, src_y, src_alt) to (rcvr_x, rcvr_y)")
-                  << " (incl_min, incl_max, bnc_min,"
-                  << '\n' << '\t' << "             bnc_max, bounces, verbose, iterations, damping, tolerance, az_dev_lim, incl_step_min,"
-                  << '\n' << '\t' << "             incl_step_max)" << '\n';
-        std::cout << '\t' << "-eig_direct  one eigenray near (incl_est, az_est) with a given bounce count" << '\n';
-    }
+    std::cout << '\t' << "-eig_search  eigenrays from " << (sph ? "(src_lat, src_lon, src_alt) to (rcvr_lat, rcvr_lon)"
+                                                                   : "(src_x, src_y, src_alt) to (rcvr_x, rcvr_y)")
+              << " (incl_min, incl_max, bnc_min,"
+              << '\n' << '\t' << "             bnc_max, bounces, verbose, iterations, damping, tolerance, az_dev_lim, incl_step_min,"
+              << '\n' << '\t' << "             incl_step_max)" << '\n';
+    std::cout << '\t' << "-eig_direct  one eigenray near (incl_est, az_est) with a given bounce count" << '\n';
     std::cout << '\t' << "Common: freq, abs_coeff, z_grnd, prof_format, reverse_winds, output_id, calc_amp, max_alt, max_rng,"
               << '\n' << '\t' << "        " << (sph ? "min_lat, max_lat, min_lon, max_lon, max_time" : "min_x, max_x, min_y, max_y")
               << ", min_ds, max_ds, max_s" << (rd ? ", topo_file" : "") << '\n';
@@ -687,7 +685,7 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
     PropOpts po;
     double freq = ep.fan.freq;
     const char* val;
-    for (int i = 3; i < argc; i++) {
+    for (int i = is_rngdep(v) ? 5 : 3; i < argc; i++) {
         const char* a = argv[i];
         if (!direct && key2(a, "incl_min=", "min_incl=", &val)) ep.incl_min = atof(val);
         else if (!direct && key2(a, "incl_max=", "max_incl=", &val)) ep.incl_max = atof(val);
@@ -731,24 +729,45 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     const char* topo = nullptr;
     iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo);
     if (!atmo) return 0;
-    const bool sph = is_sph(v);
+    const bool sph = is_sph(v), rd = is_rngdep(v), has_topo = topo != nullptr;
     iga_eig_params ep;
     int rc = iga_eig_params_default(atmo, &ep);
-    if (!rc && sph) rc = iga_fan_params_init(atmo, IGA_GEOM_SPH, &ep.fan);
+    if (!rc && (sph || rd)) rc = iga_fan_params_init(atmo, sph ? IGA_GEOM_SPH : IGA_GEOM_3D, &ep.fan);
     if (rc) return fail("parameters", rc);
     print_region(v, ep.fan);
     EigOpts o;
-    o.verbose = direct && !sph;   // infraga-sph's -eig_direct is quiet by default
-    if (sph) {   // main.infraga.sph.cpp:788-789
+    o.verbose = direct && !sph;   // the spherical -eig_direct is quiet by default
+    double incl_est = 10.0, az_est = 0.0;
+    // source and receiver defaults of run_eig_search / run_eig_direct
+    if (v == Variant::kSph || (v == Variant::kSphRngdep && !has_topo)) {   // main.infraga.sph.cpp:788-789
         o.src[0] = 30.0; o.src[1] = 0.0; o.src[2] = 0.0;
         o.rcvr[0] = 30.0; o.rcvr[1] = -2.5;
+    } else if (rd) {   // the centre of the region (main.infraga.3d.rngdep.cpp:816-817, sph.rngdep :821-822)
+        double a0, a1, b0, b1;
+        iga_atmo_region(atmo, &a0, &a1, &b0, &b1);
+        o.src[0] = (a1 + a0) / 2.0; o.src[1] = (b1 + b0) / 2.0; o.src[2] = 0.0;
+        o.rcvr[0] = sph ? o.src[0] : o.src[0] + 250.0;
+        o.rcvr[1] = sph ? o.src[1] + 5.0 : o.src[1];
     }
-    double incl_est = 10.0, az_est = 0.0;
+    // the range-dependent -eig_direct keep their inclination estimate in radians
+    // when none is given: 0.5 (3D) and 10 (spherical)
+    if (v == Variant::k3DRngdep) incl_est = 0.5 * (180.0 / Pi);
+    if (v == Variant::kSphRngdep) incl_est = 10.0 * (180.0 / Pi);
     bool az_given = false;
     int bounces = 0;
-    if (!parse_eig(argc, argv, v, direct, ep, o, false, incl_est, az_est, az_given, bounces)) return 0;
-    o.src[2] = std::max(ep.fan.z_grnd, o.src[2]);
-    const double z_rcvr = ep.fan.z_grnd;
+    if (!parse_eig(argc, argv, v, direct, ep, o, has_topo, incl_est, az_est, az_given, bounces)) return 0;
+    // topo::z under the source and the receiver: the flat ground, the terrain,
+    // or 0 for the 3D range-dependent solver without terrain
+    auto ground = [&](double x, double y) {
+        if (has_topo) {
+            double zz = 0.0;
+            iga_atmo_terrain(atmo, sph ? x * (Pi / 180.0) : x, sph ? y * (Pi / 180.0) : y, &zz, nullptr, nullptr);
+            return zz;
+        }
+        return v == Variant::k3DRngdep ? 0.0 : ep.fan.z_grnd;
+    };
+    o.src[2] = std::max(ground(o.src[0], o.src[1]), o.src[2]);
+    const double z_rcvr = ground(o.rcvr[0], o.rcvr[1]);
     if (!o.output_id) {
         strip_extension(argv[2]);
         o.output_id = argv[2];
@@ -785,7 +804,7 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
         std::cout << '\t' << "inclination range: " << ep.incl_min << ", " << ep.incl_max << '\n';
         std::cout << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
     }
-    std::cout << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+    if (!has_topo) std::cout << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
     std::cout << '\t' << "damping:" << ep.damping << '\n';
     std::cout << '\t' << "frequency: " << ep.fan.freq << '\n';
     std::cout << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << '\n';
@@ -799,13 +818,15 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     } else {
         std::ofstream res((id + ".arrivals.dat").c_str());
         res << "# " << variant_name(v) << " -eig_search summary:" << '\n';
-        res << "# " << '\t' << "profile: " << argv[2] << '\n';
+        res << "# " << '\t' << (rd ? "profile prefix: " : "profile: ") << argv[2] << '\n';
+        if (v == Variant::k3DRngdep) res << "# " << '\t' << "profile grid files: " << argv[3] << ", " << argv[4] << '\n';
         res << "# " << '\t' << loc_s << es[0] << ", " << es[1] << ", " << es[2] << '\n';
         res << "# " << '\t' << loc_r << er[0] << ", " << er[1] << ", " << z_rcvr << '\n';
         res << "# " << '\t' << "inclination range: " << ep.incl_min * (Pi / 180.0) * (180.0 / Pi) << ", "
             << ep.incl_max * (Pi / 180.0) * (180.0 / Pi) << '\n';
         res << "# " << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
-        res << "#" << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+        if (!has_topo) res << "#" << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+        else res << "#" << '\t' << "topo file:" << topo << '\n';
         res << "# " << '\t' << "damping: " << ep.damping << '\n';
         res << "# " << '\t' << "frequency: " << ep.fan.freq << '\n';
         // infraga-sph writes no blank line after the summary (main.infraga.sph.cpp:944)
@@ -866,11 +887,9 @@ int run(int argc, char** argv, Variant v) {
     else if (strncmp(o, "-back_proj", 10) == 0 || strncmp(o, "-b", 2) == 0)
         std::cout << "-back_proj is not provided by the GPU front end." << '\n';
     else if (strncmp(o, "-eig_search", 11) == 0 || strncmp(o, "-s", 2) == 0) {
-        if (!is_rngdep(v)) return run_eig(argc, argv, v, false);
-        std::cout << "-eig_search is provided for infraga-3d and infraga-sph only by the GPU front end." << '\n';
+        return run_eig(argc, argv, v, false);
     } else if (strncmp(o, "-eig_direct", 11) == 0 || strncmp(o, "-d", 2) == 0) {
-        if (!is_rngdep(v)) return run_eig(argc, argv, v, true);
-        std::cout << "-eig_direct is provided for infraga-3d and infraga-sph only by the GPU front end." << '\n';
+        return run_eig(argc, argv, v, true);
     } else if (strncmp(o, "-wnl_wvfrm", 10) == 0 || strncmp(o, "-w", 2) == 0)
         std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
     else

@@ -340,9 +340,11 @@ void newton_step(Chain& c, const Settings& S, const Fan3DArgs& a, const TraceRes
 }
 
 // One iteration of the spherical find_eigenray Newton loop
-// (geoac.eigenray.sph.cpp:176-371) on flat ground, where the terrain slope
-// terms vanish.  The reference's long double block is done in double.
-void newton_step_sph(Chain& c, const Settings& S, const TraceResSph& res) {
+// (geoac.eigenray.sph.cpp:176-371).  The trace returns the ground under its
+// last row (radius, gradient, sound speed there; flat ground gives a zero
+// gradient, and the terrain terms then vanish exactly).  The reference's long
+// double block is done in double.
+void newton_step_sph(Chain& c, const Settings& S, const TraceRes18& res) {
     if (res.escaped) {
         c.theta -= c.ndth * c.step_sc;
         c.phi_n -= c.ndph * c.step_sc;
@@ -360,16 +362,59 @@ void newton_step_sph(Chain& c, const Settings& S, const TraceResSph& res) {
         } else {
             c.step_sc = std::min(1.0, c.step_sc * 1.25);
             const double dlat = c.rx - s[1], dlon = c.ry - s[2];
-            const double r_grnd = S.r_grnd, c_grnd = S.c_grnd, c_src = S.c_src;
+            const double r_grnd = res.z_grnd, c_grnd = res.c_grnd, c_src = res.c_src;
             const double rc = r_grnd * cos(s[1]);
-            const double ds_dth = -c_src / c_grnd * s[6] / s[3];
-            const double ds_dph = -c_src / c_grnd * s[12] / s[3];
+            const double dzg_dlat = res.dzg[0] / r_grnd, dzg_dlon = res.dzg[1] / rc;
+            const double ds_norm = s[3] - dzg_dlat * s[4] - dzg_dlon * s[5];
+            const double ds_dth = -c_src / c_grnd * (s[6] - dzg_dlat * r_grnd * s[7] - dzg_dlon * rc * s[8]) / ds_norm;
+            const double ds_dph = -c_src / c_grnd * (s[12] - dzg_dlat * r_grnd * s[13] - dzg_dlon * rc * s[14]) / ds_norm;
             const double dlat_dth = s[7] + s[4] / r_grnd * ds_dth, dlon_dth = s[8] + s[5] / rc * ds_dth;
             const double dlat_dph = s[13] + s[4] / r_grnd * ds_dph, dlon_dph = s[14] + s[5] / rc * ds_dph;
             // (1 + damping)^2 multiplies the first product only, as written in the reference
             const double det = pow(1.0 + S.damping, 2) * dlat_dth * dlon_dph - dlat_dph * dlon_dth;
             c.ndth = ((1.0 + S.damping) * dlon_dph * dlat - dlat_dph * dlon) / det;
             c.ndph = ((1.0 + S.damping) * dlat_dth * dlon - dlon_dth * dlat) / det;
+            c.theta += c.ndth * c.step_sc;
+            c.phi_n += c.ndph * c.step_sc;
+            c.dr_prev = dr;
+        }
+    }
+    if (sqrt(c.ndth * c.ndth + c.ndph * c.ndph) * c.step_sc < 1.0e-12) { search_continue(c, S); return; }
+    c.n++;
+}
+
+// One iteration of the 3D find_eigenray Newton loop on a range-dependent
+// atmosphere with terrain (geoac.eigenray.3d.cpp:320-355, the is_topo
+// branch; without terrain the gradient is zero and it reduces exactly to the
+// flat form), 18-state layout.
+void newton_step_3dr(Chain& c, const Settings& S, const TraceRes18& res) {
+    if (res.escaped) {
+        c.theta -= c.ndth * c.step_sc;
+        c.phi_n -= c.ndph * c.step_sc;
+        c.step_sc /= 2.0;
+    } else {
+        const double* s = res.y;
+        const double x = s[0], dx = c.rx - x;
+        const double y = s[1], dy = c.ry - y;
+        const double dr = sqrt(pow(dx, 2) + pow(dy, 2));
+        if (dr < S.tolerance) {
+            c.phase = Chain::kRecordTrace;
+            return;
+        } else if (c.n > 0 && dr > c.dr_prev) {
+            c.theta -= c.ndth * c.step_sc;
+            c.phi_n -= c.ndph * c.step_sc;
+            c.step_sc /= 2.0;
+        } else {
+            c.step_sc = std::min(1.0, c.step_sc * 1.25);
+            const double c_src = res.c_src, c_grnd = res.c_grnd, gx = res.dzg[0], gy = res.dzg[1];
+            const double den = s[5] - gx * s[3] - gy * s[4];
+            const double ds_dth = -c_src / c_grnd * (s[8] - gx * s[6] - gy * s[7]) / den;
+            const double ds_dph = -c_src / c_grnd * (s[14] - gx * s[12] - gy * s[13]) / den;
+            const double dx_dth = s[6] + s[3] * ds_dth, dy_dth = s[7] + s[4] * ds_dth;
+            const double dx_dph = s[12] + s[3] * ds_dph, dy_dph = s[13] + s[4] * ds_dph;
+            const double det = pow(1.0 + S.damping, 2) * (dx_dth * dy_dph - dx_dph * dy_dth);
+            c.ndth = ((1.0 + S.damping) * dy_dph * dx - dx_dph * dy) / det;
+            c.ndph = ((1.0 + S.damping) * dx_dth * dy - dy_dth * dx) / det;
             c.theta += c.ndth * c.step_sc;
             c.phi_n += c.ndph * c.step_sc;
             c.dr_prev = dr;
@@ -388,7 +433,10 @@ using namespace iga_internal;
 extern "C" int iga_eig_params_default(iga_atmo_t h, iga_eig_params* p) {
     if (!h || !p) return IGA_E_INVALID;
     memset(p, 0, sizeof(*p));
-    int rc = iga_fan_params_default(h, &p->fan);
+    // propagation defaults of the handle's own solver (range-dependent: its
+    // geometry, region and source at the region's centre)
+    int rc = h->kind == 0 ? iga_fan_params_default(h, &p->fan)
+                          : iga_fan_params_init(h, h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D, &p->fan);
     if (rc) return rc;
     p->incl_min = 0.5; p->incl_max = 45.0;
     p->incl_step_min = 0.001; p->incl_step_max = 0.1;
@@ -416,32 +464,44 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     fp.write_rays = 1;
     int rc = validate(&fp, 1);
     if (rc) return rc;
-    if (h->kind != 0) {
-        g_cuda_err = "eigenray search: stratified atmospheres only";
+    // range-dependent handles (kind 1 spherical, 2 Cartesian) search in the
+    // geometry they were loaded for
+    const bool rngdep = h->kind != 0;
+    if (rngdep && sph != (h->kind == 1)) {
+        g_cuda_err = "range-dependent atmosphere: eigenray search in the geometry it was loaded for";
         return IGA_E_UNSUPPORTED;
     }
-    if (sph && fp.precision != IGA_FP64) {
-        g_cuda_err = "spherical eigenray search: FP64 only";
+    if ((sph || rngdep) && fp.precision != IGA_FP64) {
+        g_cuda_err = "spherical and range-dependent eigenray searches: FP64 only";
         return IGA_E_UNSUPPORTED;
     }
+    // 18-state traces: spherical and range-dependent solvers
+    const bool wide = sph || rngdep;
     if (P->bnc_min < 0 || P->bnc_max < P->bnc_min || P->iterations < 0 || !(P->tolerance > 0.0) ||
         !(P->incl_step_max > 0.0) || !(P->incl_step_min > 0.0) || !(P->incl_max > P->incl_min))
         return IGA_E_INVALID;
     if (n_pairs == 0) return IGA_OK;
-    for (int i = 1; i < n_pairs; i++)
+    for (int i = 1; i < n_pairs; i++) {
         if (pairs[i].src[2] != pairs[0].src[2]) {
             g_cuda_err = "iga_eig_run: all pairs of one call must share the source altitude";
             return IGA_E_UNSUPPORTED;
         }
+        if (rngdep && (pairs[i].src[0] != pairs[0].src[0] || pairs[i].src[1] != pairs[0].src[1])) {
+            g_cuda_err = "iga_eig_run: range-dependent searches of one call must share the source";
+            return IGA_E_UNSUPPORTED;
+        }
+    }
     IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
     // the launch arguments carry the source altitude; each trace request
     // carries its own source x, y (latitude, longitude)
-    fp.src[0] = sph ? pairs[0].src[0] : 0.0; fp.src[1] = sph ? pairs[0].src[1] : 0.0; fp.src[2] = pairs[0].src[2];
+    fp.src[0] = (sph || rngdep) ? pairs[0].src[0] : 0.0;
+    fp.src[1] = (sph || rngdep) ? pairs[0].src[1] : 0.0;
+    fp.src[2] = pairs[0].src[2];
     Fan3DArgs a;
     rc = build_args(h, &fp, a);
     if (rc) return rc;
     double c_incl_src = 0.0;   // spherical find_eigenray: c at radius = source altitude, i.e. the lowest knot
-    if (sph) {
+    if (sph && !rngdep) {
         double f, d1, d2;
         iga::spline_eval(h->prof.z, h->prof.c, h->prof.cs, h->prof.z.front(), f, d1, d2);
         c_incl_src = f;
@@ -458,8 +518,27 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     S.sph = sph;
     S.r_grnd = a.r_grnd; S.c_src = a.c0; S.c_grnd = a.c_gnd;
     double theta_min = P->incl_min * (kPi / 180.0);
-    if (sph) {   // run_eig_search's theta_grnd for flat ground (main.infraga.sph.cpp:965-981)
-        const double theta_grnd = pairs[0].src[2] - fp.z_grnd < 0.01 ? 0.1 * (kPi / 180.0) : -89.9 * (kPi / 180.0);
+    if (sph) {   // run_eig_search's theta_grnd (main.infraga.sph.cpp:965-981, sph.rngdep the same)
+        double theta_grnd;
+        if (rngdep && h->has_topo) {
+            // over terrain the reference takes the steepest ground slope over
+            // azimuths 0, 3, ..., 357 deg plus 0.1, in DEGREES, and compares it
+            // with the inclination bounds in radians; kept as written
+            double zt, dz[2];
+            iga::terrain_eval1(h->topo, a.src_x, a.src_y, zt, dz);
+            if (a.src_z - zt < 0.01) {
+                theta_grnd = 0.0;
+                const double dzgdx = 1.0 / (kEarthRadiusKm * cos(a.src_x)) * dz[1];
+                const double dzgdy = 1.0 / kEarthRadiusKm * dz[0];
+                for (double pv = 0.0; pv < 360.0; pv += 3.0)
+                    theta_grnd = std::max(theta_grnd, atan(dzgdx * sin(pv * kPi / 180.0) + dzgdy * cos(pv * kPi / 180.0)) *
+                                                          (180.0 / kPi) + 0.1);
+            } else {
+                theta_grnd = -89.9 * (kPi / 180.0);
+            }
+        } else {
+            theta_grnd = a.src_z - (a.r_grnd - a.r_earth) < 0.01 ? 0.1 * (kPi / 180.0) : -89.9 * (kPi / 180.0);
+        }
         theta_min = std::max(theta_min, theta_grnd);
     }
 
@@ -494,8 +573,8 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     }
 
     TraceReq* d_req = nullptr;
-    unsigned char* d_res = nullptr;   // TraceRes or TraceResSph records
-    const size_t res_bytes = sph ? sizeof(TraceResSph) : sizeof(TraceRes);
+    unsigned char* d_res = nullptr;   // TraceRes or TraceRes18 records
+    const size_t res_bytes = wide ? sizeof(TraceRes18) : sizeof(TraceRes);
     SegRes* d_seg = nullptr;
     size_t cap_req = 0;
     long long steps_tot = 0;
@@ -510,7 +589,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
 
     std::vector<TraceReq> req6, req18;
     std::vector<TraceRes> res18;
-    std::vector<TraceResSph> res18s;
+    std::vector<TraceRes18> res18s;
     std::vector<SegRes> seg6;
     // searches of one pair for different bounce counts sweep the same launch
     // angles until their first bracket: one trace serves them all
@@ -576,7 +655,11 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (!req6.empty()) {
             e = cudaMemcpyAsync(d_req, req6.data(), req6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
-                e = sph ? launch_trace_sph(a, d_req, reinterpret_cast<TraceResSph*>(d_res), (int)req6.size(), false, st,
+                e = h->kind == 1 ? launch_trace_sphr(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false,
+                                                     st, d_seg, max_seg)
+                    : h->kind == 2 ? launch_trace_3dr(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false,
+                                                      st, d_seg, max_seg)
+                    : sph ? launch_trace_sph(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false, st,
                                            d_seg, max_seg, c_incl_src)
                     : f32 ? launch_trace_fp32c(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), false, st,
                                                d_seg, max_seg)
@@ -586,18 +669,22 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (e == cudaSuccess && !req18.empty()) {
             e = cudaMemcpyAsync(d_req18, req18.data(), req18.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
-                e = sph ? launch_trace_sph(a, d_req18, reinterpret_cast<TraceResSph*>(d_res18), (int)req18.size(), true,
+                e = h->kind == 1 ? launch_trace_sphr(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(),
+                                                     true, st, nullptr, 0)
+                    : h->kind == 2 ? launch_trace_3dr(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(),
+                                                      true, st, nullptr, 0)
+                    : sph ? launch_trace_sph(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(), true,
                                            st, nullptr, 0, c_incl_src)
                     : f32 ? launch_trace_fp32c(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), true, st)
                           : launch_trace<true>(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), st);
         }
         seg6.resize(req6.size() * max_seg);
-        res18.resize(sph ? 0 : req18.size());
-        res18s.resize(sph ? req18.size() : 0);
+        res18.resize(wide ? 0 : req18.size());
+        res18s.resize(wide ? req18.size() : 0);
         if (e == cudaSuccess && !req6.empty())
             e = cudaMemcpyAsync(seg6.data(), d_seg, seg6.size() * sizeof(SegRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && !req18.empty())
-            e = sph ? cudaMemcpyAsync(res18s.data(), d_res18, res18s.size() * sizeof(TraceResSph), cudaMemcpyDeviceToHost, st)
+            e = wide ? cudaMemcpyAsync(res18s.data(), d_res18, res18s.size() * sizeof(TraceRes18), cudaMemcpyDeviceToHost, st)
                     : cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
@@ -647,10 +734,11 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
                 }
             } else if (c.phase == Chain::kNewton) {
                 if (sph) newton_step_sph(c, S, res18s[c.req0]);
+                else if (rngdep) newton_step_3dr(c, S, res18s[c.req0]);
                 else newton_step(c, S, a, res18[c.req0]);
             } else if (c.phase == Chain::kRecordTrace && sph) {
                 // eig_results row of geoac.eigenray.sph.cpp:303-315
-                const TraceResSph& t = res18s[c.req0];
+                const TraceRes18& t = res18s[c.req0];
                 std::vector<double> row(IGA_ARRIVAL_COLS);
                 row[0] = c.theta * (180.0 / kPi);
                 row[1] = 90.0 - c.phi_n * (180.0 / kPi);
@@ -659,7 +747,25 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
                 row[4] = t.y[2] * 180.0 / kPi;
                 row[5] = t.tt;
                 row[6] = gc_dist_h(t.y[1], t.y[2], c.sx, c.sy) / t.tt;
-                row[7] = t.rmax;
+                row[7] = t.zmax;
+                row[8] = t.incl;
+                row[9] = t.baz;
+                row[10] = t.amp_db;
+                row[11] = -2.0 * t.att;
+                c.rows.push_back(std::move(row));
+                search_continue(c, S);
+            } else if (c.phase == Chain::kRecordTrace && rngdep) {
+                // eig_results row of geoac.eigenray.3d.cpp:296-308, 18-state layout
+                const TraceRes18& t = res18s[c.req0];
+                std::vector<double> row(IGA_ARRIVAL_COLS);
+                row[0] = c.theta * (180.0 / kPi);
+                row[1] = 90.0 - c.phi_n * (180.0 / kPi);
+                row[2] = c.nb;
+                row[3] = t.y[0];
+                row[4] = t.y[1];
+                row[5] = t.tt;
+                row[6] = sqrt(pow(t.y[0] - c.sx, 2) + pow(t.y[1] - c.sy, 2)) / t.tt;
+                row[7] = t.zmax;
                 row[8] = t.incl;
                 row[9] = t.baz;
                 row[10] = t.amp_db;

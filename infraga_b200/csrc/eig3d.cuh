@@ -35,22 +35,36 @@ struct SegRes {
     int pad;
 };
 
-// Result of a spherical trace (eigsph.cu): the last row in the 18-state
-// spherical layout (r, lat, lon, nu, X_th, mu_th, X_ph, mu_ph), and in record
-// mode the arrival columns find_eigenray forms on the device.
-struct TraceResSph {
+// Result of a trace in the full 18-state layout (spherical: r, lat, lon,
+// nu, X_th, mu_th, X_ph, mu_ph; 3D range-dependent: x, y, z, nu, ...): the
+// last row; in record mode the arrival columns find_eigenray forms on the
+// device; after an amplitude trace the ground under the last row that
+// find_eigenray's Newton derivatives use (sound speeds at the source and on
+// the ground, the ground height -- a radius in the spherical layout -- and
+// its gradient).
+struct TraceRes18 {
     double y[18];
-    double tt, att, rmax, amp_db, incl, baz;
+    double tt, att, zmax, amp_db, incl, baz;
+    double c_src, c_grnd, z_grnd, dzg[2];
+    double pad_d;
     long long steps;
     int escaped;
     int pad;
 };
 
-// Spherical stratified traces; source latitude/longitude per request (x0, y0,
-// radians), altitude from the launch arguments.  c_incl_src is the sound
-// speed find_eigenray divides by in its arrival inclination.
-cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceResSph* d_res, int n, bool amp,
+// Spherical stratified traces (eigsph.cu); source latitude/longitude per
+// request (x0, y0, radians), altitude from the launch arguments.
+// c_incl_src is the sound speed find_eigenray divides by in its arrival
+// inclination.
+cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
                              cudaStream_t st, SegRes* seg_out, int seg_stride, double c_incl_src);
+
+// Range-dependent traces with terrain (fan3dr_fp64.cu, fansphr_fp64.cu): the
+// source is the launch arguments' (all requests of a launch share it).
+cudaError_t launch_trace_3dr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
+                             cudaStream_t st, SegRes* seg_out, int seg_stride);
+cudaError_t launch_trace_sphr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
+                              cudaStream_t st, SegRes* seg_out, int seg_stride);
 
 // FP32-compensated traces (same contract as the FP64 trace kernel).  With
 // seg_out != null, segment j of request r also writes seg_out[r * seg_stride + j].

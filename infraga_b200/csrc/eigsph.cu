@@ -21,7 +21,7 @@ constexpr int kSphTraceThreads = 128;
 template <bool AMP>
 __global__ void __launch_bounds__(kSphTraceThreads) tracesph_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                          const TraceReq* __restrict__ reqs,
-                                                                         TraceResSph* __restrict__ out, int n,
+                                                                         TraceRes18* __restrict__ out, int n,
                                                                          SegRes* __restrict__ seg_out, int seg_stride,
                                                                          double c_incl_src) {
     constexpr int N = DimSph<AMP>::n;
@@ -134,13 +134,15 @@ __global__ void __launch_bounds__(kSphTraceThreads) tracesph_fp64_kernel(const _
             y[16] = p[16]; y[17] = p[17];
         }
     }
-    TraceResSph& o = out[r];
+    TraceRes18& o = out[r];
 #pragma unroll
     for (int i = 0; i < 18; i++) o.y[i] = i < N ? acc[i] : 0.0;
     o.steps = steps;
     o.escaped = esc ? 1 : 0;
+    // flat ground under every row
+    o.c_src = a.c0; o.c_grnd = a.c_gnd; o.z_grnd = a.r_grnd; o.dzg[0] = 0.0; o.dzg[1] = 0.0;
     if (record) {
-        o.tt = tt; o.att = att; o.rmax = rmax;
+        o.tt = tt; o.att = att; o.zmax = rmax;
         o.amp_db = AMP ? amp_db_sph(tab, a, seg, acc, q.theta, q.phi, nullptr) : 0.0;
         const double ze = fmin(fmax(acc[0] - a.r_earth, a.z_lo), a.z_hi);
         seg = seg_walk(tab, a.n_knots, ze, seg);
@@ -152,12 +154,12 @@ __global__ void __launch_bounds__(kSphTraceThreads) tracesph_fp64_kernel(const _
         while (baz > 180.0) baz -= 360.0;
         o.baz = baz;
     } else {
-        o.tt = o.att = o.rmax = o.amp_db = o.incl = o.baz = 0.0;
+        o.tt = o.att = o.zmax = o.amp_db = o.incl = o.baz = 0.0;
     }
 }
 
 template <bool AMP>
-cudaError_t launch_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceResSph* d_res, int n, cudaStream_t st,
+cudaError_t launch_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, cudaStream_t st,
                         SegRes* seg_out, int seg_stride, double c_incl_src) {
     if (n <= 0) return cudaSuccess;
     auto kern = tracesph_fp64_kernel<AMP>;
@@ -172,7 +174,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceResSph* 
 
 }  // namespace
 
-cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceResSph* d_res, int n, bool amp,
+cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
                              cudaStream_t st, SegRes* seg_out, int seg_stride, double c_incl_src) {
     return amp ? launch_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride, c_incl_src)
                : launch_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride, c_incl_src);

@@ -58,6 +58,18 @@ CASES = {
     "3dr_calc_amp": ("infraga-3d-rngdep", "3dr", 0,
                      ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "inclination=12", "azimuth=100",
                       "bounces=1", "calc_amp=true", "write_rays=false", "output_id=amp"]),
+    "3dr_eig": ("infraga-3d-rngdep", "3dr", 0,
+                ["-eig_search", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "rcvr_x=210",
+                 "rcvr_y=0", "incl_min=12", "incl_max=24"]),
+    "3dr_direct": ("infraga-3d-rngdep", "3dr", 0,
+                   ["-eig_direct", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "rcvr_x=210",
+                    "rcvr_y=0", "incl_est=18", "az_est=90", "bounces=0", "output_id=direct"]),
+    "sphr_eig": ("infraga-sph-rngdep", "sphr", 0,
+                 ["-eig_search", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "src_alt=3",
+                  "rcvr_lat=32.98", "rcvr_lon=-104.6", "incl_min=10", "incl_max=30"]),
+    "sphr_eig_ground": ("infraga-sph-rngdep", "sphr", 0,
+                        ["-s", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "rcvr_lat=32.98",
+                         "rcvr_lon=-104.6", "output_id=ground"]),
     "sphr_prop": ("infraga-sph-rngdep", "sphr", 0,
                   ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "incl_min=6",
                    "incl_max=26", "incl_step=10", "az_min=90", "az_max=270", "az_step=180", "bounces=1",

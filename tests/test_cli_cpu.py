@@ -54,7 +54,7 @@ def test_cli_fixtures_complete():
         for rel in c["files"]:
             assert os.path.getsize(os.path.join(CLI, name, rel)) > 0, (name, rel)
         arr = [f for f in c["files"] if f.endswith(".arrivals.dat")]
-        if arr:
+        if arr and not name.endswith("_ground"):   # *_ground: a case whose reference result is empty
             rows = [ln for ln in open(os.path.join(CLI, name, arr[0])) if ln.strip() and not ln.startswith("#")]
             assert rows, f"{name}: fixture without arrivals"
 
