@@ -553,6 +553,180 @@ def run_serving(args):
     return 0
 
 
+# ---------------------------------------------------------------- config 2
+def ref_sphr_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "iga_ref_sphr_fast")
+    return p if os.path.exists(p) else None
+
+
+def cpu_baseline_sphr(files):
+    """The reference's spherical range-dependent solver (oracle/_ref) on a
+    bounded sample: azimuth 90 deg, `procs` inclinations spread over the
+    fan's range, one single-threaded process each, all 20 bounces."""
+    exe = ref_sphr_binary()
+    if not exe:
+        return None
+    from infraga_b200 import workloads as wl
+    procs = max(1, min(8, os.cpu_count() or 1))
+    incls = np.linspace(5.0, 45.0, procs)
+    prefix, lat_f, lon_f, topo = files
+    f = wl.SPHR_FAN
+    cmds = [[exe, "prop", prefix, lat_f, lon_f, f"topo_file={topo}", f"inclination={x:.2f}", "azimuth=90",
+             f"bounces={f['bounces']}", f"max_rng={f['rng_max']}", "write_rays=false"] for x in incls]
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for c in cmds]
+    outs = [p.communicate(timeout=600)[0] for p in ps]
+    wall = time.perf_counter() - t0
+    steps = sum(parse_ref_steps(o)[0] for o in outs)
+    return {"value": steps / wall, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"azimuth 90 deg x {procs} inclinations 5..45 deg, 20 bounces, one process each; "
+                      f"{steps} ray-steps in {wall:.1f} s"}
+
+
+def run_sphr(args):
+    """Config 2: spherical range-dependent fan over a 21x21 node grid with
+    0.05-deg fractal terrain (workloads.py), FP64, ray-steps/s."""
+    import torch
+    import infraga_b200 as ig
+    from infraga_b200 import workloads as wl
+    dev = torch.device("cuda", 0)
+    files = wl.sphr_files()
+    atmo = ig.Atmosphere.load_rngdep(files[0], files[1], files[2], topo_file=files[3], geometry=ig.GEOM_SPH)
+    th, ph = wl.sphr_angles()
+    n = th.size
+    f = wl.SPHR_FAN
+    nb = f["bounces"] + 1
+    d_th = torch.tensor(th, dtype=torch.float64, device=dev)
+    d_ph = torch.tensor(ph, dtype=torch.float64, device=dev)
+    arr = torch.empty((n, nb, 12), dtype=torch.float64, device=dev)
+    na = torch.empty(n, dtype=torch.int32, device=dev)
+    st = torch.empty(n, dtype=torch.int64, device=dev)
+    ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    legs = {}
+    for amp in (1, 0):
+        params = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"],
+                                     write_rays=0, calc_amp=amp)
+        times, steps = [], 0
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ig.fan_run_device(atmo, params, d_th.data_ptr(), d_ph.data_ptr(), n, arr.data_ptr(), na.data_ptr(),
+                              st.data_ptr(), 0, ws.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1) * 1e-3)
+                steps = int(st.sum().item())
+        t = sum(times) / len(times)
+        legs["amp" if amp else "noamp"] = {"ray_steps": steps, "s_per_fan": t, "value": steps / t}
+    cpu = None if args.no_cpu else cpu_baseline_sphr(files)
+    head = legs["amp"]
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * head["s_per_fan"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sph-rngdep-fan-{n}rays-21x21grid-401x401terrain-20bnc-3000km-fp64",
+                       "rays": n, "l2": "flushed (256 MiB write) between timed steps"},
+            "legs": legs, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- config 3
+def cpu_baseline_eig(mets, pairs_by_seed, bnc_max):
+    """The reference eigenray search (oracle/_ref iga_ref_3d_fast eig mode) on a
+    bounded sample: up to 8 pairs of the first seed, one process per pair,
+    bounce counts 0..bnc_max (the caller bounds it: the reference spends
+    minutes per pair on 0..8)."""
+    exe = ref_binary()
+    if not exe:
+        return None
+    procs = max(1, min(8, os.cpu_count() or 1))
+    cmds = []
+    for k, (src, rcv) in enumerate(pairs_by_seed[0][:procs]):
+        cmds.append([exe, "eig", mets[0], f"rcvr_x={rcv[0]:.6f}", f"rcvr_y={rcv[1]:.6f}", "bnc_min=0",
+                     f"bnc_max={bnc_max}", f"out=/tmp/iga_eig_cpu_{os.getpid()}_{k}.dat",
+                     f"out_id=/tmp/iga_eig_cpu_{os.getpid()}_{k}"])
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for c in cmds]
+    outs = [p.communicate(timeout=1200)[0] for p in ps]
+    wall = time.perf_counter() - t0
+    n_eig = 0
+    for o in outs:
+        for line in o.splitlines():
+            if line.startswith("# eigenrays"):
+                n_eig += int(line.split()[2])
+    return {"value": n_eig / wall, "unit": "eigenrays/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} pairs of seed 1, bounces 0..{bnc_max}, one process per pair; "
+                      f"{n_eig} eigenrays in {wall:.1f} s"}
+
+
+def run_eigen(args):
+    """Config 3: batched 3D eigenray search, 8 seeds x 128 pairs, 0..8
+    bounces, FP64 and FP32-compensated traces; eigenrays/s over wall time."""
+    import infraga_b200 as ig
+    from infraga_b200 import workloads as wl
+    seeds = list(range(1, 9))
+    bmax = wl.EIG["bnc_max"]
+    mets = [wl.profile_met(sd) for sd in seeds]
+    atmos = [ig.Atmosphere.load(m) for m in mets]
+    pairs = [wl.eig_pairs(sd) for sd in seeds]
+    # warm-up: a small search per precision (kernel loading, allocator)
+    for prec in (ig.FP64, ig.FP32C):
+        p = ig.eig_params(atmos[0], bnc_min=0, bnc_max=1)
+        p.fan.precision = prec
+        ig.eig_run(atmos[0], p, pairs[0][:4])
+    legs, rows = {}, {}
+    for name, prec in (("fp64", ig.FP64), ("fp32c", ig.FP32C)):
+        n_eig, steps, t_tot = 0, 0, 0.0
+        rows[name] = []
+        for a, pr in zip(atmos, pairs):
+            p = ig.eig_params(a, bnc_min=0, bnc_max=bmax)
+            p.fan.precision = prec
+            t0 = time.perf_counter()
+            r = ig.eig_run(a, p, pr)
+            t_tot += time.perf_counter() - t0
+            n_eig += r["eigenrays"].shape[0]
+            steps += r["total_steps"]
+            rows[name].append((r["eigenrays"], r["pair_index"]))
+        legs[name] = {"eigenrays": n_eig, "seconds": t_tot, "value": n_eig / t_tot, "ray_steps": steps}
+    # FP32C eigenrays against the FP64 ones: matched by pair, bounce count and
+    # launch inclination (within 0.05 deg)
+    d_pos, d_t, n_match = [], [], 0
+    for (r64, i64), (r32, i32) in zip(rows["fp64"], rows["fp32c"]):
+        for k in range(r64.shape[0]):
+            cand = np.where((i32 == i64[k]) & (r32[:, 2] == r64[k, 2]) & (np.abs(r32[:, 0] - r64[k, 0]) < 0.05))[0]
+            if cand.size:
+                j = cand[np.argmin(np.abs(r32[cand, 0] - r64[k, 0]))]
+                n_match += 1
+                d_pos.append(np.hypot(r32[j, 3] - r64[k, 3], r32[j, 4] - r64[k, 4]))
+                d_t.append(abs(r32[j, 5] - r64[k, 5]))
+    def pct(v, q):
+        v = np.asarray(v, dtype=np.float64)
+        v = v[np.isfinite(v)]
+        return float(np.percentile(v, q)) if v.size else None
+
+    nonfinite = {k: int(sum(int((~np.isfinite(r[:, :12])).any(axis=1).sum()) for r, _ in rows[k])) for k in rows}
+    err = {"matched": n_match, "fp64_eigenrays": legs["fp64"]["eigenrays"],
+           "fp32c_eigenrays": legs["fp32c"]["eigenrays"],
+           "landing_km_p50": pct(d_pos, 50), "landing_km_p99": pct(d_pos, 99),
+           "time_s_p50": pct(d_t, 50), "time_s_p99": pct(d_t, 99),
+           "rows_with_nonfinite_columns": nonfinite}
+    cpu = None if args.no_cpu else cpu_baseline_eig(mets, pairs, 1)
+    head = legs["fp32c"]
+    line = {"metric": "eigenrays/s", "value": head["value"], "unit": "eigenrays/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": 1e3 * head["seconds"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-compensated (f64 Newton)", "data": "synthetic",
+            "config": {"workload": f"3d-strat-eigen-8seeds-x-{wl.EIG['pairs']}pairs-bnc0-{bmax}",
+                       "timing": "wall clock of iga_eig_run over all seeds (host-driven search)"},
+            "legs": legs, "fp32c_vs_fp64": err, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -570,9 +744,17 @@ def main():
                     help="run the request-server benchmark (Poisson stream of fan and eigen requests) instead")
     ap.add_argument("--serve-rate", type=float, default=SERVE["rate"], help="request arrival rate [1/s]")
     ap.add_argument("--serve-requests", type=int, default=SERVE["requests"], help="requests in the stream")
+    ap.add_argument("--sphr", action="store_true",
+                    help="time the spherical range-dependent fan with terrain (config 2) instead")
+    ap.add_argument("--eigen", action="store_true",
+                    help="time the batched 3D eigenray search (config 3, FP64 and FP32C) instead")
     args = ap.parse_args()
     if args.serving:
         return run_serving(args)
+    if args.sphr:
+        return run_sphr(args)
+    if args.eigen:
+        return run_eigen(args)
     if args.az_step != FAN["az"][2]:
         FAN["az"] = (FAN["az"][0], FAN["az"][1], args.az_step)
     if args.impl == "reference":

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define IGA_ABI_VERSION 2
+#define IGA_ABI_VERSION 3
 
 /* ---- status codes ---- */
 enum iga_status {
@@ -297,6 +297,9 @@ typedef struct iga_eig_params {
     int bnc_min, bnc_max;        /* bounce counts searched (0, 0) */
     int iterations;              /* Newton iteration limit (25) */
     int chunk;                   /* sweep inclinations traced per search per GPU round (0 = automatic) */
+    int streams;                 /* pair groups searched concurrently, each on its own host thread and
+                                    CUDA stream (0 = automatic = 1: on large searches the sweep launches
+                                    already fill the GPU, and more groups measured slower) */
 } iga_eig_params;
 
 /* Defaults of run_eig_search after set_region (fan as iga_fan_params_default;

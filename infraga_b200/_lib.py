@@ -56,7 +56,7 @@ class EigParams(ctypes.Structure):
                 ("incl_step_min", ctypes.c_double), ("incl_step_max", ctypes.c_double),
                 ("damping", ctypes.c_double), ("tolerance", ctypes.c_double), ("az_err_lim", ctypes.c_double),
                 ("bnc_min", ctypes.c_int), ("bnc_max", ctypes.c_int), ("iterations", ctypes.c_int),
-                ("chunk", ctypes.c_int)]
+                ("chunk", ctypes.c_int), ("streams", ctypes.c_int)]
 
 
 class EigPair(ctypes.Structure):

@@ -17,6 +17,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "eig3d.cuh"
@@ -585,7 +587,12 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (d_seg) cudaFreeAsync(d_seg, st);
         d_req = nullptr; d_res = nullptr; d_seg = nullptr;
     };
-    auto fail = [&](int code) { release(); return code; };
+    cudaEvent_t round_done = nullptr;
+    {
+        cudaError_t e = cudaEventCreateWithFlags(&round_done, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate(eigen round)");
+    }
+    auto fail = [&](int code) { release(); cudaEventDestroy(round_done); return code; };
 
     std::vector<TraceReq> req6, req18;
     std::vector<TraceRes> res18;
@@ -686,7 +693,11 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (e == cudaSuccess && !req18.empty())
             e = wide ? cudaMemcpyAsync(res18s.data(), d_res18, res18s.size() * sizeof(TraceRes18), cudaMemcpyDeviceToHost, st)
                     : cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        // wait on a blocking-sync event: the host thread sleeps instead of
+        // spinning, so concurrent searches (pair groups, server workers) leave
+        // the host cores to each other and to the driver
+        if (e == cudaSuccess) e = cudaEventRecord(round_done, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(round_done);
         if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
         // each search's view of its sweep traces: the entry of its own
         // segment count, or the earlier entry where the trace escaped
@@ -793,6 +804,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         }
     }
     release();
+    cudaEventDestroy(round_done);
     if (verbose) {
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_begin).count();
         fprintf(stderr, "eig_search: %zu chains, %lld rounds, sweep traces %lld (%lld steps), "
@@ -832,15 +844,86 @@ extern "C" int iga_eig_direct(iga_atmo_t h, const iga_eig_params* P, const iga_e
     return IGA_OK;
 }
 
+namespace {
+
+// Searches of different pairs are independent: pair groups can run
+// concurrently, each on its own host thread and stream, so that their rounds
+// overlap on the GPU.  Pairs are dealt round-robin (uneven pairs spread over
+// the groups); the rows are merged back in pair order.
+int eig_search_groups(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs, int groups,
+                      std::vector<double>& rows, std::vector<int>& pidx, long long& steps) {
+    rows.clear(); pidx.clear(); steps = 0;
+    if (groups <= 1) return eig_search(h, P, pairs, n_pairs, h->stream, rows, pidx, steps);
+    struct Part {
+        std::vector<int> idx;
+        std::vector<iga_eig_pair> pairs;
+        std::vector<double> rows;
+        std::vector<int> pidx;
+        long long steps = 0;
+        int rc = IGA_OK;
+        std::string err;
+    };
+    std::vector<Part> parts(groups);
+    for (int i = 0; i < n_pairs; i++) {
+        parts[i % groups].idx.push_back(i);
+        parts[i % groups].pairs.push_back(pairs[i]);
+    }
+    std::vector<std::thread> threads;
+    for (int g = 0; g < groups; g++) {
+        threads.emplace_back([&, g]() {
+            Part& pt = parts[g];
+            cudaStream_t s = nullptr;
+            cudaError_t e = cudaSetDevice(h->device);
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            if (e != cudaSuccess) {
+                pt.rc = cuda_fail(e, "eigen search stream");
+            } else {
+                pt.rc = eig_search(h, P, pt.pairs.data(), (int)pt.pairs.size(), s, pt.rows, pt.pidx, pt.steps);
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+            if (pt.rc) pt.err = g_cuda_err;
+        });
+    }
+    for (auto& t : threads) t.join();
+    for (auto& pt : parts)
+        if (pt.rc) {
+            g_cuda_err = pt.err;
+            return pt.rc;
+        }
+    // merge in pair order (within a pair the group kept the search order)
+    std::vector<std::vector<std::pair<int, int>>> by_pair(n_pairs);   // (group, row)
+    for (int g = 0; g < groups; g++) {
+        steps += parts[g].steps;
+        for (size_t r = 0; r < parts[g].pidx.size(); r++) by_pair[parts[g].idx[parts[g].pidx[r]]].push_back({g, (int)r});
+    }
+    for (int i = 0; i < n_pairs; i++)
+        for (auto& gr : by_pair[i]) {
+            const double* src = &parts[gr.first].rows[(size_t)gr.second * IGA_ARRIVAL_COLS];
+            rows.insert(rows.end(), src, src + IGA_ARRIVAL_COLS);
+            pidx.push_back(i);
+        }
+    return IGA_OK;
+}
+
+}  // namespace
+
 extern "C" int iga_eig_run(iga_atmo_t h, const iga_eig_params* P, const iga_eig_pair* pairs, int n_pairs,
                            double* eigenrays, int cap, int* n_out, int* pair_index, long long* total_steps) {
     if (!h || !P || !n_out || n_pairs < 0 || (n_pairs > 0 && !pairs) || (cap > 0 && !eigenrays)) return IGA_E_INVALID;
     *n_out = 0;
     if (total_steps) *total_steps = 0;
+    if (P->streams < 0) return IGA_E_INVALID;
     std::vector<double> rows;
     std::vector<int> pidx;
     long long steps = 0;
-    int rc = eig_search(h, P, pairs, n_pairs, h->stream, rows, pidx, steps);
+    // automatic: one group.  Measured on a config-3 seed (128 pairs, 0-8 bounces),
+    // 4 and 16 concurrent groups took 1.8x and 3.8x longer than one: the rounds'
+    // big sweep launches already fill the GPU, and concurrent launches only
+    // stretch each other's longest trace
+    int groups = P->streams > 0 ? P->streams : 1;
+    groups = std::max(1, std::min(groups, n_pairs));
+    int rc = eig_search_groups(h, P, pairs, n_pairs, groups, rows, pidx, steps);
     if (rc) return rc;
     const int w = (int)pidx.size();
     for (int i = 0; i < w && i < cap; i++) {

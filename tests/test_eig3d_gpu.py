@@ -70,6 +70,21 @@ def test_eigen_batch_equals_single_pairs(dev):
         np.testing.assert_array_equal(batch["eigenrays"][batch["pair_index"] == i], single["eigenrays"])
 
 
+def test_eigen_pair_groups_equal_one_stream(dev):
+    """Pair groups searched concurrently on their own streams give exactly the
+    single-stream rows, in pair order."""
+    atmo = ig.Atmosphere.load(profile_path(0))
+    g = np.random.default_rng(5)
+    rng, az = g.uniform(150.0, 400.0, 10), g.uniform(0.0, 2 * np.pi, 10)
+    pairs = [((0.0, 0.0, 0.0), (float(r * np.cos(a)), float(r * np.sin(a)))) for r, a in zip(rng, az)]
+    one = ig.eig_run(atmo, ig.eig_params(atmo, bnc_min=0, bnc_max=1, streams=1), pairs)
+    many = ig.eig_run(atmo, ig.eig_params(atmo, bnc_min=0, bnc_max=1, streams=4), pairs)
+    assert one["eigenrays"].shape[0] > 0
+    np.testing.assert_array_equal(many["eigenrays"], one["eigenrays"])
+    np.testing.assert_array_equal(many["pair_index"], one["pair_index"])
+    assert many["total_steps"] == one["total_steps"]
+
+
 # FP32-compensated ray integration with FP64 bracket/Newton updates: the same
 # eigenrays within the search tolerance.  A trace's FP32 rounding moves its
 # landing point by metres, so the Newton iteration stops at a slightly
