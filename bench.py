@@ -604,10 +604,14 @@ def run_sphr(args):
     ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
+    # launch shape picked by the autotuner (iga_fan_tune) on this fan
+    tp = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"], write_rays=0)
+    best, tune_s = ig.fan_tune(atmo, tp, th, ph)
     legs = {}
-    for amp in (1, 0):
+    for amp, block in ((1, best), (0, best), (1, 0)):
         params = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"],
                                      write_rays=0, calc_amp=amp)
+        params.block = block
         times, steps = [], 0
         for i in range(args.warmup + args.steps):
             flush.zero_()
@@ -621,7 +625,8 @@ def run_sphr(args):
                 times.append(e0.elapsed_time(e1) * 1e-3)
                 steps = int(st.sum().item())
         t = sum(times) / len(times)
-        legs["amp" if amp else "noamp"] = {"ray_steps": steps, "s_per_fan": t, "value": steps / t}
+        name = ("amp" if amp else "noamp") + ("" if block else "_default_block128")
+        legs[name] = {"ray_steps": steps, "s_per_fan": t, "value": steps / t, "block": block or 128}
     cpu = None if args.no_cpu else cpu_baseline_sphr(files)
     head = legs["amp"]
     line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -629,7 +634,7 @@ def run_sphr(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"sph-rngdep-fan-{n}rays-21x21grid-401x401terrain-20bnc-3000km-fp64",
                        "rays": n, "l2": "flushed (256 MiB write) between timed steps"},
-            "legs": legs, "cpu_baseline": cpu}
+            "legs": legs, "autotune": {"block": best, "seconds_per_candidate": tune_s}, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -97,7 +97,8 @@ typedef struct iga_fan_params {
     int write_rays;          /* 1: sum time/absorption per step like the CLI's
                                 write_rays=true path (all segments but the last of
                                 each bounce, main.infraga.3d.cpp:451-453) */
-    int reserved;
+    int block;               /* threads per CTA of the fan launch: 0 = 128, else 32, 64, 96 or 128
+                                (iga_fan_tune picks one by timing the fan) */
     double src[3];           /* 3D: source x, y [km], altitude [km];
                                 SPH: source latitude, longitude [deg], altitude [km] */
     double ds_min, ds_max, s_max;
@@ -205,6 +206,17 @@ int iga_fan_run(iga_atmo_t atmo, const iga_fan_params* params,
                 double* arrivals, int cap, int* n_out, int* ray_index,
                 long long* ray_steps, int* ray_status, long long* total_steps,
                 double* arrival_aux);
+
+/* Launch-shape autotuner (no counterpart in the reference, whose CPU loop has
+ * no launch shape): runs the fan once per candidate CTA size (32, 64, 96 and
+ * 128 threads; after one untimed warm-up run) and returns the fastest in
+ * *best_block, to be passed as params->block to later runs of that fan (or
+ * fans of the same size and kind).  seconds (nullable, 4 doubles) gets each
+ * candidate's device time.  The persistent fan kernels give each resident
+ * thread one ray at a time: small fans leave SMs idle with large CTAs, while
+ * large fans fill the GPU either way. */
+int iga_fan_tune(iga_atmo_t atmo, const iga_fan_params* params, const double* theta_deg, const double* phi_deg,
+                 int n_rays, int* best_block, double* seconds);
 
 /* Bytes of device workspace iga_fan_run_device needs (ray queue counters). */
 size_t iga_fan_workspace_bytes(void);

@@ -5,9 +5,9 @@ the C ABI in include/infraga_gpu.h); this package is a thin host binding.
 """
 from ._lib import (ARRIVAL_COLS, CAUSTIC_COLS, FP32C, FP64, GEOM_3D, GEOM_SPH, PATH_COLS, PATH_RAYS, PATH_TERRAIN,
                    RAY_STATUS, Atmosphere, EigParams, FanParams, IgaError, NativeLibraryError, Server, eig_direct,
-                   eig_params, eig_run, fan_paths, fan_run, fan_run_device, fan_workspace_bytes, lib)
+                   eig_params, eig_run, fan_paths, fan_run, fan_run_device, fan_tune, fan_workspace_bytes, lib)
 
 __all__ = ["ARRIVAL_COLS", "CAUSTIC_COLS", "FP32C", "FP64", "GEOM_3D", "GEOM_SPH", "PATH_COLS", "PATH_RAYS",
            "PATH_TERRAIN", "RAY_STATUS", "Atmosphere", "EigParams", "FanParams", "IgaError", "NativeLibraryError",
-           "Server", "eig_direct", "eig_params", "eig_run", "fan_paths", "fan_run", "fan_run_device",
+           "Server", "eig_direct", "eig_params", "eig_run", "fan_paths", "fan_run", "fan_run_device", "fan_tune",
            "fan_workspace_bytes", "lib"]

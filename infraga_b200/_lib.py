@@ -36,7 +36,7 @@ class FanParams(ctypes.Structure):
     """Mirror of iga_fan_params."""
     _fields_ = [
         ("geometry", ctypes.c_int), ("precision", ctypes.c_int), ("bounces", ctypes.c_int),
-        ("calc_amp", ctypes.c_int), ("write_rays", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("calc_amp", ctypes.c_int), ("write_rays", ctypes.c_int), ("block", ctypes.c_int),
         ("src", ctypes.c_double * 3),
         ("ds_min", ctypes.c_double), ("ds_max", ctypes.c_double), ("s_max", ctypes.c_double),
         ("alt_max", ctypes.c_double), ("rng_max", ctypes.c_double),
@@ -126,6 +126,7 @@ _SIGS = {
     "iga_fan_paths": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _I, _P(_LL), _P(_D), _LL, _P(_LL), _P(_LL),
                            _P(_D), _LL, _P(_LL), _P(_I)]),
     "iga_atmo_terrain": (_I, [_VP, _D, _D, _P(_D), _P(_D), _P(_D)]),
+    "iga_fan_tune": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_I), _P(_D)]),
 }
 
 
@@ -374,6 +375,17 @@ def fan_paths(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, mode: int
             out["caustics"] = crow[:n_caus.value]
             out["caustic_ray"] = cray[:n_caus.value]
         return out
+
+
+def fan_tune(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg):
+    """Times the fan at each candidate CTA size; returns (best block, {block: seconds})."""
+    th = np.ascontiguousarray(theta_deg, dtype=np.float64)
+    ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
+    best = _I()
+    secs = np.zeros(4, dtype=np.float64)
+    _check(lib().iga_fan_tune(atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph), th.size, ctypes.byref(best),
+                              _dptr(secs)), "iga_fan_tune")
+    return int(best.value), dict(zip((32, 64, 96, 128), secs.tolist()))
 
 
 def fan_workspace_bytes() -> int:

@@ -160,6 +160,7 @@ int validate(const iga_fan_params* p, int n_rays) {
     if (!std::isfinite(p->s_max / p->ds_min) || p->s_max / p->ds_min > 2.0e9) return IGA_E_INVALID;
     if (!(p->freq > 0.0) || !(p->tweak_abs >= 0.0)) return IGA_E_INVALID;
     for (int i = 0; i < 3; i++) if (!std::isfinite(p->src[i])) return IGA_E_INVALID;
+    if (p->block != 0 && (p->block < 32 || p->block > 128 || p->block % 32 != 0)) return IGA_E_INVALID;
     return IGA_OK;
 }
 
@@ -411,6 +412,7 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
     a.arrivals = d_arr; a.n_arr = d_n; a.ray_steps = d_steps; a.ray_status = d_status; a.aux = d_aux;
     a.queue = static_cast<unsigned int*>(d_ws);
     a.grid_cap = grid_cap;
+    a.block = p->block;
     if (ps) {
         if (p->precision != IGA_FP64) {
             g_cuda_err = "sampled ray paths: FP64 only";
@@ -652,6 +654,67 @@ int iga_fan_params_init(iga_atmo_t h, int geometry, iga_fan_params* p) {
 }
 
 size_t iga_fan_workspace_bytes(void) { return 256; }
+
+// Launch-shape autotuner: the persistent fan kernels keep every resident
+// thread busy with one ray at a time, so a fan with fewer rays than resident
+// thread slots leaves SMs idle at the kernel's largest CTA size, while
+// smaller CTAs spread the same rays over more SMs (and fit more CTAs per SM
+// where registers limit occupancy).  Which wins depends on the fan (rays,
+// ray lengths, kernel), so each candidate CTA size is timed on the fan itself.
+int iga_fan_tune(iga_atmo_t h, const iga_fan_params* p, const double* theta_deg, const double* phi_deg, int n_rays,
+                 int* best_block, double* seconds) {
+    if (!h || !p || !best_block || n_rays <= 0 || !theta_deg || !phi_deg) return IGA_E_INVALID;
+    int rc = validate(p, n_rays);
+    if (rc) return rc;
+    IGA_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    const int nb = p->bounces + 1;
+    const size_t n = (size_t)n_rays;
+    double *d_th = nullptr, *d_ph = nullptr, *d_arr = nullptr;
+    int* d_n = nullptr;
+    long long* d_steps = nullptr;
+    void* d_ws = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_th); cudaFree(d_ph); cudaFree(d_arr); cudaFree(d_n); cudaFree(d_steps); cudaFree(d_ws);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+    };
+    cudaError_t e = cudaMalloc(&d_th, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_ph, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_arr, n * nb * IGA_ARRIVAL_COLS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_n, n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&d_steps, n * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&d_ws, iga_fan_workspace_bytes());
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_th, theta_deg, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ph, phi_deg, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { cleanup(); return cuda_fail(e, "iga_fan_tune set-up"); }
+    const int cand[4] = {32, 64, 96, 128};
+    double best_t = 1e300;
+    int best = 0;
+    for (int k = -1; k < 4; k++) {   // k = -1: untimed warm-up (module load)
+        iga_fan_params q = *p;
+        q.block = k < 0 ? 0 : cand[k];
+        if ((e = cudaEventRecord(e0, st)) != cudaSuccess) break;
+        rc = run_device(h, &q, d_th, d_ph, n_rays, d_arr, d_n, d_steps, nullptr, nullptr, d_ws, st);
+        if (rc) { cleanup(); return rc; }
+        if ((e = cudaEventRecord(e1, st)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.0f;
+        if ((e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) break;
+        if (k < 0) continue;
+        if (seconds) seconds[k] = 1e-3 * ms;
+        if (1e-3 * ms < best_t) { best_t = 1e-3 * ms; best = cand[k]; }
+    }
+    cleanup();
+    if (e != cudaSuccess) return cuda_fail(e, "iga_fan_tune");
+    *best_block = best;
+    return IGA_OK;
+}
 
 int iga_fan_run_device(iga_atmo_t h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                        double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,

@@ -28,6 +28,8 @@ struct Fan3DArgs {
     double* aux;             // nullable: [n_rays][bounces+1][4] per-arrival diagnostics
     unsigned int* queue;     // [0] next ray (device ray queue)
     int grid_cap;            // > 0: at most this many CTAs (the request server shares the GPU)
+    int block;               // > 0: threads per CTA of the fan launch (a multiple of 32 up to the kernel's
+                             // compiled maximum); 0: that maximum
     // sampled per-step output (run_prop's write_rays / write_topo / write_caustics);
     // all null on the plain fan path
     double* path_rows;       // [path_off[n_rays]][kPathCols]

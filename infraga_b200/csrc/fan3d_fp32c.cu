@@ -149,8 +149,8 @@ template <bool AMP>
 __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = DimF<AMP>::n;
     extern __shared__ float s_memf[];
-    float* s_dprev = s_memf;                       // [N][kThreadsC] previous step's increments
-    float* s_tab = s_memf + N * kThreadsC;         // FP32 knot table
+    float* s_dprev = s_memf;                       // [N][blockDim.x] previous step's increments
+    float* s_tab = s_memf + N * blockDim.x;         // FP32 knot table
     {
         const int tot = a.n_knots * kStrideF;
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots_f[i];
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = z0f;
 #pragma unroll
-        for (int i = 0; i < N; i++) dprev[i * kThreadsC] = 0.0f;
+        for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
     };
     start_ray(ray);
 
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) dprev[i * kThreadsC] = inc[i];
+            for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
 #pragma unroll
             for (int i = 0; i < 4; i++) {   // renormalise the pair
                 const float hh = nh[i] + nl[i];
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
                 const double base = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
                 r1[i] = base;
                 rk[i] = base + (double)inc[i];
-                d1[i] = (double)dprev[i * kThreadsC];
+                d1[i] = (double)dprev[i * blockDim.x];
             }
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
             const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
     constexpr int N = DimF<AMP>::n;
     extern __shared__ float s_memf[];
     float* s_dprev = s_memf;
-    float* s_tab = s_memf + N * kThreadsC;
+    float* s_tab = s_memf + N * blockDim.x;
     {
         const int tot = a.n_knots * kStrideF;
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots_f[i];
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
         int kb = 0;
         bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) dprev[i * kThreadsC] = 0.0f;
+        for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
         while (true) {
             const float zc = y[2] + lo[2];
             if (record && kb >= 1) zmax = fmaxf(zmax, zc);
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
             }
             if (!esc && !gnd) {
 #pragma unroll
-                for (int i = 0; i < N; i++) dprev[i * kThreadsC] = inc[i];
+                for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     const float hh = nh[i] + nl[i];
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
 #pragma unroll
         for (int i = 0; i < N; i++) {
             r1[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
-            d1[i] = (double)dprev[i * kThreadsC];
+            d1[i] = (double)dprev[i * blockDim.x];
         }
         const double dz_grnd = a.z0 - r1[2];
         const double dz_k = d1[2];
@@ -622,22 +622,24 @@ cudaError_t launch_trace_c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* 
 
 template <bool AMP>
 cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    // threads per block: the caller's choice (a multiple of 32 up to kThreadsC) or kThreadsC
+    const int threads = a.block > 0 ? a.block : kThreadsC;
     auto kern = fan3d_fp32c_kernel<AMP>;
-    const size_t smem = (size_t)DimF<AMP>::n * kThreadsC * sizeof(float) + (size_t)a.n_knots * kStrideF * sizeof(float);
+    const size_t smem = (size_t)DimF<AMP>::n * threads * sizeof(float) + (size_t)a.n_knots * kStrideF * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreadsC, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    long long want = ((long long)a.n_rays + kThreadsC - 1) / kThreadsC;
+    long long want = ((long long)a.n_rays + threads - 1) / threads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, kThreadsC, smem, stream>>>(a);
+    kern<<<(unsigned)grid, threads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
     double* s_prev = s_mem;
     const double* tab;
     if (SMEM) {
-        double* s_tab = s_mem + N * kThreads;
+        double* s_tab = s_mem + N * blockDim.x;
         const int tot = a.n_knots * kStride;
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
         __syncthreads();
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
     } else {
         tab = a.knots;
     }
-    double* prev = s_prev + threadIdx.x;   // element i at prev[i * kThreads]
+    double* prev = s_prev + threadIdx.x;   // element i at prev[i * blockDim.x]
 
     const int nb = a.bounces + 1;
     const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
             if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 // row m = kb of the bounce, above the ground: z = max(z, z_g) = z
                 if (p_n < p_cap) {
@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
             // reflection from rows k-2 (prev) and k-1 (y): geoac::approx_intercept
             // and geoac::set_refl (geoac.eqset.3d.strat.cpp:110-209), flat ground
             const double dz_grnd = a.z0 - y[2];
-            const double dz_k = y[2] - prev[2 * kThreads];
+            const double dz_k = y[2] - prev[2 * blockDim.x];
             double p[N];
 #pragma unroll
-            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kThreads]) / dz_k * dz_grnd;
+            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * blockDim.x]) / dz_k * dz_grnd;
             y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
             if (AMP) {
                 y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
@@ -233,23 +233,25 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
 
 template <bool AMP, bool SMEM, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
+    const int threads = a.block > 0 ? a.block : kThreads;
     auto kern = fan3d_fp64_kernel<AMP, SMEM, PATHS>;
-    const size_t smem = (size_t)Dim<AMP>::n * kThreads * sizeof(double) +
+    const size_t smem = (size_t)Dim<AMP>::n * threads * sizeof(double) +
                         (SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    long long want = ((long long)a.n_rays + kThreads - 1) / kThreads;
+    long long want = ((long long)a.n_rays + threads - 1) / threads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, kThreads, smem, stream>>>(a);
+    kern<<<(unsigned)grid, threads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 

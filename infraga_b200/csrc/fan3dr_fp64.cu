@@ -246,10 +246,10 @@ __device__ __noinline__ void reflect_3dr(const Fan3DArgs& a, const Views& vw, Ce
         zy = t.z; dzy[0] = t.d[0]; dzy[1] = t.d[1];
     }
     const double dz_grnd = zy - y[2];
-    const double dz_k = (y[2] - prev[2 * kThreads]) - (y[0] - prev[0]) * dzy[0] - (y[1] - prev[1 * kThreads]) * dzy[1];
+    const double dz_k = (y[2] - prev[2 * blockDim.x]) - (y[0] - prev[0]) * dzy[0] - (y[1] - prev[1 * blockDim.x]) * dzy[1];
     double p[N];
 #pragma unroll
-    for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kThreads]) / dz_k * dz_grnd;
+    for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * blockDim.x]) / dz_k * dz_grnd;
 
     double zg = 0.0, A = 0.0, B = 0.0, zxx = 0.0, zxy = 0.0, zyy = 0.0;
     if (vw.has_topo) {
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
     constexpr int N = Dim3r<AMP>::n;
     extern __shared__ double s_mem[];
     double* s_prev = s_mem;
-    double* s_hz = s_mem + N * kThreads;
+    double* s_hz = s_mem + N * blockDim.x;
     double* s_hx = s_hz + a.hyb_nz;
     double* s_hy = s_hx + a.hyb_nx;
     double* s_tx = s_hy + a.hyb_ny;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
             if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 if (p_n < p_cap) {
                     double* o = a.path_rows + (p_base + p_n) * kPathCols;
@@ -557,23 +557,25 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
 
 template <bool AMP, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
+    const int threads = a.block > 0 ? a.block : kThreads;
     auto kern = fan3dr_fp64_kernel<AMP, PATHS>;
-    const size_t smem = ((size_t)Dim3r<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
+    const size_t smem = ((size_t)Dim3r<AMP>::n * threads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    long long want = ((long long)a.n_rays + kThreads - 1) / kThreads;
+    long long want = ((long long)a.n_rays + threads - 1) / threads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, kThreads, smem, stream>>>(a);
+    kern<<<(unsigned)grid, threads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
     constexpr int N = Dim3r<AMP>::n;
     extern __shared__ double s_mem[];
     double* s_prev = s_mem;
-    double* s_hz = s_mem + N * kThreads;
+    double* s_hz = s_mem + N * blockDim.x;
     double* s_hx = s_hz + a.hyb_nz;
     double* s_hy = s_hx + a.hyb_nx;
     double* s_tx = s_hy + a.hyb_ny;
@@ -629,7 +631,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
         int kb = 0;
         bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) prev[i * kThreads] = y[i];
+        for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
         while (true) {
             if (record && kb >= 1) zmax = fmax(zmax, y[2]);
             double ds = a.ds_max;
@@ -664,7 +666,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
             }
             if (!esc && !gnd) {
 #pragma unroll
-                for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+                for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
                 continue;
             }
             break;

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
     double* s_prev = s_mem;
     const double* tab;
     if (SMEM) {
-        double* s_tab = s_mem + N * kThreads;
+        double* s_tab = s_mem + N * blockDim.x;
         const int tot = a.n_knots * kStride;
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
         __syncthreads();
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
     } else {
         tab = a.knots;
     }
-    double* prev = s_prev + threadIdx.x;   // element i at prev[i * kThreads]
+    double* prev = s_prev + threadIdx.x;   // element i at prev[i * blockDim.x]
 
     const int nb = a.bounces + 1;
     const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
             if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 if (p_n < p_cap) {
                     double* o = a.path_rows + (p_base + p_n) * kPathCols;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
             const double dr_k = y[0] - prev[0];
             double p[N];
 #pragma unroll
-            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kThreads]) / dr_k * dr_grnd;
+            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * blockDim.x]) / dr_k * dr_grnd;
             y[0] = a.r_grnd; y[1] = p[1]; y[2] = p[2];
             y[3] = -p[3]; y[4] = p[4]; y[5] = p[5];
             if (AMP) {
@@ -236,23 +236,25 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
 
 template <bool AMP, bool SMEM, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
+    const int threads = a.block > 0 ? a.block : kThreads;
     auto kern = fansph_fp64_kernel<AMP, SMEM, PATHS>;
-    const size_t smem = (size_t)DimSph<AMP>::n * kThreads * sizeof(double) +
+    const size_t smem = (size_t)DimSph<AMP>::n * threads * sizeof(double) +
                         (SMEM ? (size_t)a.n_knots * kStride * sizeof(double) : 0);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    long long want = ((long long)a.n_rays + kThreads - 1) / kThreads;
+    long long want = ((long long)a.n_rays + threads - 1) / threads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, kThreads, smem, stream>>>(a);
+    kern<<<(unsigned)grid, threads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -288,11 +288,11 @@ __device__ __noinline__ void reflect_sphr(const Fan3DArgs& a, const Views& vw, C
         zy = a.r_earth + t.z; dzy[0] = t.d[0]; dzy[1] = t.d[1];
     }
     const double dr_grnd = zy - y[0];
-    const double dr_k = (y[0] - prev[0]) - (y[1] - prev[1 * kThreads]) * 1.0 / y[0] * dzy[0] -
-                        (y[2] - prev[2 * kThreads]) * 1.0 / (y[0] * cos(y[1])) * dzy[1];
+    const double dr_k = (y[0] - prev[0]) - (y[1] - prev[1 * blockDim.x]) * 1.0 / y[0] * dzy[0] -
+                        (y[2] - prev[2 * blockDim.x]) * 1.0 / (y[0] * cos(y[1])) * dzy[1];
     double p[N];
 #pragma unroll
-    for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kThreads]) / dr_k * dr_grnd;
+    for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * blockDim.x]) / dr_k * dr_grnd;
 
     double rg = a.r_grnd, dz0 = 0.0, dz1 = 0.0, zxx = 0.0, zxy = 0.0, zyy = 0.0;
     if (vw.has_topo) {
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
     extern __shared__ double s_mem[];
     double* s_prev = s_mem;
     // node coordinates in shared memory
-    double* s_hz = s_mem + N * kThreads;
+    double* s_hz = s_mem + N * blockDim.x;
     double* s_hx = s_hz + a.hyb_nz;
     double* s_hy = s_hx + a.hyb_nx;
     double* s_tx = s_hy + a.hyb_ny;
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
     vw.hyb = HybView{a.hyb_tab, s_hx, s_hy, s_hz, a.hyb_nx, a.hyb_ny, a.hyb_nz};
     vw.topo = TopoView{a.topo_tab, s_tx, s_ty, a.topo_nx, a.topo_ny};
     vw.has_topo = a.topo_tab != nullptr;
-    double* prev = s_prev + threadIdx.x;   // element i at prev[i * kThreads]
+    double* prev = s_prev + threadIdx.x;   // element i at prev[i * blockDim.x]
 
     const int nb = a.bounces + 1;
     const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+            for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
             if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 if (p_n < p_cap) {
                     double* o = a.path_rows + (p_base + p_n) * kPathCols;
@@ -581,23 +581,25 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
 
 template <bool AMP, bool PATHS>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
+    // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
+    const int threads = a.block > 0 ? a.block : kThreads;
     auto kern = fansphr_fp64_kernel<AMP, PATHS>;
-    const size_t smem = ((size_t)DimSph<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
+    const size_t smem = ((size_t)DimSph<AMP>::n * threads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    long long want = ((long long)a.n_rays + kThreads - 1) / kThreads;
+    long long want = ((long long)a.n_rays + threads - 1) / threads;
     long long grid = (long long)n_sm * per_sm;
     if (want < grid) grid = want;
     if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
-    kern<<<(unsigned)grid, kThreads, smem, stream>>>(a);
+    kern<<<(unsigned)grid, threads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -621,7 +623,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
     constexpr int N = DimSph<AMP>::n;
     extern __shared__ double s_mem[];
     double* s_prev = s_mem;
-    double* s_hz = s_mem + N * kThreads;
+    double* s_hz = s_mem + N * blockDim.x;
     double* s_hx = s_hz + a.hyb_nz;
     double* s_hy = s_hx + a.hyb_nx;
     double* s_tx = s_hy + a.hyb_ny;
@@ -655,7 +657,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
         int kb = 0;
         bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) prev[i * kThreads] = y[i];
+        for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
         while (true) {
             if (record && kb >= 1) rmax = fmax(rmax, y[0] - a.r_earth);
             double ds = a.ds_max;
@@ -696,7 +698,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
             }
             if (!esc && !gnd) {
 #pragma unroll
-                for (int i = 0; i < N; i++) { prev[i * kThreads] = y[i]; y[i] = acc[i]; }
+                for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
                 continue;
             }
             break;
