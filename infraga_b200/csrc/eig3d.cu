@@ -38,7 +38,7 @@ constexpr int kTraceThreads = 128;
 template <bool AMP>
 __global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                     const TraceReq* __restrict__ reqs,
-                                                                    TraceRes* __restrict__ out, int n,
+                                                                    TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
                                                                     SegRes* __restrict__ seg_out, int seg_stride) {
     constexpr int N = Dim<AMP>::n;
     extern __shared__ double s_mem[];
@@ -48,123 +48,128 @@ __global__ void __launch_bounds__(kTraceThreads) trace3d_fp64_kernel(const __gri
     for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots[i];
     __syncthreads();
     const double* tab = s_tab;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    double* prev = s_prev + threadIdx.x;
-    const TraceReq q = reqs[r];
-    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-    const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
+    // persistent: each thread takes the next request when its trace ends, so
+    // lanes whose trace finished early do not idle until the warp's longest one
+    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
+        double* prev = s_prev + threadIdx.x;
+        const TraceReq q = reqs[r];
+        const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+        const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
 
-    double y[N];
-    RayConst rc;
-    ray_init<AMP>(a, q.theta, q.phi, y, rc);
-    y[0] = q.x0;
-    y[1] = q.y0;
-    int seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-    double tt = 0.0, att = 0.0, zmax = 0.0;
-    long long steps = 0;
-    double acc[N];
-    bool esc = false;
-    for (int sg = 0; sg < q.n_seg; sg++) {
-        double s = 0.0, pt = 0.0, pa = 0.0;
-        int kb = 0;
-        bool capped = false;
+        double y[N];
+        RayConst rc;
+        ray_init<AMP>(a, q.theta, q.phi, y, rc);
+        y[0] = q.x0;
+        y[1] = q.y0;
+        int seg = seg_guess(fmin(fmax(y[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+        double tt = 0.0, att = 0.0, zmax = 0.0;
+        long long steps = 0;
+        double acc[N];
+        bool esc = false;
+        for (int sg = 0; sg < q.n_seg; sg++) {
+            double s = 0.0, pt = 0.0, pa = 0.0;
+            int kb = 0;
+            bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) prev[i * kTraceThreads] = y[i];
-        while (true) {
-            if (record && kb >= 1) zmax = fmax(zmax, y[2]);
-            double ds = a.ds_max;
-            if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - a.z0) / 0.2);
-            s += ds;
-            double stg[N], f[N];
-            rhs<AMP>(tab, a, seg, y, rc, f);
+            for (int i = 0; i < N; i++) prev[i * kTraceThreads] = y[i];
+            while (true) {
+                if (record && kb >= 1) zmax = fmax(zmax, y[2]);
+                double ds = a.ds_max;
+                if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - a.z0) / 0.2);
+                s += ds;
+                double stg[N], f[N];
+                rhs<AMP>(tab, a, seg, y, rc, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-            rhs<AMP>(tab, a, seg, stg, rc, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
+                rhs<AMP>(tab, a, seg, stg, rc, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-            rhs<AMP>(tab, a, seg, stg, rc, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
+                rhs<AMP>(tab, a, seg, stg, rc, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-            rhs<AMP>(tab, a, seg, stg, rc, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
+                rhs<AMP>(tab, a, seg, stg, rc, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
-            kb++;
-            if (record) {
-                double dt, da;
-                seg_increment(tab, a, seg, y, acc, rc, dt, da);
-                tt += pt; att += pa; pt = dt; pa = da;
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+                kb++;
+                if (record) {
+                    double dt, da;
+                    seg_increment(tab, a, seg, y, acc, rc, dt, da);
+                    tt += pt; att += pa; pt = dt; pa = da;
+                }
+                const double rx = acc[0] - q.x0, ry = acc[1] - q.y0;
+                esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) ||
+                      (acc[0] < a.x_min) || (acc[1] > a.y_max) || (acc[1] < a.y_min) || (acc[2] > a.alt_max);
+                const bool gnd = !esc && (acc[2] < a.z0);
+                if (!esc && !gnd) {
+                    if (kb >= a.length - 1) { capped = true; esc = true; }
+                    else if (!isfinite(acc[2]) || !isfinite(acc[3])) esc = true;
+                }
+                if (!esc && !gnd) {
+#pragma unroll
+                    for (int i = 0; i < N; i++) { prev[i * kTraceThreads] = y[i]; y[i] = acc[i]; }
+                    continue;
+                }
+                break;
             }
-            const double rx = acc[0] - q.x0, ry = acc[1] - q.y0;
-            esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) ||
-                  (acc[0] < a.x_min) || (acc[1] > a.y_max) || (acc[1] < a.y_min) || (acc[2] > a.alt_max);
-            const bool gnd = !esc && (acc[2] < a.z0);
-            if (!esc && !gnd) {
-                if (kb >= a.length - 1) { capped = true; esc = true; }
-                else if (!isfinite(acc[2]) || !isfinite(acc[3])) esc = true;
+            steps += capped ? a.length : kb;
+            if (seg_out) {
+                SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+                g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
             }
-            if (!esc && !gnd) {
+            if (sg == q.n_seg - 1 || (esc && stop)) break;
+            // reflection from rows k-2 (prev) and k-1 (y), flat ground
+            const double dz_grnd = a.z0 - y[2];
+            const double dz_k = y[2] - prev[2 * kTraceThreads];
+            double p[N];
 #pragma unroll
-                for (int i = 0; i < N; i++) { prev[i * kTraceThreads] = y[i]; y[i] = acc[i]; }
-                continue;
+            for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kTraceThreads]) / dz_k * dz_grnd;
+            y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
+            if (AMP) {
+                y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
+                y[8] = p[8]; y[9] = p[9]; y[10] = -p[10];
+                const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
+                const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
+                const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + rc.nx * a.duz_g + rc.ny * a.dvz_g);
+                y[7] = -p[7] + (-2.0 * dnuz_ds) * ds0_dth;
+                y[11] = -p[11] + (-2.0 * dnuz_ds) * ds0_dph;
             }
-            break;
         }
-        steps += capped ? a.length : kb;
-        if (seg_out) {
-            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-            g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
-        }
-        if (sg == q.n_seg - 1 || (esc && stop)) break;
-        // reflection from rows k-2 (prev) and k-1 (y), flat ground
-        const double dz_grnd = a.z0 - y[2];
-        const double dz_k = y[2] - prev[2 * kTraceThreads];
-        double p[N];
+        TraceRes& o = out[r];
 #pragma unroll
-        for (int i = 0; i < N; i++) p[i] = y[i] + (y[i] - prev[i * kTraceThreads]) / dz_k * dz_grnd;
-        y[0] = p[0]; y[1] = p[1]; y[2] = a.z0; y[3] = -p[3];
-        if (AMP) {
-            y[4] = p[4]; y[5] = p[5]; y[6] = -p[6];
-            y[8] = p[8]; y[9] = p[9]; y[10] = -p[10];
-            const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
-            const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
-            const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + rc.nx * a.duz_g + rc.ny * a.dvz_g);
-            y[7] = -p[7] + (-2.0 * dnuz_ds) * ds0_dth;
-            y[11] = -p[11] + (-2.0 * dnuz_ds) * ds0_dph;
+        for (int i = 0; i < 12; i++) o.y[i] = i < N ? acc[i] : 0.0;
+        o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
+        o.steps = steps;
+        o.escaped = esc ? 1 : 0;
+        if (record) {
+            o.tt = tt; o.att = att; o.zmax = zmax;
+            o.amp_db = AMP ? amp_db(tab, a, seg, acc, rc, q.theta, q.phi, nullptr) : 0.0;
+            // arrival inclination with c at the (clamped) below-ground altitude,
+            // as find_eigenray writes it (geoac.eigenray.3d.cpp:265)
+            const double ze = fmin(fmax(acc[2], a.z_lo), a.z_hi);
+            seg = seg_walk(tab, a.n_knots, ze, seg);
+            const double* r0 = tab + seg * kStride;
+            const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
+            o.incl = -asin(c_k / a.c0 * acc[3]) * (180.0 / kPi);
+            double baz = 90.0 - atan2(-rc.ny, -rc.nx) * (180.0 / kPi);
+            while (baz > 180.0) baz -= 360.0;
+            while (baz < -180.0) baz += 360.0;
+            o.baz = baz;
         }
-    }
-    TraceRes& o = out[r];
-#pragma unroll
-    for (int i = 0; i < 12; i++) o.y[i] = i < N ? acc[i] : 0.0;
-    o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
-    o.steps = steps;
-    o.escaped = esc ? 1 : 0;
-    if (record) {
-        o.tt = tt; o.att = att; o.zmax = zmax;
-        o.amp_db = AMP ? amp_db(tab, a, seg, acc, rc, q.theta, q.phi, nullptr) : 0.0;
-        // arrival inclination with c at the (clamped) below-ground altitude,
-        // as find_eigenray writes it (geoac.eigenray.3d.cpp:265)
-        const double ze = fmin(fmax(acc[2], a.z_lo), a.z_hi);
-        seg = seg_walk(tab, a.n_knots, ze, seg);
-        const double* r0 = tab + seg * kStride;
-        const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
-        o.incl = -asin(c_k / a.c0 * acc[3]) * (180.0 / kPi);
-        double baz = 90.0 - atan2(-rc.ny, -rc.nx) * (180.0 / kPi);
-        while (baz > 180.0) baz -= 360.0;
-        while (baz < -180.0) baz += 360.0;
-        o.baz = baz;
     }
 }
 
 template <bool AMP>
 cudaError_t launch_trace(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st,
-                         SegRes* seg_out = nullptr, int seg_stride = 0) {
+                         unsigned int* d_queue, SegRes* seg_out = nullptr, int seg_stride = 0) {
     if (n <= 0) return cudaSuccess;
     auto kern = trace3d_fp64_kernel<AMP>;
     const size_t smem = (size_t)Dim<AMP>::n * kTraceThreads * sizeof(double) + (size_t)a.n_knots * kStride * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(n + kTraceThreads - 1) / kTraceThreads, kTraceThreads, smem, st>>>(a, d_req, d_res, n, seg_out, seg_stride);
+    int grid = 0;
+    if ((e = trace_grid(kern, kTraceThreads, smem, n, grid)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    kern<<<grid, kTraceThreads, smem, st>>>(a, d_req, d_res, n, d_queue, seg_out, seg_stride);
     return cudaGetLastError();
 }
 
@@ -578,6 +583,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     unsigned char* d_res = nullptr;   // TraceRes or TraceRes18 records
     const size_t res_bytes = wide ? sizeof(TraceRes18) : sizeof(TraceRes);
     SegRes* d_seg = nullptr;
+    unsigned int* d_q = nullptr;   // request counters of the sweep and the Newton/record launches
     size_t cap_req = 0;
     long long steps_tot = 0;
     const int max_seg = P->bnc_max + 1;
@@ -585,7 +591,8 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (d_req) cudaFreeAsync(d_req, st);
         if (d_res) cudaFreeAsync(d_res, st);
         if (d_seg) cudaFreeAsync(d_seg, st);
-        d_req = nullptr; d_res = nullptr; d_seg = nullptr;
+        if (d_q) cudaFreeAsync(d_q, st);
+        d_req = nullptr; d_res = nullptr; d_seg = nullptr; d_q = nullptr;
     };
     cudaEvent_t round_done = nullptr;
     {
@@ -597,7 +604,9 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     std::vector<TraceReq> req6, req18;
     std::vector<TraceRes> res18;
     std::vector<TraceRes18> res18s;
-    std::vector<SegRes> seg6;
+    std::vector<SegRes> seg6, seg6s;   // per request (request order) / as traced (launch order)
+    std::vector<int> order6;
+    std::vector<TraceReq> sorted6;
     // searches of one pair for different bounce counts sweep the same launch
     // angles until their first bracket: one trace serves them all
     std::map<std::array<double, 4>, int> uniq;
@@ -654,42 +663,53 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
             cudaError_t e1 = cudaMallocAsync(&d_req, 2 * cap_req * sizeof(TraceReq), st);
             cudaError_t e2 = e1 == cudaSuccess ? cudaMallocAsync(&d_res, 2 * cap_req * res_bytes, st) : e1;
             cudaError_t e3 = e2 == cudaSuccess ? cudaMallocAsync(&d_seg, cap_req * max_seg * sizeof(SegRes), st) : e2;
+            if (e3 == cudaSuccess) e3 = cudaMallocAsync(&d_q, 2 * sizeof(unsigned int), st);
             if (e3 != cudaSuccess) return fail(cuda_fail(e3, "cudaMallocAsync(eigen traces)"));
         }
         TraceReq* d_req18 = d_req + cap_req;
         unsigned char* d_res18 = d_res + cap_req * res_bytes;
         cudaError_t e = cudaSuccess;
+        // sweep traces go out longest first (more segments first), so the
+        // persistent kernel's last requests are short ones
+        order6.resize(req6.size());
+        for (size_t i = 0; i < order6.size(); i++) order6[i] = (int)i;
+        std::stable_sort(order6.begin(), order6.end(), [&](int x, int y) { return req6[x].n_seg > req6[y].n_seg; });
+        sorted6.resize(req6.size());
+        for (size_t i = 0; i < order6.size(); i++) sorted6[i] = req6[order6[i]];
         if (!req6.empty()) {
-            e = cudaMemcpyAsync(d_req, req6.data(), req6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
+            e = cudaMemcpyAsync(d_req, sorted6.data(), sorted6.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
                 e = h->kind == 1 ? launch_trace_sphr(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false,
-                                                     st, d_seg, max_seg)
+                                                     st, d_seg, max_seg, d_q)
                     : h->kind == 2 ? launch_trace_3dr(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false,
-                                                      st, d_seg, max_seg)
+                                                      st, d_seg, max_seg, d_q)
                     : sph ? launch_trace_sph(a, d_req, reinterpret_cast<TraceRes18*>(d_res), (int)req6.size(), false, st,
-                                           d_seg, max_seg, c_incl_src)
+                                           d_seg, max_seg, c_incl_src, d_q)
                     : f32 ? launch_trace_fp32c(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), false, st,
-                                               d_seg, max_seg)
-                          : launch_trace<false>(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), st, d_seg,
-                                                max_seg);
+                                               d_q, d_seg, max_seg)
+                          : launch_trace<false>(a, d_req, reinterpret_cast<TraceRes*>(d_res), (int)req6.size(), st, d_q,
+                                                d_seg, max_seg);
         }
         if (e == cudaSuccess && !req18.empty()) {
             e = cudaMemcpyAsync(d_req18, req18.data(), req18.size() * sizeof(TraceReq), cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess)
                 e = h->kind == 1 ? launch_trace_sphr(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(),
-                                                     true, st, nullptr, 0)
+                                                     true, st, nullptr, 0, d_q + 1)
                     : h->kind == 2 ? launch_trace_3dr(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(),
-                                                      true, st, nullptr, 0)
+                                                      true, st, nullptr, 0, d_q + 1)
                     : sph ? launch_trace_sph(a, d_req18, reinterpret_cast<TraceRes18*>(d_res18), (int)req18.size(), true,
-                                           st, nullptr, 0, c_incl_src)
-                    : f32 ? launch_trace_fp32c(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), true, st)
-                          : launch_trace<true>(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), st);
+                                           st, nullptr, 0, c_incl_src, d_q + 1)
+                    : f32 ? launch_trace_fp32c(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), true, st,
+                                               d_q + 1)
+                          : launch_trace<true>(a, d_req18, reinterpret_cast<TraceRes*>(d_res18), (int)req18.size(), st,
+                                               d_q + 1);
         }
         seg6.resize(req6.size() * max_seg);
+        seg6s.resize(req6.size() * max_seg);
         res18.resize(wide ? 0 : req18.size());
         res18s.resize(wide ? req18.size() : 0);
         if (e == cudaSuccess && !req6.empty())
-            e = cudaMemcpyAsync(seg6.data(), d_seg, seg6.size() * sizeof(SegRes), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(seg6s.data(), d_seg, seg6s.size() * sizeof(SegRes), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && !req18.empty())
             e = wide ? cudaMemcpyAsync(res18s.data(), d_res18, res18s.size() * sizeof(TraceRes18), cudaMemcpyDeviceToHost, st)
                     : cudaMemcpyAsync(res18.data(), d_res18, res18.size() * sizeof(TraceRes), cudaMemcpyDeviceToHost, st);
@@ -699,6 +719,8 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         if (e == cudaSuccess) e = cudaEventRecord(round_done, st);
         if (e == cudaSuccess) e = cudaEventSynchronize(round_done);
         if (e != cudaSuccess) return fail(cuda_fail(e, "eigen trace round"));
+        for (size_t i = 0; i < order6.size(); i++)
+            std::copy(&seg6s[i * max_seg], &seg6s[i * max_seg] + max_seg, &seg6[(size_t)order6[i] * max_seg]);
         // each search's view of its sweep traces: the entry of its own
         // segment count, or the earlier entry where the trace escaped
         auto sweep_view = [&](int idx, int m, TraceRes& t) {

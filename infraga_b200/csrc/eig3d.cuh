@@ -2,9 +2,29 @@
 // that serve them: FP64 (eig3d.cu) and FP32-compensated (fan3d_fp32c.cu).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <algorithm>
+
 #include "fan3d.cuh"
 
 namespace iga {
+
+// Grid of a persistent trace launch: every SM filled at the kernel's
+// occupancy, fewer CTAs when the requests do not need them.  The trace
+// kernels take requests from a device counter (queue, zeroed on the stream
+// before the launch), so each thread traces until the requests run out.
+template <class Kern>
+inline cudaError_t trace_grid(Kern kern, int threads, size_t smem, int n, int& grid) {
+    int dev = 0, n_sm = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    const long long want = ((long long)n + threads - 1) / threads;
+    const long long cap = (long long)n_sm * (per_sm > 0 ? per_sm : 1);
+    grid = (int)std::max(1LL, std::min(want, cap));
+    return cudaSuccess;
+}
 
 struct TraceReq {
     double x0, y0;       // source position
@@ -57,18 +77,19 @@ struct TraceRes18 {
 // c_incl_src is the sound speed find_eigenray divides by in its arrival
 // inclination.
 cudaError_t launch_trace_sph(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
-                             cudaStream_t st, SegRes* seg_out, int seg_stride, double c_incl_src);
+                             cudaStream_t st, SegRes* seg_out, int seg_stride, double c_incl_src,
+                             unsigned int* d_queue);
 
 // Range-dependent traces with terrain (fan3dr_fp64.cu, fansphr_fp64.cu): the
 // source is the launch arguments' (all requests of a launch share it).
 cudaError_t launch_trace_3dr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
-                             cudaStream_t st, SegRes* seg_out, int seg_stride);
+                             cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue);
 cudaError_t launch_trace_sphr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
-                              cudaStream_t st, SegRes* seg_out, int seg_stride);
+                              cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue);
 
 // FP32-compensated traces (same contract as the FP64 trace kernel).  With
 // seg_out != null, segment j of request r also writes seg_out[r * seg_stride + j].
 cudaError_t launch_trace_fp32c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, bool amp,
-                               cudaStream_t st, SegRes* seg_out = nullptr, int seg_stride = 0);
+                               cudaStream_t st, unsigned int* d_queue, SegRes* seg_out = nullptr, int seg_stride = 0);
 
 }  // namespace iga

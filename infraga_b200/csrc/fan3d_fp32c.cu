@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
 template <bool AMP>
 __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a,
                                                                  const TraceReq* __restrict__ reqs,
-                                                                 TraceRes* __restrict__ out, int n,
+                                                                 TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
                                                                  SegRes* __restrict__ seg_out, int seg_stride) {
     constexpr int N = DimF<AMP>::n;
     extern __shared__ float s_memf[];
@@ -412,211 +412,216 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
         for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots_f[i];
         __syncthreads();
     }
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    const float* tab = s_tab;
-    float* dprev = s_dprev + threadIdx.x;
-    const TraceReq q = reqs[r];
-    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-    const float z0f = (float)a.z0, inv_blf = (float)a.inv_bl;
-    const float zlo = (float)a.z_lo, zhi = (float)a.z_hi;
-    const float zbl = (float)a.z_bl;
-    const float ds_max = (float)a.ds_max, ds_span = (float)(a.ds_max - a.ds_min);
-    const float tweak = (float)a.tweak_abs;
-    auto set_pair = [](double v, float& h, float& l) { h = (float)v; l = (float)(v - (double)h); };
+    // persistent: each thread takes the next request when its trace ends, so
+    // lanes whose trace finished early do not idle until the warp's longest one
+    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
+        const float* tab = s_tab;
+        float* dprev = s_dprev + threadIdx.x;
+        const TraceReq q = reqs[r];
+        const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+        const float z0f = (float)a.z0, inv_blf = (float)a.inv_bl;
+        const float zlo = (float)a.z_lo, zhi = (float)a.z_hi;
+        const float zbl = (float)a.z_bl;
+        const float ds_max = (float)a.ds_max, ds_span = (float)(a.ds_max - a.ds_min);
+        const float tweak = (float)a.tweak_abs;
+        auto set_pair = [](double v, float& h, float& l) { h = (float)v; l = (float)(v - (double)h); };
 
-    float y[N], lo[4], inc[N];
-    RayConstF rc;
-    {
-        const double theta = q.theta, phi = q.phi;
-        const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
-        const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
-        const double n0x = ct * cp, n0y = ct * sp, n0z = st;
-        const double ms = 1.0 + (n0x * mx + n0y * my);
-        const double ims = 1.0 / ms, ims2 = ims * ims;
-        set_pair(q.x0, y[0], lo[0]);
-        set_pair(q.y0, y[1], lo[1]);
-        set_pair(a.src_z, y[2], lo[2]);
-        set_pair(n0z * ims, y[3], lo[3]);
-        rc.nx = (float)(n0x * ims);
-        rc.ny = (float)(n0y * ims);
-        if (AMP) {
-            const double tx = -st * cp, ty = -st * sp, tz = ct;
-            const double px = -ct * sp, py = ct * cp;
-            const double tm = tx * mx + ty * my, pm = px * mx + py * my;
-            rc.mtx = (float)(tx * ims - n0x * ims2 * tm);
-            rc.mty = (float)(ty * ims - n0y * ims2 * tm);
-            y[7] = (float)(tz * ims - n0z * ims2 * tm);
-            rc.mpx = (float)(px * ims - n0x * ims2 * pm);
-            rc.mpy = (float)(py * ims - n0y * ims2 * pm);
-            y[11] = (float)(-n0z * ims2 * pm);
-            y[4] = y[5] = y[6] = 0.0f;
-            y[8] = y[9] = y[10] = 0.0f;
-        } else {
-            rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0f;
-        }
-    }
-    int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-    double tt = 0.0, att = 0.0;
-    float zmax = 0.0f;
-    long long steps = 0;
-    bool esc = false;
-#pragma unroll
-    for (int i = 0; i < N; i++) inc[i] = 0.0f;
-    for (int sg = 0; sg < q.n_seg; sg++) {
-        double s = 0.0, pt = 0.0, pa = 0.0;
-        int kb = 0;
-        bool capped = false;
-#pragma unroll
-        for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
-        while (true) {
-            const float zc = y[2] + lo[2];
-            if (record && kb >= 1) zmax = fmaxf(zmax, zc);
-            float ds = ds_max;
-            if (zc < zbl) ds -= ds_span * __expf(-(zc - z0f) * 5.0f);
-            s += (double)ds;
-            float stg[N], f[N];
-            rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, y, rc, f);
-#pragma unroll
-            for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] = t * (1.0f / 6.0f); stg[i] = y[i] + t * 0.5f; }
-            rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-            for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t * 0.5f; }
-            rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-            for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t; }
-            rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-            for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 6.0f); }
-            kb++;
-            if (record) {
-                const float seg_ds = sqrtf(inc[0] * inc[0] + inc[1] * inc[1] + inc[2] * inc[2]);
-                const float zm = y[2] + (lo[2] + 0.5f * inc[2]);
-                const float nzm = y[3] + (lo[3] + 0.5f * inc[3]);
-                const float ze = fminf(fmaxf(zm, zlo), zhi);
-                seg = seg_walk_f(tab, a.n_knots, ze, seg);
-                const float* r0 = tab + seg * kStrideF;
-                const CubicF cq = cubic_at_f(r0, ze);
-                const float c = cubicf_f(r0, cq, 2);
-                float sc = 1.0f;
-                if (zm < zbl) { const float X = __expf(-(zm - z0f) * inv_blf); sc = __fdividef(1.0f - X, 1.0f + X); }
-                const float u = cubicf_f(r0, cq, 6) * sc, v = cubicf_f(r0, cq, 10) * sc;
-                const float inum = rsqrtf(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
-                const float cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
-                const float dt = seg_ds * rsqrtf(cgx * cgx + cgy * cgy + cgz * cgz);
-                const float ua = (float)((double)zm - a.alpha_z0) * (float)a.alpha_inv_h;
-                int ia = (int)ua;
-                ia = ia < 0 ? 0 : (ia > a.alpha_n - 2 ? a.alpha_n - 2 : ia);
-                const float w = fminf(fmaxf(ua - (float)ia, 0.0f), 1.0f);
-                const float al0 = __ldg(a.alpha_tab + ia), al1 = __ldg(a.alpha_tab + ia + 1);
-                const float da = (al0 + w * (al1 - al0)) * tweak * seg_ds;
-                tt += pt; att += pa; pt = (double)dt; pa = (double)da;
+        float y[N], lo[4], inc[N];
+        RayConstF rc;
+        {
+            const double theta = q.theta, phi = q.phi;
+            const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
+            const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
+            const double n0x = ct * cp, n0y = ct * sp, n0z = st;
+            const double ms = 1.0 + (n0x * mx + n0y * my);
+            const double ims = 1.0 / ms, ims2 = ims * ims;
+            set_pair(q.x0, y[0], lo[0]);
+            set_pair(q.y0, y[1], lo[1]);
+            set_pair(a.src_z, y[2], lo[2]);
+            set_pair(n0z * ims, y[3], lo[3]);
+            rc.nx = (float)(n0x * ims);
+            rc.ny = (float)(n0y * ims);
+            if (AMP) {
+                const double tx = -st * cp, ty = -st * sp, tz = ct;
+                const double px = -ct * sp, py = ct * cp;
+                const double tm = tx * mx + ty * my, pm = px * mx + py * my;
+                rc.mtx = (float)(tx * ims - n0x * ims2 * tm);
+                rc.mty = (float)(ty * ims - n0y * ims2 * tm);
+                y[7] = (float)(tz * ims - n0z * ims2 * tm);
+                rc.mpx = (float)(px * ims - n0x * ims2 * pm);
+                rc.mpy = (float)(py * ims - n0y * ims2 * pm);
+                y[11] = (float)(-n0z * ims2 * pm);
+                y[4] = y[5] = y[6] = 0.0f;
+                y[8] = y[9] = y[10] = 0.0f;
+            } else {
+                rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0f;
             }
-            float nh[4], nl[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                float e;
-                two_sum(y[i], inc[i], nh[i], e);
-                nl[i] = lo[i] + e;
-            }
-            const float zn = nh[2] + nl[2];
-            const float rx = (nh[0] - (float)q.x0) + nl[0], ry = (nh[1] - (float)q.y0) + nl[1];
-            const float xn = nh[0] + nl[0], yn = nh[1] + nl[1];
-            esc = (s > a.s_max) || (sqrtf(rx * rx + ry * ry) > (float)a.rng_max) || (xn > (float)a.x_max) ||
-                  (xn < (float)a.x_min) || (yn > (float)a.y_max) || (yn < (float)a.y_min) || (zn > (float)a.alt_max);
-            const bool gnd = !esc && ((nh[2] - z0f) + nl[2] < 0.0f);
-            if (!esc && !gnd) {
-                if (kb >= a.length - 1) { capped = true; esc = true; }
-                else if (!isfinite(zn) || !isfinite(nh[3])) esc = true;
-            }
-            if (!esc && !gnd) {
-#pragma unroll
-                for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const float hh = nh[i] + nl[i];
-                    lo[i] = nl[i] - (hh - nh[i]);
-                    y[i] = hh;
-                }
-#pragma unroll
-                for (int i = 4; i < N; i++) y[i] += inc[i];
-                continue;
-            }
-            break;
         }
-        steps += capped ? a.length : kb;
-        if (seg_out) {
-            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-            g.x = (double)y[0] + (double)lo[0] + (double)inc[0];
-            g.y = (double)y[1] + (double)lo[1] + (double)inc[1];
-            g.steps = steps;
-            g.escaped = esc ? 1 : 0;
-        }
-        if (sg == q.n_seg - 1 || (esc && stop)) break;
-        // approx_intercept + flat-ground set_refl in FP64 from rows k-1 and k-2
-        double r1[12], d1[12], p[12];
-#pragma unroll
-        for (int i = 0; i < N; i++) {
-            r1[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
-            d1[i] = (double)dprev[i * blockDim.x];
-        }
-        const double dz_grnd = a.z0 - r1[2];
-        const double dz_k = d1[2];
-#pragma unroll
-        for (int i = 0; i < N; i++) p[i] = r1[i] + d1[i] / dz_k * dz_grnd;
-        set_pair(p[0], y[0], lo[0]);
-        set_pair(p[1], y[1], lo[1]);
-        set_pair(a.z0, y[2], lo[2]);
-        set_pair(-p[3], y[3], lo[3]);
-        if (AMP) {
-            y[4] = (float)p[4]; y[5] = (float)p[5]; y[6] = (float)(-p[6]);
-            y[8] = (float)p[8]; y[9] = (float)p[9]; y[10] = (float)(-p[10]);
-            const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
-            const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
-            const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + (double)rc.nx * a.duz_g + (double)rc.ny * a.dvz_g);
-            y[7] = (float)(-p[7] + (-2.0 * dnuz_ds) * ds0_dth);
-            y[11] = (float)(-p[11] + (-2.0 * dnuz_ds) * ds0_dph);
-        }
+        int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+        double tt = 0.0, att = 0.0;
+        float zmax = 0.0f;
+        long long steps = 0;
+        bool esc = false;
 #pragma unroll
         for (int i = 0; i < N; i++) inc[i] = 0.0f;
-    }
-    double rk[12];
+        for (int sg = 0; sg < q.n_seg; sg++) {
+            double s = 0.0, pt = 0.0, pa = 0.0;
+            int kb = 0;
+            bool capped = false;
 #pragma unroll
-    for (int i = 0; i < 12; i++) rk[i] = 0.0;
+            for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
+            while (true) {
+                const float zc = y[2] + lo[2];
+                if (record && kb >= 1) zmax = fmaxf(zmax, zc);
+                float ds = ds_max;
+                if (zc < zbl) ds -= ds_span * __expf(-(zc - z0f) * 5.0f);
+                s += (double)ds;
+                float stg[N], f[N];
+                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, y, rc, f);
 #pragma unroll
-    for (int i = 0; i < N; i++) rk[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0) + (double)inc[i];
-    TraceRes& o = out[r];
+                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] = t * (1.0f / 6.0f); stg[i] = y[i] + t * 0.5f; }
+                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
 #pragma unroll
-    for (int i = 0; i < 12; i++) o.y[i] = rk[i];
-    o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
-    o.steps = steps;
-    o.escaped = esc ? 1 : 0;
-    if (record) {
-        o.tt = tt; o.att = att; o.zmax = (double)zmax;
-        RayConst rcd{(double)rc.nx, (double)rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
-        int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-        o.amp_db = AMP ? amp_db(a.knots, a, segd, rk, rcd, q.theta, q.phi, nullptr) : 0.0;
-        const double ze = fmin(fmax(rk[2], a.z_lo), a.z_hi);
-        segd = seg_walk(a.knots, a.n_knots, ze, segd);
-        const double* r0 = a.knots + segd * kStride;
-        const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
-        o.incl = -asin(c_k / a.c0 * rk[3]) * (180.0 / kPi);
-        double baz = 90.0 - atan2(-rcd.ny, -rcd.nx) * (180.0 / kPi);
-        while (baz > 180.0) baz -= 360.0;
-        while (baz < -180.0) baz += 360.0;
-        o.baz = baz;
+                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t * 0.5f; }
+                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
+#pragma unroll
+                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t; }
+                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
+#pragma unroll
+                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 6.0f); }
+                kb++;
+                if (record) {
+                    const float seg_ds = sqrtf(inc[0] * inc[0] + inc[1] * inc[1] + inc[2] * inc[2]);
+                    const float zm = y[2] + (lo[2] + 0.5f * inc[2]);
+                    const float nzm = y[3] + (lo[3] + 0.5f * inc[3]);
+                    const float ze = fminf(fmaxf(zm, zlo), zhi);
+                    seg = seg_walk_f(tab, a.n_knots, ze, seg);
+                    const float* r0 = tab + seg * kStrideF;
+                    const CubicF cq = cubic_at_f(r0, ze);
+                    const float c = cubicf_f(r0, cq, 2);
+                    float sc = 1.0f;
+                    if (zm < zbl) { const float X = __expf(-(zm - z0f) * inv_blf); sc = __fdividef(1.0f - X, 1.0f + X); }
+                    const float u = cubicf_f(r0, cq, 6) * sc, v = cubicf_f(r0, cq, 10) * sc;
+                    const float inum = rsqrtf(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
+                    const float cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
+                    const float dt = seg_ds * rsqrtf(cgx * cgx + cgy * cgy + cgz * cgz);
+                    const float ua = (float)((double)zm - a.alpha_z0) * (float)a.alpha_inv_h;
+                    int ia = (int)ua;
+                    ia = ia < 0 ? 0 : (ia > a.alpha_n - 2 ? a.alpha_n - 2 : ia);
+                    const float w = fminf(fmaxf(ua - (float)ia, 0.0f), 1.0f);
+                    const float al0 = __ldg(a.alpha_tab + ia), al1 = __ldg(a.alpha_tab + ia + 1);
+                    const float da = (al0 + w * (al1 - al0)) * tweak * seg_ds;
+                    tt += pt; att += pa; pt = (double)dt; pa = (double)da;
+                }
+                float nh[4], nl[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    float e;
+                    two_sum(y[i], inc[i], nh[i], e);
+                    nl[i] = lo[i] + e;
+                }
+                const float zn = nh[2] + nl[2];
+                const float rx = (nh[0] - (float)q.x0) + nl[0], ry = (nh[1] - (float)q.y0) + nl[1];
+                const float xn = nh[0] + nl[0], yn = nh[1] + nl[1];
+                esc = (s > a.s_max) || (sqrtf(rx * rx + ry * ry) > (float)a.rng_max) || (xn > (float)a.x_max) ||
+                      (xn < (float)a.x_min) || (yn > (float)a.y_max) || (yn < (float)a.y_min) || (zn > (float)a.alt_max);
+                const bool gnd = !esc && ((nh[2] - z0f) + nl[2] < 0.0f);
+                if (!esc && !gnd) {
+                    if (kb >= a.length - 1) { capped = true; esc = true; }
+                    else if (!isfinite(zn) || !isfinite(nh[3])) esc = true;
+                }
+                if (!esc && !gnd) {
+#pragma unroll
+                    for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float hh = nh[i] + nl[i];
+                        lo[i] = nl[i] - (hh - nh[i]);
+                        y[i] = hh;
+                    }
+#pragma unroll
+                    for (int i = 4; i < N; i++) y[i] += inc[i];
+                    continue;
+                }
+                break;
+            }
+            steps += capped ? a.length : kb;
+            if (seg_out) {
+                SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+                g.x = (double)y[0] + (double)lo[0] + (double)inc[0];
+                g.y = (double)y[1] + (double)lo[1] + (double)inc[1];
+                g.steps = steps;
+                g.escaped = esc ? 1 : 0;
+            }
+            if (sg == q.n_seg - 1 || (esc && stop)) break;
+            // approx_intercept + flat-ground set_refl in FP64 from rows k-1 and k-2
+            double r1[12], d1[12], p[12];
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                r1[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
+                d1[i] = (double)dprev[i * blockDim.x];
+            }
+            const double dz_grnd = a.z0 - r1[2];
+            const double dz_k = d1[2];
+#pragma unroll
+            for (int i = 0; i < N; i++) p[i] = r1[i] + d1[i] / dz_k * dz_grnd;
+            set_pair(p[0], y[0], lo[0]);
+            set_pair(p[1], y[1], lo[1]);
+            set_pair(a.z0, y[2], lo[2]);
+            set_pair(-p[3], y[3], lo[3]);
+            if (AMP) {
+                y[4] = (float)p[4]; y[5] = (float)p[5]; y[6] = (float)(-p[6]);
+                y[8] = (float)p[8]; y[9] = (float)p[9]; y[10] = (float)(-p[10]);
+                const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
+                const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
+                const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + (double)rc.nx * a.duz_g + (double)rc.ny * a.dvz_g);
+                y[7] = (float)(-p[7] + (-2.0 * dnuz_ds) * ds0_dth);
+                y[11] = (float)(-p[11] + (-2.0 * dnuz_ds) * ds0_dph);
+            }
+#pragma unroll
+            for (int i = 0; i < N; i++) inc[i] = 0.0f;
+        }
+        double rk[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) rk[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < N; i++) rk[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0) + (double)inc[i];
+        TraceRes& o = out[r];
+#pragma unroll
+        for (int i = 0; i < 12; i++) o.y[i] = rk[i];
+        o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
+        o.steps = steps;
+        o.escaped = esc ? 1 : 0;
+        if (record) {
+            o.tt = tt; o.att = att; o.zmax = (double)zmax;
+            RayConst rcd{(double)rc.nx, (double)rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
+            int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+            o.amp_db = AMP ? amp_db(a.knots, a, segd, rk, rcd, q.theta, q.phi, nullptr) : 0.0;
+            const double ze = fmin(fmax(rk[2], a.z_lo), a.z_hi);
+            segd = seg_walk(a.knots, a.n_knots, ze, segd);
+            const double* r0 = a.knots + segd * kStride;
+            const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
+            o.incl = -asin(c_k / a.c0 * rk[3]) * (180.0 / kPi);
+            double baz = 90.0 - atan2(-rcd.ny, -rcd.nx) * (180.0 / kPi);
+            while (baz > 180.0) baz -= 360.0;
+            while (baz < -180.0) baz += 360.0;
+            o.baz = baz;
+        }
     }
 }
 
 template <bool AMP>
 cudaError_t launch_trace_c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st,
-                           SegRes* seg_out, int seg_stride) {
+                           SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
     auto kern = trace3d_fp32c_kernel<AMP>;
     const size_t smem = (size_t)DimF<AMP>::n * kThreadsC * sizeof(float) + (size_t)a.n_knots * kStrideF * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(n + kThreadsC - 1) / kThreadsC, kThreadsC, smem, st>>>(a, d_req, d_res, n, seg_out, seg_stride);
+    int grid = 0;
+    if ((e = trace_grid(kern, kThreadsC, smem, n, grid)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    kern<<<grid, kThreadsC, smem, st>>>(a, d_req, d_res, n, d_queue, seg_out, seg_stride);
     return cudaGetLastError();
 }
 
@@ -650,9 +655,9 @@ cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t s
 }
 
 cudaError_t launch_trace_fp32c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, bool amp,
-                               cudaStream_t st, SegRes* seg_out, int seg_stride) {
-    return amp ? launch_trace_c<true>(a, d_req, d_res, n, st, seg_out, seg_stride)
-               : launch_trace_c<false>(a, d_req, d_res, n, st, seg_out, seg_stride);
+                               cudaStream_t st, unsigned int* d_queue, SegRes* seg_out, int seg_stride) {
+    return amp ? launch_trace_c<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_c<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga

@@ -591,7 +591,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 template <bool AMP>
 __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                             const TraceReq* __restrict__ reqs,
-                                                                            TraceRes18* __restrict__ out, int n,
+                                                                            TraceRes18* __restrict__ out, int n, unsigned int* __restrict__ queue,
                                                                             SegRes* __restrict__ seg_out,
                                                                             int seg_stride) {
     constexpr int N = Dim3r<AMP>::n;
@@ -608,119 +608,124 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
     for (int i = threadIdx.x; i < a.topo_nx; i += blockDim.x) s_tx[i] = a.topo_x[i];
     for (int i = threadIdx.x; i < a.topo_ny; i += blockDim.x) s_ty[i] = a.topo_y[i];
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    Views vw;
-    vw.hyb = HybView{a.hyb_tab, s_hx, s_hy, s_hz, a.hyb_nx, a.hyb_ny, a.hyb_nz};
-    vw.topo = TopoView{a.topo_tab, s_tx, s_ty, a.topo_nx, a.topo_ny};
-    vw.has_topo = a.topo_tab != nullptr;
-    double* prev = s_prev + threadIdx.x;
-    const TraceReq q = reqs[r];
-    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-    const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
+    // persistent: each thread takes the next request when its trace ends, so
+    // lanes whose trace finished early do not idle until the warp's longest one
+    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
+        Views vw;
+        vw.hyb = HybView{a.hyb_tab, s_hx, s_hy, s_hz, a.hyb_nx, a.hyb_ny, a.hyb_nz};
+        vw.topo = TopoView{a.topo_tab, s_tx, s_ty, a.topo_nx, a.topo_ny};
+        vw.has_topo = a.topo_tab != nullptr;
+        double* prev = s_prev + threadIdx.x;
+        const TraceReq q = reqs[r];
+        const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+        const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
 
-    double y[N];
-    Cells cl{0, 0, 0, 0, 0};
-    ray_init_3dr<AMP>(a, q.theta, q.phi, y);
-    double tt = 0.0, att = 0.0, zmax = 0.0;
-    long long steps = 0;
-    double acc[N];
-    bool esc = false;
-    for (int sg = 0; sg < q.n_seg; sg++) {
-        double s = 0.0, pt = 0.0, pa = 0.0;
-        int kb = 0;
-        bool capped = false;
+        double y[N];
+        Cells cl{0, 0, 0, 0, 0};
+        ray_init_3dr<AMP>(a, q.theta, q.phi, y);
+        double tt = 0.0, att = 0.0, zmax = 0.0;
+        long long steps = 0;
+        double acc[N];
+        bool esc = false;
+        for (int sg = 0; sg < q.n_seg; sg++) {
+            double s = 0.0, pt = 0.0, pa = 0.0;
+            int kb = 0;
+            bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
-        while (true) {
-            if (record && kb >= 1) zmax = fmax(zmax, y[2]);
-            double ds = a.ds_max;
-            if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - topo_z(vw, cl, y[0], y[1])) / 0.2);
-            s += ds;
-            double stg[N], f[N];
-            rhs_3dr<AMP>(a, vw, cl, y, f);
+            for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
+            while (true) {
+                if (record && kb >= 1) zmax = fmax(zmax, y[2]);
+                double ds = a.ds_max;
+                if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - topo_z(vw, cl, y[0], y[1])) / 0.2);
+                s += ds;
+                double stg[N], f[N];
+                rhs_3dr<AMP>(a, vw, cl, y, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-            rhs_3dr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
+                rhs_3dr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-            rhs_3dr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
+                rhs_3dr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-            rhs_3dr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
+                rhs_3dr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
-            kb++;
-            const double rx = acc[0] - a.src_x, ry = acc[1] - a.src_y;
-            esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) || (acc[0] < a.x_min) ||
-                  (acc[1] > a.y_max) || (acc[1] < a.y_min) || (acc[2] > a.alt_max);
-            const bool gnd = !esc && (acc[2] <= a.topo_zmax) && (acc[2] < topo_z(vw, cl, acc[0], acc[1]));
-            if (record) {
-                double dt, da;
-                seg_increment_3dr(a, vw, cl, y, acc, dt, da);
-                tt += pt; att += pa; pt = dt; pa = da;
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+                kb++;
+                const double rx = acc[0] - a.src_x, ry = acc[1] - a.src_y;
+                esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) || (acc[0] < a.x_min) ||
+                      (acc[1] > a.y_max) || (acc[1] < a.y_min) || (acc[2] > a.alt_max);
+                const bool gnd = !esc && (acc[2] <= a.topo_zmax) && (acc[2] < topo_z(vw, cl, acc[0], acc[1]));
+                if (record) {
+                    double dt, da;
+                    seg_increment_3dr(a, vw, cl, y, acc, dt, da);
+                    tt += pt; att += pa; pt = dt; pa = da;
+                }
+                if (!esc && !gnd) {
+                    if (kb >= a.length - 1) { capped = true; esc = true; }
+                    else if (!isfinite(acc[2]) || !isfinite(acc[5])) esc = true;
+                }
+                if (!esc && !gnd) {
+#pragma unroll
+                    for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
+                    continue;
+                }
+                break;
             }
-            if (!esc && !gnd) {
-                if (kb >= a.length - 1) { capped = true; esc = true; }
-                else if (!isfinite(acc[2]) || !isfinite(acc[5])) esc = true;
+            steps += capped ? a.length : kb;
+            if (seg_out) {
+                SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+                g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
             }
-            if (!esc && !gnd) {
+            if (sg == q.n_seg - 1 || (esc && stop)) break;
+            reflect_3dr<N, AMP>(a, vw, cl, y, prev);
+        }
+        TraceRes18& o = out[r];
 #pragma unroll
-                for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
-                continue;
+        for (int i = 0; i < 18; i++) o.y[i] = i < N ? acc[i] : 0.0;
+        o.steps = steps;
+        o.escaped = esc ? 1 : 0;
+        o.tt = o.att = o.zmax = o.amp_db = o.incl = o.baz = 0.0;
+        o.c_src = a.c0; o.c_grnd = 0.0; o.z_grnd = 0.0; o.dzg[0] = 0.0; o.dzg[1] = 0.0;
+        if (AMP && !record) {   // ground under the last row: topo::z (0 without terrain), topo::dz, atmo::c there
+            double zg = 0.0;
+            if (vw.has_topo) {
+                TopoVal t;
+                topo_eval(vw.topo, acc[0], acc[1], 1, t, cl.tx, cl.ty);
+                zg = t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
             }
-            break;
+            AtmPt m;
+            atm_point(a, vw, cl, acc[0], acc[1], zg, m);
+            o.z_grnd = zg;
+            o.c_grnd = m.c;
         }
-        steps += capped ? a.length : kb;
-        if (seg_out) {
-            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-            g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
+        if (record) {
+            o.tt = tt; o.att = att; o.zmax = zmax;
+            o.amp_db = AMP ? amp_db_3dr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
+            AtmPt m;
+            atm_point(a, vw, cl, acc[0], acc[1], acc[2], m);
+            o.incl = -asin(m.c / a.c0 * acc[5]) * (180.0 / kPi);
+            double baz = 90.0 - atan2(-acc[4], -acc[3]) * (180.0 / kPi);
+            while (baz > 180.0) baz -= 360.0;
+            while (baz < -180.0) baz += 360.0;
+            o.baz = baz;
         }
-        if (sg == q.n_seg - 1 || (esc && stop)) break;
-        reflect_3dr<N, AMP>(a, vw, cl, y, prev);
-    }
-    TraceRes18& o = out[r];
-#pragma unroll
-    for (int i = 0; i < 18; i++) o.y[i] = i < N ? acc[i] : 0.0;
-    o.steps = steps;
-    o.escaped = esc ? 1 : 0;
-    o.tt = o.att = o.zmax = o.amp_db = o.incl = o.baz = 0.0;
-    o.c_src = a.c0; o.c_grnd = 0.0; o.z_grnd = 0.0; o.dzg[0] = 0.0; o.dzg[1] = 0.0;
-    if (AMP && !record) {   // ground under the last row: topo::z (0 without terrain), topo::dz, atmo::c there
-        double zg = 0.0;
-        if (vw.has_topo) {
-            TopoVal t;
-            topo_eval(vw.topo, acc[0], acc[1], 1, t, cl.tx, cl.ty);
-            zg = t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
-        }
-        AtmPt m;
-        atm_point(a, vw, cl, acc[0], acc[1], zg, m);
-        o.z_grnd = zg;
-        o.c_grnd = m.c;
-    }
-    if (record) {
-        o.tt = tt; o.att = att; o.zmax = zmax;
-        o.amp_db = AMP ? amp_db_3dr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
-        AtmPt m;
-        atm_point(a, vw, cl, acc[0], acc[1], acc[2], m);
-        o.incl = -asin(m.c / a.c0 * acc[5]) * (180.0 / kPi);
-        double baz = 90.0 - atan2(-acc[4], -acc[3]) * (180.0 / kPi);
-        while (baz > 180.0) baz -= 360.0;
-        while (baz < -180.0) baz += 360.0;
-        o.baz = baz;
     }
 }
 
 template <bool AMP>
 cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, cudaStream_t st,
-                              SegRes* seg_out, int seg_stride) {
+                              SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
     auto kern = trace3dr_fp64_kernel<AMP>;
     const size_t smem = ((size_t)Dim3r<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(n + kThreads - 1) / kThreads, kThreads, smem, st>>>(a, d_req, d_res, n, seg_out, seg_stride);
+    int grid = 0;
+    if ((e = trace_grid(kern, kThreads, smem, n, grid)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    kern<<<grid, kThreads, smem, st>>>(a, d_req, d_res, n, d_queue, seg_out, seg_stride);
     return cudaGetLastError();
 }
 
@@ -733,9 +738,9 @@ cudaError_t launch_fan3dr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t s
 }
 
 cudaError_t launch_trace_3dr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
-                             cudaStream_t st, SegRes* seg_out, int seg_stride) {
-    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride)
-               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride);
+                             cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
+    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga

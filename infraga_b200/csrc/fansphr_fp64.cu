@@ -617,7 +617,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 template <bool AMP>
 __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                               const TraceReq* __restrict__ reqs,
-                                                                              TraceRes18* __restrict__ out, int n,
+                                                                              TraceRes18* __restrict__ out, int n, unsigned int* __restrict__ queue,
                                                                               SegRes* __restrict__ seg_out,
                                                                               int seg_stride) {
     constexpr int N = DimSph<AMP>::n;
@@ -634,128 +634,133 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
     for (int i = threadIdx.x; i < a.topo_nx; i += blockDim.x) s_tx[i] = a.topo_x[i];
     for (int i = threadIdx.x; i < a.topo_ny; i += blockDim.x) s_ty[i] = a.topo_y[i];
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    Views vw;
-    vw.hyb = HybView{a.hyb_tab, s_hx, s_hy, s_hz, a.hyb_nx, a.hyb_ny, a.hyb_nz};
-    vw.topo = TopoView{a.topo_tab, s_tx, s_ty, a.topo_nx, a.topo_ny};
-    vw.has_topo = a.topo_tab != nullptr;
-    double* prev = s_prev + threadIdx.x;
-    const TraceReq q = reqs[r];
-    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-    const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
+    // persistent: each thread takes the next request when its trace ends, so
+    // lanes whose trace finished early do not idle until the warp's longest one
+    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
+        Views vw;
+        vw.hyb = HybView{a.hyb_tab, s_hx, s_hy, s_hz, a.hyb_nx, a.hyb_ny, a.hyb_nz};
+        vw.topo = TopoView{a.topo_tab, s_tx, s_ty, a.topo_nx, a.topo_ny};
+        vw.has_topo = a.topo_tab != nullptr;
+        double* prev = s_prev + threadIdx.x;
+        const TraceReq q = reqs[r];
+        const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+        const double c_third = 1.0 / 3.0, c_sixth = 1.0 / 6.0;
 
-    double y[N];
-    Cells cl{0, 0, 0, 0, 0};
-    ray_init_sph<AMP>(a, q.theta, q.phi, y);
-    double tt = 0.0, att = 0.0, rmax = 0.0;
-    long long steps = 0;
-    double acc[N];
-    bool esc = false;
-    for (int sg = 0; sg < q.n_seg; sg++) {
-        double s = 0.0, pt = 0.0, pa = 0.0;
-        int kb = 0;
-        bool capped = false;
+        double y[N];
+        Cells cl{0, 0, 0, 0, 0};
+        ray_init_sph<AMP>(a, q.theta, q.phi, y);
+        double tt = 0.0, att = 0.0, rmax = 0.0;
+        long long steps = 0;
+        double acc[N];
+        bool esc = false;
+        for (int sg = 0; sg < q.n_seg; sg++) {
+            double s = 0.0, pt = 0.0, pa = 0.0;
+            int kb = 0;
+            bool capped = false;
 #pragma unroll
-        for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
-        while (true) {
-            if (record && kb >= 1) rmax = fmax(rmax, y[0] - a.r_earth);
-            double ds = a.ds_max;
-            if (y[0] - a.r_earth < a.z_bl)
-                ds -= (a.ds_max - a.ds_min) * exp(-(y[0] - topo_r(a, vw, cl, y[1], y[2])) / 0.2);
-            s += ds;
-            double stg[N], f[N];
-            rhs_sphr<AMP>(a, vw, cl, y, f);
+            for (int i = 0; i < N; i++) prev[i * blockDim.x] = y[i];
+            while (true) {
+                if (record && kb >= 1) rmax = fmax(rmax, y[0] - a.r_earth);
+                double ds = a.ds_max;
+                if (y[0] - a.r_earth < a.z_bl)
+                    ds -= (a.ds_max - a.ds_min) * exp(-(y[0] - topo_r(a, vw, cl, y[1], y[2])) / 0.2);
+                s += ds;
+                double stg[N], f[N];
+                rhs_sphr<AMP>(a, vw, cl, y, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-            rhs_sphr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
+                rhs_sphr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-            rhs_sphr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
+                rhs_sphr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-            rhs_sphr<AMP>(a, vw, cl, stg, f);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
+                rhs_sphr<AMP>(a, vw, cl, stg, f);
 #pragma unroll
-            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
-            kb++;
-            esc = s > a.s_max;
-            if (!esc) {
-                if (acc[2] > kPi) acc[2] -= 2.0 * kPi;
-                else if (acc[2] < -kPi) acc[2] += 2.0 * kPi;
-                esc = (acc[1] < -kPi / 2.0 || acc[1] > kPi / 2.0) || (acc[0] - a.r_earth > a.alt_max) ||
-                      beyond_range(a, acc[1], acc[2]) || (acc[1] < a.lat_min || acc[1] > a.lat_max) ||
-                      (acc[2] < a.lon_min || acc[2] > a.lon_max);
+                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+                kb++;
+                esc = s > a.s_max;
+                if (!esc) {
+                    if (acc[2] > kPi) acc[2] -= 2.0 * kPi;
+                    else if (acc[2] < -kPi) acc[2] += 2.0 * kPi;
+                    esc = (acc[1] < -kPi / 2.0 || acc[1] > kPi / 2.0) || (acc[0] - a.r_earth > a.alt_max) ||
+                          beyond_range(a, acc[1], acc[2]) || (acc[1] < a.lat_min || acc[1] > a.lat_max) ||
+                          (acc[2] < a.lon_min || acc[2] > a.lon_max);
+                }
+                const bool gnd = !esc && (acc[0] - a.r_earth <= a.topo_zmax) && (acc[0] < topo_r(a, vw, cl, acc[1], acc[2]));
+                if (record) {
+                    double dt, da;
+                    seg_increment_sphr(a, vw, cl, y, acc, dt, da);
+                    tt += pt; att += pa; pt = dt; pa = da;
+                }
+                if (!esc && !gnd) {
+                    if (kb >= a.length - 1) { capped = true; esc = true; }
+                    else if (!isfinite(acc[0]) || !isfinite(acc[1]) || !isfinite(acc[3])) esc = true;
+                }
+                if (!esc && !gnd) {
+#pragma unroll
+                    for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
+                    continue;
+                }
+                break;
             }
-            const bool gnd = !esc && (acc[0] - a.r_earth <= a.topo_zmax) && (acc[0] < topo_r(a, vw, cl, acc[1], acc[2]));
-            if (record) {
-                double dt, da;
-                seg_increment_sphr(a, vw, cl, y, acc, dt, da);
-                tt += pt; att += pa; pt = dt; pa = da;
+            steps += capped ? a.length : kb;
+            if (seg_out) {
+                SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+                g.x = acc[1]; g.y = acc[2]; g.steps = steps; g.escaped = esc ? 1 : 0;
             }
-            if (!esc && !gnd) {
-                if (kb >= a.length - 1) { capped = true; esc = true; }
-                else if (!isfinite(acc[0]) || !isfinite(acc[1]) || !isfinite(acc[3])) esc = true;
-            }
-            if (!esc && !gnd) {
-#pragma unroll
-                for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
-                continue;
-            }
-            break;
+            if (sg == q.n_seg - 1 || (esc && stop)) break;
+            reflect_sphr<N, AMP>(a, vw, cl, y, prev);
         }
-        steps += capped ? a.length : kb;
-        if (seg_out) {
-            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-            g.x = acc[1]; g.y = acc[2]; g.steps = steps; g.escaped = esc ? 1 : 0;
-        }
-        if (sg == q.n_seg - 1 || (esc && stop)) break;
-        reflect_sphr<N, AMP>(a, vw, cl, y, prev);
-    }
-    TraceRes18& o = out[r];
+        TraceRes18& o = out[r];
 #pragma unroll
-    for (int i = 0; i < 18; i++) o.y[i] = i < N ? acc[i] : 0.0;
-    o.steps = steps;
-    o.escaped = esc ? 1 : 0;
-    o.tt = o.att = o.zmax = o.amp_db = o.incl = o.baz = 0.0;
-    o.c_src = a.c0; o.c_grnd = 0.0; o.z_grnd = 0.0; o.dzg[0] = 0.0; o.dzg[1] = 0.0;
-    if (AMP && !record) {   // topo::z (a radius), topo::dz and atmo::c on the ground under the last row
-        double rg = a.r_grnd;
-        if (vw.has_topo) {
-            TopoVal t;
-            topo_eval(vw.topo, acc[1], acc[2], 1, t, cl.tx, cl.ty);
-            rg = a.r_earth + t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
+        for (int i = 0; i < 18; i++) o.y[i] = i < N ? acc[i] : 0.0;
+        o.steps = steps;
+        o.escaped = esc ? 1 : 0;
+        o.tt = o.att = o.zmax = o.amp_db = o.incl = o.baz = 0.0;
+        o.c_src = a.c0; o.c_grnd = 0.0; o.z_grnd = 0.0; o.dzg[0] = 0.0; o.dzg[1] = 0.0;
+        if (AMP && !record) {   // topo::z (a radius), topo::dz and atmo::c on the ground under the last row
+            double rg = a.r_grnd;
+            if (vw.has_topo) {
+                TopoVal t;
+                topo_eval(vw.topo, acc[1], acc[2], 1, t, cl.tx, cl.ty);
+                rg = a.r_earth + t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
+            }
+            HybLoc L;
+            hyb_locate(vw.hyb, acc[1], acc[2], rg - a.r_earth, L, cl.hx, cl.hy, cl.hz);
+            o.z_grnd = rg;
+            o.c_grnd = hyb_f(vw.hyb, L, 0);
         }
-        HybLoc L;
-        hyb_locate(vw.hyb, acc[1], acc[2], rg - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-        o.z_grnd = rg;
-        o.c_grnd = hyb_f(vw.hyb, L, 0);
-    }
-    if (record) {
-        o.tt = tt; o.att = att; o.zmax = rmax;
-        o.amp_db = AMP ? amp_db_sphr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
-        HybLoc L;
-        hyb_locate(vw.hyb, acc[1], acc[2], acc[0] - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-        const double c_k = hyb_f(vw.hyb, L, 0);
-        hyb_locate(vw.hyb, a.src_x, a.src_y, a.src_z - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-        const double c_s = hyb_f(vw.hyb, L, 0);
-        o.incl = -asin(c_k / c_s * acc[3]) * 180.0 / kPi;
-        double baz = 90.0 - atan2(-acc[4], -acc[5]) * (180.0 / kPi);
-        while (baz < -180.0) baz += 360.0;
-        while (baz > 180.0) baz -= 360.0;
-        o.baz = baz;
+        if (record) {
+            o.tt = tt; o.att = att; o.zmax = rmax;
+            o.amp_db = AMP ? amp_db_sphr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
+            HybLoc L;
+            hyb_locate(vw.hyb, acc[1], acc[2], acc[0] - a.r_earth, L, cl.hx, cl.hy, cl.hz);
+            const double c_k = hyb_f(vw.hyb, L, 0);
+            hyb_locate(vw.hyb, a.src_x, a.src_y, a.src_z - a.r_earth, L, cl.hx, cl.hy, cl.hz);
+            const double c_s = hyb_f(vw.hyb, L, 0);
+            o.incl = -asin(c_k / c_s * acc[3]) * 180.0 / kPi;
+            double baz = 90.0 - atan2(-acc[4], -acc[5]) * (180.0 / kPi);
+            while (baz < -180.0) baz += 360.0;
+            while (baz > 180.0) baz -= 360.0;
+            o.baz = baz;
+        }
     }
 }
 
 template <bool AMP>
 cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, cudaStream_t st,
-                              SegRes* seg_out, int seg_stride) {
+                              SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
     auto kern = tracesphr_fp64_kernel<AMP>;
     const size_t smem = ((size_t)DimSph<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(n + kThreads - 1) / kThreads, kThreads, smem, st>>>(a, d_req, d_res, n, seg_out, seg_stride);
+    int grid = 0;
+    if ((e = trace_grid(kern, kThreads, smem, n, grid)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st)) != cudaSuccess) return e;
+    kern<<<grid, kThreads, smem, st>>>(a, d_req, d_res, n, d_queue, seg_out, seg_stride);
     return cudaGetLastError();
 }
 
@@ -768,9 +773,9 @@ cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t 
 }
 
 cudaError_t launch_trace_sphr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
-                              cudaStream_t st, SegRes* seg_out, int seg_stride) {
-    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride)
-               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride);
+                              cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
+    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga
