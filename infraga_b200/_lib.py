@@ -105,6 +105,7 @@ _SIGS = {
     "iga_atmo_load_rngdep": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                   _I, _I, _P(_VP)]),
     "iga_atmo_region": (_I, [_VP, _P(_D), _P(_D), _P(_D), _P(_D)]),
+    "iga_atmo_load_topo": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I, _I, _P(_VP)]),
     "iga_server_config_default": (_I, [_P(ServerConfig)]),
     "iga_server_create": (_I, [_P(ServerConfig), _P(_VP)]),
     "iga_server_submit_fan": (_I, [_VP, _VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_LL)]),
@@ -200,6 +201,18 @@ class Atmosphere:
                                           str(topo_file).encode() if topo_file else None, fmt.encode(),
                                           int(reverse_winds), int(geometry), ctypes.byref(h)),
                f"iga_atmo_load_rngdep({prefix})")
+        return cls(h)
+
+    @classmethod
+    def load_topo(cls, met_path: str, topo_file: str, fmt: str = "zTuvdp", reverse_winds: bool = False,
+                  geometry: int = GEOM_3D) -> "Atmosphere":
+        """A .met profile over a terrain file of "x y z" rows [km]: infraga-3d's
+        set_region with topo_file (atmo_io.3d.strat.cpp:146-258).  The handle
+        runs FP64 3D fans and eigenray searches like a range-dependent one."""
+        h = _VP()
+        _check(lib().iga_atmo_load_topo(str(met_path).encode(), str(topo_file).encode(), fmt.encode(),
+                                        int(reverse_winds), int(geometry), ctypes.byref(h)),
+               f"iga_atmo_load_topo({met_path}, {topo_file})")
         return cls(h)
 
     def region(self):

@@ -74,6 +74,18 @@ int upload(iga_atmo_s* h) {
     return IGA_OK;
 }
 
+// terrain node records, then node x (lat), y (lon)
+int upload_terrain(iga_atmo_s* h) {
+    if (!h->has_topo) return IGA_OK;
+    const iga::Terrain& t = h->topo;
+    std::vector<double> tb(t.table);
+    tb.insert(tb.end(), t.x.begin(), t.x.end());
+    tb.insert(tb.end(), t.y.begin(), t.y.end());
+    IGA_CUDA(cudaMalloc(&h->d_topo, tb.size() * sizeof(double)), "cudaMalloc(terrain)");
+    IGA_CUDA(cudaMemcpy(h->d_topo, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(terrain)");
+    return IGA_OK;
+}
+
 int upload_rngdep(iga_atmo_s* h) {
     int dev;
     IGA_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
@@ -86,14 +98,8 @@ int upload_rngdep(iga_atmo_s* h) {
     buf.insert(buf.end(), g.z.begin(), g.z.end());
     IGA_CUDA(cudaMalloc(&h->d_hyb, buf.size() * sizeof(double)), "cudaMalloc(hybrid tables)");
     IGA_CUDA(cudaMemcpy(h->d_hyb, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(hybrid)");
-    if (h->has_topo) {
-        const iga::Terrain& t = h->topo;
-        std::vector<double> tb(t.table);
-        tb.insert(tb.end(), t.x.begin(), t.x.end());
-        tb.insert(tb.end(), t.y.begin(), t.y.end());
-        IGA_CUDA(cudaMalloc(&h->d_topo, tb.size() * sizeof(double)), "cudaMalloc(terrain)");
-        IGA_CUDA(cudaMemcpy(h->d_topo, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(terrain)");
-    }
+    int rc = upload_terrain(h);
+    if (rc) return rc;
     IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     return IGA_OK;
 }
@@ -287,11 +293,58 @@ int build_args_sphr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     return IGA_OK;
 }
 
+int set_terrain_args(iga_atmo_s* h, iga::Fan3DArgs& a) {
+    const iga::Terrain& t = h->topo;
+    a.topo_tab = h->d_topo;
+    a.topo_x = h->d_topo + (size_t)t.nx * t.ny * 4;
+    a.topo_y = a.topo_x + t.nx;
+    a.topo_nx = t.nx; a.topo_ny = t.ny;
+    return IGA_OK;
+}
+
+// infraga-3d over terrain: run_prop of main.infraga.3d.cpp:199-357 with a
+// topo_file, set_initial (eqset.3d.strat.cpp:58-105) at the source raised to
+// the ground, topo::set_bndlyr (atmo_state.3d.strat.cpp:36-49: the terrain
+// maximum, from 0, plus 0.1 km is the ground-check ceiling, 2 km above it the
+// boundary-layer top), topo::z0 = the first profile altitude (set_limits,
+// atmo_io.3d.strat.cpp:24-37).  The fan runs the 3D terrain kernel with the
+// 1D knot table in place of the hybrid grid.
+int build_args_3dt(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const StratProfile& P = h->prof;
+    a.knots = h->d_knots;
+    a.n_knots = (int)P.z.size();
+    a.uniform = P.uniform ? 1 : 0;
+    a.z_lo = P.z.front(); a.z_hi = P.z.back(); a.inv_dz = P.inv_dz;
+    a.src_x = p->src[0]; a.src_y = p->src[1];
+    a.x_min = p->x_min; a.x_max = p->x_max; a.y_min = p->y_min; a.y_max = p->y_max;
+    a.z0 = P.z.front();
+    a.topo_zmax = h->topo.z_max + 0.1;
+    a.z_bl = a.topo_zmax + 2.0;
+    a.x_cut = a.topo_zmax + 40.0;
+    double zt = 0.0, dz[2];
+    iga::terrain_eval1(h->topo, a.src_x, a.src_y, zt, dz);
+    a.src_z = std::max(p->src[2], zt);
+    double sc = 1.0;
+    if (a.src_z < a.z_bl) {
+        const double X = std::exp(-(a.src_z - zt) / 0.1);
+        sc = (1.0 - X) / (1.0 + X);
+    }
+    double f, d1, d2;
+    iga::spline_eval(P.z, P.c, P.cs, a.src_z, f, d1, d2); a.c0 = f;
+    iga::spline_eval(P.z, P.u, P.us, a.src_z, f, d1, d2); a.u0s = f * sc;
+    iga::spline_eval(P.z, P.v, P.vs, a.src_z, f, d1, d2); a.v0s = f * sc;
+    iga::spline_eval(P.z, P.rho, P.rhos, a.src_z, f, d1, d2); a.rho0 = f;
+    a.hyb_tab = nullptr; a.hyb_x = a.hyb_y = a.hyb_z = nullptr;
+    a.hyb_nx = a.hyb_ny = a.hyb_nz = 0;
+    return set_terrain_args(h, a);
+}
+
 // 3D range-dependent launch constants (run_prop of infraga-3d-rngdep,
 // main.infraga.3d.rngdep.cpp:235-309; set_initial; topo::set_bndlyr).
 // Without terrain topo::z is 0 in this solver (atmo_state.3d.rngdep.cpp:45-51).
 int build_args_3dr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     const iga::RngdepGrid& g = h->grid;
+    if (h->strat_topo) return build_args_3dt(h, p, a);
     a.src_x = p->src[0]; a.src_y = p->src[1];
     a.x_min = p->x_min; a.x_max = p->x_max; a.y_min = p->y_min; a.y_max = p->y_max;
     a.z0 = p->z_grnd;
@@ -524,6 +577,29 @@ int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_f
     return IGA_OK;
 }
 
+int iga_atmo_load_topo(const char* met_path, const char* topo_file, const char* format, int reverse_winds,
+                       int geometry, iga_atmo_t* out) {
+    if (!met_path || !topo_file || !out) return IGA_E_INVALID;
+    if (geometry != IGA_GEOM_3D && geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
+    *out = nullptr;
+    if (geometry == IGA_GEOM_SPH) {
+        g_err = "stratified profile over terrain: 3D Cartesian geometry only";
+        return IGA_E_UNSUPPORTED;
+    }
+    iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
+    if (!h) return IGA_E_NOMEM;
+    h->kind = 2;
+    h->strat_topo = true;
+    int rc = iga::load_terrain(topo_file, false, h->topo, g_err);
+    h->has_topo = (rc == IGA_OK);
+    if (rc == IGA_OK) rc = iga::load_met(met_path, format ? format : "zTuvdp", reverse_winds != 0, h->prof, g_err);
+    if (rc == IGA_OK) rc = upload(h);
+    if (rc == IGA_OK) rc = upload_terrain(h);
+    if (rc != IGA_OK) { iga_atmo_destroy(h); return rc; }
+    *out = h;
+    return IGA_OK;
+}
+
 int iga_atmo_terrain(iga_atmo_t h, double x, double y, double* z, double* dz_dx, double* dz_dy) {
     if (!h) return IGA_E_INVALID;
     if (!h->has_topo) return IGA_E_UNSUPPORTED;
@@ -538,7 +614,12 @@ int iga_atmo_terrain(iga_atmo_t h, double x, double y, double* z, double* dz_dx,
 int iga_atmo_region(iga_atmo_t h, double* lat_min, double* lat_max, double* lon_min, double* lon_max) {
     if (!h) return IGA_E_INVALID;
     double r[4] = {-90.0, 90.0, -180.0, 180.0};
-    if (h->kind == 2) {
+    if (h->kind == 2 && h->strat_topo) {
+        // geoac::set_limits with terrain (atmo_io.3d.strat.cpp:24-30): terrain extent less 0.001 km
+        const double buf = 0.001;
+        r[0] = h->topo.x.front() + buf; r[1] = h->topo.x.back() - buf;
+        r[2] = h->topo.y.front() + buf; r[3] = h->topo.y.back() - buf;
+    } else if (h->kind == 2) {
         // geoac::set_limits (atmo_io.3d.rngdep.cpp:25-40): grid (and terrain) extent less 0.001 km
         const double buf = 0.001;
         double a0 = h->grid.x.front() + buf, a1 = h->grid.x.back() - buf;

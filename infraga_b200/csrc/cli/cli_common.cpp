@@ -160,14 +160,25 @@ iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_o
     *topo_out = topo;
     iga_atmo_t a = nullptr;
     int rc;
-    if (!is_rngdep(v)) {
-        std::cout << "Interpolating atmosphere data in '" << argv[2] << "' using format '" << fmt << "'..." << '\n';
+    if (!is_rngdep(v) && topo) {
+        // set_region(atmo_file, topo_file, ...) (atmo_io.3d.strat.cpp:146-258)
+        std::cout << "Interpolating atmosphere data in '" << argv[2] << "' and topography data in '" << topo << "'..."
+                  << '\n';
         if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
-        if (topo) {
-            std::cout << '\t' << "ERROR: terrain (topo_file) with a stratified profile is not provided by the GPU front end;"
-                      << " use " << (is_sph(v) ? "infraga-sph-rngdep" : "infraga-3d-rngdep") << '\n' << '\n';
+        if (is_sph(v)) {
+            std::cout << '\t' << "ERROR: terrain (topo_file) with a spherical stratified profile is not provided by the"
+                      << " GPU front end; use infraga-sph-rngdep" << '\n' << '\n';
             return nullptr;
         }
+        rc = iga_atmo_load_topo(argv[2], topo, fmt, rev ? 1 : 0, IGA_GEOM_3D, &a);
+        if (rc == IGA_E_IO) {
+            std::cout << '\t' << "ERROR: Invalid terrain file or atmospheric specification (" << topo << ", " << argv[2]
+                      << ")" << '\n' << '\n';
+            return nullptr;
+        }
+    } else if (!is_rngdep(v)) {
+        std::cout << "Interpolating atmosphere data in '" << argv[2] << "' using format '" << fmt << "'..." << '\n';
+        if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
         rc = iga_atmo_load(argv[2], fmt, rev ? 1 : 0, &a);
         if (rc == IGA_E_IO) {
             std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\n';
@@ -742,6 +753,11 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     if (v == Variant::kSph || (v == Variant::kSphRngdep && !has_topo)) {   // main.infraga.sph.cpp:788-789
         o.src[0] = 30.0; o.src[1] = 0.0; o.src[2] = 0.0;
         o.rcvr[0] = 30.0; o.rcvr[1] = -2.5;
+    } else if (v == Variant::k3D && has_topo) {   // main.infraga.3d.cpp:812-815, :992-995
+        double a0, a1, b0, b1;
+        iga_atmo_region(atmo, &a0, &a1, &b0, &b1);
+        o.src[0] = (a1 + a0) / 2.0; o.src[1] = (b1 + b0) / 2.0;
+        o.rcvr[0] = o.src[0] - 250.0; o.rcvr[1] = o.src[1];
     } else if (rd) {   // the centre of the region (main.infraga.3d.rngdep.cpp:816-817, sph.rngdep :821-822)
         double a0, a1, b0, b1;
         iga_atmo_region(atmo, &a0, &a1, &b0, &b1);

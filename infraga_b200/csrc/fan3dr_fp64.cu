@@ -9,6 +9,16 @@
 // (src/main.infraga.3d.rngdep.cpp:204-535).  Two reference details carried
 // over: without terrain topo::z is 0 (not z_grnd, atmo_state.3d.rngdep.cpp:45-51),
 // and the azimuth variation of v is added into dv[3] (eqset.3d.rngdep.cpp:288).
+//
+// ST instantiations run infraga-3d's stratified profile over terrain
+// (topo_file=): c, u, v, rho from the 1D knot table at the clamped altitude
+// (atmo_state.3d.strat.cpp:148-233, calc_uvw :462-734) with the same terrain,
+// boundary-layer scaling, reflection and bounce loop (geoac.eqset.3d.strat.cpp
+// and run_prop, main.infraga.3d.cpp:199-357, have the same forms).  Their
+// differences from the range-dependent solver are kept: the Hessian-times-
+// Jacobian sums of update_refs run over m >= n only (eqset.3d.strat.cpp:305-310)
+// and the turning height starts from topo::z0, the profile's first altitude
+// (main.infraga.3d.cpp:427).
 #include "eig3d.cuh"
 #include "fan3d.cuh"
 #include "fan3d_common.cuh"
@@ -49,20 +59,49 @@ __device__ __forceinline__ double topo_z(const Views& v, Cells& cl, double x, do
     return t.z;
 }
 
+// sum_{k >= i} X[k] H[k], accumulated from k = i like the reference's loop
+__device__ __forceinline__ double hsum_from(int i, const double* X, const double* H) {
+    return i == 0 ? X[0] * H[0] + X[1] * H[1] + X[2] * H[2] : (i == 1 ? X[1] * H[1] + X[2] * H[2] : X[2] * H[2]);
+}
+
 struct AtmFull {
     double c, dc[3], ddc[3][3];
     double u, du[3], ddu[3][3];
     double v, dv[3], ddv[3][3];
 };
 
-// update_refs' atmosphere (atmo::c/dc/ddc and calc_uvw, atmo_state.3d.rngdep.cpp:148-170, 400-700)
-template <bool AMP>
+// Stratified profile row at z clamped to the knot range (interp::in_interval);
+// cl.hz caches the segment.
+__device__ __forceinline__ const double* strat_at(const Fan3DArgs& a, Cells& cl, double z, Cubic& q) {
+    const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
+    cl.hz = seg_walk(a.knots, a.n_knots, ze, cl.hz);
+    const double* r0 = a.knots + cl.hz * kStride;
+    q = cubic_at(r0, ze);
+    return r0;
+}
+
+// update_refs' atmosphere (atmo::c/dc/ddc and calc_uvw, atmo_state.3d.rngdep.cpp:148-170, 400-700;
+// ST: atmo_state.3d.strat.cpp:148-233, 462-734)
+template <bool AMP, bool ST>
 __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Cells& cl, double x, double y, double z,
                                          AtmFull& m) {
+    HybF2 c2 = {}, u2 = {}, v2 = {};   // hybrid index order: d[0] is d/dz
+    if (ST) {
+        Cubic q;
+        const double* r0 = strat_at(a, cl, z, q);
+        if (AMP) {
+            cubic_f2(r0, q, 2, c2.f, c2.d[0], c2.dd[0][0]);
+            cubic_f2(r0, q, 4, u2.f, u2.d[0], u2.dd[0][0]);
+            cubic_f2(r0, q, 6, v2.f, v2.d[0], v2.dd[0][0]);
+        } else {
+            cubic_f1(r0, q, 2, c2.f, c2.d[0]);
+            cubic_f1(r0, q, 4, u2.f, u2.d[0]);
+            cubic_f1(r0, q, 6, v2.f, v2.d[0]);
+        }
+    } else {
     HybLoc L;
     hyb_locate(vw.hyb, x, y, z, L, cl.hx, cl.hy, cl.hz);
     L.zq_raw = L.zq;   // the Cartesian calls pass the clamped z to every block
-    HybF2 c2, u2, v2;
     if (AMP) {
         hyb_f2(vw.hyb, L, 0, c2);
         hyb_f2(vw.hyb, L, 1, u2);
@@ -72,6 +111,7 @@ __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Ce
         hyb_f1(vw.hyb, L, 0, t); c2.f = t.f; c2.d[0] = t.d[0]; c2.d[1] = t.d[1]; c2.d[2] = t.d[2];
         hyb_f1(vw.hyb, L, 1, t); u2.f = t.f; u2.d[0] = t.d[0]; u2.d[1] = t.d[1]; u2.d[2] = t.d[2];
         hyb_f1(vw.hyb, L, 2, t); v2.f = t.f; v2.d[0] = t.d[0]; v2.d[1] = t.d[1]; v2.d[2] = t.d[2];
+    }
     }
     double zg = 0.0, dzg[2] = {0.0, 0.0}, ddzg[3] = {0.0, 0.0, 0.0};
     double X = 0.0;
@@ -125,11 +165,11 @@ __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Ce
     }
 }
 
-// update_refs + eval_src_eq (geoac.eqset.3d.rngdep.cpp:226-388), w = 0
-template <bool AMP>
+// update_refs + eval_src_eq (geoac.eqset.3d.rngdep.cpp:226-388; ST: eqset.3d.strat.cpp:225-389), w = 0
+template <bool AMP, bool ST>
 __device__ __forceinline__ void rhs_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y, double* f) {
     AtmFull m;
-    atm_full<AMP>(a, vw, cl, y[0], y[1], y[2], m);
+    atm_full<AMP, ST>(a, vw, cl, y[0], y[1], y[2], m);
     const double n0 = y[3], n1 = y[4], n2 = y[5];
     const double num = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
     const double inum = 1.0 / num;
@@ -166,9 +206,10 @@ __device__ __forceinline__ void rhs_3dr(const Fan3DArgs& a, const Views& vw, Cel
             const double dm = (cg[0] * g[0] + cg[1] * g[1] + cg[2] * g[2]) * icg;
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                const double ddc = Xv[0] * m.ddc[i][0] + Xv[1] * m.ddc[i][1] + Xv[2] * m.ddc[i][2];
-                const double ddu = Xv[0] * m.ddu[i][0] + Xv[1] * m.ddu[i][1] + Xv[2] * m.ddu[i][2];
-                const double ddv = Xv[0] * m.ddv[i][0] + Xv[1] * m.ddv[i][1] + Xv[2] * m.ddv[i][2];
+                // ST: the stratified update_refs sums m = i..2 only (eqset.3d.strat.cpp:305-310)
+                const double ddc = ST ? hsum_from(i, Xv, m.ddc[i]) : Xv[0] * m.ddc[i][0] + Xv[1] * m.ddc[i][1] + Xv[2] * m.ddc[i][2];
+                const double ddu = ST ? hsum_from(i, Xv, m.ddu[i]) : Xv[0] * m.ddu[i][0] + Xv[1] * m.ddu[i][1] + Xv[2] * m.ddu[i][2];
+                const double ddv = ST ? hsum_from(i, Xv, m.ddv[i]) : Xv[0] * m.ddv[i][0] + Xv[1] * m.ddv[i][1] + Xv[2] * m.ddv[i][2];
                 f[6 + 6 * j + i] = g[i] * icg - cg[i] * icg2 * dm;
                 f[9 + 6 * j + i] = icg2 * dm * K[i] -
                                    icg * (dnu * m.dc[i] + num * ddc + mu[0] * m.du[i] + mu[1] * m.dv[i] + n0 * ddu + n1 * ddv);
@@ -181,15 +222,25 @@ __device__ __forceinline__ void rhs_3dr(const Fan3DArgs& a, const Views& vw, Cel
 struct AtmPt {
     double c, u, v, rho;
 };
+template <bool ST>
 __device__ __forceinline__ void atm_point(const Fan3DArgs& a, const Views& vw, Cells& cl, double x, double y, double z,
                                           AtmPt& o) {
-    HybLoc L;
-    hyb_locate(vw.hyb, x, y, z, L, cl.hx, cl.hy, cl.hz);
     double sc = 1.0;
     if (z < a.z_bl) {
         const double X = exp(-(z - topo_z(vw, cl, x, y)) * a.inv_bl);
         sc = (1.0 - X) / (1.0 + X);
     }
+    if (ST) {
+        Cubic q;
+        const double* r0 = strat_at(a, cl, z, q);
+        o.c = cubic_f(r0, q, 2);
+        o.u = cubic_f(r0, q, 4) * sc;
+        o.v = cubic_f(r0, q, 6) * sc;
+        o.rho = cubic_f(r0, q, 8);
+        return;
+    }
+    HybLoc L;
+    hyb_locate(vw.hyb, x, y, z, L, cl.hx, cl.hy, cl.hz);
     o.c = hyb_f(vw.hyb, L, 0);
     o.u = hyb_f(vw.hyb, L, 1) * sc;
     o.v = hyb_f(vw.hyb, L, 2) * sc;
@@ -197,6 +248,7 @@ __device__ __forceinline__ void atm_point(const Fan3DArgs& a, const Views& vw, C
 }
 
 // travel_time / atten of one segment at its midpoint (eqset.3d.rngdep.cpp:487-514, 689-702)
+template <bool ST>
 __device__ __forceinline__ void seg_increment_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y0,
                                                   const double* y1, double& dt_out, double& da_out) {
     const double dx = y1[0] - y0[0], dy = y1[1] - y0[1], dz = y1[2] - y0[2];
@@ -207,7 +259,7 @@ __device__ __forceinline__ void seg_increment_3dr(const Fan3DArgs& a, const View
     const double n2 = y0[5] + (y1[5] - y0[5]) * 0.5;
     const double num = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
     AtmPt m;
-    atm_point(a, vw, cl, xm, ym, zm, m);
+    atm_point<ST>(a, vw, cl, xm, ym, zm, m);
     const double inum = 1.0 / num;
     const double c0 = m.c * n0 * inum + m.u, c1 = m.c * n1 * inum + m.v, c2 = m.c * n2 * inum;
     dt_out = ds / sqrt(c0 * c0 + c1 * c1 + c2 * c2);
@@ -215,10 +267,11 @@ __device__ __forceinline__ void seg_increment_3dr(const Fan3DArgs& a, const View
 }
 
 // geoac::amp with geoac::jacobian at the below-ground row (eqset.3d.rngdep.cpp:704-748)
+template <bool ST>
 __device__ __noinline__ double amp_db_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y, double theta,
                                           double phi, double* jac_out) {
     AtmPt m;
-    atm_point(a, vw, cl, y[0], y[1], y[2], m);
+    atm_point<ST>(a, vw, cl, y[0], y[1], y[2], m);
     const double num = sqrt(y[3] * y[3] + y[4] * y[4] + y[5] * y[5]);
     const double num0 = 1.0 - (y[3] * a.u0s + y[4] * a.v0s + y[5] * 0.0) / a.c0;
     const double cp[3] = {m.c * y[3] / num + m.u, m.c * y[4] / num + m.v, m.c * y[5] / num};
@@ -237,7 +290,7 @@ __device__ __noinline__ double amp_db_3dr(const Fan3DArgs& a, const Views& vw, C
 }
 
 // approx_intercept + set_refl (eqset.3d.rngdep.cpp:111-209), general terrain
-template <int N, bool AMP>
+template <int N, bool AMP, bool ST>
 __device__ __noinline__ void reflect_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, double* y, const double* prev) {
     double zy = 0.0, dzy[2] = {0.0, 0.0};
     if (vw.has_topo) {
@@ -268,13 +321,21 @@ __device__ __noinline__ void reflect_3dr(const Fan3DArgs& a, const Views& vw, Ce
     q[4] = C1y * p[4] + C2y * (p[5] - p[3] * A);
     q[5] = -C1z * p[5] + p[3] * C2x + p[4] * C2y;
     if (AMP) {
-        HybLoc L;
-        hyb_locate(vw.hyb, p[0], p[1], zg, L, cl.hx, cl.hy, cl.hz);
-        L.zq_raw = L.zq;
-        HybF1 cc, uu, vv;
-        hyb_f1(vw.hyb, L, 0, cc);
-        hyb_f1(vw.hyb, L, 1, uu);
-        hyb_f1(vw.hyb, L, 2, vv);
+        HybF1 cc = {}, uu = {}, vv = {};
+        if (ST) {   // atmo::c, dc, du, dv at the ground point (atmo_state.3d.strat.cpp:153-218)
+            Cubic qz;
+            const double* r0 = strat_at(a, cl, zg, qz);
+            cubic_f1(r0, qz, 2, cc.f, cc.d[0]);
+            cubic_f1(r0, qz, 4, uu.f, uu.d[0]);
+            cubic_f1(r0, qz, 6, vv.f, vv.d[0]);
+        } else {
+            HybLoc L;
+            hyb_locate(vw.hyb, p[0], p[1], zg, L, cl.hx, cl.hy, cl.hz);
+            L.zq_raw = L.zq;
+            hyb_f1(vw.hyb, L, 0, cc);
+            hyb_f1(vw.hyb, L, 1, uu);
+            hyb_f1(vw.hyb, L, 2, vv);
+        }
         const double c_grnd = cc.f;
         // atmo::du/dv at the ground point: the scaling there has X = exp(-(zg - zg)/bl) = 1
         const double Xg = exp(-(zg - zg) * a.inv_bl);
@@ -359,7 +420,7 @@ __device__ __forceinline__ void ray_init_3dr(const Fan3DArgs& a, double theta, d
 // PATHS: also write the sampled per-step rows and caustic points of
 // run_prop's write_rays / write_topo / write_caustics output
 // (main.infraga.3d.rngdep.cpp:440-488); the fan results are unchanged.
-template <bool AMP, bool PATHS>
+template <bool AMP, bool PATHS, bool ST>
 __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = Dim3r<AMP>::n;
     extern __shared__ double s_mem[];
@@ -401,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         ray_init_3dr<AMP>(a, theta, phi, y);
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
-        zmax = 0.0;
+        zmax = ST ? a.z0 : 0.0;   // run_prop's z_max = topo::z0 (0 in the range-dependent main)
         if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
@@ -412,7 +473,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - topo_z(vw, cl, y[0], y[1])) / 0.2);
         s += ds;
         double acc[N], stg[N], f[N];
-        rhs_3dr<AMP>(a, vw, cl, y, f);
+        rhs_3dr<AMP, ST>(a, vw, cl, y, f);
         if (AMP && (a.aux || (PATHS && a.caus_rows)) && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
             const double* Xt = y + 6;
             const double* Xp = y + 12;
@@ -433,13 +494,13 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         }
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-        rhs_3dr<AMP>(a, vw, cl, stg, f);
+        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-        rhs_3dr<AMP>(a, vw, cl, stg, f);
+        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-        rhs_3dr<AMP>(a, vw, cl, stg, f);
+        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
         kb++;
@@ -451,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         const bool gnd = !esc && (acc[2] <= a.topo_zmax) && (acc[2] < topo_z(vw, cl, acc[0], acc[1]));
 
         double dt, da;
-        seg_increment_3dr(a, vw, cl, y, acc, dt, da);
+        seg_increment_3dr<ST>(a, vw, cl, y, acc, dt, da);
         if (a.write_rays) { tt += pt; att += pa; pt = dt; pa = da; }
         else { pt += dt; pa += da; }
 
@@ -471,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
                     o[0] = y[0]; o[1] = y[1];
                     o[2] = a.path_mode == kPathRays ? fmax(y[2], zg) : zg;
                     o[3] = (AMP && a.path_mode == kPathRays)
-                               ? amp_db_3dr(a, vw, c2, y, a.theta_deg[ray] * kPi / 180.0,
+                               ? amp_db_3dr<ST>(a, vw, c2, y, a.theta_deg[ray] * kPi / 180.0,
                                             kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0, nullptr)
                                : 0.0;
                     o[4] = -2.0 * (att + pa); o[5] = tt + pt; o[6] = (double)bnc;
@@ -495,7 +556,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
             const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
             const double zgk = topo_z(vw, cl, acc[0], acc[1]);
             AtmPt mg;
-            atm_point(a, vw, cl, acc[0], acc[1], zgk, mg);
+            atm_point<ST>(a, vw, cl, acc[0], acc[1], zgk, mg);
             const double incl = -asin(mg.c / a.c0 * acc[5]) * 180.0 / kPi;
             double baz = 90.0 - atan2(-acc[4], -acc[3]) * 180.0 / kPi;
             if (baz < -180.0) baz += 360.0;
@@ -511,7 +572,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
             out[8] = incl;
             out[9] = baz;
             double jac = 0.0;
-            out[10] = AMP ? amp_db_3dr(a, vw, cl, acc, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0, &jac) : 0.0;
+            out[10] = AMP ? amp_db_3dr<ST>(a, vw, cl, acc, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0, &jac) : 0.0;
             out[11] = -2.0 * att;
             if (a.aux) {
                 double* ax = a.aux + ((size_t)ray * nb + na) * 4;
@@ -537,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
                 }
             }
             na++;
-            reflect_3dr<N, AMP>(a, vw, cl, y, prev);
+            reflect_3dr<N, AMP, ST>(a, vw, cl, y, prev);
             bnc++;
             if (bnc > a.bounces) status = 0;
         }
@@ -555,11 +616,11 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
     }
 }
 
-template <bool AMP, bool PATHS>
+template <bool AMP, bool PATHS, bool ST>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
     const int threads = a.block > 0 ? a.block : kThreads;
-    auto kern = fan3dr_fp64_kernel<AMP, PATHS>;
+    auto kern = fan3dr_fp64_kernel<AMP, PATHS, ST>;
     const size_t smem = ((size_t)Dim3r<AMP>::n * threads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -588,7 +649,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 // (:334-342): c at the source and on the ground, the ground height and its
 // gradient.  Same block size as the fan kernel (reflect_3dr reads row k-2
 // from shared memory with that stride).
-template <bool AMP>
+template <bool AMP, bool ST>
 __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                             const TraceReq* __restrict__ reqs,
                                                                             TraceRes18* __restrict__ out, int n, unsigned int* __restrict__ queue,
@@ -639,16 +700,16 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
                 if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - topo_z(vw, cl, y[0], y[1])) / 0.2);
                 s += ds;
                 double stg[N], f[N];
-                rhs_3dr<AMP>(a, vw, cl, y, f);
+                rhs_3dr<AMP, ST>(a, vw, cl, y, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-                rhs_3dr<AMP>(a, vw, cl, stg, f);
+                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-                rhs_3dr<AMP>(a, vw, cl, stg, f);
+                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-                rhs_3dr<AMP>(a, vw, cl, stg, f);
+                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
                 kb++;
@@ -658,7 +719,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
                 const bool gnd = !esc && (acc[2] <= a.topo_zmax) && (acc[2] < topo_z(vw, cl, acc[0], acc[1]));
                 if (record) {
                     double dt, da;
-                    seg_increment_3dr(a, vw, cl, y, acc, dt, da);
+                    seg_increment_3dr<ST>(a, vw, cl, y, acc, dt, da);
                     tt += pt; att += pa; pt = dt; pa = da;
                 }
                 if (!esc && !gnd) {
@@ -678,7 +739,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
                 g.x = acc[0]; g.y = acc[1]; g.steps = steps; g.escaped = esc ? 1 : 0;
             }
             if (sg == q.n_seg - 1 || (esc && stop)) break;
-            reflect_3dr<N, AMP>(a, vw, cl, y, prev);
+            reflect_3dr<N, AMP, ST>(a, vw, cl, y, prev);
         }
         TraceRes18& o = out[r];
 #pragma unroll
@@ -695,15 +756,15 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
                 zg = t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
             }
             AtmPt m;
-            atm_point(a, vw, cl, acc[0], acc[1], zg, m);
+            atm_point<ST>(a, vw, cl, acc[0], acc[1], zg, m);
             o.z_grnd = zg;
             o.c_grnd = m.c;
         }
         if (record) {
             o.tt = tt; o.att = att; o.zmax = zmax;
-            o.amp_db = AMP ? amp_db_3dr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
+            o.amp_db = AMP ? amp_db_3dr<ST>(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
             AtmPt m;
-            atm_point(a, vw, cl, acc[0], acc[1], acc[2], m);
+            atm_point<ST>(a, vw, cl, acc[0], acc[1], acc[2], m);
             o.incl = -asin(m.c / a.c0 * acc[5]) * (180.0 / kPi);
             double baz = 90.0 - atan2(-acc[4], -acc[3]) * (180.0 / kPi);
             while (baz > 180.0) baz -= 360.0;
@@ -713,11 +774,11 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
     }
 }
 
-template <bool AMP>
+template <bool AMP, bool ST>
 cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, cudaStream_t st,
                               SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
-    auto kern = trace3dr_fp64_kernel<AMP>;
+    auto kern = trace3dr_fp64_kernel<AMP, ST>;
     const size_t smem = ((size_t)Dim3r<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -729,18 +790,27 @@ cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRe
     return cudaGetLastError();
 }
 
+// a.knots set (no hybrid tables): stratified profile over terrain
+template <bool ST>
+cudaError_t launch_fan(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
+    if (a.path_rows || a.caus_rows)
+        return calc_amp ? launch_impl<true, true, ST>(a, stream, grid_used) : launch_impl<false, true, ST>(a, stream, grid_used);
+    return calc_amp ? launch_impl<true, false, ST>(a, stream, grid_used) : launch_impl<false, false, ST>(a, stream, grid_used);
+}
+
 }  // namespace
 
 cudaError_t launch_fan3dr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
-    if (a.path_rows || a.caus_rows)
-        return calc_amp ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<false, true>(a, stream, grid_used);
-    return calc_amp ? launch_impl<true, false>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
+    return a.knots ? launch_fan<true>(a, calc_amp, stream, grid_used) : launch_fan<false>(a, calc_amp, stream, grid_used);
 }
 
 cudaError_t launch_trace_3dr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
                              cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
-    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
-               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    if (a.knots)
+        return amp ? launch_trace_impl<true, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+                   : launch_trace_impl<false, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    return amp ? launch_trace_impl<true, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_impl<false, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga

@@ -17,8 +17,11 @@ using iga::StratProfile;
 
 struct iga_atmo_s {
     int device = 0;
-    // 0: stratified profile (prof); 1: range-dependent grid (grid, optional topo)
+    // 0: stratified profile (prof); 1: spherical range-dependent grid (grid,
+    // optional topo); 2: 3D range-dependent grid (grid, optional topo), or with
+    // strat_topo a stratified profile (prof, d_knots) over terrain (topo)
     int kind = 0;
+    bool strat_topo = false;
     StratProfile prof;        // range-dependent: z only (knot altitudes)
     iga::RngdepGrid grid;
     iga::Terrain topo;
