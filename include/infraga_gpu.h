@@ -143,12 +143,14 @@ int iga_atmo_load_rngdep(const char* prefix, const char* x_file, const char* y_f
                          const char* format, int reverse_winds, int geometry, iga_atmo_t* out);
 
 /* Replaces set_region(atmo_file, topo_file, format, invert_winds) of
- * infraga-3d (src/atmo/atmo_io.3d.strat.cpp:146-258): a .met profile as
- * iga_atmo_load over a terrain file of rows "x y z" [km] (x major, as for
- * iga_atmo_load_rngdep).  The handle behaves as a 3D range-dependent one
- * (iga_atmo_region gives the terrain extent less 0.001 km, iga_atmo_terrain
- * works, FP64 only) and runs the stratified solver's equations over the
- * terrain.  geometry must be IGA_GEOM_3D (IGA_E_UNSUPPORTED otherwise). */
+ * infraga-3d and infraga-sph (src/atmo/atmo_io.3d.strat.cpp:146-258,
+ * src/atmo/atmo_io.sph.strat.cpp): a .met profile as iga_atmo_load over a
+ * terrain file of rows "x y z" [km] (IGA_GEOM_3D) or "lat lon z" [deg, deg,
+ * km] (IGA_GEOM_SPH), first coordinate major as for iga_atmo_load_rngdep.
+ * The handle behaves as a range-dependent one of that geometry
+ * (iga_atmo_region gives the terrain extent less 0.001 km or 1e-3 deg,
+ * iga_atmo_terrain works, FP64 only) and runs the stratified solver's
+ * equations over the terrain. */
 int iga_atmo_load_topo(const char* met_path, const char* topo_file, const char* format, int reverse_winds,
                        int geometry, iga_atmo_t* out);
 

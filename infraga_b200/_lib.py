@@ -206,9 +206,11 @@ class Atmosphere:
     @classmethod
     def load_topo(cls, met_path: str, topo_file: str, fmt: str = "zTuvdp", reverse_winds: bool = False,
                   geometry: int = GEOM_3D) -> "Atmosphere":
-        """A .met profile over a terrain file of "x y z" rows [km]: infraga-3d's
-        set_region with topo_file (atmo_io.3d.strat.cpp:146-258).  The handle
-        runs FP64 3D fans and eigenray searches like a range-dependent one."""
+        """A .met profile over a terrain file: infraga-3d's set_region with
+        topo_file (atmo_io.3d.strat.cpp:146-258; rows "x y z" in km) or, with
+        geometry=GEOM_SPH, infraga-sph's (rows "lat lon z" in deg, deg, km).
+        The handle runs FP64 fans and eigenray searches of that geometry like a
+        range-dependent one."""
         h = _VP()
         _check(lib().iga_atmo_load_topo(str(met_path).encode(), str(topo_file).encode(), fmt.encode(),
                                         int(reverse_winds), int(geometry), ctypes.byref(h)),

@@ -230,7 +230,10 @@ int build_args_sph(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
 // Range-dependent spherical launch constants (run_prop of infraga-sph-rngdep,
 // main.infraga.sph.rngdep.cpp:310-320; set_initial; topo::set_bndlyr
 // atmo_state.sph.rngdep.cpp:22-33).
+int build_args_spht(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a);
+
 int build_args_sphr(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    if (h->strat_topo) return build_args_spht(h, p, a);
     const iga::RngdepGrid& g = h->grid;
     const double d2r = iga::kPi / 180.0;
     a.r_earth = iga::kEarthRadiusKm;
@@ -334,6 +337,53 @@ int build_args_3dt(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
     iga::spline_eval(P.z, P.u, P.us, a.src_z, f, d1, d2); a.u0s = f * sc;
     iga::spline_eval(P.z, P.v, P.vs, a.src_z, f, d1, d2); a.v0s = f * sc;
     iga::spline_eval(P.z, P.rho, P.rhos, a.src_z, f, d1, d2); a.rho0 = f;
+    a.hyb_tab = nullptr; a.hyb_x = a.hyb_y = a.hyb_z = nullptr;
+    a.hyb_nx = a.hyb_ny = a.hyb_nz = 0;
+    return set_terrain_args(h, a);
+}
+
+// infraga-sph over terrain: run_prop of main.infraga.sph.cpp:200-360 with a
+// topo_file, set_initial at the source raised to the ground, topo::set_bndlyr
+// (atmo_state.sph.strat.cpp:41-54: ground-check ceiling = terrain maximum,
+// from 0, plus 0.01 km; boundary-layer top 2 km above that ceiling),
+// topo::z0 = the first profile altitude (set_limits, atmo_io.sph.strat.cpp:27-39).
+// The fan runs the spherical terrain kernel with the 1D knot table.
+int build_args_spht(iga_atmo_s* h, const iga_fan_params* p, iga::Fan3DArgs& a) {
+    const StratProfile& P = h->prof;
+    const double d2r = iga::kPi / 180.0;
+    a.knots = h->d_knots;
+    a.n_knots = (int)P.z.size();
+    a.uniform = P.uniform ? 1 : 0;
+    a.z_lo = P.z.front(); a.z_hi = P.z.back(); a.inv_dz = P.inv_dz;
+    a.r_earth = iga::kEarthRadiusKm;
+    a.src_x = p->src[0] * d2r;
+    a.src_y = p->src[1] * d2r;
+    a.cos_lat_src = std::cos(a.src_x);
+    a.lat_min = p->lat_min * d2r; a.lat_max = p->lat_max * d2r;
+    a.lon_min = p->lon_min * d2r; a.lon_max = p->lon_max * d2r;
+    a.time_max_h = p->time_max;
+    const double half_ang = p->rng_max / (2.0 * a.r_earth);
+    a.rng_exact_only = (half_ang > 0.0 && half_ang < 0.5 * iga::kPi - 1e-6) ? 0 : 1;
+    a.hav_rng = a.rng_exact_only ? 0.0 : std::pow(std::sin(half_ang), 2);
+    a.z0 = P.z.front();
+    a.r_grnd = a.r_earth + a.z0;
+    a.topo_zmax = h->topo.z_max + 0.01;
+    a.z_bl = a.topo_zmax + 2.0;
+    a.x_cut = a.topo_zmax + 40.0;
+    double zt = 0.0, dz[2];
+    iga::terrain_eval1(h->topo, a.src_x, a.src_y, zt, dz);
+    a.src_z = std::max(p->src[2], zt);
+    double sc = 1.0;
+    if (a.src_z < a.z_bl) {
+        const double X = std::exp(-((a.r_earth + a.src_z) - (a.r_earth + zt)) / 0.1);
+        sc = (1.0 - X) / (1.0 + X);
+    }
+    double f, d1, d2;
+    iga::spline_eval(P.z, P.c, P.cs, a.src_z, f, d1, d2); a.c0 = f;
+    iga::spline_eval(P.z, P.u, P.us, a.src_z, f, d1, d2); a.u0s = f * sc;
+    iga::spline_eval(P.z, P.v, P.vs, a.src_z, f, d1, d2); a.v0s = f * sc;
+    iga::spline_eval(P.z, P.rho, P.rhos, a.src_z, f, d1, d2); a.rho0 = f;
+    a.refl_mcr = 0.0;   // position dependent: formed in the kernel
     a.hyb_tab = nullptr; a.hyb_x = a.hyb_y = a.hyb_z = nullptr;
     a.hyb_nx = a.hyb_ny = a.hyb_nz = 0;
     return set_terrain_args(h, a);
@@ -582,15 +632,12 @@ int iga_atmo_load_topo(const char* met_path, const char* topo_file, const char* 
     if (!met_path || !topo_file || !out) return IGA_E_INVALID;
     if (geometry != IGA_GEOM_3D && geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
     *out = nullptr;
-    if (geometry == IGA_GEOM_SPH) {
-        g_err = "stratified profile over terrain: 3D Cartesian geometry only";
-        return IGA_E_UNSUPPORTED;
-    }
     iga_atmo_s* h = new (std::nothrow) iga_atmo_s();
     if (!h) return IGA_E_NOMEM;
-    h->kind = 2;
+    const bool sph = geometry == IGA_GEOM_SPH;
+    h->kind = sph ? 1 : 2;
     h->strat_topo = true;
-    int rc = iga::load_terrain(topo_file, false, h->topo, g_err);
+    int rc = iga::load_terrain(topo_file, sph, h->topo, g_err);
     h->has_topo = (rc == IGA_OK);
     if (rc == IGA_OK) rc = iga::load_met(met_path, format ? format : "zTuvdp", reverse_winds != 0, h->prof, g_err);
     if (rc == IGA_OK) rc = upload(h);
@@ -629,6 +676,11 @@ int iga_atmo_region(iga_atmo_t h, double* lat_min, double* lat_max, double* lon_
             b0 = std::max(b0, h->topo.y.front() + buf); b1 = std::min(b1, h->topo.y.back() - buf);
         }
         r[0] = a0; r[1] = a1; r[2] = b0; r[3] = b1;
+    } else if (h->kind == 1 && h->strat_topo) {
+        // geoac::set_limits with terrain (atmo_io.sph.strat.cpp:27-31): terrain extent less 1e-3 deg
+        const double buf = 1.0e-3 * (iga::kPi / 180.0), r2d = 180.0 / iga::kPi;
+        r[0] = (h->topo.x.front() + buf) * r2d; r[1] = (h->topo.x.back() - buf) * r2d;
+        r[2] = (h->topo.y.front() + buf) * r2d; r[3] = (h->topo.y.back() - buf) * r2d;
     } else if (h->kind == 1) {
         // geoac::set_limits (atmo_io.sph.rngdep.cpp:27-43): grid (and terrain) extent less 1e-3 deg
         const double buf = 1.0e-3 * (iga::kPi / 180.0);
@@ -728,7 +780,8 @@ int iga_fan_params_init(iga_atmo_t h, int geometry, iga_fan_params* p) {
             const double d2r = iga::kPi / 180.0, r2d = 180.0 / iga::kPi;
             p->src[0] = (p->lat_max * d2r + p->lat_min * d2r) / 2.0 * r2d;
             p->src[1] = (p->lon_max * d2r + p->lon_min * d2r) / 2.0 * r2d;
-            p->bounces = 2;
+            // infraga-sph over terrain keeps its 10 bounces (main.infraga.sph.cpp:209)
+            p->bounces = h->strat_topo ? 10 : 2;
         }
     }
     return IGA_OK;

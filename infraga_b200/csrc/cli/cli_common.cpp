@@ -161,16 +161,11 @@ iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_o
     iga_atmo_t a = nullptr;
     int rc;
     if (!is_rngdep(v) && topo) {
-        // set_region(atmo_file, topo_file, ...) (atmo_io.3d.strat.cpp:146-258)
+        // set_region(atmo_file, topo_file, ...) (atmo_io.3d.strat.cpp:146-258, atmo_io.sph.strat.cpp)
         std::cout << "Interpolating atmosphere data in '" << argv[2] << "' and topography data in '" << topo << "'..."
                   << '\n';
         if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
-        if (is_sph(v)) {
-            std::cout << '\t' << "ERROR: terrain (topo_file) with a spherical stratified profile is not provided by the"
-                      << " GPU front end; use infraga-sph-rngdep" << '\n' << '\n';
-            return nullptr;
-        }
-        rc = iga_atmo_load_topo(argv[2], topo, fmt, rev ? 1 : 0, IGA_GEOM_3D, &a);
+        rc = iga_atmo_load_topo(argv[2], topo, fmt, rev ? 1 : 0, is_sph(v) ? IGA_GEOM_SPH : IGA_GEOM_3D, &a);
         if (rc == IGA_E_IO) {
             std::cout << '\t' << "ERROR: Invalid terrain file or atmospheric specification (" << topo << ", " << argv[2]
                       << ")" << '\n' << '\n';
@@ -750,7 +745,7 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     o.verbose = direct && !sph;   // the spherical -eig_direct is quiet by default
     double incl_est = 10.0, az_est = 0.0;
     // source and receiver defaults of run_eig_search / run_eig_direct
-    if (v == Variant::kSph || (v == Variant::kSphRngdep && !has_topo)) {   // main.infraga.sph.cpp:788-789
+    if (is_sph(v) && !has_topo) {   // main.infraga.sph.cpp:788-789
         o.src[0] = 30.0; o.src[1] = 0.0; o.src[2] = 0.0;
         o.rcvr[0] = 30.0; o.rcvr[1] = -2.5;
     } else if (v == Variant::k3D && has_topo) {   // main.infraga.3d.cpp:812-815, :992-995
@@ -758,12 +753,13 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
         iga_atmo_region(atmo, &a0, &a1, &b0, &b1);
         o.src[0] = (a1 + a0) / 2.0; o.src[1] = (b1 + b0) / 2.0;
         o.rcvr[0] = o.src[0] - 250.0; o.rcvr[1] = o.src[1];
-    } else if (rd) {   // the centre of the region (main.infraga.3d.rngdep.cpp:816-817, sph.rngdep :821-822)
+    } else if (rd || sph) {   // the centre of the region (main.infraga.3d.rngdep.cpp:816-817, sph.rngdep :821-822,
+                              // infraga-sph over terrain main.infraga.sph.cpp:825-828 with the receiver 2.5 deg east)
         double a0, a1, b0, b1;
         iga_atmo_region(atmo, &a0, &a1, &b0, &b1);
         o.src[0] = (a1 + a0) / 2.0; o.src[1] = (b1 + b0) / 2.0; o.src[2] = 0.0;
         o.rcvr[0] = sph ? o.src[0] : o.src[0] + 250.0;
-        o.rcvr[1] = sph ? o.src[1] + 5.0 : o.src[1];
+        o.rcvr[1] = sph ? o.src[1] + (rd ? 5.0 : 2.5) : o.src[1];
     }
     // the range-dependent -eig_direct keep their inclination estimate in radians
     // when none is given: 0.5 (3D) and 10 (spherical)

@@ -15,6 +15,14 @@
 // (no boundary-layer vertical wind: topo_use_BLw=false, the default), its RK4
 // driver (src/util/rk4solver.cpp:14-85) and run_prop
 // (src/main.infraga.sph.rngdep.cpp:412-545).
+//
+// ST instantiations run infraga-sph's stratified profile over terrain
+// (topo_file=): c, u, v, rho from the 1D knot table at the clamped altitude
+// (atmo_state.sph.strat.cpp:166-245, calc_uvw :498-800) with the same terrain,
+// boundary-layer scaling, equations (geoac.eqset.sph.strat.cpp differs from
+// the range-dependent set only in where the atmosphere comes from) and bounce
+// loop; run_prop of infraga-sph records the arrival inclination as -asin(...)
+// (main.infraga.sph.cpp:523) where the range-dependent one has +asin.
 #include "eig3d.cuh"
 #include "fan3d.cuh"
 #include "fansph_common.cuh"
@@ -61,12 +69,35 @@ struct AtmFull {
     double v, dv[3], ddv[3][3];
 };
 
-template <bool AMP>
+// Stratified profile row at the altitude r - r_earth clamped to the knot
+// range (interp::in_interval); cl.hz caches the segment.
+__device__ __forceinline__ const double* strat_at(const Fan3DArgs& a, Cells& cl, double r, Cubic& q) {
+    const double ze = fmin(fmax(r - a.r_earth, a.z_lo), a.z_hi);
+    cl.hz = seg_walk(a.knots, a.n_knots, ze, cl.hz);
+    const double* r0 = a.knots + cl.hz * kStride;
+    q = cubic_at(r0, ze);
+    return r0;
+}
+
+template <bool AMP, bool ST>
 __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Cells& cl, double r, double lat, double lon,
                                          AtmFull& m) {
+    HybF2 c2 = {}, u2 = {}, v2 = {};
+    if (ST) {   // derivatives in r only
+        Cubic q;
+        const double* r0 = strat_at(a, cl, r, q);
+        if (AMP) {
+            cubic_f2(r0, q, 2, c2.f, c2.d[0], c2.dd[0][0]);
+            cubic_f2(r0, q, 4, u2.f, u2.d[0], u2.dd[0][0]);
+            cubic_f2(r0, q, 6, v2.f, v2.d[0], v2.dd[0][0]);
+        } else {
+            cubic_f1(r0, q, 2, c2.f, c2.d[0]);
+            cubic_f1(r0, q, 4, u2.f, u2.d[0]);
+            cubic_f1(r0, q, 6, v2.f, v2.d[0]);
+        }
+    } else {
     HybLoc L;
     hyb_locate(vw.hyb, lat, lon, r - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-    HybF2 c2, u2, v2;
     if (AMP) {
         hyb_f2(vw.hyb, L, 0, c2);
         hyb_f2(vw.hyb, L, 1, u2);
@@ -76,6 +107,7 @@ __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Ce
         hyb_f1(vw.hyb, L, 0, t); c2.f = t.f; c2.d[0] = t.d[0]; c2.d[1] = t.d[1]; c2.d[2] = t.d[2];
         hyb_f1(vw.hyb, L, 1, t); u2.f = t.f; u2.d[0] = t.d[0]; u2.d[1] = t.d[1]; u2.d[2] = t.d[2];
         hyb_f1(vw.hyb, L, 2, t); v2.f = t.f; v2.d[0] = t.d[0]; v2.d[1] = t.d[1]; v2.d[2] = t.d[2];
+    }
     }
     // boundary-layer scaling over the terrain (or flat ground)
     const double zr = r - a.r_earth;
@@ -132,10 +164,10 @@ __device__ __forceinline__ void atm_full(const Fan3DArgs& a, const Views& vw, Ce
 
 // RHS with full gradients: update_refs + eval_src_eq
 // (geoac.eqset.sph.rngdep.cpp:238-437), w = 0.
-template <bool AMP>
+template <bool AMP, bool ST>
 __device__ __forceinline__ void rhs_sphr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y, double* f) {
     AtmFull m;
-    atm_full<AMP>(a, vw, cl, y[0], y[1], y[2], m);
+    atm_full<AMP, ST>(a, vw, cl, y[0], y[1], y[2], m);
     const double r = y[0];
     double st, ct;
     sincos(y[1], &st, &ct);
@@ -207,8 +239,19 @@ __device__ __forceinline__ double bl_sc(const Fan3DArgs& a, const Views& vw, Cel
 struct AtmPt {
     double c, u, v, rho;
 };
+template <bool ST>
 __device__ __forceinline__ void atm_point(const Fan3DArgs& a, const Views& vw, Cells& cl, double r, double lat, double lon,
                                           AtmPt& o) {
+    if (ST) {
+        const double sc = bl_sc(a, vw, cl, r, lat, lon);
+        Cubic q;
+        const double* r0 = strat_at(a, cl, r, q);
+        o.c = cubic_f(r0, q, 2);
+        o.u = cubic_f(r0, q, 4) * sc;
+        o.v = cubic_f(r0, q, 6) * sc;
+        o.rho = cubic_f(r0, q, 8);
+        return;
+    }
     HybLoc L;
     hyb_locate(vw.hyb, lat, lon, r - a.r_earth, L, cl.hx, cl.hy, cl.hz);
     const double sc = bl_sc(a, vw, cl, r, lat, lon);
@@ -218,9 +261,23 @@ __device__ __forceinline__ void atm_point(const Fan3DArgs& a, const Views& vw, C
     o.rho = hyb_f(vw.hyb, L, 3);
 }
 
+// atmo::c alone at (r, lat, lon)
+template <bool ST>
+__device__ __forceinline__ double c_at(const Fan3DArgs& a, const Views& vw, Cells& cl, double r, double lat, double lon) {
+    if (ST) {
+        Cubic q;
+        const double* r0 = strat_at(a, cl, r, q);
+        return cubic_f(r0, q, 2);
+    }
+    HybLoc L;
+    hyb_locate(vw.hyb, lat, lon, r - a.r_earth, L, cl.hx, cl.hy, cl.hz);
+    return hyb_f(vw.hyb, L, 0);
+}
+
 // travel_time / atten segment (geoac.eqset.sph.rngdep.cpp:547-579, 775-796):
 // the atmosphere is read at (r, lat, lon) of the segment midpoint with the
 // longitude midpoint taken before the +-2 pi wrap of dp.
+template <bool ST>
 __device__ __forceinline__ void seg_increment_sphr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y0,
                                                    const double* y1, double& dt_out, double& da_out) {
     const double dr = y1[0] - y0[0], rm = y0[0] + dr * 0.5;
@@ -236,7 +293,7 @@ __device__ __forceinline__ void seg_increment_sphr(const Fan3DArgs& a, const Vie
     const double n2 = y0[5] + (y1[5] - y0[5]) * 0.5;
     const double num = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
     AtmPt m;
-    atm_point(a, vw, cl, rm, tm, pm, m);
+    atm_point<ST>(a, vw, cl, rm, tm, pm, m);
     const double inum = 1.0 / num;
     const double cp0 = m.c * n0 * inum, cp1 = m.c * n1 * inum + m.v, cp2 = m.c * n2 * inum + m.u;
     dt_out = ds / sqrt(cp0 * cp0 + cp1 * cp1 + cp2 * cp2);
@@ -244,10 +301,11 @@ __device__ __forceinline__ void seg_increment_sphr(const Fan3DArgs& a, const Vie
 }
 
 // geoac::amp / jacobian at the below-ground row (geoac.eqset.sph.rngdep.cpp:798-850)
+template <bool ST>
 __device__ __noinline__ double amp_db_sphr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y, double theta,
                                            double phi, double* jac_out) {
     AtmPt m;
-    atm_point(a, vw, cl, y[0], y[1], y[2], m);
+    atm_point<ST>(a, vw, cl, y[0], y[1], y[2], m);
     const double r = y[0], n0 = y[3], n1 = y[4], n2 = y[5];
     double st, ct, sp, cp;
     sincos(theta, &st, &ct);
@@ -278,7 +336,7 @@ __device__ __noinline__ double amp_db_sphr(const Fan3DArgs& a, const Views& vw, 
 
 // approx_intercept + set_refl (geoac.eqset.sph.rngdep.cpp:117-224), general
 // terrain; p = row k-2 on entry (the shared-memory copy), y = row k-1 (in/out).
-template <int N, bool AMP>
+template <int N, bool AMP, bool ST>
 __device__ __noinline__ void reflect_sphr(const Fan3DArgs& a, const Views& vw, Cells& cl, double* y, const double* prev) {
     // approx_intercept with the terrain slope at row k-1
     double zy = a.r_grnd, dzy[2] = {0.0, 0.0};
@@ -318,12 +376,20 @@ __device__ __noinline__ void reflect_sphr(const Fan3DArgs& a, const Views& vw, C
         // atmosphere at the intercept: c and its gradient (atmo::c/dc), and
         // du, dv = df * sc + f * dsc with the scaling at the ground itself
         // (X = 1: sc = 0, dsc = (1/bl)/2 * (1, -dz_lat, -dz_lon))
-        HybLoc L;
-        hyb_locate(vw.hyb, p[1], p[2], rg - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-        HybF1 cc, uu, vv;
-        hyb_f1(vw.hyb, L, 0, cc);
-        hyb_f1(vw.hyb, L, 1, uu);
-        hyb_f1(vw.hyb, L, 2, vv);
+        HybF1 cc = {}, uu = {}, vv = {};
+        if (ST) {   // atmo::c, dc, du, dv at the ground point (atmo_state.sph.strat.cpp:172-234)
+            Cubic qz;
+            const double* r0 = strat_at(a, cl, rg, qz);
+            cubic_f1(r0, qz, 2, cc.f, cc.d[0]);
+            cubic_f1(r0, qz, 4, uu.f, uu.d[0]);
+            cubic_f1(r0, qz, 6, vv.f, vv.d[0]);
+        } else {
+            HybLoc L;
+            hyb_locate(vw.hyb, p[1], p[2], rg - a.r_earth, L, cl.hx, cl.hy, cl.hz);
+            hyb_f1(vw.hyb, L, 0, cc);
+            hyb_f1(vw.hyb, L, 1, uu);
+            hyb_f1(vw.hyb, L, 2, vv);
+        }
         const double c_grnd = cc.f;
         const double Xg = exp(-(rg - rg) * a.inv_bl);
         const double scg = (1.0 - Xg) / (1.0 + Xg);
@@ -396,7 +462,7 @@ __device__ __noinline__ void reflect_sphr(const Fan3DArgs& a, const Views& vw, C
 // PATHS: also write the sampled per-step rows and caustic points of
 // run_prop's write_rays / write_topo / write_caustics output
 // (main.infraga.sph.rngdep.cpp:450-503); the fan results are unchanged.
-template <bool AMP, bool PATHS>
+template <bool AMP, bool PATHS, bool ST>
 __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(const __grid_constant__ Fan3DArgs a) {
     constexpr int N = DimSph<AMP>::n;
     extern __shared__ double s_mem[];
@@ -452,7 +518,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
             ds -= (a.ds_max - a.ds_min) * exp(-(y[0] - topo_r(a, vw, cl, y[1], y[2])) / 0.2);
         s += ds;
         double acc[N], stg[N], f[N];
-        rhs_sphr<AMP>(a, vw, cl, y, f);
+        rhs_sphr<AMP, ST>(a, vw, cl, y, f);
         if (AMP && (a.aux || (PATHS && a.caus_rows)) && kb >= 1) {
             const double D = ray_det_sph(f, y);
             if (kb >= 2 && D * D_prev < 0.0) {
@@ -470,13 +536,13 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         }
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-        rhs_sphr<AMP>(a, vw, cl, stg, f);
+        rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-        rhs_sphr<AMP>(a, vw, cl, stg, f);
+        rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-        rhs_sphr<AMP>(a, vw, cl, stg, f);
+        rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
         kb++;
@@ -493,7 +559,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
         const bool gnd = !esc && (acc[0] - a.r_earth <= a.topo_zmax) && (acc[0] < topo_r(a, vw, cl, acc[1], acc[2]));
 
         double dt, da;
-        seg_increment_sphr(a, vw, cl, y, acc, dt, da);
+        seg_increment_sphr<ST>(a, vw, cl, y, acc, dt, da);
         if (a.write_rays) { tt += pt; att += pa; pt = dt; pa = da; }
         else { pt += dt; pa += da; }
 
@@ -512,7 +578,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
                     o[0] = y[1] * rad2deg; o[1] = y[2] * rad2deg;
                     o[2] = a.path_mode == kPathRays ? y[0] - a.r_earth : topo_r(a, vw, c2, y[1], y[2]) - a.r_earth;
                     o[3] = (AMP && a.path_mode == kPathRays)
-                               ? amp_db_sphr(a, vw, c2, y, a.theta_deg[ray] * (kPi / 180.0),
+                               ? amp_db_sphr<ST>(a, vw, c2, y, a.theta_deg[ray] * (kPi / 180.0),
                                              kPi / 2.0 - a.phi_deg[ray] * (kPi / 180.0), nullptr)
                                : 0.0;
                     o[4] = -2.0 * (att + pa); o[5] = tt + pt; o[6] = (double)bnc;
@@ -536,9 +602,10 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
             const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
             AtmPt mk;
-            atm_point(a, vw, cl, acc[0], acc[1], acc[2], mk);
-            // the range-dependent run_prop records +asin(...) (main.infraga.sph.rngdep.cpp:514)
-            const double incl = asin(mk.c / a.c0 * acc[3]) * 180.0 / kPi;
+            atm_point<ST>(a, vw, cl, acc[0], acc[1], acc[2], mk);
+            // the range-dependent run_prop records +asin(...) (main.infraga.sph.rngdep.cpp:514),
+            // infraga-sph -asin(...) (main.infraga.sph.cpp:523)
+            const double incl = (ST ? -1.0 : 1.0) * asin(mk.c / a.c0 * acc[3]) * 180.0 / kPi;
             double baz = 90.0 - atan2(-acc[4], -acc[5]) * 180.0 / kPi;
             if (baz < -180.0) baz += 360.0;
             else if (baz > 180.0) baz -= 360.0;
@@ -553,7 +620,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
             out[8] = incl;
             out[9] = baz;
             double jac = 0.0;
-            out[10] = AMP ? amp_db_sphr(a, vw, cl, acc, th_deg * (kPi / 180.0), kPi / 2.0 - ph_deg * (kPi / 180.0), &jac) : 0.0;
+            out[10] = AMP ? amp_db_sphr<ST>(a, vw, cl, acc, th_deg * (kPi / 180.0), kPi / 2.0 - ph_deg * (kPi / 180.0), &jac) : 0.0;
             out[11] = -2.0 * att;
             if (a.aux) {
                 double* ax = a.aux + ((size_t)ray * nb + na) * 4;
@@ -561,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
                 else ax[0] = ax[1] = ax[2] = ax[3] = 0.0;
             }
             na++;
-            reflect_sphr<N, AMP>(a, vw, cl, y, prev);
+            reflect_sphr<N, AMP, ST>(a, vw, cl, y, prev);
             bnc++;
             if (bnc > a.bounces) status = 0;
         }
@@ -579,11 +646,11 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) fansphr_fp64_kernel(c
     }
 }
 
-template <bool AMP, bool PATHS>
+template <bool AMP, bool PATHS, bool ST>
 cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     // threads per block: the caller's choice (a multiple of 32 up to kThreads) or kThreads
     const int threads = a.block > 0 ? a.block : kThreads;
-    auto kern = fansphr_fp64_kernel<AMP, PATHS>;
+    auto kern = fansphr_fp64_kernel<AMP, PATHS, ST>;
     const size_t smem = ((size_t)DimSph<AMP>::n * threads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -614,7 +681,7 @@ cudaError_t launch_impl(const Fan3DArgs& a, cudaStream_t stream, int* grid_used)
 // source and on the ground, the ground radius and the terrain gradient.
 // Same block size as the fan kernel (reflect_sphr reads row k-2 from shared
 // memory with that stride).
-template <bool AMP>
+template <bool AMP, bool ST>
 __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel(const __grid_constant__ Fan3DArgs a,
                                                                               const TraceReq* __restrict__ reqs,
                                                                               TraceRes18* __restrict__ out, int n, unsigned int* __restrict__ queue,
@@ -666,16 +733,16 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
                     ds -= (a.ds_max - a.ds_min) * exp(-(y[0] - topo_r(a, vw, cl, y[1], y[2])) / 0.2);
                 s += ds;
                 double stg[N], f[N];
-                rhs_sphr<AMP>(a, vw, cl, y, f);
+                rhs_sphr<AMP, ST>(a, vw, cl, y, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-                rhs_sphr<AMP>(a, vw, cl, stg, f);
+                rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-                rhs_sphr<AMP>(a, vw, cl, stg, f);
+                rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-                rhs_sphr<AMP>(a, vw, cl, stg, f);
+                rhs_sphr<AMP, ST>(a, vw, cl, stg, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
                 kb++;
@@ -690,7 +757,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
                 const bool gnd = !esc && (acc[0] - a.r_earth <= a.topo_zmax) && (acc[0] < topo_r(a, vw, cl, acc[1], acc[2]));
                 if (record) {
                     double dt, da;
-                    seg_increment_sphr(a, vw, cl, y, acc, dt, da);
+                    seg_increment_sphr<ST>(a, vw, cl, y, acc, dt, da);
                     tt += pt; att += pa; pt = dt; pa = da;
                 }
                 if (!esc && !gnd) {
@@ -710,7 +777,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
                 g.x = acc[1]; g.y = acc[2]; g.steps = steps; g.escaped = esc ? 1 : 0;
             }
             if (sg == q.n_seg - 1 || (esc && stop)) break;
-            reflect_sphr<N, AMP>(a, vw, cl, y, prev);
+            reflect_sphr<N, AMP, ST>(a, vw, cl, y, prev);
         }
         TraceRes18& o = out[r];
 #pragma unroll
@@ -726,19 +793,14 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
                 topo_eval(vw.topo, acc[1], acc[2], 1, t, cl.tx, cl.ty);
                 rg = a.r_earth + t.z; o.dzg[0] = t.d[0]; o.dzg[1] = t.d[1];
             }
-            HybLoc L;
-            hyb_locate(vw.hyb, acc[1], acc[2], rg - a.r_earth, L, cl.hx, cl.hy, cl.hz);
             o.z_grnd = rg;
-            o.c_grnd = hyb_f(vw.hyb, L, 0);
+            o.c_grnd = c_at<ST>(a, vw, cl, rg, acc[1], acc[2]);
         }
         if (record) {
             o.tt = tt; o.att = att; o.zmax = rmax;
-            o.amp_db = AMP ? amp_db_sphr(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
-            HybLoc L;
-            hyb_locate(vw.hyb, acc[1], acc[2], acc[0] - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-            const double c_k = hyb_f(vw.hyb, L, 0);
-            hyb_locate(vw.hyb, a.src_x, a.src_y, a.src_z - a.r_earth, L, cl.hx, cl.hy, cl.hz);
-            const double c_s = hyb_f(vw.hyb, L, 0);
+            o.amp_db = AMP ? amp_db_sphr<ST>(a, vw, cl, acc, q.theta, q.phi, nullptr) : 0.0;
+            const double c_k = c_at<ST>(a, vw, cl, acc[0], acc[1], acc[2]);
+            const double c_s = c_at<ST>(a, vw, cl, a.src_z, a.src_x, a.src_y);   // r = the source altitude
             o.incl = -asin(c_k / c_s * acc[3]) * 180.0 / kPi;
             double baz = 90.0 - atan2(-acc[4], -acc[5]) * (180.0 / kPi);
             while (baz < -180.0) baz += 360.0;
@@ -748,11 +810,11 @@ __global__ void __launch_bounds__(kThreads, IGA_SPHR_MINB) tracesphr_fp64_kernel
     }
 }
 
-template <bool AMP>
+template <bool AMP, bool ST>
 cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, cudaStream_t st,
                               SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
-    auto kern = tracesphr_fp64_kernel<AMP>;
+    auto kern = tracesphr_fp64_kernel<AMP, ST>;
     const size_t smem = ((size_t)DimSph<AMP>::n * kThreads + a.hyb_nz + a.hyb_nx + a.hyb_ny + a.topo_nx + a.topo_ny) *
                         sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -764,18 +826,27 @@ cudaError_t launch_trace_impl(const Fan3DArgs& a, const TraceReq* d_req, TraceRe
     return cudaGetLastError();
 }
 
+// a.knots set (no hybrid tables): stratified profile over terrain
+template <bool ST>
+cudaError_t launch_fan(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
+    if (a.path_rows || a.caus_rows)
+        return calc_amp ? launch_impl<true, true, ST>(a, stream, grid_used) : launch_impl<false, true, ST>(a, stream, grid_used);
+    return calc_amp ? launch_impl<true, false, ST>(a, stream, grid_used) : launch_impl<false, false, ST>(a, stream, grid_used);
+}
+
 }  // namespace
 
 cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
-    if (a.path_rows || a.caus_rows)
-        return calc_amp ? launch_impl<true, true>(a, stream, grid_used) : launch_impl<false, true>(a, stream, grid_used);
-    return calc_amp ? launch_impl<true, false>(a, stream, grid_used) : launch_impl<false, false>(a, stream, grid_used);
+    return a.knots ? launch_fan<true>(a, calc_amp, stream, grid_used) : launch_fan<false>(a, calc_amp, stream, grid_used);
 }
 
 cudaError_t launch_trace_sphr(const Fan3DArgs& a, const TraceReq* d_req, TraceRes18* d_res, int n, bool amp,
                               cudaStream_t st, SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
-    return amp ? launch_trace_impl<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
-               : launch_trace_impl<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    if (a.knots)
+        return amp ? launch_trace_impl<true, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+                   : launch_trace_impl<false, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    return amp ? launch_trace_impl<true, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_impl<false, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga

@@ -28,7 +28,8 @@ OUT = os.path.join(HERE, "cli")
 # name -> (binary, atmosphere kind, seed of the 1D profile, argv after the binary)
 # kinds: "1d" = profiles/gen{seed}.met staged as atmo.met;
 #        "sphr" / "3dr" = the rngdep/ or rngdep3d/ grid staged as grid/node*, grid/x.dat, grid/y.dat, topo.dat;
-#        "1dt" = profiles/gen{seed}.met as atmo.met over the rngdep3d/ terrain as topo.dat
+#        "1dt" / "1dts" = profiles/gen{seed}.met as atmo.met over the rngdep3d/ (x, y) or rngdep/ (lat, lon)
+#        terrain as topo.dat
 CASES = {
     "3d_prop": ("infraga-3d", "1d", 0,
                 ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=90",
@@ -78,6 +79,16 @@ CASES = {
     "3dt_direct": ("infraga-3d", "1dt", 0,
                    ["-eig_direct", "atmo.met", "topo_file=topo.dat", "rcvr_x=240", "rcvr_y=0", "incl_est=20",
                     "bounces=0", "output_id=direct"]),
+    "spht_prop": ("infraga-sph", "1dts", 0,
+                  ["-prop", "atmo.met", "topo_file=topo.dat", "incl_min=6", "incl_max=26", "incl_step=10", "az_min=90",
+                   "az_max=270", "az_step=180", "bounces=1", "max_rng=400", "max_ds=0.25", "write_caustics=true",
+                   "write_topo=true"]),
+    "spht_noamp": ("infraga-sph", "1dts", 1,
+                   ["-p", "atmo.met", "topo_file=topo.dat", "incl_min=10", "incl_max=30", "incl_step=5", "azimuth=-60",
+                    "bounces=2", "max_rng=500", "calc_amp=false", "write_rays=false", "freq=0.3"]),
+    "spht_eig": ("infraga-sph", "1dts", 0,
+                 ["-eig_search", "atmo.met", "topo_file=topo.dat", "src_alt=3", "rcvr_lat=32.98", "rcvr_lon=-104.6",
+                  "incl_min=10", "incl_max=30"]),
     "sphr_eig": ("infraga-sph-rngdep", "sphr", 0,
                  ["-eig_search", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "src_alt=3",
                   "rcvr_lat=32.98", "rcvr_lon=-104.6", "incl_min=10", "incl_max=30"]),
@@ -93,10 +104,11 @@ CASES = {
 
 def stage(work: str, kind: str, seed: int) -> None:
     """Input files of a case in `work` under fixed relative names."""
-    if kind in ("1d", "1dt"):
+    if kind in ("1d", "1dt", "1dts"):
         shutil.copy(os.path.join(HERE, "profiles", f"gen{seed}.met"), os.path.join(work, "atmo.met"))
-        if kind == "1dt":
-            shutil.copy(os.path.join(HERE, "rngdep3d", "topo.dat"), os.path.join(work, "topo.dat"))
+        if kind != "1d":
+            shutil.copy(os.path.join(HERE, "rngdep3d" if kind == "1dt" else "rngdep", "topo.dat"),
+                        os.path.join(work, "topo.dat"))
         return
     src = os.path.join(HERE, "rngdep" if kind == "sphr" else "rngdep3d")
     ax = ("node_lat.dat", "node_lon.dat") if kind == "sphr" else ("node_x.dat", "node_y.dat")
