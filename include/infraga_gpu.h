@@ -264,14 +264,27 @@ int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
  * main.infraga.3d.cpp:470-475; the 3D range-dependent CLI also writes a
  * 0.0 column before the time, main.infraga.3d.rngdep.cpp:467-471). */
 #define IGA_CAUSTIC_COLS 5
+/* Back-projection row (.projection.dat of run_back_proj,
+ * main.infraga.3d.cpp:673-690 and :711-735): x, y, z [km], time [s],
+ * X_incl, Y_incl, Z_incl [km/deg], T_incl [s/deg], X_az, Y_az, Z_az [km/deg],
+ * T_az [s/deg], group velocity x, y, z [km/s].  The T columns are the
+ * reference's travel_time_var sums (geoac.eqset.3d.strat.cpp:597-670), kept
+ * as written: they are decremented, and the last d|c_g| term multiplies where
+ * it should add. */
+#define IGA_PROJ_COLS 15
 enum iga_path_mode {
     IGA_PATH_RAYS = 0,       /* rows m == 1 and m % 15 == 0 of every bounce (write_rays) */
-    IGA_PATH_TERRAIN = 1     /* rows m % 10 == 1 (write_topo) */
+    IGA_PATH_TERRAIN = 1,    /* rows m % 10 == 1 (write_topo) */
+    IGA_PATH_PROJ = 2        /* rows m == 1 and m % 5 == 0, IGA_PROJ_COLS wide (-back_proj);
+                                3D stratified flat-ground handles, calc_amp = 1, no caustics */
 };
 
 /* Replaces the write_rays / write_topo / write_caustics branches of run_prop's
  * per-ray loop (src/main.infraga.3d.cpp:443-497, main.infraga.sph.cpp:455-510,
- * main.infraga.3d.rngdep.cpp:440-488, main.infraga.sph.rngdep.cpp:450-503):
+ * main.infraga.3d.rngdep.cpp:440-488, main.infraga.sph.rngdep.cpp:450-503)
+ * and, with IGA_PATH_PROJ, the projection rows of run_back_proj
+ * (main.infraga.3d.cpp:701-741; the caller passes the reversed-wind
+ * atmosphere, the receiver as src and turn_ht_min = -1e30):
  * for every ray of the fan, the RK4 rows m (1 <= m < k of each bounce
  * segment) that the reference samples, with time and absorption summed per
  * step as the reference does whenever it writes paths (params->write_rays is
@@ -284,7 +297,8 @@ enum iga_path_mode {
  *               (nullable, n_rays + 1) = first row of each ray and the total.
  *               The rows of ray i number at most
  *               (bounces + 1) + ray_steps[i] / 15 (IGA_PATH_RAYS; / 10 for
- *               IGA_PATH_TERRAIN) + 1.
+ *               IGA_PATH_TERRAIN, / 5 for IGA_PATH_PROJ) + 1; IGA_PATH_PROJ
+ *               rows are IGA_PROJ_COLS wide.
  *   caustic_rows nullable: caustic_cap rows of IGA_CAUSTIC_COLS, ray by ray
  *               in step order; *n_caustic = rows produced; caustic_ray
  *               (nullable, caustic_cap) the ray of each row.

@@ -350,25 +350,26 @@ def eig_direct(atmo: Atmosphere, params: EigParams, src, rcvr, incl_est: float, 
     return row if found.value else None
 
 
-PATH_RAYS, PATH_TERRAIN = 0, 1
-PATH_COLS, CAUSTIC_COLS = 7, 5
+PATH_RAYS, PATH_TERRAIN, PATH_PROJ = 0, 1, 2
+PATH_COLS, CAUSTIC_COLS, PROJ_COLS = 7, 5, 15
 
 
 def fan_paths(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, mode: int = PATH_RAYS,
               caustics: bool = False, ray_steps=None):
-    """Sampled ray-path rows (run_prop's write_rays / write_topo rows) and,
-    with ``caustics``, caustic points of a fan.  Returns a dict with
-    ``paths`` [n, 7], ``path_start`` [n_rays + 1] and, with caustics,
-    ``caustics`` [m, 5] and ``caustic_ray`` [m]."""
+    """Sampled ray-path rows (run_prop's write_rays / write_topo rows, or
+    run_back_proj's projection rows with mode=PATH_PROJ) and, with
+    ``caustics``, caustic points of a fan.  Returns a dict with ``paths``
+    [n, 7] ([n, 15] for PATH_PROJ), ``path_start`` [n_rays + 1] and, with
+    caustics, ``caustics`` [m, 5] and ``caustic_ray`` [m]."""
     th = np.ascontiguousarray(theta_deg, dtype=np.float64)
     ph = np.ascontiguousarray(phi_deg, dtype=np.float64)
     n = th.size
     if ray_steps is None:
         ray_steps = fan_run(atmo, params, th, ph)["ray_steps"]
     steps = np.ascontiguousarray(ray_steps, dtype=np.int64)
-    div = 15 if mode == PATH_RAYS else 10
+    div = {PATH_RAYS: 15, PATH_TERRAIN: 10, PATH_PROJ: 5}[mode]
     cap = int(np.sum(params.bounces + 1 + steps // div + 1))
-    rows = np.zeros((max(cap, 1), PATH_COLS), dtype=np.float64)
+    rows = np.zeros((max(cap, 1), PROJ_COLS if mode == PATH_PROJ else PATH_COLS), dtype=np.float64)
     start = np.zeros(n + 1, dtype=np.int64)
     n_path = _LL()
     ccap = 4096 if caustics else 0

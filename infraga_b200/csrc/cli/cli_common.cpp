@@ -119,9 +119,12 @@ void usage(Variant v) {
     std::cout << '\t' << "-eig_direct  one eigenray near (incl_est, az_est) with a given bounce count" << '\n';
     std::cout << '\t' << "Common: freq, abs_coeff, z_grnd, prof_format, reverse_winds, output_id, calc_amp, max_alt, max_rng,"
               << '\n' << '\t' << "        " << (sph ? "min_lat, max_lat, min_lon, max_lon, max_time" : "min_x, max_x, min_y, max_y")
-              << ", min_ds, max_ds, max_s" << (rd ? ", topo_file" : "") << '\n';
-    std::cout << '\t' << "-back_proj, -wnl_wvfrm and the reference's MPI builds are not provided by the GPU front end." << '\n'
-              << '\n';
+              << ", min_ds, max_ds, max_s, topo_file" << '\n';
+    if (v == Variant::k3D)
+        std::cout << '\t' << "-back_proj   one ray from (rcvr_x, rcvr_y) at (inclination, azimuth) through the reversed"
+                  << " winds (bounces)" << '\n';
+    std::cout << '\t' << (v == Variant::k3D ? "" : "-back_proj, ")
+              << "-wnl_wvfrm and the reference's MPI builds are not provided by the GPU front end." << '\n' << '\n';
 }
 
 void version() {
@@ -884,6 +887,126 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     return 0;
 }
 
+// ------------------------------------------------------------------------
+// -back_proj (infraga-3d, flat ground): run_back_proj, main.infraga.3d.cpp:559-770
+// ------------------------------------------------------------------------
+
+// One ray from the receiver through the reversed winds; {id}.projection.dat
+// holds its rows m == 1 and m % 5 == 0 with the inclination / azimuth
+// derivatives of position and travel time and the group velocity
+// (iga_fan_paths, IGA_PATH_PROJ), the console the arrival at the last bounce.
+int run_back(int argc, char** argv, Variant v) {
+    if (v != Variant::k3D) {
+        std::cout << "-back_proj is not provided by the GPU front end." << '\n';
+        return 0;
+    }
+    banner(v, "Back Projection");
+    const char* fmt = "zTuvdp";
+    const char* topo = nullptr;
+    const char* val;
+    for (int i = 3; i < argc; i++) {
+        if (key(argv[i], "prof_format=", &val)) fmt = val;
+        else if (key(argv[i], "topo_file=", &val)) topo = val;
+    }
+    if (topo) {
+        std::cout << '\t' << "ERROR: -back_proj over terrain is not provided by the GPU front end" << '\n';
+        return 0;
+    }
+    std::cout << "Interpolating atmosphere data in '" << argv[2] << "' using format '" << fmt << "'..." << '\n';
+    std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
+    iga_atmo_t atmo = nullptr;
+    int rc = iga_atmo_load(argv[2], fmt, 1, &atmo);   // set_region(..., true): winds reversed
+    if (rc == IGA_E_IO) {
+        std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\n';
+        return 0;
+    }
+    if (rc) return fail("loading the atmosphere", rc);
+    iga_fan_params p;
+    if ((rc = iga_fan_params_default(atmo, &p))) return fail("parameters", rc);
+    print_region(v, p);
+    PropOpts o;
+    double incl = 15.0, az = 90.0, xr = 0.0, yr = 0.0, freq = 0.1;
+    int bounces = 0;
+    for (int i = 3; i < argc; i++) {
+        const char* a = argv[i];
+        if (key(a, "inclination=", &val)) incl = atof(val);
+        else if (key(a, "azimuth=", &val)) az = atof(val);
+        else if (key(a, "bounces=", &val)) bounces = std::max(0, atoi(val));
+        else if (key2(a, "rcvr_x=", "x_rcvr=", &val)) xr = atof(val);
+        else if (key2(a, "rcvr_y=", "y_rcvr=", &val)) yr = atof(val);
+        else if (common_key(v, a, p, o, false, freq)) {}
+        else if (!confirm_unknown(a, false)) return 0;
+    }
+    if (o.use_blw) {
+        std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
+        return 0;
+    }
+    if (o.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
+    const double zr = std::max(p.z_grnd, 0.0);   // z_rcvr = max(topo::z, 0)
+    // the reference echoes geoac::theta / phi converted back to degrees
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "inclination: " << incl * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "azimuth: " << 90.0 - (Pi / 2.0 - az * (Pi / 180.0)) * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "bounces: " << bounces << '\n';
+    std::cout << '\t' << "receiver location: " << xr << ", " << yr << ", " << zr << '\n';
+    std::cout << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    std::cout << '\t' << "frequency: " << freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n' << '\n';
+    if (!o.output_id) {
+        strip_extension(argv[2]);
+        o.output_id = argv[2];
+    }
+    const std::string id = o.output_id;
+    p.bounces = bounces;
+    p.calc_amp = 1;
+    p.write_rays = 1;
+    p.src[0] = xr; p.src[1] = yr; p.src[2] = zr;
+    p.freq = freq;
+    p.turn_ht_min = -1.0e30;   // run_back_proj has no turning-height cut
+    p.precision = IGA_FP64;
+    const int nb = bounces + 1;
+    std::vector<double> arr((size_t)nb * IGA_ARRIVAL_COLS);
+    long long st = 0;
+    int n_out = 0;
+    rc = iga_fan_run(atmo, &p, &incl, &az, 1, arr.data(), nb, &n_out, nullptr, &st, nullptr, nullptr, nullptr);
+    if (rc) return fail("back projection", rc);
+    const long long cap = (long long)nb + st / 5 + 1;
+    std::vector<double> rows((size_t)cap * IGA_PROJ_COLS);
+    long long np = 0;
+    rc = iga_fan_paths(atmo, &p, &incl, &az, 1, IGA_PATH_PROJ, &st, rows.data(), cap, &np, nullptr, nullptr, 0, nullptr,
+                       nullptr);
+    if (rc) return fail("back projection rows", rc);
+    std::ofstream f((id + ".projection.dat").c_str());
+    f << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "time [s]" << '\t' << "X^{(incl)} [km/deg]" << '\t'
+      << "Y^{(incl)} [km/deg]" << '\t' << "Z^{(incl)} [km/deg]" << '\t' << "T^{(incl)} [s/deg]" << '\t'
+      << "X^{(az)} [km/deg]" << '\t' << "Y^{(az)} [km/deg]" << '\t' << "Z^{(az)} [km/deg]" << '\t' << "T^{(az)} [s/deg]"
+      << '\t' << "c_{g,x} [m/s]" << '\t' << "c_{g,y} [m/s]" << '\t' << "c_{g,z} [m/s]" << '\n';
+    for (long long j = 0; j < np; j++) {
+        const double* q = &rows[(size_t)j * IGA_PROJ_COLS];
+        f << q[0];
+        for (int c = 1; c < IGA_PROJ_COLS; c++) f << '\t' << q[c];
+        f << '\n';
+    }
+    // the arrival after the last bounce, as run_back_proj prints it
+    if (n_out == nb) {
+        const double* q = &arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS];
+        std::cout << '\t' << "Back projected arrival:" << '\n';
+        std::cout << '\t' << '\t' << "x [km E-W] = " << q[3] << '\n';
+        std::cout << '\t' << '\t' << "y [km N-S] = " << q[4] << '\n';
+        std::cout << '\t' << '\t' << "time [s] = " << q[5] << '\n';
+        std::cout << '\t' << '\t' << "celerity [km/s] = " << q[6] << '\n';
+        std::cout << '\t' << '\t' << "turning height [km] = " << q[7] << '\n';
+        std::cout << '\t' << '\t' << "arrival inclination [deg] = " << q[8] << '\n';
+        std::cout << '\t' << '\t' << "back azimuth = " << q[9] << '\n';
+        std::cout << '\t' << '\t' << "trans. coeff. [dB] = " << q[10] << '\n';
+        std::cout << '\t' << '\t' << "absorption [dB] = " << q[11] << '\n' << '\n';
+    } else {
+        std::cout << '\n' << '\t' << '\t' << "Ray path does not return to the ground." << '\n' << '\n';
+    }
+    iga_atmo_destroy(atmo);
+    return 0;
+}
+
 }  // namespace
 
 int run(int argc, char** argv, Variant v) {
@@ -897,7 +1020,7 @@ int run(int argc, char** argv, Variant v) {
     else if (strncmp(o, "-usage", 6) == 0 || strncmp(o, "-u", 2) == 0) usage(v);
     else if (strncmp(o, "-prop", 5) == 0 || strncmp(o, "-p", 2) == 0) return run_prop(argc, argv, v);
     else if (strncmp(o, "-back_proj", 10) == 0 || strncmp(o, "-b", 2) == 0)
-        std::cout << "-back_proj is not provided by the GPU front end." << '\n';
+        return run_back(argc, argv, v);
     else if (strncmp(o, "-eig_search", 11) == 0 || strncmp(o, "-s", 2) == 0) {
         return run_eig(argc, argv, v, false);
     } else if (strncmp(o, "-eig_direct", 11) == 0 || strncmp(o, "-d", 2) == 0) {

@@ -96,19 +96,26 @@ constexpr int kStrideF = 14;  // floats per segment row of the FP32 table
 // [dB] (0 without calc_amp or in terrain mode), absorption [dB] (-2 x the
 // running sum), travel time [s], bounce.  Caustic rows: position (3), time,
 // bounce, ray, and the ray's step index of the row (for ordering).
+// Back-projection rows (kPathProj, 3D stratified flat-ground kernel only):
+// x, y, z [km], time [s], X_incl (3) [km/deg], T_incl [s/deg], X_az (3),
+// T_az, group velocity (3) [km/s].
 constexpr int kPathCols = 7;
+constexpr int kProjCols = 15;
 constexpr int kCausCols = 7;
 constexpr int kPathRays = 0;      // rows m == 1 and m % 15 == 0 of each bounce (raypaths)
 constexpr int kPathTerrain = 1;   // rows m % 10 == 1 (terrain under the ray)
+constexpr int kPathProj = 2;      // rows m == 1 and m % 5 == 0 (back projection)
 
 __host__ __device__ inline bool path_sampled(int mode, int m) {
-    return mode == kPathRays ? (m == 1 || m % 15 == 0) : (m % 10 == 1);
+    return mode == kPathRays ? (m == 1 || m % 15 == 0) : (mode == kPathTerrain ? (m % 10 == 1) : (m == 1 || m % 5 == 0));
 }
+
+__host__ __device__ inline int path_cols(int mode) { return mode == kPathProj ? kProjCols : kPathCols; }
 
 // Upper bound on the path rows of a ray that took `steps` RK4 steps over at
 // most `segments` bounce segments: each segment of K rows samples m in 1..K-1.
 inline long long path_rows_bound(int mode, long long steps, int segments) {
-    return (long long)segments + steps / (mode == kPathRays ? 15 : 10) + 1;
+    return (long long)segments + steps / (mode == kPathRays ? 15 : (mode == kPathTerrain ? 10 : 5)) + 1;
 }
 
 cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);

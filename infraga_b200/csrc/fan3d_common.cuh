@@ -138,6 +138,54 @@ static __device__ __forceinline__ void seg_increment(const double* __restrict__ 
     da = sb_alpha_cart(c, rho, zm, a.freq, a.tweak_abs, a.sb) * ds;
 }
 
+// geoac::travel_time_var of one segment, the (k1, k2) form run_back_proj
+// calls (geoac.eqset.3d.strat.cpp:597-670): the inclination and azimuth
+// variations of the travel-time increment from the midpoint state, with that
+// form's sign (the sums are decremented, :644 and :668) and its product in
+// place of a sum in the last term of d|c_g| (dcg[1] * cg[1] * dcg[2] * cg[2]).
+// Flat ground: dc, du, dv have only z components, w = 0.
+static __device__ __forceinline__ void seg_time_var(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                                    const double* y0, const double* y1, const RayConst& rc,
+                                                    double& dvar_t, double& dvar_p) {
+    const double dx = y1[0] - y0[0], dy = y1[1] - y0[1], dz = y1[2] - y0[2];
+    const double zm = y0[2] + dz / 2.0;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    const double nu[3] = {rc.nx, rc.ny, y0[3] + (y1[3] - y0[3]) / 2.0};
+    const double num = sqrt(nu[0] * nu[0] + nu[1] * nu[1] + nu[2] * nu[2]);
+    const double ze = fmin(fmax(zm, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    double c, cz, u0, u0z, v0, v0z;
+    cubic_f1(r0, q, 2, c, cz);
+    cubic_f1(r0, q, 4, u0, u0z);
+    cubic_f1(r0, q, 6, v0, v0z);
+    double sc = 1.0, dsc = 0.0;   // bndlyr_sc, bndlyr_dsc(n = 2) (atmo_state.3d.strat.cpp:87-112)
+    if (zm < a.z_bl) {
+        const double X = exp(-(zm - a.z0) * a.inv_bl);
+        sc = (1.0 - X) / (1.0 + X);
+        dsc = -2.0 * (-X * a.inv_bl) / ((1.0 + X) * (1.0 + X));
+    }
+    const double cg[3] = {c * nu[0] / num + u0 * sc, c * nu[1] / num + v0 * sc, c * nu[2] / num};
+    const double cgm = sqrt(cg[0] * cg[0] + cg[1] * cg[1] + cg[2] * cg[2]);
+    const double duz = u0 * dsc + u0z * sc, dvz = v0 * dsc + v0z * sc;
+    const double den = cgm * cgm * cgm;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int o = 4 * j;   // reduced state: X at 4..6 / 8..10, mu_z at 7 / 11
+        const double X2 = y0[6 + o] + (y1[6 + o] - y0[6 + o]) / 2.0;
+        const double mu[3] = {j == 0 ? rc.mtx : rc.mpx, j == 0 ? rc.mty : rc.mpy, y0[7 + o] + (y1[7 + o] - y0[7 + o]) / 2.0};
+        const double s = X2 * cz - c / (num * num) * (mu[0] * nu[0] + mu[1] * nu[1] + mu[2] * nu[2]);
+        double dcg[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) dcg[i] = nu[i] / num * s + c / num * mu[i];
+        dcg[0] += X2 * duz;
+        dcg[1] += X2 * dvz;
+        const double v = -((dcg[0] * cg[0] + dcg[1] * cg[1] * dcg[2] * cg[2]) / den * ds);
+        if (j == 0) dvar_t = v; else dvar_p = v;
+    }
+}
+
 // Launch state of a ray: geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105).
 template <bool AMP>
 static __device__ __forceinline__ void ray_init(const Fan3DArgs& a, double theta, double phi, double* y, RayConst& rc) {

@@ -70,6 +70,9 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
     // sums (bulk mode) or the pending last-segment increments (write_rays mode)
     double s, tt, att, pt, pa, zmax;
     long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
+    // PATHS, back projection: travel-time variations (sums and pending increments as tt / pt)
+    double tvt = 0.0, tvp = 0.0, ptvt = 0.0, ptvp = 0.0;
+    const bool proj = PATHS && AMP && a.path_rows && a.path_mode == kPathProj;
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
@@ -79,6 +82,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = a.z0;
+        tvt = tvp = ptvt = ptvp = 0.0;
         if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
@@ -123,6 +127,11 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         seg_increment(tab, a, seg, y, acc, rc, dt, da);
         if (a.write_rays) {   // all segments but the bounce's last (main.infraga.3d.cpp:451-453)
             tt += pt; att += pa; pt = dt; pa = da;
+            if (proj) {       // run_back_proj sums travel_time_var the same way (main.infraga.3d.cpp:706-708)
+                double vt, vp;
+                seg_time_var(tab, a, seg, y, acc, rc, vt, vp);
+                tvt += ptvt; tvp += ptvp; ptvt = vt; ptvp = vp;
+            }
         } else {              // per-bounce sum added at the end (main.infraga.3d.cpp:486-487)
             pt += dt; pa += da;
         }
@@ -141,7 +150,27 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         if (!esc && !gnd) {
 #pragma unroll
             for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
-            if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
+            if (proj && path_sampled(a.path_mode, kb)) {
+                // projection row (main.infraga.3d.cpp:711-735): derivatives per degree
+                // (x pi/180), the group velocity at the row
+                if (p_n < p_cap) {
+                    double* o = a.path_rows + (p_base + p_n) * kProjCols;
+                    const double d2r = kPi / 180.0;
+                    o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; o[3] = tt + pt;
+                    o[4] = y[4] * d2r; o[5] = y[5] * d2r; o[6] = y[6] * d2r; o[7] = (tvt + ptvt) * d2r;
+                    o[8] = y[8] * d2r; o[9] = y[9] * d2r; o[10] = y[10] * d2r; o[11] = (tvp + ptvp) * d2r;
+                    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + y[3] * y[3]);
+                    const double ze = fmin(fmax(y[2], a.z_lo), a.z_hi);
+                    int sg = seg_walk(tab, a.n_knots, ze, seg);
+                    const double* r0 = tab + sg * kStride;
+                    const Cubic q = cubic_at(r0, ze);
+                    const double c = cubic_f(r0, q, 2), sc = bl_scale(a, y[2]);
+                    o[12] = c * rc.nx / num + cubic_f(r0, q, 4) * sc;
+                    o[13] = c * rc.ny / num + cubic_f(r0, q, 6) * sc;
+                    o[14] = c * y[3] / num;
+                }
+                p_n++;
+            } else if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 // row m = kb of the bounce, above the ground: z = max(z, z_g) = z
                 if (p_n < p_cap) {
                     double* o = a.path_rows + (p_base + p_n) * kPathCols;
@@ -164,6 +193,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         steps += K;
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
+        ptvt = 0.0; ptvp = 0.0;
         int status = -1;
         if (zmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);

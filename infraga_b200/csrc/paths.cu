@@ -55,7 +55,7 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
     if (!h || !p) return IGA_E_INVALID;
     int rc = validate(p, n_rays);
     if (rc) return rc;
-    if (path_mode != IGA_PATH_RAYS && path_mode != IGA_PATH_TERRAIN) return IGA_E_INVALID;
+    if (path_mode != IGA_PATH_RAYS && path_mode != IGA_PATH_TERRAIN && path_mode != IGA_PATH_PROJ) return IGA_E_INVALID;
     if (n_rays > 0 && (!theta_deg || !phi_deg)) return IGA_E_INVALID;
     const bool want_path = path_rows != nullptr || n_path != nullptr;
     const bool want_caus = caustic_rows != nullptr || n_caustic != nullptr;
@@ -67,6 +67,15 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
         return IGA_E_INVALID;
     }
     if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
+    if (path_mode == IGA_PATH_PROJ) {   // run_back_proj exists here for the 3D stratified flat-ground solver
+        if (want_caus || !p->calc_amp) return IGA_E_INVALID;
+        if (h->kind != 0 || p->geometry != IGA_GEOM_3D) {
+            g_err = "back projection rows: 3D stratified flat-ground atmospheres only";
+            return IGA_E_UNSUPPORTED;
+        }
+    }
+    const int pcols = iga::path_cols(path_mode);           // device row width
+    const int ucols = path_mode == IGA_PATH_PROJ ? IGA_PROJ_COLS : IGA_PATH_COLS;   // caller's row width
     if (n_path) *n_path = 0;
     if (n_caustic) *n_caustic = 0;
     if (path_start) std::fill(path_start, path_start + n_rays + 1, 0LL);
@@ -118,7 +127,7 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
     ps.mode = path_mode;
     long long* d_off = nullptr;
     if (want_path) {
-        if ((rc = mem.get(&ps.rows, (size_t)off[n] * iga::kPathCols)) || (rc = mem.get(&d_off, n + 1)) ||
+        if ((rc = mem.get(&ps.rows, (size_t)off[n] * pcols)) || (rc = mem.get(&d_off, n + 1)) ||
             (rc = mem.get(&ps.n, n)))
             return rc;
         ps.off = d_off;
@@ -154,7 +163,7 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
     std::vector<double> rows;
     if (want_path) {
         pn.resize(n);
-        rows.resize((size_t)off[n] * iga::kPathCols);
+        rows.resize((size_t)off[n] * pcols);
         IGA_CUDA(cudaMemcpyAsync(pn.data(), ps.n, sizeof(long long) * n, cudaMemcpyDeviceToHost, st), "D2H path counts");
         IGA_CUDA(cudaMemcpyAsync(rows.data(), ps.rows, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
                  "D2H path rows");
@@ -176,8 +185,7 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
             if (path_start) path_start[i] = w;
             for (long long j = 0; j < pn[i]; j++, w++)
                 if (w < path_cap)
-                    memcpy(path_rows + (size_t)w * IGA_PATH_COLS, &rows[(size_t)(off[i] + j) * iga::kPathCols],
-                           sizeof(double) * IGA_PATH_COLS);
+                    memcpy(path_rows + (size_t)w * ucols, &rows[(size_t)(off[i] + j) * pcols], sizeof(double) * ucols);
         }
         if (path_start) path_start[n] = w;
         *n_path = w;

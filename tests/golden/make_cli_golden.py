@@ -43,6 +43,10 @@ CASES = {
     "3d_direct": ("infraga-3d", "1d", 0,
                   ["-eig_direct", "atmo.met", "rcvr_x=240", "rcvr_y=30", "incl_est=8", "bounces=0",
                    "output_id=direct"]),
+    "3d_back_proj": ("infraga-3d", "1d", 0,
+                     ["-back_proj", "atmo.met", "inclination=12", "azimuth=60", "bounces=1", "rcvr_x=10", "max_ds=0.25",
+                      "freq=0.2"]),
+    "3d_back_proj_dflt": ("infraga-3d", "1d", 1, ["-b", "atmo.met", "max_ds=0.5", "output_id=bp"]),
     "sph_prop": ("infraga-sph", "1d", 1,
                  ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=180",
                   "az_step=180", "bounces=1", "src_lat=20", "src_lon=-40", "max_rng=700", "max_ds=0.25", "write_caustics=true",

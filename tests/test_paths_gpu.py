@@ -85,3 +85,27 @@ def test_paths_reject_fp32c_and_caustics_without_amp(dev):
     params.calc_amp = 0
     with pytest.raises(ig.IgaError):
         ig.fan_paths(atmo, params, th[:2], ph[:2], caustics=True, ray_steps=np.array([10, 10]))
+
+
+def test_projection_rows_match_fan_and_reject_other_solvers(dev):
+    """IGA_PATH_PROJ (-back_proj rows): 15 columns, time growing along the ray,
+    the last row before each arrival at most the arrival time; other handles,
+    caustics and calc_amp = 0 are refused.  File-level parity with the
+    reference's .projection.dat is in test_cli_gpu.py (3d_back_proj*)."""
+    atmo = ig.Atmosphere.load(profile_path(0), reverse_winds=True)
+    params = atmo.default_params(bounces=1, src=(10.0, 0.0, 0.0), turn_ht_min=-1e30)
+    params.write_rays = 1
+    th, ph = np.array([12.0]), np.array([60.0])
+    fan = ig.fan_run(atmo, params, th, ph)
+    rows = ig.fan_paths(atmo, params, th, ph, mode=ig.PATH_PROJ, ray_steps=fan["ray_steps"])["paths"]
+    assert rows.shape[1] == ig.PROJ_COLS and rows.shape[0] > 10
+    assert np.all(np.diff(rows[:, 3]) > 0.0) and np.all(rows[:, 2] >= 0.0)
+    assert rows[-1, 3] <= fan["arrivals"][-1, 5]
+    with pytest.raises(ig.IgaError):
+        ig.fan_paths(atmo, params, th, ph, mode=ig.PATH_PROJ, caustics=True, ray_steps=fan["ray_steps"])
+    params.calc_amp = 0
+    with pytest.raises(ig.IgaError):
+        ig.fan_paths(atmo, params, th, ph, mode=ig.PATH_PROJ, ray_steps=fan["ray_steps"])
+    sph = atmo.default_params(geometry=ig.GEOM_SPH)
+    with pytest.raises(ig.IgaError):
+        ig.fan_paths(atmo, sph, th, ph, mode=ig.PATH_PROJ, ray_steps=np.array([100]))
