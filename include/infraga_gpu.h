@@ -168,6 +168,17 @@ int iga_atmo_region(iga_atmo_t atmo, double* lat_min, double* lat_max, double* l
  * 3D: x, y [km], gradient per km.  IGA_E_UNSUPPORTED without terrain. */
 int iga_atmo_terrain(iga_atmo_t atmo, double x, double y, double* z, double* dz_dx, double* dz_dy);
 
+/* atmo::c, u, v, rho as the reference's point functions return them
+ * (atmo_state.*.cpp: the splines at the clamped altitude, u and v scaled by
+ * topo::bndlyr_sc over the handle's ground or terrain), at the horizontal point
+ * (x, y) [km; IGA_GEOM_SPH: lat, lon in deg] and altitudes z[0..n) [km]; out
+ * gets n rows of c [km/s], u, v [km/s], rho [g/cm^3].  params gives the
+ * geometry and the flat ground height (z_grnd).  Host-side FP64; used for the
+ * write_atmo profile dump (geoac::write_prof, geoac.interface.3d.cpp:47-66,
+ * geoac.interface.sph.cpp:55-73). */
+int iga_atmo_sample(iga_atmo_t atmo, const iga_fan_params* params, double x, double y, const double* z, int n,
+                    double* out);
+
 /* Same as iga_atmo_load from arrays already in solver units. */
 int iga_atmo_create(const iga_profile* profile, iga_atmo_t* out);
 

@@ -106,6 +106,7 @@ _SIGS = {
                                   _I, _I, _P(_VP)]),
     "iga_atmo_region": (_I, [_VP, _P(_D), _P(_D), _P(_D), _P(_D)]),
     "iga_atmo_load_topo": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I, _I, _P(_VP)]),
+    "iga_atmo_sample": (_I, [_VP, _P(FanParams), _D, _D, _P(_D), _I, _P(_D)]),
     "iga_server_config_default": (_I, [_P(ServerConfig)]),
     "iga_server_create": (_I, [_P(ServerConfig), _P(_VP)]),
     "iga_server_submit_fan": (_I, [_VP, _VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_LL)]),
@@ -216,6 +217,16 @@ class Atmosphere:
                                         int(reverse_winds), int(geometry), ctypes.byref(h)),
                f"iga_atmo_load_topo({met_path}, {topo_file})")
         return cls(h)
+
+    def sample(self, params: FanParams, x: float, y: float, z) -> np.ndarray:
+        """atmo::c, u, v, rho at (x, y) [km; lat, lon in deg for GEOM_SPH params]
+        and altitudes z [km], as the reference's point functions return them
+        (host FP64; the write_atmo profile).  Returns [n, 4]."""
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+        out = np.zeros((max(zz.size, 1), 4), dtype=np.float64)
+        _check(lib().iga_atmo_sample(self._h, ctypes.byref(params), float(x), float(y), _dptr(zz), zz.size, _dptr(out)),
+               "iga_atmo_sample")
+        return out[:zz.size]
 
     def region(self):
         """(lat_min, lat_max, lon_min, lon_max) [deg] of geoac::set_limits."""

@@ -658,6 +658,51 @@ int iga_atmo_terrain(iga_atmo_t h, double x, double y, double* z, double* dz_dx,
     return IGA_OK;
 }
 
+int iga_atmo_sample(iga_atmo_t h, const iga_fan_params* p, double x, double y, const double* z, int n, double* out) {
+    if (!h || !p || n < 0 || (n > 0 && (!z || !out))) return IGA_E_INVALID;
+    const bool sph = p->geometry == IGA_GEOM_SPH;
+    if (h->kind != 0 && sph != (h->kind == 1)) return IGA_E_UNSUPPORTED;
+    iga::Fan3DArgs a;   // host-side launch constants: ground, boundary-layer top
+    int rc = build_args(h, p, a);
+    if (rc) return rc;
+    const double d2r = iga::kPi / 180.0;
+    const double hx = sph ? x * d2r : x, hy = sph ? y * d2r : y;   // grid / terrain units
+    // topo::z under the point (an altitude): terrain, else the flat ground (0 for
+    // the 3D range-dependent solver without terrain, atmo_state.3d.rngdep.cpp:45-51)
+    double zg = a.z0;
+    if (h->has_topo) {
+        double dz[2];
+        iga::terrain_eval1(h->topo, hx, hy, zg, dz);
+    } else if (h->kind == 2) {
+        zg = 0.0;
+    }
+    const bool hybrid = h->kind != 0 && !h->strat_topo;
+    const StratProfile& P = h->prof;
+    for (int i = 0; i < n; i++) {
+        double sc = 1.0;   // topo::bndlyr_sc
+        if (z[i] < a.z_bl) {
+            const double X = std::exp(-(z[i] - zg) / a.bl);
+            sc = (1.0 - X) / (1.0 + X);
+        }
+        double f[4];
+        if (hybrid) {
+            double df[3];
+            for (int k = 0; k < 4; k++) iga::hybrid_eval1(h->grid, k, hx, hy, z[i], f[k], df);
+        } else {
+            double d1, d2;
+            iga::spline_eval(P.z, P.c, P.cs, z[i], f[0], d1, d2);
+            iga::spline_eval(P.z, P.u, P.us, z[i], f[1], d1, d2);
+            iga::spline_eval(P.z, P.v, P.vs, z[i], f[2], d1, d2);
+            iga::spline_eval(P.z, P.rho, P.rhos, z[i], f[3], d1, d2);
+        }
+        out[4 * i + 0] = f[0];
+        out[4 * i + 1] = f[1] * sc;
+        out[4 * i + 2] = f[2] * sc;
+        out[4 * i + 3] = f[3];
+    }
+    return IGA_OK;
+}
+
 int iga_atmo_region(iga_atmo_t h, double* lat_min, double* lat_max, double* lon_min, double* lon_max) {
     if (!h) return IGA_E_INVALID;
     double r[4] = {-90.0, 90.0, -180.0, 180.0};

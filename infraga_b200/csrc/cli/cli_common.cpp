@@ -309,6 +309,26 @@ struct Ground {
     }
 };
 
+// write_atmo=true: geoac::write_prof (geoac.interface.3d.cpp:47-66,
+// geoac.interface.sph.cpp:55-73) into ./atmo.dat: for z = m / 10 km, m < alt_max * 10,
+// c, u, v [m/s], rho and the effective sound speed c + cos(az) u + sin(az) v [m/s]
+// at the source (x, y [km] or lat, lon [deg]); 3D rows end with a tab.
+int write_atmo_file(iga_atmo_t atmo, const iga_fan_params& p, double x, double y, double azimuth) {
+    const bool sph = p.geometry == IGA_GEOM_SPH;
+    std::vector<double> z;
+    for (int m = 0; m < p.alt_max * 10.0; m++) z.push_back(sph ? (kR0 + m / 10.0) - kR0 : m / 10.0);
+    std::vector<double> v(z.size() * 4);
+    const int rc = iga_atmo_sample(atmo, &p, x, y, z.data(), (int)z.size(), v.data());
+    if (rc) return rc;
+    std::ofstream f("atmo.dat");
+    for (size_t m = 0; m < z.size(); m++) {
+        const double* q = &v[4 * m];
+        f << (double)m / 10.0 << '\t' << q[0] * 1000.0 << '\t' << q[1] * 1000.0 << '\t' << q[2] * 1000.0 << '\t' << q[3]
+          << '\t' << (q[0] + cos(azimuth) * q[1] + sin(azimuth) * q[2]) * 1000.0 << (sph ? "\n" : "\t\n");
+    }
+    return IGA_OK;
+}
+
 // Rows of one ray of a fan as the library returned them.
 struct FanChunk {
     std::vector<double> arr;     // arrivals
@@ -370,13 +390,14 @@ int run_prop(int argc, char** argv, Variant v) {
         std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
         return 0;
     }
-    if (o.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
     if (o.print_resid) std::cout << '\t' << "Note: print_resid is not provided by the GPU front end" << '\n';
 
     // source: degrees on the command line, radians inside (spherical)
     const double lat_r = xs * (Pi / 180.0), lon_r = ys * (Pi / 180.0);
     Ground g{v, atmo, has_topo, p.z_grnd};
     zs = sph ? std::max(zs, g.z(lat_r, lon_r)) : std::max(zs, g.z(xs, ys));
+    if (o.write_atmo && (rc = write_atmo_file(atmo, p, xs, ys, (90.0 - o.phi_min) * Pi / 180.0)))
+        return fail("write_atmo", rc);
     if (o.write_caustics) calc_amp = true;
 
     const char* sum_src = sph ? "source location (lat, lon, alt): " : "source location: ";
@@ -620,6 +641,7 @@ struct EigOpts {
     double src[3] = {0.0, 0.0, 0.0};
     double rcvr[2] = {-250.0, 0.0};
     bool verbose = false;
+    bool write_atmo = false;
     const char* output_id = nullptr;
 };
 
@@ -729,7 +751,7 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
         std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
         return false;
     }
-    if (po.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
+    o.write_atmo = po.write_atmo;
     return true;
 }
 
@@ -783,6 +805,19 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
     };
     o.src[2] = std::max(ground(o.src[0], o.src[1]), o.src[2]);
     const double z_rcvr = ground(o.rcvr[0], o.rcvr[1]);
+    if (o.write_atmo) {   // the azimuth argument of each main's write_prof call
+        double az_w;
+        if (sph) {        // globe::bearing(src, rcvr), radians (main.infraga.sph.cpp:892, :1097)
+            const double la1 = o.src[0] * (Pi / 180.0), lo1 = o.src[1] * (Pi / 180.0);
+            const double la2 = o.rcvr[0] * (Pi / 180.0), lo2 = o.rcvr[1] * (Pi / 180.0);
+            az_w = atan2(sin(lo2 - lo1), cos(la1) * tan(la2) - sin(la1) * cos(lo2 - lo1));
+        } else if (direct && az_given) {   // phi_est (main.infraga.3d.cpp:1050-1056)
+            az_w = Pi / 2.0 - az_est * (Pi / 180.0);
+        } else {          // atan2(rcvr - src) (main.infraga.3d.cpp:875)
+            az_w = atan2(o.rcvr[1] - o.src[1], o.rcvr[0] - o.src[0]);
+        }
+        if ((rc = write_atmo_file(atmo, ep.fan, o.src[0], o.src[1], az_w))) return fail("write_atmo", rc);
+    }
     if (!o.output_id) {
         strip_extension(argv[2]);
         o.output_id = argv[2];
@@ -941,8 +976,9 @@ int run_back(int argc, char** argv, Variant v) {
         std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
         return 0;
     }
-    if (o.write_atmo) std::cout << '\t' << "Note: write_atmo is not provided by the GPU front end (no atmo.dat written)" << '\n';
     const double zr = std::max(p.z_grnd, 0.0);   // z_rcvr = max(topo::z, 0)
+    if (o.write_atmo && (rc = write_atmo_file(atmo, p, xr, yr, Pi / 2.0 - az * (Pi / 180.0))))
+        return fail("write_atmo", rc);
     // the reference echoes geoac::theta / phi converted back to degrees
     std::cout << '\n' << "Parameter summary:" << '\n';
     std::cout << '\t' << "inclination: " << incl * (Pi / 180.0) * (180.0 / Pi) << '\n';

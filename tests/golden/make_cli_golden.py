@@ -47,6 +47,15 @@ CASES = {
                      ["-back_proj", "atmo.met", "inclination=12", "azimuth=60", "bounces=1", "rcvr_x=10", "max_ds=0.25",
                       "freq=0.2"]),
     "3d_back_proj_dflt": ("infraga-3d", "1d", 1, ["-b", "atmo.met", "max_ds=0.5", "output_id=bp"]),
+    "3d_atmo": ("infraga-3d", "1d", 1,
+                ["-prop", "atmo.met", "inclination=20", "azimuth=30", "bounces=0", "write_rays=false", "write_atmo=true",
+                 "max_alt=120", "z_grnd=0.3"]),
+    "3d_direct_atmo": ("infraga-3d", "1d", 0,
+                       ["-eig_direct", "atmo.met", "rcvr_x=240", "rcvr_y=30", "incl_est=8", "az_est=80", "bounces=0",
+                        "write_atmo=true", "output_id=direct"]),
+    "sph_atmo": ("infraga-sph", "1d", 0,
+                 ["-prop", "atmo.met", "inclination=20", "azimuth=30", "bounces=0", "write_rays=false",
+                  "write_atmo=true", "src_lat=20", "src_lon=-40"]),
     "sph_prop": ("infraga-sph", "1d", 1,
                  ["-prop", "atmo.met", "incl_min=4", "incl_max=24", "incl_step=10", "az_min=0", "az_max=180",
                   "az_step=180", "bounces=1", "src_lat=20", "src_lon=-40", "max_rng=700", "max_ds=0.25", "write_caustics=true",
@@ -93,6 +102,12 @@ CASES = {
     "spht_eig": ("infraga-sph", "1dts", 0,
                  ["-eig_search", "atmo.met", "topo_file=topo.dat", "src_alt=3", "rcvr_lat=32.98", "rcvr_lon=-104.6",
                   "incl_min=10", "incl_max=30"]),
+    "3dr_atmo": ("infraga-3d-rngdep", "3dr", 0,
+                 ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "inclination=12",
+                  "azimuth=100", "bounces=0", "write_rays=false", "write_atmo=true"]),
+    "sphr_atmo": ("infraga-sph-rngdep", "sphr", 0,
+                  ["-prop", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "inclination=12",
+                   "azimuth=100", "bounces=0", "write_rays=false", "write_atmo=true"]),
     "sphr_eig": ("infraga-sph-rngdep", "sphr", 0,
                  ["-eig_search", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "src_alt=3",
                   "rcvr_lat=32.98", "rcvr_lon=-104.6", "incl_min=10", "incl_max=30"]),
