@@ -17,6 +17,7 @@
 using iga::StratProfile;
 
 #include "handle.h"
+#include "nvtx.h"
 
 namespace iga_internal {
 thread_local std::string g_cuda_err;
@@ -508,6 +509,7 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         g_cuda_err = "range-dependent atmosphere: FP64, with the geometry it was loaded for";
         return IGA_E_UNSUPPORTED;
     }
+    NvtxRange nv(ps ? "iga_fan_paths launch" : "iga_fan launch");
     iga::Fan3DArgs a;
     int rc = build_args(h, p, a);
     if (rc) return rc;

@@ -24,6 +24,7 @@
 #include "eig3d.cuh"
 #include "fan3d_common.cuh"
 #include "handle.h"
+#include "nvtx.h"
 
 namespace iga {
 namespace {
@@ -616,7 +617,9 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
     const bool per_round = vb && vb[0] == '2';
     long long n_rounds = 0, n6 = 0, n18 = 0, st6 = 0, st18 = 0;
     const auto t_begin = std::chrono::steady_clock::now();
+    NvtxRange nv_search(direct ? "iga_eig_direct" : "iga_eig_search");
     while (true) {
+        NvtxRange nv_round("eig round");
         req6.clear(); req18.clear(); uniq.clear();
         int sweeping = 0;
         for (auto& c : chains) if (c.phase == Chain::kEst && c.iterations < S.fixed_step_iters()) sweeping++;
