@@ -160,7 +160,9 @@ int load_met(const char* path, const char* format, bool reverse_winds, StratProf
         out.z.push_back(z); out.c.push_back(c); out.u.push_back(u); out.v.push_back(vv); out.rho.push_back(rho);
         row++;
     }
-    return finalize_profile(out, err);
+    // a file whose values fail the checks is a malformed file
+    const int rc = finalize_profile(out, err);
+    return rc == IGA_E_INVALID ? IGA_E_IO : rc;
 }
 
 }  // namespace iga

@@ -171,7 +171,7 @@ iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_o
         rc = iga_atmo_load_topo(argv[2], topo, fmt, rev ? 1 : 0, is_sph(v) ? IGA_GEOM_SPH : IGA_GEOM_3D, &a);
         if (rc == IGA_E_IO) {
             std::cout << '\t' << "ERROR: Invalid terrain file or atmospheric specification (" << topo << ", " << argv[2]
-                      << ")" << '\n' << '\n';
+                      << ")" << '\n' << '\t' << iga_strerror(rc) << '\n' << '\n';
             return nullptr;
         }
     } else if (!is_rngdep(v)) {
@@ -179,7 +179,8 @@ iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_o
         if (rev) std::cout << '\t' << "Inverting wind fields for back projection analysis..." << '\n';
         rc = iga_atmo_load(argv[2], fmt, rev ? 1 : 0, &a);
         if (rc == IGA_E_IO) {
-            std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\n';
+            std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\t'
+                      << iga_strerror(rc) << '\n' << '\n';
             return nullptr;
         }
     } else {
@@ -193,7 +194,8 @@ iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_o
                                   is_sph(v) ? IGA_GEOM_SPH : IGA_GEOM_3D, &a);
         if (rc == IGA_E_IO) {
             std::cout << '\t' << "ERROR: Invalid grid, profile or terrain files (" << argv[2] << "*, " << argv[3] << ", "
-                      << argv[4] << (topo ? ", " : "") << (topo ? topo : "") << ")" << '\n' << '\n';
+                      << argv[4] << (topo ? ", " : "") << (topo ? topo : "") << ")" << '\n' << '\t' << iga_strerror(rc)
+                      << '\n' << '\n';
             return nullptr;
         }
     }
@@ -952,7 +954,8 @@ int run_back(int argc, char** argv, Variant v) {
     iga_atmo_t atmo = nullptr;
     int rc = iga_atmo_load(argv[2], fmt, 1, &atmo);   // set_region(..., true): winds reversed
     if (rc == IGA_E_IO) {
-        std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\n';
+        std::cout << '\t' << "ERROR: Invalid atmospheric specification (" << argv[2] << ")" << '\n' << '\t'
+                  << iga_strerror(rc) << '\n' << '\n';
         return 0;
     }
     if (rc) return fail("loading the atmosphere", rc);
