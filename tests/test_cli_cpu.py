@@ -73,7 +73,8 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "infraga-3d")), reason="compiled reference not present")
-@pytest.mark.parametrize("name", ["3d_prop_noamp", "3dr_calc_amp"])
+@pytest.mark.parametrize("name", ["3d_prop_noamp", "3dr_calc_amp", "3dt_noamp", "spht_noamp", "3d_back_proj_dflt",
+                                  "3d_atmo", "sphr_atmo"])
 def test_reference_binaries_reproduce_fixtures(name):
     c = mk.CASES[name]
     got = mk.run_case(REF, name, c)
