@@ -47,6 +47,18 @@ def test_invalid_arguments_rejected_without_device():
     n = ctypes.c_int()
     assert L.iga_fan_run(None, None, None, None, 0, None, 0, ctypes.byref(n), None, None, None, None, None) == _lib.IGA_E_INVALID
     assert L.iga_atmo_load(None, b"zTuvdp", 0, None) == _lib.IGA_E_INVALID
+    h = ctypes.c_void_p()
+    met = os.path.join(ROOT, "tests", "golden", "profiles", "gen0.met").encode()
+    assert L.iga_atmo_load_topo(None, b"t.dat", b"zTuvdp", 0, 0, ctypes.byref(h)) == _lib.IGA_E_INVALID
+    assert L.iga_atmo_load_topo(met, b"t.dat", b"zTuvdp", 0, 7, ctypes.byref(h)) == _lib.IGA_E_INVALID
+    # a missing terrain file fails in the host loader, before any device call
+    assert L.iga_atmo_load_topo(met, b"/nonexistent/t.dat", b"zTuvdp", 0, 0, ctypes.byref(h)) == _lib.IGA_E_IO
+    assert not h.value
+    z = (ctypes.c_double * 1)(0.0)
+    out = (ctypes.c_double * 4)()
+    assert L.iga_atmo_sample(None, None, 0.0, 0.0, z, 1, out) == _lib.IGA_E_INVALID
+    assert L.iga_fan_paths(None, None, None, None, 0, 2, None, None, 0, None, None, None, 0, None, None) == \
+        _lib.IGA_E_INVALID
 
 
 def test_no_silent_cpu_fallback_when_no_gpu():
