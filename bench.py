@@ -37,15 +37,13 @@ METRIC = "ray-steps/s"
 UNIT = "ray-steps/s"
 SEEDS = (1, 2, 3, 4)
 FAN = dict(incl=(0.5, 60.01, 0.1), az=(0.0, 357.0, 3.0), bounces=10, rng_max=2000.0)
-# Algorithmic FP64 work of one RK4 ray-step with amplitude (4 RHS stages of the
-# 12 varying equations, the midpoint travel-time increment and one
-# Sutherland-Bass evaluation), counting add/sub/mul as 1, FMA as 2,
-# div/sqrt/reciprocal as 4 and exp/exp10/log/cbrt as 20 FLOPs.
-FLOPS_PER_STEP = 2600.0
-# The FP32-compensated path runs the same equations but reads the absorption
-# from a tabulated alpha(z) (one lerp instead of the ~1,000-FLOP Sutherland-Bass
-# evaluation) and adds the hi/lo TwoSum updates: ~1,650 per ray-step.
-FLOPS_PER_STEP_FP32C = 1650.0
+# Algorithmic work per accepted RK4 ray-step (FLOP-equivalents: add/sub/mul 1,
+# div/sqrt 4, exp/log/pow/trig 20), counted by running the reference algorithm
+# (the oracle restatement) with an operation-counting scalar; roofline.json
+# holds the counts, the weights and the sample they came from.
+with open(os.path.join(ROOT, "roofline.json")) as _f:
+    ROOFLINE = json.load(_f)
+FLOPS_PER_STEP = {"fp64": ROOFLINE["variants"]["fp64_amp"], "fp32c": ROOFLINE["variants"]["fp32c_amp"]}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per fan launch of the dominant kernel, from the ncu
 # captures summarised in profiles/ (None until captured).
@@ -356,11 +354,13 @@ def run_ours(args):
 
     # e2e: the public host-buffer C ABI (iga_fan_run: H2D of the launch angles
     # from pinned memory, kernel, D2H of the arrival records), one host thread
-    # per seed fan so the four calls overlap on the GPU, wall-clocked per step.
+    # per seed fan so the four calls overlap on the GPU, wall-clocked per step;
+    # the max over ranks of the wall time.  Run for every precision leg.
     th_p = torch.from_numpy(th).pin_memory().numpy()
     ph_p = torch.from_numpy(ph).pin_memory().numpy()
-    e2e_steps, e2e_t, d2h = 0, 0.0, 0
-    if not args.no_e2e:
+
+    def measure_e2e(params):
+        e2e_steps, e2e_t = 0, 0.0
         for k, a in enumerate(atmos):
             ig.fan_run(a, params[k], th_p, ph_p)   # size the handles' device buffers
         for _ in range(args.steps):
@@ -378,17 +378,23 @@ def run_ours(args):
                 t_.join()
             e2e_t += time.perf_counter() - t0
             e2e_steps += sum(r["total_steps"] for r in out)
-            d2h = sum(r["arrivals"].nbytes + n * (4 + 4 + 8) for r in out)
-    if world > 1:
-        t = torch.tensor([float(e2e_steps), e2e_t], dtype=torch.float64, device=dev)
-        s = t.clone()
-        dist.all_reduce(s[:1], op=dist.ReduceOp.SUM)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
-        e2e_steps, e2e_t = int(s[0].item()), float(t[1].item())
+        if world > 1:
+            t = torch.tensor([float(e2e_steps), e2e_t], dtype=torch.float64, device=dev)
+            s_ = t.clone()
+            dist.all_reduce(s_[:1], op=dist.ReduceOp.SUM)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
+            e2e_steps, e2e_t = int(s_[0].item()), float(t[1].item())
+        # bytes iga_fan_run copies per call: the launch angles in; the arrival
+        # slots [n][bounces+1][12], per-ray counts, status and step counts out
+        return {"value": e2e_steps / e2e_t if e2e_t > 0 else None, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * 8 * n * len(atmos),
+                "d2h_bytes_per_step": len(atmos) * (n * nb * 12 * 8 + n * (4 + 4 + 8))}
+
+    e2e = {k: measure_e2e(all_params[k]) for k in legs} if not args.no_e2e else {}
 
     result = None
     if rank == 0:
-        fps = FLOPS_PER_STEP_FP32C if head == "fp32c" else FLOPS_PER_STEP
+        fps = FLOPS_PER_STEP[head]
         achieved = fps * my_steps / kern_s / 1e12
         peak = peaks.get(head)
         line = {
@@ -399,8 +405,7 @@ def run_ours(args):
             "data": "synthetic",
             "config": config_dict({"parallelism": f"independent fans per GPU x{world}", "precision": head,
                                    "ray_steps_per_step": tot_steps / args.steps / world}),
-            "e2e": {"value": e2e_steps / e2e_t if e2e_t > 0 else None, "unit": UNIT,
-                    "h2d_bytes_per_step": 2 * 8 * n * len(atmos), "d2h_bytes_per_step": int(d2h)},
+            "e2e": e2e.get(head, {"value": None, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}),
             "gpu_launches": args.steps * len(atmos),
             "roofline": {"bound": "fp32" if head == "fp32c" else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": TRAFFIC.get(head),
@@ -409,8 +414,8 @@ def run_ours(args):
                                          " 8192^3 via torch.matmul, best of 5"),
                          "flops_per_step": fps},
             "legs": {k: {"value": v["value"], "ms_per_step": v["ms_per_step"], "clocks": v["clocks"],
-                         "roofline_frac": ((FLOPS_PER_STEP_FP32C if k == "fp32c" else FLOPS_PER_STEP) *
-                                           v["my_steps"] / v["kern_s"] / 1e12 / peaks[k]) if k in peaks else None}
+                         "roofline_frac": (FLOPS_PER_STEP[k] * v["my_steps"] / v["kern_s"] / 1e12 / peaks[k])
+                         if k in peaks else None, "e2e": e2e.get(k)}
                      for k, v in res.items()},
             "clocks": clocks,
             "wall_s_timed_region": wall,
@@ -732,6 +737,79 @@ def run_eigen(args):
 
 
 
+# ---------------------------------------------------------------- profiling cases
+# Small, self-contained runs of each kernel for ncu captures (summaries under
+# profiles/): each case traces one modest workload once per repetition, so a
+# capture with ``-k regex:<kernel> -c 1`` sees a representative launch of a few
+# hundred milliseconds at most.  ``python bench.py --profile-case <case>``.
+def _profile_case(name):
+    import infraga_b200 as ig
+    from infraga_b200 import synth
+    from infraga_b200 import workloads as wl
+    golden = os.path.join(ROOT, "tests", "golden")
+    if name == "fansph":       # spherical stratified fan (fansph_fp64_kernel): 1,440 rays
+        atmo = ig.Atmosphere.load(wl.profile_met(1))
+        th, ph = synth.fan_angles(0.5, 60.0, 0.5, 0.0, 330.0, 30.0)
+        p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=5, rng_max=2000.0, src=(30.0, 0.0, 0.0))
+        return lambda: ig.fan_run(atmo, p, th, ph)
+    if name == "fansphr":      # 21x21 grid with terrain (fansphr_fp64_kernel): 408 rays, 1 bounce, 600 km
+        f = wl.sphr_files()
+        atmo = ig.Atmosphere.load_rngdep(f[0], f[1], f[2], topo_file=f[3], geometry=ig.GEOM_SPH)
+        th, ph = synth.fan_angles(0.5, 50.0, 3.0, 0.0, 345.0, 15.0)
+        p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=1, rng_max=600.0)
+        return lambda: ig.fan_run(atmo, p, th, ph)
+    if name == "fan3dr":       # committed 5x5 grid with terrain (fan3dr_fp64_kernel): 1,080 rays
+        d = os.path.join(golden, "rngdep3d")
+        atmo = ig.Atmosphere.load_rngdep(os.path.join(d, "node"), os.path.join(d, "node_x.dat"),
+                                         os.path.join(d, "node_y.dat"), topo_file=os.path.join(d, "topo.dat"),
+                                         geometry=ig.GEOM_3D)
+        th, ph = synth.fan_angles(0.5, 45.0, 0.5, 0.0, 330.0, 30.0)
+        p = atmo.default_params(bounces=2, rng_max=600.0)
+        return lambda: ig.fan_run(atmo, p, th, ph)
+    if name == "paths":        # 3D stratified fan with sampled ray paths (PATHS instantiation)
+        atmo = ig.Atmosphere.load(wl.profile_met(1))
+        th, ph = synth.fan_angles(1.0, 45.0, 1.0, 0.0, 330.0, 30.0)
+        p = atmo.default_params(bounces=3, rng_max=1000.0, write_rays=1)
+        steps = ig.fan_run(atmo, p, th, ph)["ray_steps"]
+        return lambda: ig.fan_paths(atmo, p, th, ph, caustics=True, ray_steps=steps)
+    if name == "eig3d":        # 3D eigenray search, 16 pairs (trace3d_fp64_kernel)
+        atmo = ig.Atmosphere.load(wl.profile_met(1))
+        pairs = wl.eig_pairs(1, 16)
+        p = ig.eig_params(atmo, bnc_min=0, bnc_max=2, streams=1)
+        return lambda: ig.eig_run(atmo, p, pairs)
+    if name == "eigsph":       # spherical eigenray search, 8 pairs (tracesph_fp64_kernel)
+        atmo = ig.Atmosphere.load(wl.profile_met(1))
+        pairs = [((30.0, 0.0, 0.0), (30.0 + 2.0 * k / 8.0, 2.5 + 0.25 * k)) for k in range(8)]
+        p = ig.eig_params(atmo, geometry=ig.GEOM_SPH, bnc_min=0, bnc_max=1, streams=1)
+        return lambda: ig.eig_run(atmo, p, pairs)
+    raise SystemExit(f"unknown profiling case {name!r} (one of {', '.join(PROFILE_CASES)})")
+
+
+PROFILE_CASES = ("fansph", "fansphr", "fan3dr", "paths", "eig3d", "eigsph")
+
+
+def run_profile_case(args):
+    run = _profile_case(args.profile_case)
+    for _ in range(args.reps):
+        run()
+    print(f"{args.profile_case}: ok")
+    return 0
+
+
+def launch_ranks(n):
+    """`--gpus N` without an external launcher: start N ranks (one process per
+    GPU, RANK / LOCAL_RANK / WORLD_SIZE set by torch.distributed.run on
+    127.0.0.1) running this script with the same arguments; exit with the
+    launcher's status."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -753,7 +831,14 @@ def main():
                     help="time the spherical range-dependent fan with terrain (config 2) instead")
     ap.add_argument("--eigen", action="store_true",
                     help="time the batched 3D eigenray search (config 3, FP64 and FP32C) instead")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES,
+                    help="run one small profiling workload of a single kernel (for ncu captures) instead")
+    ap.add_argument("--reps", type=int, default=1, help="repetitions of --profile-case")
     args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     if args.serving:
         return run_serving(args)
     if args.sphr:

@@ -286,8 +286,16 @@ int iga_fan_run_device(iga_atmo_t atmo, const iga_fan_params* params,
 enum iga_path_mode {
     IGA_PATH_RAYS = 0,       /* rows m == 1 and m % 15 == 0 of every bounce (write_rays) */
     IGA_PATH_TERRAIN = 1,    /* rows m % 10 == 1 (write_topo) */
-    IGA_PATH_PROJ = 2        /* rows m == 1 and m % 5 == 0, IGA_PROJ_COLS wide (-back_proj);
+    IGA_PATH_PROJ = 2,       /* rows m == 1 and m % 5 == 0, IGA_PROJ_COLS wide (-back_proj);
                                 3D stratified flat-ground handles, calc_amp = 1, no caustics */
+    IGA_PATH_RESID = 3       /* one row per bounce segment (prop_rk4 call) at its row k - 1
+                                (print_resid, main.infraga.3d.cpp:437-441): eikonal residual,
+                                auxiliary-parameter residual, bounce, then zeros
+                                (geoac::eval_eikonal / eval_eikonal_deriv,
+                                geoac.eqset.3d.strat.cpp:393-432); 3D stratified flat-ground
+                                handles, no caustics.  Without calc_amp the auxiliary
+                                residual is 0: the reference reads it from solution
+                                columns 6..17 that its 6-equation rows do not have. */
 };
 
 /* Replaces the write_rays / write_topo / write_caustics branches of run_prop's
@@ -309,7 +317,8 @@ enum iga_path_mode {
  *               The rows of ray i number at most
  *               (bounces + 1) + ray_steps[i] / 15 (IGA_PATH_RAYS; / 10 for
  *               IGA_PATH_TERRAIN, / 5 for IGA_PATH_PROJ) + 1; IGA_PATH_PROJ
- *               rows are IGA_PROJ_COLS wide.
+ *               rows are IGA_PROJ_COLS wide; IGA_PATH_RESID gives at most
+ *               bounces + 1 rows per ray.
  *   caustic_rows nullable: caustic_cap rows of IGA_CAUSTIC_COLS, ray by ray
  *               in step order; *n_caustic = rows produced; caustic_ray
  *               (nullable, caustic_cap) the ray of each row.
@@ -407,7 +416,15 @@ int iga_eig_direct(iga_atmo_t atmo, const iga_eig_params* params, const iga_eig_
  *     (iga_fan_workspace_bytes()) exceeds IGA_FAN_STATIC_SCRATCH_BYTES.
  *   - The first call on a device looks up that device's address of the array
  *     (one-time set-up, serialised internally); make that first call before
- *     any stream capture starts.
+ *     any stream capture starts.  That first call is also when the driver
+ *     loads the library's device code and its static array and reserves the
+ *     local (stack) memory the fan kernel needs: one-time allocations by the
+ *     driver, not by this library.  Make one warm-up call during set-up, before
+ *     latency-critical work; later calls leave device memory use unchanged.
+ *   - The address is kept per device for the life of the process.  A
+ *     cudaDeviceReset of that device invalidates it, together with every
+ *     atmosphere handle on the device: reload the library's handles and do not
+ *     call this entry point on a device that was reset.
  *   - All calls share the one array (the call clears it on `stream` before
  *     launching), so calls whose work overlaps on the GPU race: issue them on
  *     one stream or otherwise order them.

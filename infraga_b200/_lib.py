@@ -361,14 +361,15 @@ def eig_direct(atmo: Atmosphere, params: EigParams, src, rcvr, incl_est: float, 
     return row if found.value else None
 
 
-PATH_RAYS, PATH_TERRAIN, PATH_PROJ = 0, 1, 2
+PATH_RAYS, PATH_TERRAIN, PATH_PROJ, PATH_RESID = 0, 1, 2, 3
 PATH_COLS, CAUSTIC_COLS, PROJ_COLS = 7, 5, 15
 
 
 def fan_paths(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, mode: int = PATH_RAYS,
               caustics: bool = False, ray_steps=None):
     """Sampled ray-path rows (run_prop's write_rays / write_topo rows, or
-    run_back_proj's projection rows with mode=PATH_PROJ) and, with
+    run_back_proj's projection rows with mode=PATH_PROJ, or print_resid's
+    per-segment residual rows with mode=PATH_RESID) and, with
     ``caustics``, caustic points of a fan.  Returns a dict with ``paths``
     [n, 7] ([n, 15] for PATH_PROJ), ``path_start`` [n_rays + 1] and, with
     caustics, ``caustics`` [m, 5] and ``caustic_ray`` [m]."""
@@ -378,8 +379,11 @@ def fan_paths(atmo: Atmosphere, params: FanParams, theta_deg, phi_deg, mode: int
     if ray_steps is None:
         ray_steps = fan_run(atmo, params, th, ph)["ray_steps"]
     steps = np.ascontiguousarray(ray_steps, dtype=np.int64)
-    div = {PATH_RAYS: 15, PATH_TERRAIN: 10, PATH_PROJ: 5}[mode]
-    cap = int(np.sum(params.bounces + 1 + steps // div + 1))
+    if mode == PATH_RESID:
+        cap = int(n * (params.bounces + 1))
+    else:
+        div = {PATH_RAYS: 15, PATH_TERRAIN: 10, PATH_PROJ: 5}[mode]
+        cap = int(np.sum(params.bounces + 1 + steps // div + 1))
     rows = np.zeros((max(cap, 1), PROJ_COLS if mode == PATH_PROJ else PATH_COLS), dtype=np.float64)
     start = np.zeros(n + 1, dtype=np.int64)
     n_path = _LL()

@@ -130,7 +130,11 @@ int ensure_alpha(iga_atmo_s* h, double freq, iga_atmo_s::AlphaTab& out) {
     iga_atmo_s::AlphaTab t;
     t.n = n; t.z0 = z0; t.inv_h = 1.0 / kAlphaStepKm;
     IGA_CUDA(cudaMalloc(&t.d, n * sizeof(float)), "cudaMalloc(alpha)");
-    IGA_CUDA(cudaMemcpy(t.d, tab.data(), n * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(alpha)");
+    const cudaError_t ce = cudaMemcpy(t.d, tab.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+        cudaFree(t.d);   // not yet owned by the handle
+        return cuda_fail(ce, "cudaMemcpy(alpha)");
+    }
     h->alpha[freq] = t;
     out = t;
     return IGA_OK;

@@ -392,7 +392,10 @@ int run_prop(int argc, char** argv, Variant v) {
         std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
         return 0;
     }
-    if (o.print_resid) std::cout << '\t' << "Note: print_resid is not provided by the GPU front end" << '\n';
+    // print_resid: residuals of every bounce segment, from the library's
+    // residual rows (3D stratified flat ground; the other solvers do not have them)
+    const bool resid = o.print_resid && v == Variant::k3D && !has_topo;
+    if (o.print_resid && !resid) std::cout << '\t' << "Note: print_resid is not provided by the GPU front end for this solver" << '\n';
 
     // source: degrees on the command line, radians inside (spherical)
     const double lat_r = xs * (Pi / 180.0), lon_r = ys * (Pi / 180.0);
@@ -560,10 +563,27 @@ int run_prop(int argc, char** argv, Variant v) {
                 s0 = s1;
             }
         }
+        std::vector<double> res_rows;
+        std::vector<long long> res_start;
+        if (resid) {
+            res_rows.assign(m * nb * IGA_PATH_COLS, 0.0);
+            res_start.assign(m + 1, 0);
+            long long n_res = 0;
+            rc = iga_fan_paths(atmo, &p, &th[r0], &ph[r0], (int)m, IGA_PATH_RESID, c.steps.data(), res_rows.data(),
+                               (long long)(m * nb), &n_res, res_start.data(), nullptr, 0, nullptr, nullptr);
+            if (rc) return fail("residuals", rc);
+        }
         size_t w = 0;   // next arrival row
         for (size_t i = 0; i < m; i++) {
             const size_t r = r0 + i;
             std::cout << "Calculating ray path: " << th[r] << " degrees inclination, " << ph[r] << " degrees azimuth." << '\n';
+            for (long long j = resid ? res_start[i] : 0; resid && j < res_start[i + 1]; j++) {
+                // after each prop_rk4 call (main.infraga.3d.cpp:437-441)
+                const double* q = &res_rows[(size_t)j * IGA_PATH_COLS];
+                std::cout << '\t' << "Residuals at Ray Termination (region boundary or reflection):" << '\n';
+                std::cout << '\t' << '\t' << "Eikonal residual: " << q[0] << '\n';
+                std::cout << '\t' << '\t' << "Aux. param. residual: " << q[1] << '\n';
+            }
             for (const double* q = path_rows[i].data(); q < path_rows[i].data() + path_rows[i].size(); q += IGA_PATH_COLS) {
                 if (sph) raypath << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1];
                 else raypath << q[0] << '\t' << q[1];

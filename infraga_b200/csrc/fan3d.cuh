@@ -105,8 +105,10 @@ constexpr int kCausCols = 7;
 constexpr int kPathRays = 0;      // rows m == 1 and m % 15 == 0 of each bounce (raypaths)
 constexpr int kPathTerrain = 1;   // rows m % 10 == 1 (terrain under the ray)
 constexpr int kPathProj = 2;      // rows m == 1 and m % 5 == 0 (back projection)
+constexpr int kPathResid = 3;     // one row per bounce segment: residuals at its row k - 1 (print_resid)
 
 __host__ __device__ inline bool path_sampled(int mode, int m) {
+    if (mode == kPathResid) return false;   // written at the segment end, not per step
     return mode == kPathRays ? (m == 1 || m % 15 == 0) : (mode == kPathTerrain ? (m % 10 == 1) : (m == 1 || m % 5 == 0));
 }
 
@@ -115,6 +117,7 @@ __host__ __device__ inline int path_cols(int mode) { return mode == kPathProj ? 
 // Upper bound on the path rows of a ray that took `steps` RK4 steps over at
 // most `segments` bounce segments: each segment of K rows samples m in 1..K-1.
 inline long long path_rows_bound(int mode, long long steps, int segments) {
+    if (mode == kPathResid) return segments;
     return (long long)segments + steps / (mode == kPathRays ? 15 : (mode == kPathTerrain ? 10 : 5)) + 1;
 }
 

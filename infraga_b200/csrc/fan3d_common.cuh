@@ -245,6 +245,51 @@ static __device__ __noinline__ double amp_db(const double* __restrict__ tab, con
 }
 
 
+// geoac::eval_eikonal and geoac::eval_eikonal_deriv (geoac.eqset.3d.strat.cpp:
+// 393-432) at state y (12-state layout) over flat ground, the print_resid
+// diagnostics: eik = |nu| - c0 / c + (u nu_x + v nu_y) / c, and aux = the norm
+// of the inclination and azimuth residuals of the auxiliary parameters.  The
+// horizontal derivatives of c, u and v vanish over flat ground and w = 0, so
+// only the z terms of the reference's sums remain; u, v and their
+// z-derivatives carry the boundary-layer scaling as atmo::u / atmo::du do.
+template <bool AMP>
+__device__ __noinline__ void eikonal_resid(const double* __restrict__ tab, const Fan3DArgs& a, int seg, const double* y,
+                                           const RayConst& rc, double& eik, double& aux) {
+    const double z = y[2];
+    const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    double c, cz, u0, u0z, v0, v0z;
+    cubic_f1(r0, q, 2, c, cz);
+    cubic_f1(r0, q, 4, u0, u0z);
+    cubic_f1(r0, q, 6, v0, v0z);
+    double sc = 1.0, dsc = 0.0;   // bndlyr_sc / bndlyr_dsc(n = 2) (atmo_state.3d.strat.cpp:85-112)
+    if (z < a.z_bl) {
+        const double X = exp(-(z - a.z0) / a.bl);
+        sc = (1.0 - X) / (1.0 + X);
+        dsc = -2.0 * (-X / a.bl) / ((1.0 + X) * (1.0 + X));
+    }
+    const double u = u0 * sc, v = v0 * sc;
+    const double nu[3] = {rc.nx, rc.ny, y[3]};
+    const double num = sqrt(nu[0] * nu[0] + nu[1] * nu[1] + nu[2] * nu[2]);
+    eik = num - a.c0 / c + (u * nu[0] + v * nu[1]) / c;
+    aux = 0.0;
+    if (AMP) {
+        const double uz = u0 * dsc + u0z * sc, vz = v0 * dsc + v0z * sc;
+        double r[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int o = 4 * j;   // X at 4..6 / 8..10, mu_z at 7 / 11
+            const double Xz = y[6 + o];
+            const double mu[3] = {j == 0 ? rc.mtx : rc.mpx, j == 0 ? rc.mty : rc.mpy, y[7 + o]};
+            r[j] = (nu[0] * mu[0] + nu[1] * mu[1] + nu[2] * mu[2]) / num + num / c * (Xz * cz) +
+                   1.0 / c * (mu[0] * u + mu[1] * v + nu[0] * (Xz * uz) + nu[1] * (Xz * vz));
+        }
+        aux = sqrt(r[0] * r[0] + r[1] * r[1]);
+    }
+}
+
 // Per-arrival diagnostics at the below-ground row y (12-state layout,
 // flat ground): launch-angle derivatives of the ground intercept as
 // find_eigenray forms them (geoac.eigenray.3d.cpp:334-348), the Jacobian D

@@ -191,6 +191,15 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         // ---- end of a bounce segment (main.infraga.3d.cpp:436-538) ----
         const int K = capped ? a.length : kb;
         steps += K;
+        if (PATHS && a.path_rows && a.path_mode == kPathResid) {
+            // print_resid (main.infraga.3d.cpp:437-441): residuals at row k - 1
+            if (p_n < p_cap) {
+                double* o = a.path_rows + (p_base + p_n) * kPathCols;
+                eikonal_resid<AMP>(tab, a, seg, y, rc, o[0], o[1]);
+                o[2] = (double)bnc; o[3] = 0.0; o[4] = 0.0; o[5] = 0.0; o[6] = 0.0;
+            }
+            p_n++;
+        }
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
         ptvt = 0.0; ptvp = 0.0;

@@ -55,7 +55,9 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
     if (!h || !p) return IGA_E_INVALID;
     int rc = validate(p, n_rays);
     if (rc) return rc;
-    if (path_mode != IGA_PATH_RAYS && path_mode != IGA_PATH_TERRAIN && path_mode != IGA_PATH_PROJ) return IGA_E_INVALID;
+    if (path_mode != IGA_PATH_RAYS && path_mode != IGA_PATH_TERRAIN && path_mode != IGA_PATH_PROJ &&
+        path_mode != IGA_PATH_RESID)
+        return IGA_E_INVALID;
     if (n_rays > 0 && (!theta_deg || !phi_deg)) return IGA_E_INVALID;
     const bool want_path = path_rows != nullptr || n_path != nullptr;
     const bool want_caus = caustic_rows != nullptr || n_caustic != nullptr;
@@ -71,6 +73,13 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
         if (want_caus || !p->calc_amp) return IGA_E_INVALID;
         if (h->kind != 0 || p->geometry != IGA_GEOM_3D) {
             g_err = "back projection rows: 3D stratified flat-ground atmospheres only";
+            return IGA_E_UNSUPPORTED;
+        }
+    }
+    if (path_mode == IGA_PATH_RESID) {   // print_resid exists here for the 3D stratified flat-ground solver
+        if (want_caus) return IGA_E_INVALID;
+        if (h->kind != 0 || p->geometry != IGA_GEOM_3D) {
+            g_err = "residual rows: 3D stratified flat-ground atmospheres only";
             return IGA_E_UNSUPPORTED;
         }
     }

@@ -1,5 +1,5 @@
 """Seeded synthetic workloads of the measured configurations, shared by
-bench.py and the profiling cases (infraga_b200/profile_cases.py).
+bench.py's timed legs and its profiling cases (``--profile-case``).
 
 * spherical range-dependent fan: a 21 x 21 node grid at 1 deg (each node a
   751-level profile whose jet amplitudes vary smoothly across the grid),

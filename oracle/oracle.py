@@ -33,10 +33,12 @@ class FanCfg(ctypes.Structure):
 
 
 def build() -> None:
-    """Compile the oracle restatement (and, where the reference is present, oracle/_ref)."""
+    """Compile the oracle restatement and, where the reference checkout is present
+    (IGA_REFERENCE_DIR, default /root/reference), oracle/_ref from its sources."""
     subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = os.environ.get("IGA_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
 def lib():

@@ -298,6 +298,9 @@ double sb_alpha_cart(double c_kms, double rho_gcc, double z, double freq, double
 }
 
 static double SB_alpha(Ray& r, double x, double y, double z, double freq) {
+#ifdef ORC_REGION_ABSORPTION
+    ORC_REGION_ABSORPTION;   // operation-counting build only (oracle/opcount)
+#endif
     double c = a_c(r, x, y, z);
     return sb_alpha_cart(c, a_rho(r, x, y, z), z, freq, r.A->tweak_abs);
 }

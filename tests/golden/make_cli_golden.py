@@ -121,6 +121,34 @@ CASES = {
 }
 
 
+# Console output cases: the lines of the reference's stdout that the
+# print_resid diagnostic writes (with the ray lines they follow), kept as
+# cli/NAME/stdout.txt.  name -> same tuple as CASES.
+STDOUT_CASES = {
+    "3d_resid": ("infraga-3d", "1d", 0,
+                 ["-prop", "atmo.met", "incl_min=5", "incl_max=35", "incl_step=10", "az_min=0", "az_max=90",
+                  "az_step=45", "bounces=2", "max_rng=900", "write_rays=false", "print_resid=true"]),
+    "3d_resid_noamp": ("infraga-3d", "1d", 2,
+                       ["-prop", "atmo.met", "incl_min=8", "incl_max=20", "incl_step=6", "azimuth=-30", "bounces=3",
+                        "max_rng=1200", "calc_amp=false", "write_rays=false", "print_resid=true"]),
+}
+RESID_MARKERS = ("Calculating ray path", "Residuals at Ray Termination", "Eikonal residual", "Aux. param. residual")
+
+
+def resid_lines(stdout: str) -> list[str]:
+    return [ln for ln in stdout.splitlines() if any(m in ln for m in RESID_MARKERS)]
+
+
+def run_case_stdout(binary_dir: str, spec) -> str:
+    """Runs one console case; returns its print_resid lines."""
+    binary, kind, seed, argv = spec
+    with tempfile.TemporaryDirectory() as work:
+        stage(work, kind, seed)
+        r = subprocess.run([os.path.join(binary_dir, binary), *argv], cwd=work, stdin=subprocess.DEVNULL,
+                           capture_output=True, text=True, check=True, timeout=600)
+        return "\n".join(resid_lines(r.stdout)) + "\n"
+
+
 def stage(work: str, kind: str, seed: int) -> None:
     """Input files of a case in `work` under fixed relative names."""
     if kind in ("1d", "1dt", "1dts"):
@@ -180,6 +208,15 @@ def main(names: list[str]) -> None:
                 f.write(text)
         meta[name] = {"binary": spec[0], "kind": spec[1], "seed": spec[2], "argv": spec[3], "files": sorted(files)}
         print(name, sorted(files), sum(len(t) for t in files.values()), "bytes")
+    for name, spec in STDOUT_CASES.items():
+        if names and name not in names:
+            continue
+        text = run_case_stdout(REF, spec)
+        d = os.path.join(OUT, name)
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "stdout.txt"), "w") as f:
+            f.write(text)
+        print(name, text.count("\n"), "console lines")
     os.makedirs(OUT, exist_ok=True)
     with open(meta_path, "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)

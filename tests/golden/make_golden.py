@@ -126,6 +126,21 @@ EIG_CASES = {
     "3d_eig_none": (2, ["rcvr_x=180", "rcvr_y=-30", "bnc_min=0", "bnc_max=1"]),
 }
 
+# Config-3 searches at the full bounce range: the first six receivers of the
+# batched eigenray workload's seeds 1 and 2 (infraga_b200.workloads.eig_pairs:
+# source at the origin, receivers on the ground 50..800 km away), bounces
+# 0..8, on the same seeded profiles.  Run concurrently (minutes per pair).
+def _eig8_cases():
+    from infraga_b200 import workloads
+    cases = {}
+    for seed in (1, 2):
+        for k, (_, (rx, ry)) in enumerate(workloads.eig_pairs(seed)[:6]):
+            cases[f"3d_eig8_s{seed}_p{k}"] = (seed, [f"rcvr_x={rx:.6f}", f"rcvr_y={ry:.6f}", "bnc_min=0", "bnc_max=8"])
+    return cases
+
+
+EIG8_CASES = _eig8_cases()
+
 # Spherical eigenray searches through oracle/harness/harness_sph.cpp (degrees
 # as on the infraga-sph command line).  name -> (profile seed, argv)
 SPH_EIG_CASES = {
@@ -212,6 +227,33 @@ def main():
             f.write(r.stdout)
         meta[name] = {"binary": "iga_ref_3d", "mode": "eig", "seed": seed, "args": args}
         print(name, r.stdout.strip().splitlines()[-1])
+    todo = [(n, a) for n, a in EIG8_CASES.items() if want(n)]
+    if todo:
+        from concurrent.futures import ThreadPoolExecutor
+
+        def run_eig8(item):
+            name, (seed, args) = item
+            out = os.path.join(HERE, name + ".txt")
+            if os.path.exists(out):
+                os.remove(out)
+            cmd = [os.path.join(REF, "iga_ref_3d"), "eig", profile_path(seed), *args, "out=" + out,
+                   "out_id=" + os.path.join("/tmp", name)]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:   # the reference crashes on some inputs: no fixture
+                if os.path.exists(out):
+                    os.remove(out)
+                return name, seed, args, None, f"reference exited with {r.returncode}"
+            with open(out, "a") as f:
+                f.write(r.stdout)
+            return name, seed, args, r.stdout.strip().splitlines()[-1], None
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+            for name, seed, args, last, err in ex.map(run_eig8, todo):
+                if err:
+                    meta.pop(name, None)
+                    print(name, "skipped:", err)
+                    continue
+                meta[name] = {"binary": "iga_ref_3d", "mode": "eig", "seed": seed, "args": args}
+                print(name, last)
     for name, (seed, args) in SPH_EIG_CASES.items():
         if not want(name):
             continue

@@ -67,3 +67,16 @@ def test_no_silent_cpu_fallback_when_no_gpu():
         pytest.skip("GPU present")
     with pytest.raises(ig.IgaError):
         ig.Atmosphere.load(os.path.join(ROOT, "tests", "golden", "profiles", "gen0.met"))
+
+
+def test_static_scratch_covers_fan_workspace():
+    """iga_fan_run_device_noalloc refuses fans whose scratch need exceeds its
+    static array; the fan's need is a constant that must fit."""
+    text = open(os.path.join(ROOT, "include", "infraga_gpu.h")).read()
+    m = re.search(r"#define\s+IGA_FAN_STATIC_SCRATCH_BYTES\s+(\d+)", text)
+    assert m, "IGA_FAN_STATIC_SCRATCH_BYTES not defined in the header"
+    assert 0 < ig.fan_workspace_bytes() <= int(m.group(1))
+    # without a device the entry point fails on its arguments, before any CUDA call
+    L = ig.lib()
+    assert L.iga_fan_run_device_noalloc(None, None, None, None, 0, None, None, None, None, None, None) == \
+        _lib.IGA_E_INVALID

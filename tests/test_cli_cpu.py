@@ -80,3 +80,10 @@ def test_reference_binaries_reproduce_fixtures(name):
     got = mk.run_case(REF, name, c)
     for rel, text in got.items():
         assert text == open(os.path.join(CLI, name, rel)).read(), rel
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "infraga-3d")), reason="compiled reference not present")
+@pytest.mark.parametrize("name", sorted(mk.STDOUT_CASES))
+def test_reference_binaries_reproduce_console_fixtures(name):
+    with open(os.path.join(CLI, name, "stdout.txt")) as f:
+        assert mk.run_case_stdout(REF, mk.STDOUT_CASES[name]) == f.read()
