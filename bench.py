@@ -127,9 +127,37 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU legs
+_REF_PROBED = {}
+
+
+def _ref_build(stem):
+    """The fastest build of a reference driver (oracle/_ref) that runs on this
+    host: -O3 -march=sapphirerapids (the GPU host's CPU) when it starts here,
+    else the portable -O3 build.  Returns (path, flags) or (None, None)."""
+    if stem in _REF_PROBED:
+        return _REF_PROBED[stem]
+    out = (None, None)
+    for suffix, flags in (("_native", "-O3 -march=sapphirerapids"), ("_fast", "-O3")):
+        exe = os.path.join(ROOT, "oracle", "_ref", stem + suffix)
+        if not os.path.exists(exe):
+            continue
+        try:   # one short ray through the solver on the committed config-0 profile
+            met = os.path.join(ROOT, "tests", "golden", "profiles", "gen0.met")
+            args = ([met, "inclination=10", "azimuth=90", "bounces=0", "max_rng=100", "write_rays=false"]
+                    if stem == "iga_ref_3d" else [])
+            r = subprocess.run([exe, "prop", *args] if args else [exe], stdout=subprocess.DEVNULL,
+                               stderr=subprocess.DEVNULL, timeout=60)
+            if r.returncode == (0 if args else 2):
+                out = (exe, flags)
+                break
+        except (OSError, subprocess.TimeoutExpired):
+            continue
+    _REF_PROBED[stem] = out
+    return out
+
+
 def ref_binary():
-    p = os.path.join(ROOT, "oracle", "_ref", "iga_ref_3d_fast")
-    return p if os.path.exists(p) else None
+    return _ref_build("iga_ref_3d")[0]
 
 
 def parse_ref_steps(text):
@@ -180,6 +208,7 @@ def cpu_baseline(met):
         steps, wall = cpu_sample_port(met, [90.0], 2.0, 1)
         kind = "port"
     return {"value": steps / wall, "unit": UNIT, "cores": 1, "kind": kind,
+            "flags": _ref_build("iga_ref_3d")[1] if kind == "reference" else None,
             "sample": f"1 azimuth (90 deg) x 30 inclinations (0.5..60 step 2), seed {SEEDS[0]}, "
                       f"{steps} ray-steps in {wall:.1f} s"}
 
@@ -212,7 +241,8 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / max(1, args.steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_dict({"reference_sample": sample}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                             "flags": _ref_build("iga_ref_3d")[1] if kind == "reference" else None},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     shutil.rmtree(tmp, ignore_errors=True)
@@ -401,7 +431,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * max_t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32c (fp32 state/RHS, hi/lo positions, fp64 sums)" if head == "fp32c" else "f64",
+            "dtype": "f32c (fp64 ray equations, fp32 Jacobian auxiliaries with compensated sums)" if head == "fp32c" else "f64",
             "data": "synthetic",
             "config": config_dict({"parallelism": f"independent fans per GPU x{world}", "precision": head,
                                    "ray_steps_per_step": tot_steps / args.steps / world}),
@@ -424,6 +454,8 @@ def run_ours(args):
             line["fp32c_over_fp64"] = res["fp32c"]["value"] / res["fp64"]["value"]
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(mets[0])
+        if world == 1 and not args.no_extra:
+            line.update(extra_configs(gpu_id))
         result = line
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -560,8 +592,7 @@ def run_serving(args):
 
 # ---------------------------------------------------------------- config 2
 def ref_sphr_binary():
-    p = os.path.join(ROOT, "oracle", "_ref", "iga_ref_sphr_fast")
-    return p if os.path.exists(p) else None
+    return _ref_build("iga_ref_sphr")[0]
 
 
 def cpu_baseline_sphr(files):
@@ -588,13 +619,17 @@ def cpu_baseline_sphr(files):
                       f"{steps} ray-steps in {wall:.1f} s"}
 
 
-def run_sphr(args):
+def sphr_measure(steps, warmup, shapes=((1, None), (0, None), (1, 0))):
     """Config 2: spherical range-dependent fan over a 21x21 node grid with
-    0.05-deg fractal terrain (workloads.py), FP64, ray-steps/s."""
+    0.05-deg fractal terrain (workloads.py), FP64.  The autotuner
+    (iga_fan_tune) picks the CTA size first; each (calc_amp, block) in
+    `shapes` (block None = the tuned one, 0 = the default 128) is timed over
+    `steps` launches with CUDA events after `warmup`, L2 flushed between.
+    Returns (legs, tuned block, seconds per tuning candidate, rays, files)."""
     import torch
     import infraga_b200 as ig
     from infraga_b200 import workloads as wl
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     files = wl.sphr_files()
     atmo = ig.Atmosphere.load_rngdep(files[0], files[1], files[2], topo_file=files[3], geometry=ig.GEOM_SPH)
     th, ph = wl.sphr_angles()
@@ -609,16 +644,16 @@ def run_sphr(args):
     ws = torch.zeros(ig.fan_workspace_bytes(), dtype=torch.uint8, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
-    # launch shape picked by the autotuner (iga_fan_tune) on this fan
     tp = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"], write_rays=0)
     best, tune_s = ig.fan_tune(atmo, tp, th, ph)
     legs = {}
-    for amp, block in ((1, best), (0, best), (1, 0)):
+    for amp, block in shapes:
+        block = best if block is None else block
         params = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"],
                                      write_rays=0, calc_amp=amp)
         params.block = block
-        times, steps = [], 0
-        for i in range(args.warmup + args.steps):
+        times, n_steps = [], 0
+        for i in range(warmup + steps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -626,12 +661,20 @@ def run_sphr(args):
                               st.data_ptr(), 0, ws.data_ptr(), stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
-            if i >= args.warmup:
+            if i >= warmup:
                 times.append(e0.elapsed_time(e1) * 1e-3)
-                steps = int(st.sum().item())
+                n_steps = int(st.sum().item())
         t = sum(times) / len(times)
-        name = ("amp" if amp else "noamp") + ("" if block else "_default_block128")
-        legs[name] = {"ray_steps": steps, "s_per_fan": t, "value": steps / t, "block": block or 128}
+        name = ("amp" if amp else "noamp") + ("" if block == best else f"_block{block or 128}")
+        legs[name] = {"ray_steps": n_steps, "s_per_fan": t, "value": n_steps / t, "block": block or 128}
+    atmo.close()
+    return legs, best, tune_s, n, files
+
+
+def run_sphr(args):
+    """Config 2 on its own line (``--sphr``): tuned and default launch shapes,
+    with and without amplitude, and the reference's CPU rate."""
+    legs, best, tune_s, n, files = sphr_measure(args.steps, args.warmup)
     cpu = None if args.no_cpu else cpu_baseline_sphr(files)
     head = legs["amp"]
     line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -673,12 +716,13 @@ def cpu_baseline_eig(mets, pairs_by_seed, bnc_max):
                       f"{n_eig} eigenrays in {wall:.1f} s"}
 
 
-def run_eigen(args):
-    """Config 3: batched 3D eigenray search, 8 seeds x 128 pairs, 0..8
-    bounces, FP64 and FP32-compensated traces; eigenrays/s over wall time."""
+def eigen_measure(seeds):
+    """Config 3: batched 3D eigenray search, 128 pairs per seed, bounces
+    0..8, FP64 and FP32-compensated traces; eigenrays/s over the wall time of
+    iga_eig_run, and the FP32C eigenrays against the FP64 ones.  Returns
+    (legs, comparison, profile paths, pairs per seed)."""
     import infraga_b200 as ig
     from infraga_b200 import workloads as wl
-    seeds = list(range(1, 9))
     bmax = wl.EIG["bnc_max"]
     mets = [wl.profile_met(sd) for sd in seeds]
     atmos = [ig.Atmosphere.load(m) for m in mets]
@@ -713,6 +757,7 @@ def run_eigen(args):
                 n_match += 1
                 d_pos.append(np.hypot(r32[j, 3] - r64[k, 3], r32[j, 4] - r64[k, 4]))
                 d_t.append(abs(r32[j, 5] - r64[k, 5]))
+
     def pct(v, q):
         v = np.asarray(v, dtype=np.float64)
         v = v[np.isfinite(v)]
@@ -724,17 +769,50 @@ def run_eigen(args):
            "landing_km_p50": pct(d_pos, 50), "landing_km_p99": pct(d_pos, 99),
            "time_s_p50": pct(d_t, 50), "time_s_p99": pct(d_t, 99),
            "rows_with_nonfinite_columns": nonfinite}
+    for a in atmos:
+        a.close()
+    return legs, err, mets, pairs
+
+
+def run_eigen(args):
+    """Config 3 on its own line (``--eigen``): 8 seeds x 128 pairs, 0..8
+    bounces, and the reference's CPU rate on a bounded sample."""
+    from infraga_b200 import workloads as wl
+    legs, err, mets, pairs = eigen_measure(list(range(1, 9)))
     cpu = None if args.no_cpu else cpu_baseline_eig(mets, pairs, 1)
     head = legs["fp32c"]
     line = {"metric": "eigenrays/s", "value": head["value"], "unit": "eigenrays/s", "n_gpus": 1, "steps": 1,
             "warmup": 1, "ms_per_step": 1e3 * head["seconds"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32-compensated (f64 Newton)", "data": "synthetic",
-            "config": {"workload": f"3d-strat-eigen-8seeds-x-{wl.EIG['pairs']}pairs-bnc0-{bmax}",
+            "config": {"workload": f"3d-strat-eigen-8seeds-x-{wl.EIG['pairs']}pairs-bnc0-{wl.EIG['bnc_max']}",
                        "timing": "wall clock of iga_eig_run over all seeds (host-driven search)"},
             "legs": legs, "fp32c_vs_fp64": err, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     return 0
 
+
+def extra_configs(gpu_id):
+    """Compact measurements of configs 2 and 3 carried in the default line,
+    each with the clocks sampled during it: the config-2 fan at the tuned CTA
+    size (2 timed launches after 1 warm-up) and one config-3 seed (128 pairs,
+    bounces 0..8) at both precisions."""
+    from infraga_b200 import workloads as wl
+    out = {}
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    legs, best, tune_s, n, _ = sphr_measure(2, 1, shapes=((1, None),))
+    out["config2"] = {"metric": METRIC, "unit": UNIT, "value": legs["amp"]["value"], "dtype": "f64",
+                      "workload": f"sph-rngdep-fan-{n}rays-21x21grid-401x401terrain-20bnc-3000km",
+                      "timing": "CUDA events, mean of 2 launches after 1 warm-up, L2 flushed",
+                      "block": best, "s_per_fan": legs["amp"]["s_per_fan"], "clocks": sampler.stop()}
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    legs3, err, _, _ = eigen_measure([1])
+    out["config3"] = {"metric": "eigenrays/s", "unit": "eigenrays/s",
+                      "workload": f"3d-strat-eigen-1seed-x-{wl.EIG['pairs']}pairs-bnc0-{wl.EIG['bnc_max']}",
+                      "timing": "wall clock of iga_eig_run", "legs": legs3, "fp32c_vs_fp64": err,
+                      "clocks": sampler.stop()}
+    return out
 
 
 # ---------------------------------------------------------------- profiling cases
@@ -819,6 +897,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API leg")
     ap.add_argument("--no-peak", action="store_true", help="skip the GEMM peak measurements")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="leave the compact config-2 / config-3 measurements out of the default line")
     ap.add_argument("--precision", choices=["both", "fp32c", "fp64"], default="both",
                     help="fan precision(s) to time; the headline is fp32c unless only fp64 is run")
     ap.add_argument("--az-step", type=float, default=FAN["az"][2],

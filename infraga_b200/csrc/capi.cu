@@ -43,35 +43,35 @@ int upload(iga_atmo_s* h) {
     IGA_CUDA(cudaMalloc(&h->d_knots, bytes), "cudaMalloc(knots)");
     IGA_CUDA(cudaMemcpy(h->d_knots, h->prof.table.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(knots)");
     IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    // FP32 segment rows: z_k, 1/dz, then for c, u, v the power-basis
-    // coefficients of the Hermite cubic f = a0 + a1 X + a2 X^2 + a3 X^3
-    // (X = (z - z_k)/dz), formed in FP64.  With A = s0 dx - df and
-    // B = -s1 dx + df (interpolation.cpp:213-221): a1 = df + A = s0 dx,
-    // a2 = B - 2A, a3 = A - B.  Rounding these to FP32 keeps ~7 digits in the
-    // derivatives, where FP32 knot values would lose ~4 to cancellation.
+    // Power-basis segment rows of the FP32-compensated kernels: z_k, 1/dz,
+    // then for c, u, v the coefficients of the Hermite cubic written as
+    // f = a0 + a1 X + a2 X^2 + a3 X^3 (X = (z - z_k)/dz).  With
+    // A = s0 dx - df and B = -s1 dx + df (interpolation.cpp:213-221):
+    // a1 = df + A = s0 dx, a2 = B - 2A, a3 = A - B; one row per evaluation
+    // instead of the two knot rows the Hermite form reads.
     const StratProfile& P = h->prof;
     const size_t n = P.z.size();
-    std::vector<float> tf(n * iga::kStrideF, 0.0f);
+    std::vector<double> tc(n * iga::kStrideC, 0.0);
     const std::vector<double>* fv[3] = {&P.c, &P.u, &P.v};
     const std::vector<double>* sv[3] = {&P.cs, &P.us, &P.vs};
     for (size_t k = 0; k < n; k++) {
-        float* o = &tf[k * iga::kStrideF];
-        o[0] = (float)P.z[k];
+        double* o = &tc[k * iga::kStrideC];
+        o[0] = P.z[k];
         if (k + 1 == n) break;
         const double dx = P.z[k + 1] - P.z[k];
-        o[1] = (float)(1.0 / dx);
+        o[1] = 1.0 / dx;
         for (int f = 0; f < 3; f++) {
             const double f0 = (*fv[f])[k], f1 = (*fv[f])[k + 1];
             const double s0 = (*sv[f])[k], s1 = (*sv[f])[k + 1];
             const double df = f1 - f0, A = s0 * dx - df, B = -s1 * dx + df;
-            o[2 + 4 * f] = (float)f0;
-            o[3 + 4 * f] = (float)(s0 * dx);
-            o[4 + 4 * f] = (float)(B - 2.0 * A);
-            o[5 + 4 * f] = (float)(A - B);
+            o[2 + 4 * f] = f0;
+            o[3 + 4 * f] = s0 * dx;
+            o[4 + 4 * f] = B - 2.0 * A;
+            o[5 + 4 * f] = A - B;
         }
     }
-    IGA_CUDA(cudaMalloc(&h->d_knots_f, tf.size() * sizeof(float)), "cudaMalloc(knots_f)");
-    IGA_CUDA(cudaMemcpy(h->d_knots_f, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(knots_f)");
+    IGA_CUDA(cudaMalloc(&h->d_knots_c, tc.size() * sizeof(double)), "cudaMalloc(knots_c)");
+    IGA_CUDA(cudaMemcpy(h->d_knots_c, tc.data(), tc.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(knots_c)");
     return IGA_OK;
 }
 
@@ -534,7 +534,7 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         iga_atmo_s::AlphaTab t;
         rc = ensure_alpha(h, p->freq, t);
         if (rc) return rc;
-        a.knots_f = h->d_knots_f;
+        a.knots_c = h->d_knots_c;
         a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
     }
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
@@ -559,7 +559,7 @@ int fp32c_setup(iga_atmo_s* h, double freq, iga::Fan3DArgs& a) {
     iga_atmo_s::AlphaTab t;
     int rc = ensure_alpha(h, freq, t);
     if (rc) return rc;
-    a.knots_f = h->d_knots_f;
+    a.knots_c = h->d_knots_c;
     a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
     return IGA_OK;
 }
@@ -780,7 +780,7 @@ int iga_atmo_destroy(iga_atmo_t h) {
     if (h->d_knots) cudaFree(h->d_knots);
     if (h->d_buf) cudaFree(h->d_buf);
     if (h->stream) cudaStreamDestroy(h->stream);
-    if (h->d_knots_f) cudaFree(h->d_knots_f);
+    if (h->d_knots_c) cudaFree(h->d_knots_c);
     if (h->d_hyb) cudaFree(h->d_hyb);
     if (h->d_topo) cudaFree(h->d_topo);
     for (auto& kv : h->alpha) cudaFree(kv.second.d);

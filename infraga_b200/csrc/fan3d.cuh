@@ -82,14 +82,15 @@ struct Fan3DArgs {
     double topo_zmax;        // topo::z_max of ground_check (max terrain + 0.01, or z0)
     double x_cut;            // r - r_earth above which exp(-(r - z_g)/bl) < 1e-173 everywhere
     // FP32-compensated path only
-    const float* knots_f;    // [n_knots][kStrideF]: per segment z_k, 1/dz and the power-basis
-                             // cubic coefficients a0..a3 of c, u, v (last row: z only)
+    const double* knots_c;   // [n_knots][kStrideC]: per segment z_k, 1/dz and the power-basis
+                             // cubic coefficients a0..a3 of c, u, v in X = (z - z_k)/dz
+                             // (last row: z only)
     const float* alpha_tab;  // Sutherland-Bass alpha(z) [dB/km, tweak_abs = 1] on a uniform grid
     int alpha_n;
     double alpha_z0, alpha_inv_h;
 };
 
-constexpr int kStrideF = 14;  // floats per segment row of the FP32 table
+constexpr int kStrideC = 14;  // doubles per segment row of the FP32-compensated path's power-basis table
 
 // Sampled output rows.  Path rows: horizontal position (x, y [km] or lat, lon
 // [deg]), altitude [km] (terrain mode: the ground height there), amplitude

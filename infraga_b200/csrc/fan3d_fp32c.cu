@@ -1,17 +1,31 @@
-// FP32-compensated ray-fan kernel: 3D Cartesian, stratified, flat ground.
+// FP32-compensated ray-fan and eigenray-trace kernels: 3D Cartesian,
+// stratified, flat ground.
 //
 // Same ray/Jacobian equations, RK4 driver, stop checks and bounce logic as
 // the FP64 kernel (fan3d_fp64.cu, following geoac.eqset.3d.strat.cpp and
 // rk4solver.cpp), with the arithmetic split by what each quantity needs:
-//   * RK4 stages and spline evaluation in FP32 (SFU exp/rsqrt);
-//   * x, y, z and nu_z carried as hi/lo float pairs updated with TwoSum, so
-//     2000 km of 1 m..50 m steps accumulate without FP32 drift;
-//   * segment vectors taken from the RK4 increments themselves (not from
-//     differences of large coordinates), path length, travel time and
-//     absorption summed in FP64;
-//   * Sutherland-Bass absorption from an FP64-built table of alpha(z) (a
-//     stratified profile makes alpha a function of altitude only);
-//   * ground intercept, reflection and amplitude in FP64 (rare events).
+//
+//   * the four ray equations (x, y, z, nu_z) and the spline values and slopes
+//     they read (c, u, v) in FP64, from a power-basis FP64 table in shared
+//     memory; square roots and reciprocals from an FP32 estimate refined by
+//     one Newton step in FP64;
+//   * the eight Jacobian auxiliaries (X_th, mu_th_z, X_ph, mu_ph_z) in FP32:
+//     their right-hand side in FP32 and their state summed with TwoSum
+//     (hi/lo pairs), so the sum of ~1e5 small increments keeps FP64-like
+//     accuracy;
+//   * boundary-layer scaling and set_ds's exponential in FP32; Sutherland-Bass
+//     absorption from an FP64-built table of alpha(z) (a stratified profile
+//     makes alpha a function of altitude only);
+//   * travel time, absorption, ground intercept, reflection and amplitude in
+//     FP64.
+//
+// The ray equations stay in FP64 because rays that graze a duct boundary have
+// launch sensitivities |d(range)/d(inclination)| of 1e6..7e7 km/rad: an FP32
+// ray state (whose ulp is ~6e-8 of the launch angle itself) moves their ground
+// intercept by hundreds of metres.  With the ray equations in FP64 the
+// intercept, travel time and turning height follow the FP64 kernel to
+// rounding; the auxiliaries only set the amplitude, which tolerates FP32
+// arithmetic once their state is summed with compensation.
 #include "eig3d.cuh"
 #include "fan3d.cuh"
 #include "fan3d_common.cuh"
@@ -21,314 +35,407 @@ namespace iga {
 namespace {
 
 #ifndef IGA_FANC_THREADS
-#define IGA_FANC_THREADS 128
+#define IGA_FANC_THREADS 192
 #endif
 #ifndef IGA_FANC_MINB
-#define IGA_FANC_MINB 4
+#define IGA_FANC_MINB 2
 #endif
 constexpr int kThreadsC = IGA_FANC_THREADS;
-// Above this height X = exp(-(z-zg)/0.1) < 2e-22 and drops out of every FP32 term.
-constexpr float kBlCutoffKmF = 5.0f;
+// Above this height X = exp(-(z-zg)/0.1) < 2e-22: S = (1-X)/(1+X) rounds to 1
+// in FP64 and the X-terms of S' and S'' vanish against the spline slopes.
+constexpr float kBlCutoffC = 5.0f;
 
-template <bool AMP> struct DimF { static constexpr int n = AMP ? 12 : 4; };
+template <bool AMP> struct AuxN { static constexpr int n = AMP ? 8 : 1; };
 
-struct RayConstF {
-    float nx, ny, mtx, mty, mpx, mpy;
+// Per-ray constants: nu_x, nu_y and |nu_h|^2 in FP64 for the ray equations,
+// FP32 copies and the mu_x, mu_y components for the auxiliaries.
+struct RayConstC {
+    double nx, ny, nh2;
+    float nxf, nyf, mtx, mty, mpx, mpy;
 };
 
-__device__ __forceinline__ int seg_walk_f(const float* __restrict__ tab, int n, float z, int k) {
-    while (k > 0 && z < tab[k * kStrideF]) --k;
-    while (k < n - 2 && z > tab[(k + 1) * kStrideF]) ++k;
+__device__ __forceinline__ int seg_walk_c(const double* __restrict__ tab, int n, double z, int k) {
+    while (k > 0 && z < tab[k * kStrideC]) --k;
+    while (k < n - 2 && z > tab[(k + 1) * kStrideC]) ++k;
     return k;
 }
 
-struct CubicF {
-    float X, idx;
+// 1/sqrt(x) for x in the normal FP32 range: the FP32 estimate refined by one
+// Newton step in FP64 (relative error below 1e-13).
+__device__ __forceinline__ double rsqrt_c(double x) {
+    const double r = (double)rsqrtf((float)x);
+    const double h = 0.5 * x * r;
+    return r * fma(-h, r, 1.5);
+}
+
+// Knuth's TwoSum: adds inc to the pair (hi, lo) and renormalises it.
+__device__ __forceinline__ void acc_pair(float& hi, float& lo, float inc) {
+    const float s = hi + inc;
+    const float bb = s - hi;
+    const float e = (hi - (s - bb)) + (inc - bb);
+    const float l = lo + e;
+    hi = s + l;
+    lo = l - (hi - s);
+}
+
+// No-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-h/bl) over flat
+// ground (bndlyr_sc / bndlyr_dsc, atmo_state.3d.strat.cpp:85-142) and its
+// first two h-derivatives, in FP32.
+struct BlScale {
+    float s0, ds, dds;
 };
 
-__device__ __forceinline__ CubicF cubic_at_f(const float* __restrict__ r0, float z) {
-    CubicF q;
-    q.idx = r0[1];
-    q.X = (z - r0[0]) * q.idx;
-    return q;
-}
-
-// Power-basis cubic of one field on the segment: col = 2 (c), 6 (u), 10 (v).
-__device__ __forceinline__ float cubicf_f(const float* __restrict__ r0, const CubicF& q, int col) {
-    const float a0 = r0[col], a1 = r0[col + 1], a2 = r0[col + 2], a3 = r0[col + 3];
-    return a0 + q.X * (a1 + q.X * (a2 + q.X * a3));
-}
-
 template <bool D2>
-__device__ __forceinline__ void cubicf_d(const float* __restrict__ r0, const CubicF& q, int col, float& f, float& d1, float& d2) {
-    const float a0 = r0[col], a1 = r0[col + 1], a2 = r0[col + 2], a3 = r0[col + 3];
-    const float X = q.X;
-    f = a0 + X * (a1 + X * (a2 + X * a3));
-    d1 = (a1 + X * (2.0f * a2 + 3.0f * a3 * X)) * q.idx;
-    if (D2) d2 = (2.0f * a2 + 6.0f * a3 * X) * (q.idx * q.idx);
-}
-
-// Knuth's TwoSum: s + e == a + b exactly.
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-    s = a + b;
-    const float bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
-}
-
-// RHS of the 12 (or 4) varying equations in FP32; see rhs() in fan3d_fp64.cu
-// for the derivation from update_refs / eval_src_eq.
-template <bool AMP>
-__device__ __forceinline__ void rhs_f(const float* __restrict__ tab, const Fan3DArgs& a, float z0f, float inv_blf,
-                                      float zlo, float zhi, int& seg, const float* y, const RayConstF& rc, float* f) {
-    const float z = y[2];
-    const float ze = fminf(fmaxf(z, zlo), zhi);
-    seg = seg_walk_f(tab, a.n_knots, ze, seg);
-    const float* r0 = tab + seg * kStrideF;
-    const CubicF q = cubic_at_f(r0, ze);
-    float c, cz, czz = 0.f, u0, u0z, u0zz = 0.f, v0, v0z, v0zz = 0.f;
-    cubicf_d<AMP>(r0, q, 2, c, cz, czz);
-    cubicf_d<AMP>(r0, q, 6, u0, u0z, u0zz);
-    cubicf_d<AMP>(r0, q, 10, v0, v0z, v0zz);
-    const float hz = z - z0f;
-    float sc0 = 1.0f, dsc2 = 0.0f, ddsc22 = 0.0f;
-    if (hz < kBlCutoffKmF) {
-        const float Xb = __expf(-hz * inv_blf);
-        const float iop = __fdividef(1.0f, 1.0f + Xb);
-        sc0 = (1.0f - Xb) * iop;
-        const float dX2 = -Xb * inv_blf;
-        dsc2 = -2.0f * dX2 * (iop * iop);
-        if (AMP) ddsc22 = -2.0f * (Xb * inv_blf * inv_blf * (iop * iop) - 2.0f * dX2 * dX2 * (iop * iop * iop));
+__device__ __forceinline__ BlScale bl_scale_c(float hz, float inv_bl) {
+    BlScale b{1.0f, 0.0f, 0.0f};
+    if (hz < kBlCutoffC) {
+        const float X = __expf(-hz * inv_bl);
+        const float iop = __fdividef(1.0f, 1.0f + X);
+        b.s0 = (1.0f - X) * iop;
+        const float dX = -X * inv_bl;
+        b.ds = -2.0f * dX * (iop * iop);
+        if (D2) b.dds = -2.0f * (X * inv_bl * inv_bl * (iop * iop) - 2.0f * dX * dX * (iop * iop * iop));
     }
-    const float u = u0 * sc0, v = v0 * sc0;
-    const float uz = u0z * sc0 + u0 * dsc2;
-    const float vz = v0z * sc0 + v0 * dsc2;
-    const float nz = y[3];
-    const float num2 = rc.nx * rc.nx + rc.ny * rc.ny + nz * nz;
-    const float inum = rsqrtf(num2);
-    const float num = num2 * inum;
-    const float cgx = c * rc.nx * inum + u;
-    const float cgy = c * rc.ny * inum + v;
-    const float cgz = c * nz * inum;
-    const float icg = rsqrtf(cgx * cgx + cgy * cgy + cgz * cgz);
-    f[0] = cgx * icg;
-    f[1] = cgy * icg;
-    f[2] = cgz * icg;
-    const float Kz = num * cz + rc.nx * uz + rc.ny * vz;
-    f[3] = -icg * Kz;
+    return b;
+}
+
+// Right-hand side at state (yd, ya): update_refs (geoac.eqset.3d.strat.cpp:
+// 225-328) + eval_src_eq (:333-389) on flat ground, the same algebra as rhs()
+// in fan3d_common.cuh; ray part fd[0..3] in FP64, auxiliaries fa[0..7]
+// (X_th, mu_th_z, X_ph, mu_ph_z) in FP32.
+template <bool AMP>
+__device__ __forceinline__ void rhs_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf, int& seg,
+                                      const double* yd, const float* ya, const RayConstC& rc, double* fd, float* fa) {
+    const double z = yd[2];
+    const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
+    seg = seg_walk_c(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStrideC;
+    const double idx = r0[1];
+    const double X = (ze - r0[0]) * idx;
+    // power basis f = a0 + X (a1 + X (a2 + X a3)), f' = (a1 + X (2 a2 + 3 a3 X)) / dz
+    const double c = fma(X, fma(X, fma(X, r0[5], r0[4]), r0[3]), r0[2]);
+    const double cz = fma(X, fma(3.0 * r0[5], X, 2.0 * r0[4]), r0[3]) * idx;
+    const double u0 = fma(X, fma(X, fma(X, r0[9], r0[8]), r0[7]), r0[6]);
+    const double u0z = fma(X, fma(3.0 * r0[9], X, 2.0 * r0[8]), r0[7]) * idx;
+    const double v0 = fma(X, fma(X, fma(X, r0[13], r0[12]), r0[11]), r0[10]);
+    const double v0z = fma(X, fma(3.0 * r0[13], X, 2.0 * r0[12]), r0[11]) * idx;
+    const BlScale bl = bl_scale_c<AMP>((float)(z - a.z0), inv_blf);
+    const double sc0 = (double)bl.s0, dsc = (double)bl.ds;
+    const double u = u0 * sc0, v = v0 * sc0;
+    const double uz = u0z * sc0 + u0 * dsc;
+    const double vz = v0z * sc0 + v0 * dsc;
+    const double nz = yd[3];
+    const double num2 = rc.nh2 + nz * nz;
+    const double inum = rsqrt_c(num2);
+    const double num = num2 * inum;
+    const double cin = c * inum;
+    const double cgx = cin * rc.nx + u;
+    const double cgy = cin * rc.ny + v;
+    const double cgz = cin * nz;
+    const double icg = rsqrt_c(cgx * cgx + cgy * cgy + cgz * cgz);
+    fd[0] = cgx * icg;
+    fd[1] = cgy * icg;
+    fd[2] = cgz * icg;
+    const double Kz = num * cz + rc.nx * uz + rc.ny * vz;
+    fd[3] = -icg * Kz;
     if (AMP) {
-        const float uzz = u0zz * sc0 + 2.0f * u0z * dsc2 + u0 * ddsc22;
-        const float vzz = v0zz * sc0 + 2.0f * v0z * dsc2 + v0 * ddsc22;
-        const float Xtz = y[6], Xpz = y[10], mtz = y[7], mpz = y[11];
-        const float dc3 = Xtz * cz, dc4 = Xpz * cz;
-        const float du3 = Xtz * uz, du4 = Xpz * uz;
-        const float dv3 = Xtz * vz + Xpz * vz;   // reference's dv[3]/dv[4] accumulation (eqset.3d.strat.cpp:298)
-        const float dnu0 = (rc.nx * rc.mtx + rc.ny * rc.mty + nz * mtz) * inum;
-        const float dnu1 = (rc.nx * rc.mpx + rc.ny * rc.mpy + nz * mpz) * inum;
-        const float cin = c * inum, cin2 = cin * inum;
-        const float g0x = rc.nx * inum * dc3 + cin * rc.mtx - cin2 * rc.nx * dnu0 + du3;
-        const float g0y = rc.ny * inum * dc3 + cin * rc.mty - cin2 * rc.ny * dnu0 + dv3;
-        const float g0z = nz * inum * dc3 + cin * mtz - cin2 * nz * dnu0;
-        const float g1x = rc.nx * inum * dc4 + cin * rc.mpx - cin2 * rc.nx * dnu1 + du4;
-        const float g1y = rc.ny * inum * dc4 + cin * rc.mpy - cin2 * rc.ny * dnu1;
-        const float g1z = nz * inum * dc4 + cin * mpz - cin2 * nz * dnu1;
-        const float dm0 = (cgx * g0x + cgy * g0y + cgz * g0z) * icg;
-        const float dm1 = (cgx * g1x + cgy * g1y + cgz * g1z) * icg;
-        const float icg2 = icg * icg;
-        f[4] = g0x * icg - cgx * icg2 * dm0;
-        f[5] = g0y * icg - cgy * icg2 * dm0;
-        f[6] = g0z * icg - cgz * icg2 * dm0;
-        f[8] = g1x * icg - cgx * icg2 * dm1;
-        f[9] = g1y * icg - cgy * icg2 * dm1;
-        f[10] = g1z * icg - cgz * icg2 * dm1;
-        f[7] = dm0 * icg2 * Kz - icg * (dnu0 * cz + num * (Xtz * czz) + rc.mtx * uz + rc.mty * vz + rc.nx * (Xtz * uzz) + rc.ny * (Xtz * vzz));
-        f[11] = dm1 * icg2 * Kz - icg * (dnu1 * cz + num * (Xpz * czz) + rc.mpx * uz + rc.mpy * vz + rc.nx * (Xpz * uzz) + rc.ny * (Xpz * vzz));
+        const double idx2 = idx * idx;
+        const float czz = (float)(fma(6.0 * r0[5], X, 2.0 * r0[4]) * idx2);
+        const float u0zz = (float)(fma(6.0 * r0[9], X, 2.0 * r0[8]) * idx2);
+        const float v0zz = (float)(fma(6.0 * r0[13], X, 2.0 * r0[12]) * idx2);
+        const float uzz = u0zz * bl.s0 + 2.0f * (float)u0z * bl.ds + (float)u0 * bl.dds;
+        const float vzz = v0zz * bl.s0 + 2.0f * (float)v0z * bl.ds + (float)v0 * bl.dds;
+        const float czf = (float)cz, uzf = (float)uz, vzf = (float)vz;
+        const float inumf = (float)inum, icgf = (float)icg, numf = (float)num, Kzf = (float)Kz;
+        const float cgxf = (float)cgx, cgyf = (float)cgy, cgzf = (float)cgz, nzf = (float)nz;
+        const float cinf = (float)cin, cin2 = cinf * inumf;
+        const float Xtz = ya[2], Xpz = ya[6], mtz = ya[3], mpz = ya[7];
+        const float dc3 = Xtz * czf, dc4 = Xpz * czf;
+        const float du3 = Xtz * uzf, du4 = Xpz * uzf;
+        const float dv3 = Xtz * vzf + Xpz * vzf;   // reference's dv[3]/dv[4] accumulation (eqset.3d.strat.cpp:298)
+        const float dnu0 = (rc.nxf * rc.mtx + rc.nyf * rc.mty + nzf * mtz) * inumf;
+        const float dnu1 = (rc.nxf * rc.mpx + rc.nyf * rc.mpy + nzf * mpz) * inumf;
+        const float g0x = rc.nxf * inumf * dc3 + cinf * rc.mtx - cin2 * rc.nxf * dnu0 + du3;
+        const float g0y = rc.nyf * inumf * dc3 + cinf * rc.mty - cin2 * rc.nyf * dnu0 + dv3;
+        const float g0z = nzf * inumf * dc3 + cinf * mtz - cin2 * nzf * dnu0;
+        const float g1x = rc.nxf * inumf * dc4 + cinf * rc.mpx - cin2 * rc.nxf * dnu1 + du4;
+        const float g1y = rc.nyf * inumf * dc4 + cinf * rc.mpy - cin2 * rc.nyf * dnu1;
+        const float g1z = nzf * inumf * dc4 + cinf * mpz - cin2 * nzf * dnu1;
+        const float dm0 = (cgxf * g0x + cgyf * g0y + cgzf * g0z) * icgf;
+        const float dm1 = (cgxf * g1x + cgyf * g1y + cgzf * g1z) * icgf;
+        const float icg2 = icgf * icgf;
+        fa[0] = g0x * icgf - cgxf * icg2 * dm0;
+        fa[1] = g0y * icgf - cgyf * icg2 * dm0;
+        fa[2] = g0z * icgf - cgzf * icg2 * dm0;
+        fa[4] = g1x * icgf - cgxf * icg2 * dm1;
+        fa[5] = g1y * icgf - cgyf * icg2 * dm1;
+        fa[6] = g1z * icgf - cgzf * icg2 * dm1;
+        fa[3] = dm0 * icg2 * Kzf - icgf * (dnu0 * czf + numf * (Xtz * czz) + rc.mtx * uzf + rc.mty * vzf +
+                                           rc.nxf * (Xtz * uzz) + rc.nyf * (Xtz * vzz));
+        fa[7] = dm1 * icg2 * Kzf - icgf * (dnu1 * czf + numf * (Xpz * czz) + rc.mpx * uzf + rc.mpy * vzf +
+                                           rc.nxf * (Xpz * uzz) + rc.nyf * (Xpz * vzz));
     }
 }
 
+// One RK4 step (rk4solver.cpp:30-55) of size ds from (yd, ya): the increments
+// incd (FP64) and inca (FP32), and the stage-1 direction f1 = c_g/|c_g| for the
+// caustic test.
 template <bool AMP>
-__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
-    constexpr int N = DimF<AMP>::n;
-    extern __shared__ float s_memf[];
-    float* s_dprev = s_memf;                       // [N][blockDim.x] previous step's increments
-    float* s_tab = s_memf + N * blockDim.x;         // FP32 knot table
-    {
-        const int tot = a.n_knots * kStrideF;
-        for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots_f[i];
-        __syncthreads();
+__device__ __forceinline__ void rk4_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf, int& seg,
+                                      double ds, const double* yd, const float* ya, const RayConstC& rc,
+                                      double* incd, float* inca, double* f1) {
+    constexpr int NA = AuxN<AMP>::n;
+    const float dsf = (float)ds;
+    double stgd[4], fd[4];
+    float stga[NA], fa[NA];
+    rhs_c<AMP>(tab, a, inv_blf, seg, yd, ya, rc, fd, fa);
+#pragma unroll
+    for (int i = 0; i < 3; i++) f1[i] = fd[i];
+#pragma unroll
+    for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] = t * (1.0 / 6.0); stgd[i] = yd[i] + t * 0.5; }
+    if (AMP) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] = t * (1.0f / 6.0f); stga[i] = ya[i] + t * 0.5f; }
     }
-    const float* tab = s_tab;
-    float* dprev = s_dprev + threadIdx.x;
+    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+#pragma unroll
+    for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] += t * (1.0 / 3.0); stgd[i] = yd[i] + t * 0.5; }
+    if (AMP) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] += t * (1.0f / 3.0f); stga[i] = ya[i] + t * 0.5f; }
+    }
+    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+#pragma unroll
+    for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] += t * (1.0 / 3.0); stgd[i] = yd[i] + t; }
+    if (AMP) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] += t * (1.0f / 3.0f); stga[i] = ya[i] + t; }
+    }
+    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+#pragma unroll
+    for (int i = 0; i < 4; i++) incd[i] += (ds * fd[i]) * (1.0 / 6.0);
+    if (AMP) {
+#pragma unroll
+        for (int i = 0; i < NA; i++) inca[i] += (dsf * fa[i]) * (1.0f / 6.0f);
+    }
+}
+
+// set_ds (geoac.eqset.3d.strat.cpp:214-220), the exponential in FP32.
+__device__ __forceinline__ double step_c(const Fan3DArgs& a, double z) {
+    double ds = a.ds_max;
+    if (z < a.z_bl) ds -= (a.ds_max - a.ds_min) * (double)__expf(-(float)(z - a.z0) * 5.0f);
+    return ds;
+}
+
+// Travel-time and absorption increments of the step yd -> yd + incd at its
+// midpoint (travel_time :486-511, c, u, v in FP64; atten :688-699 with
+// alpha(z) from the FP64-built table, tweak_abs applied here).
+__device__ __forceinline__ void seg_increment_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf,
+                                                int& seg, const double* yd, const double* incd, const RayConstC& rc,
+                                                double& dt, double& da) {
+    const double seg_ds = sqrt(incd[0] * incd[0] + incd[1] * incd[1] + incd[2] * incd[2]);
+    const double zm = yd[2] + 0.5 * incd[2];
+    const double nzm = yd[3] + 0.5 * incd[3];
+    const double ze = fmin(fmax(zm, a.z_lo), a.z_hi);
+    seg = seg_walk_c(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStrideC;
+    const double X = (ze - r0[0]) * r0[1];
+    const double c = fma(X, fma(X, fma(X, r0[5], r0[4]), r0[3]), r0[2]);
+    const double sc = (double)bl_scale_c<false>((float)(zm - a.z0), inv_blf).s0;
+    const double u = fma(X, fma(X, fma(X, r0[9], r0[8]), r0[7]), r0[6]) * sc;
+    const double v = fma(X, fma(X, fma(X, r0[13], r0[12]), r0[11]), r0[10]) * sc;
+    const double cin = c * rsqrt_c(rc.nh2 + nzm * nzm);
+    const double cgx = cin * rc.nx + u, cgy = cin * rc.ny + v, cgz = cin * nzm;
+    dt = seg_ds * rsqrt_c(cgx * cgx + cgy * cgy + cgz * cgz);
+    const float ua = (float)(zm - a.alpha_z0) * (float)a.alpha_inv_h;
+    int ia = (int)ua;
+    ia = ia < 0 ? 0 : (ia > a.alpha_n - 2 ? a.alpha_n - 2 : ia);
+    const float w = fminf(fmaxf(ua - (float)ia, 0.0f), 1.0f);
+    const float al0 = __ldg(a.alpha_tab + ia), al1 = __ldg(a.alpha_tab + ia + 1);
+    da = (double)((al0 + w * (al1 - al0)) * (float)a.tweak_abs) * seg_ds;
+}
+
+// geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105) from (x0, y0, src_z)
+// into the split state.
+template <bool AMP>
+__device__ __forceinline__ void init_c(const Fan3DArgs& a, double theta, double phi, double x0, double y0, double* yd,
+                                       float* ya, float* yl, RayConstC& rc) {
+    double y[12];
+    RayConst r;
+    ray_init<AMP>(a, theta, phi, y, r);
+    y[0] = x0; y[1] = y0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) yd[i] = y[i];
+    if (AMP) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) { ya[i] = (float)y[4 + i]; yl[i] = (float)(y[4 + i] - (double)ya[i]); }
+    }
+    rc.nx = r.nx; rc.ny = r.ny; rc.nh2 = r.nx * r.nx + r.ny * r.ny;
+    rc.nxf = (float)r.nx; rc.nyf = (float)r.ny;
+    rc.mtx = (float)r.mtx; rc.mty = (float)r.mty; rc.mpx = (float)r.mpx; rc.mpy = (float)r.mpy;
+}
+
+// Rows k-1 (r1) and the step k-2 -> k-1 (d1) in FP64, 12-state layout.
+template <bool AMP>
+__device__ __forceinline__ void last_rows_c(const double* yd, const float* ya, const float* yl, const double* dprev,
+                                            const float* dprevf, double* r1, double* d1) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) { r1[i] = yd[i]; d1[i] = dprev[i * blockDim.x]; }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        r1[4 + i] = AMP ? (double)ya[i] + (double)yl[i] : 0.0;
+        d1[4 + i] = AMP ? (double)dprevf[i * blockDim.x] : 0.0;
+    }
+}
+
+// approx_intercept + flat-ground set_refl (geoac.eqset.3d.strat.cpp:110-209)
+// in FP64 from rows k-1 and k-2, into the split state.
+template <bool AMP>
+__device__ __forceinline__ void reflect_c(const Fan3DArgs& a, const double* r1, const double* d1, const RayConstC& rc,
+                                          double* yd, float* ya, float* yl) {
+    const double dz_grnd = a.z0 - r1[2];
+    const double dz_k = d1[2];
+    double p[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) p[i] = r1[i] + d1[i] / dz_k * dz_grnd;
+    yd[0] = p[0]; yd[1] = p[1]; yd[2] = a.z0; yd[3] = -p[3];
+    if (AMP) {
+        const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
+        const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
+        const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + rc.nx * a.duz_g + rc.ny * a.dvz_g);
+        const double q[8] = {p[4], p[5], -p[6], -p[7] + (-2.0 * dnuz_ds) * ds0_dth,
+                             p[8], p[9], -p[10], -p[11] + (-2.0 * dnuz_ds) * ds0_dph};
+#pragma unroll
+        for (int i = 0; i < 8; i++) { ya[i] = (float)q[i]; yl[i] = (float)(q[i] - (double)ya[i]); }
+    }
+}
+
+// Shared memory of a launch: the FP64 table (SMEM; otherwise it is read from
+// global memory through the read-only cache), then per lane the previous
+// step's increments ([4][blockDim.x] FP64, [8][blockDim.x] FP32).
+constexpr size_t kSmemTableMax = 160 * 1024;   // larger tables (profiles over ~1,800 knots) stay in global memory
+
+inline bool table_in_smem(const Fan3DArgs& a) { return (size_t)a.n_knots * kStrideC * sizeof(double) <= kSmemTableMax; }
+
+inline size_t smem_c(const Fan3DArgs& a, int threads, bool smem_table) {
+    return (smem_table ? (size_t)a.n_knots * kStrideC * sizeof(double) : 0) +
+           (size_t)threads * (4 * sizeof(double) + 8 * sizeof(float));
+}
+
+template <bool SMEM>
+__device__ __forceinline__ const double* stage_table_c(const Fan3DArgs& a, double* s_mem) {
+    if (!SMEM) return a.knots_c;
+    const int tot = a.n_knots * kStrideC;
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) s_mem[i] = a.knots_c[i];
+    __syncthreads();
+    return s_mem;
+}
+
+template <bool AMP, bool SMEM>
+__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
+    constexpr int NA = AuxN<AMP>::n;
+    extern __shared__ double s_memc[];
+    const double* tab = stage_table_c<SMEM>(a, s_memc);
+    double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
+    double* dprev = s_lane + threadIdx.x;
+    float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
 
     const int nb = a.bounces + 1;
-    const float z0f = (float)a.z0, inv_blf = (float)a.inv_bl;
-    const float zlo = (float)a.z_lo, zhi = (float)a.z_hi;
-    const float zbl = (float)a.z_bl;
-    const float ds_max = (float)a.ds_max, ds_span = (float)(a.ds_max - a.ds_min);
-    const float tweak = (float)a.tweak_abs;
+    const float inv_blf = (float)a.inv_bl;
 
     int ray = (int)atomicAdd(a.queue, 1u);
     if (ray >= a.n_rays) return;
 
-    float y[N];         // hi parts for 0..3; plain FP32 for the auxiliaries
-    float lo[4];        // lo parts of x, y, z, nu_z
-    RayConstF rc;
+    double yd[4];
+    float ya[NA], yl[NA];
+    RayConstC rc;
     int seg, bnc, kb, na, caustics;
     float D_prev = 0.0f;
     long long steps;
-    double s, tt, att, pt, pa;
-    float zmax;
-
-    auto set_pair = [](double v, float& h, float& l) { h = (float)v; l = (float)(v - (double)h); };
+    // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
+    // sums (bulk mode) or the pending last-segment increments (write_rays mode)
+    double s, tt, att, pt, pa, zmax;
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
         const double phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
-        // geoac::set_initial in FP64, then split
-        const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
-        const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
-        const double n0x = ct * cp, n0y = ct * sp, n0z = st;
-        const double ms = 1.0 + (n0x * mx + n0y * my);
-        const double ims = 1.0 / ms, ims2 = ims * ims;
-        set_pair(a.src_x, y[0], lo[0]);
-        set_pair(a.src_y, y[1], lo[1]);
-        set_pair(a.src_z, y[2], lo[2]);
-        set_pair(n0z * ims, y[3], lo[3]);
-        rc.nx = (float)(n0x * ims);
-        rc.ny = (float)(n0y * ims);
-        if (AMP) {
-            const double tx = -st * cp, ty = -st * sp, tz = ct;
-            const double px = -ct * sp, py = ct * cp;
-            const double tm = tx * mx + ty * my, pm = px * mx + py * my;
-            rc.mtx = (float)(tx * ims - n0x * ims2 * tm);
-            rc.mty = (float)(ty * ims - n0y * ims2 * tm);
-            y[7] = (float)(tz * ims - n0z * ims2 * tm);
-            rc.mpx = (float)(px * ims - n0x * ims2 * pm);
-            rc.mpy = (float)(py * ims - n0y * ims2 * pm);
-            y[11] = (float)(-n0z * ims2 * pm);
-            y[4] = y[5] = y[6] = 0.0f;
-            y[8] = y[9] = y[10] = 0.0f;
-        } else {
-            rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0f;
-        }
+        init_c<AMP>(a, theta, phi, a.src_x, a.src_y, yd, ya, yl, rc);
         seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
-        zmax = z0f;
+        zmax = a.z0;
 #pragma unroll
-        for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
+        for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
+        if (AMP) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
+        }
     };
     start_ray(ray);
 
     while (true) {
-        const float zc = y[2] + lo[2];
-        zmax = fmaxf(zmax, zc);
-        float ds = ds_max;   // set_ds (geoac.eqset.3d.strat.cpp:214-220)
-        if (zc < zbl) ds -= ds_span * __expf(-(zc - z0f) * 5.0f);
-        s += (double)ds;
-        float inc[N], stg[N], f[N];
-        rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, y, rc, f);
-        if (AMP && a.aux && kb >= 1) {   // caustics between rows 1..k-1 of the bounce
-            const float D = ray_jacobian(f, y);
+        zmax = fmax(zmax, yd[2]);
+        const double ds = step_c(a, yd[2]);
+        s += ds;
+        double incd[4], f1[3];
+        float inca[NA];
+        rk4_c<AMP>(tab, a, inv_blf, seg, ds, yd, ya, rc, incd, inca, f1);
+        if (AMP && a.aux && kb >= 1) {   // caustics: sign changes of D between rows 1..k-1 of the bounce
+            const float f0 = (float)f1[0], g1 = (float)f1[1], g2 = (float)f1[2];
+            const float D = f0 * (ya[1] * ya[6] - ya[5] * ya[2]) - ya[0] * (g1 * ya[6] - g2 * ya[5]) +
+                            ya[4] * (g1 * ya[2] - g2 * ya[1]);
             if (kb >= 2 && D * D_prev < 0.0f) caustics++;
             D_prev = D;
         }
-#pragma unroll
-        for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] = t * (1.0f / 6.0f); stg[i] = y[i] + t * 0.5f; }
-        rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t * 0.5f; }
-        rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t; }
-        rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 6.0f); }
         kb++;
-
-        // segment increments at the midpoint, from the step vector itself
         {
-            const float seg_ds = sqrtf(inc[0] * inc[0] + inc[1] * inc[1] + inc[2] * inc[2]);
-            const float zm = y[2] + (lo[2] + 0.5f * inc[2]);
-            const float nzm = y[3] + (lo[3] + 0.5f * inc[3]);
-            const float ze = fminf(fmaxf(zm, zlo), zhi);
-            seg = seg_walk_f(tab, a.n_knots, ze, seg);
-            const float* r0 = tab + seg * kStrideF;
-            const CubicF q = cubic_at_f(r0, ze);
-            const float c = cubicf_f(r0, q, 2);
-            float sc = 1.0f;
-            if (zm < zbl) { const float X = __expf(-(zm - z0f) * inv_blf); sc = __fdividef(1.0f - X, 1.0f + X); }
-            const float u = cubicf_f(r0, q, 6) * sc, v = cubicf_f(r0, q, 10) * sc;
-            const float inum = rsqrtf(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
-            const float cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
-            const float dt = seg_ds * rsqrtf(cgx * cgx + cgy * cgy + cgz * cgz);
-            // alpha(z) table (linear), tweak_abs applied here
-            const float ua = (float)((double)zm - a.alpha_z0) * (float)a.alpha_inv_h;
-            int ia = (int)ua;
-            ia = ia < 0 ? 0 : (ia > a.alpha_n - 2 ? a.alpha_n - 2 : ia);
-            const float w = fminf(fmaxf(ua - (float)ia, 0.0f), 1.0f);
-            const float al0 = __ldg(a.alpha_tab + ia), al1 = __ldg(a.alpha_tab + ia + 1);
-            const float da = (al0 + w * (al1 - al0)) * tweak * seg_ds;
-            if (a.write_rays) { tt += pt; att += pa; pt = (double)dt; pa = (double)da; }
-            else { pt += (double)dt; pa += (double)da; }
+            double dt, da;
+            seg_increment_c(tab, a, inv_blf, seg, yd, incd, rc, dt, da);
+            if (a.write_rays) { tt += pt; att += pa; pt = dt; pa = da; }   // main.infraga.3d.cpp:451-453
+            else { pt += dt; pa += da; }                                    // :486-487
         }
-
-        // new row (not yet committed): hi/lo for 0..3
-        float nh[4], nl[4];
+        double nd[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            float e;
-            two_sum(y[i], inc[i], nh[i], e);
-            nl[i] = lo[i] + e;
-        }
-        const float zn = nh[2] + nl[2];
-        const float rx = (nh[0] - (float)a.src_x) + nl[0], ry = (nh[1] - (float)a.src_y) + nl[1];
-        const float xn = nh[0] + nl[0], yn = nh[1] + nl[1];
-        bool esc = (s > a.s_max) || (sqrtf(rx * rx + ry * ry) > (float)a.rng_max) ||
-                   (xn > (float)a.x_max) || (xn < (float)a.x_min) || (yn > (float)a.y_max) || (yn < (float)a.y_min) ||
-                   (zn > (float)a.alt_max);
-        const bool gnd = !esc && ((nh[2] - z0f) + nl[2] < 0.0f);
+        for (int i = 0; i < 4; i++) nd[i] = yd[i] + incd[i];
+        // stop checks (rk4solver.cpp:57-75, break/ground_check :438-453)
+        const double rx = nd[0] - a.src_x, ry = nd[1] - a.src_y;
+        bool esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (nd[0] > a.x_max) || (nd[0] < a.x_min) ||
+                   (nd[1] > a.y_max) || (nd[1] < a.y_min) || (nd[2] > a.alt_max);
+        const bool gnd = !esc && (nd[2] < a.z0);
         bool capped = false, bad = false;
         if (!esc && !gnd) {
             if (kb >= a.length - 1) { capped = true; esc = true; }
-            else if (!isfinite(zn) || !isfinite(nh[3])) { bad = true; esc = true; }
+            else if (!isfinite(nd[2]) || !isfinite(nd[3])) { bad = true; esc = true; }
         }
         if (!esc && !gnd) {
 #pragma unroll
-            for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
+            for (int i = 0; i < 4; i++) { dprev[i * blockDim.x] = incd[i]; yd[i] = nd[i]; }
+            if (AMP) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {   // renormalise the pair
-                const float hh = nh[i] + nl[i];
-                lo[i] = nl[i] - (hh - nh[i]);
-                y[i] = hh;
+                for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
             }
-#pragma unroll
-            for (int i = 4; i < N; i++) y[i] += inc[i];
             continue;
         }
 
+        // ---- end of a bounce segment (main.infraga.3d.cpp:436-538) ----
         const int K = capped ? a.length : kb;
         steps += K;
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
         int status = -1;
-        if (zmax < z0f + (float)a.turn_ht_min) status = 2;
+        if (zmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);
         else if (K < 2) status = 3;
         if (status < 0) {
-            // rows K-1 (y/lo), K (y + inc) and the step K-2 -> K-1 (dprev), in FP64
-            double r1[12], rk[12], d1[12];
+            // arrival record from the first below-ground row K (rk)
+            double r1[12], d1[12], rk[12];
+            last_rows_c<AMP>(yd, ya, yl, dprev, dprevf, r1, d1);
 #pragma unroll
-            for (int i = 0; i < N; i++) {
-                const double base = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
-                r1[i] = base;
-                rk[i] = base + (double)inc[i];
-                d1[i] = (double)dprev[i * blockDim.x];
-            }
+            for (int i = 0; i < 12; i++) rk[i] = r1[i] + (i < 4 ? incd[i] : (AMP ? (double)inca[i - 4] : 0.0));
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
             const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
-            const double nxd = rc.nx, nyd = rc.ny;
             const double incl = -asin(a.c_ratio * rk[3]) * 180.0 / kPi;
-            double baz = 90.0 - atan2(-nyd, -nxd) * 180.0 / kPi;
+            double baz = 90.0 - atan2(-rc.ny, -rc.nx) * 180.0 / kPi;
             if (baz < -180.0) baz += 360.0;
             else if (baz > 180.0) baz -= 360.0;
             const double ex = rk[0] - a.src_x, ey = rk[1] - a.src_y;
@@ -339,10 +446,10 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             out[4] = rk[1];
             out[5] = tt;
             out[6] = sqrt(ex * ex + ey * ey) / tt;
-            out[7] = (double)zmax;
+            out[7] = zmax;
             out[8] = incl;
             out[9] = baz;
-            RayConst rcd{nxd, nyd, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
+            const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
             double jac = 0.0;
             if (AMP) {
                 int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
@@ -357,25 +464,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
                 else ax[0] = ax[1] = ax[2] = ax[3] = 0.0;
             }
             na++;
-            // approx_intercept + set_refl (geoac.eqset.3d.strat.cpp:110-209) in FP64
-            const double dz_grnd = a.z0 - r1[2];
-            const double dz_k = d1[2];
-            double p[12];
-#pragma unroll
-            for (int i = 0; i < N; i++) p[i] = r1[i] + d1[i] / dz_k * dz_grnd;
-            set_pair(p[0], y[0], lo[0]);
-            set_pair(p[1], y[1], lo[1]);
-            set_pair(a.z0, y[2], lo[2]);
-            set_pair(-p[3], y[3], lo[3]);
-            if (AMP) {
-                y[4] = (float)p[4]; y[5] = (float)p[5]; y[6] = (float)(-p[6]);
-                y[8] = (float)p[8]; y[9] = (float)p[9]; y[10] = (float)(-p[10]);
-                const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
-                const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
-                const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + nxd * a.duz_g + nyd * a.dvz_g);
-                y[7] = (float)(-p[7] + (-2.0 * dnuz_ds) * ds0_dth);
-                y[11] = (float)(-p[11] + (-2.0 * dnuz_ds) * ds0_dph);
-            }
+            reflect_c<AMP>(a, r1, d1, rc, yd, ya, yl);
             bnc++;
             if (bnc > a.bounces) status = 0;
         }
@@ -383,6 +472,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             s = 0.0; kb = 0;
             continue;
         }
+        // ray finished: record and take the next one from the queue
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
         if (a.ray_status) a.ray_status[ray] = status;
@@ -393,154 +483,78 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
 }
 
 // Eigenray-search traces in FP32-compensated form: one request per thread,
-// n_seg prop_rk4 segments with flat-ground reflections, the last row in FP64
-// (same contract as trace3d_fp64_kernel in eig3d.cu, including the record
-// mode's per-step time/absorption sums and turning height from 0 over rows
-// 1..k-1, geoac.eigenray.3d.cpp:229-262).  The search's bracket and Newton
-// updates stay in FP64 on the host.
-template <bool AMP>
-__global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a,
-                                                                 const TraceReq* __restrict__ reqs,
-                                                                 TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
-                                                                 SegRes* __restrict__ seg_out, int seg_stride) {
-    constexpr int N = DimF<AMP>::n;
-    extern __shared__ float s_memf[];
-    float* s_dprev = s_memf;
-    float* s_tab = s_memf + N * blockDim.x;
-    {
-        const int tot = a.n_knots * kStrideF;
-        for (int i = threadIdx.x; i < tot; i += blockDim.x) s_tab[i] = a.knots_f[i];
-        __syncthreads();
-    }
+// n_seg prop_rk4 segments with flat-ground reflections (same contract as
+// trace3d_fp64_kernel in eig3d.cu, including the record mode's per-step
+// time/absorption sums and turning height from 0 over rows 1..k-1,
+// geoac.eigenray.3d.cpp:229-262).  The search's bracket and Newton updates
+// stay in FP64 on the host.
+template <bool AMP, bool SMEM>
+__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB)
+    trace3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a, const TraceReq* __restrict__ reqs,
+                         TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
+                         SegRes* __restrict__ seg_out, int seg_stride) {
+    constexpr int NA = AuxN<AMP>::n;
+    extern __shared__ double s_memc[];
+    const double* tab = stage_table_c<SMEM>(a, s_memc);
+    double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
+    double* dprev = s_lane + threadIdx.x;
+    float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
+    const float inv_blf = (float)a.inv_bl;
     // persistent: each thread takes the next request when its trace ends, so
     // lanes whose trace finished early do not idle until the warp's longest one
     for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
-        const float* tab = s_tab;
-        float* dprev = s_dprev + threadIdx.x;
         const TraceReq q = reqs[r];
         const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-        const float z0f = (float)a.z0, inv_blf = (float)a.inv_bl;
-        const float zlo = (float)a.z_lo, zhi = (float)a.z_hi;
-        const float zbl = (float)a.z_bl;
-        const float ds_max = (float)a.ds_max, ds_span = (float)(a.ds_max - a.ds_min);
-        const float tweak = (float)a.tweak_abs;
-        auto set_pair = [](double v, float& h, float& l) { h = (float)v; l = (float)(v - (double)h); };
-
-        float y[N], lo[4], inc[N];
-        RayConstF rc;
-        {
-            const double theta = q.theta, phi = q.phi;
-            const double st = sin(theta), ct = cos(theta), sp = sin(phi), cp = cos(phi);
-            const double mx = a.u0s / a.c0, my = a.v0s / a.c0;
-            const double n0x = ct * cp, n0y = ct * sp, n0z = st;
-            const double ms = 1.0 + (n0x * mx + n0y * my);
-            const double ims = 1.0 / ms, ims2 = ims * ims;
-            set_pair(q.x0, y[0], lo[0]);
-            set_pair(q.y0, y[1], lo[1]);
-            set_pair(a.src_z, y[2], lo[2]);
-            set_pair(n0z * ims, y[3], lo[3]);
-            rc.nx = (float)(n0x * ims);
-            rc.ny = (float)(n0y * ims);
-            if (AMP) {
-                const double tx = -st * cp, ty = -st * sp, tz = ct;
-                const double px = -ct * sp, py = ct * cp;
-                const double tm = tx * mx + ty * my, pm = px * mx + py * my;
-                rc.mtx = (float)(tx * ims - n0x * ims2 * tm);
-                rc.mty = (float)(ty * ims - n0y * ims2 * tm);
-                y[7] = (float)(tz * ims - n0z * ims2 * tm);
-                rc.mpx = (float)(px * ims - n0x * ims2 * pm);
-                rc.mpy = (float)(py * ims - n0y * ims2 * pm);
-                y[11] = (float)(-n0z * ims2 * pm);
-                y[4] = y[5] = y[6] = 0.0f;
-                y[8] = y[9] = y[10] = 0.0f;
-            } else {
-                rc.mtx = rc.mty = rc.mpx = rc.mpy = 0.0f;
-            }
-        }
+        double yd[4], incd[4] = {0.0, 0.0, 0.0, 0.0};
+        float ya[NA], yl[NA], inca[NA];
+        RayConstC rc;
+        init_c<AMP>(a, q.theta, q.phi, q.x0, q.y0, yd, ya, yl, rc);
+#pragma unroll
+        for (int i = 0; i < NA; i++) inca[i] = 0.0f;
         int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-        double tt = 0.0, att = 0.0;
-        float zmax = 0.0f;
+        double tt = 0.0, att = 0.0, zmax = 0.0;
         long long steps = 0;
         bool esc = false;
-#pragma unroll
-        for (int i = 0; i < N; i++) inc[i] = 0.0f;
         for (int sg = 0; sg < q.n_seg; sg++) {
             double s = 0.0, pt = 0.0, pa = 0.0;
             int kb = 0;
             bool capped = false;
 #pragma unroll
-            for (int i = 0; i < N; i++) dprev[i * blockDim.x] = 0.0f;
+            for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
+            if (AMP) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
+            }
             while (true) {
-                const float zc = y[2] + lo[2];
-                if (record && kb >= 1) zmax = fmaxf(zmax, zc);
-                float ds = ds_max;
-                if (zc < zbl) ds -= ds_span * __expf(-(zc - z0f) * 5.0f);
-                s += (double)ds;
-                float stg[N], f[N];
-                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, y, rc, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] = t * (1.0f / 6.0f); stg[i] = y[i] + t * 0.5f; }
-                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t * 0.5f; }
-                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 3.0f); stg[i] = y[i] + t; }
-                rhs_f<AMP>(tab, a, z0f, inv_blf, zlo, zhi, seg, stg, rc, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const float t = ds * f[i]; inc[i] += t * (1.0f / 6.0f); }
+                if (record && kb >= 1) zmax = fmax(zmax, yd[2]);
+                const double ds = step_c(a, yd[2]);
+                s += ds;
+                double f1[3];
+                rk4_c<AMP>(tab, a, inv_blf, seg, ds, yd, ya, rc, incd, inca, f1);
                 kb++;
                 if (record) {
-                    const float seg_ds = sqrtf(inc[0] * inc[0] + inc[1] * inc[1] + inc[2] * inc[2]);
-                    const float zm = y[2] + (lo[2] + 0.5f * inc[2]);
-                    const float nzm = y[3] + (lo[3] + 0.5f * inc[3]);
-                    const float ze = fminf(fmaxf(zm, zlo), zhi);
-                    seg = seg_walk_f(tab, a.n_knots, ze, seg);
-                    const float* r0 = tab + seg * kStrideF;
-                    const CubicF cq = cubic_at_f(r0, ze);
-                    const float c = cubicf_f(r0, cq, 2);
-                    float sc = 1.0f;
-                    if (zm < zbl) { const float X = __expf(-(zm - z0f) * inv_blf); sc = __fdividef(1.0f - X, 1.0f + X); }
-                    const float u = cubicf_f(r0, cq, 6) * sc, v = cubicf_f(r0, cq, 10) * sc;
-                    const float inum = rsqrtf(rc.nx * rc.nx + rc.ny * rc.ny + nzm * nzm);
-                    const float cgx = c * rc.nx * inum + u, cgy = c * rc.ny * inum + v, cgz = c * nzm * inum;
-                    const float dt = seg_ds * rsqrtf(cgx * cgx + cgy * cgy + cgz * cgz);
-                    const float ua = (float)((double)zm - a.alpha_z0) * (float)a.alpha_inv_h;
-                    int ia = (int)ua;
-                    ia = ia < 0 ? 0 : (ia > a.alpha_n - 2 ? a.alpha_n - 2 : ia);
-                    const float w = fminf(fmaxf(ua - (float)ia, 0.0f), 1.0f);
-                    const float al0 = __ldg(a.alpha_tab + ia), al1 = __ldg(a.alpha_tab + ia + 1);
-                    const float da = (al0 + w * (al1 - al0)) * tweak * seg_ds;
-                    tt += pt; att += pa; pt = (double)dt; pa = (double)da;
+                    double dt, da;
+                    seg_increment_c(tab, a, inv_blf, seg, yd, incd, rc, dt, da);
+                    tt += pt; att += pa; pt = dt; pa = da;
                 }
-                float nh[4], nl[4];
+                double nd[4];
 #pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    float e;
-                    two_sum(y[i], inc[i], nh[i], e);
-                    nl[i] = lo[i] + e;
-                }
-                const float zn = nh[2] + nl[2];
-                const float rx = (nh[0] - (float)q.x0) + nl[0], ry = (nh[1] - (float)q.y0) + nl[1];
-                const float xn = nh[0] + nl[0], yn = nh[1] + nl[1];
-                esc = (s > a.s_max) || (sqrtf(rx * rx + ry * ry) > (float)a.rng_max) || (xn > (float)a.x_max) ||
-                      (xn < (float)a.x_min) || (yn > (float)a.y_max) || (yn < (float)a.y_min) || (zn > (float)a.alt_max);
-                const bool gnd = !esc && ((nh[2] - z0f) + nl[2] < 0.0f);
+                for (int i = 0; i < 4; i++) nd[i] = yd[i] + incd[i];
+                const double rx = nd[0] - q.x0, ry = nd[1] - q.y0;
+                esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (nd[0] > a.x_max) ||
+                      (nd[0] < a.x_min) || (nd[1] > a.y_max) || (nd[1] < a.y_min) || (nd[2] > a.alt_max);
+                const bool gnd = !esc && (nd[2] < a.z0);
                 if (!esc && !gnd) {
                     if (kb >= a.length - 1) { capped = true; esc = true; }
-                    else if (!isfinite(zn) || !isfinite(nh[3])) esc = true;
+                    else if (!isfinite(nd[2]) || !isfinite(nd[3])) esc = true;
                 }
                 if (!esc && !gnd) {
 #pragma unroll
-                    for (int i = 0; i < N; i++) dprev[i * blockDim.x] = inc[i];
+                    for (int i = 0; i < 4; i++) { dprev[i * blockDim.x] = incd[i]; yd[i] = nd[i]; }
+                    if (AMP) {
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const float hh = nh[i] + nl[i];
-                        lo[i] = nl[i] - (hh - nh[i]);
-                        y[i] = hh;
+                        for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
                     }
-#pragma unroll
-                    for (int i = 4; i < N; i++) y[i] += inc[i];
                     continue;
                 }
                 break;
@@ -548,44 +562,25 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
             steps += capped ? a.length : kb;
             if (seg_out) {
                 SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-                g.x = (double)y[0] + (double)lo[0] + (double)inc[0];
-                g.y = (double)y[1] + (double)lo[1] + (double)inc[1];
+                g.x = yd[0] + incd[0];
+                g.y = yd[1] + incd[1];
                 g.steps = steps;
                 g.escaped = esc ? 1 : 0;
             }
             if (sg == q.n_seg - 1 || (esc && stop)) break;
-            // approx_intercept + flat-ground set_refl in FP64 from rows k-1 and k-2
-            double r1[12], d1[12], p[12];
+            double r1[12], d1[12];
+            last_rows_c<AMP>(yd, ya, yl, dprev, dprevf, r1, d1);
+            reflect_c<AMP>(a, r1, d1, rc, yd, ya, yl);
 #pragma unroll
-            for (int i = 0; i < N; i++) {
-                r1[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0);
-                d1[i] = (double)dprev[i * blockDim.x];
-            }
-            const double dz_grnd = a.z0 - r1[2];
-            const double dz_k = d1[2];
+            for (int i = 0; i < 4; i++) incd[i] = 0.0;
 #pragma unroll
-            for (int i = 0; i < N; i++) p[i] = r1[i] + d1[i] / dz_k * dz_grnd;
-            set_pair(p[0], y[0], lo[0]);
-            set_pair(p[1], y[1], lo[1]);
-            set_pair(a.z0, y[2], lo[2]);
-            set_pair(-p[3], y[3], lo[3]);
-            if (AMP) {
-                y[4] = (float)p[4]; y[5] = (float)p[5]; y[6] = (float)(-p[6]);
-                y[8] = (float)p[8]; y[9] = (float)p[9]; y[10] = (float)(-p[10]);
-                const double ds0_dth = -a.c0 / a.c_gnd * p[6] / p[3];
-                const double ds0_dph = -a.c0 / a.c_gnd * p[10] / p[3];
-                const double dnuz_ds = -1.0 / a.c_gnd * (a.c0 / a.c_gnd * a.dcz_g + (double)rc.nx * a.duz_g + (double)rc.ny * a.dvz_g);
-                y[7] = (float)(-p[7] + (-2.0 * dnuz_ds) * ds0_dth);
-                y[11] = (float)(-p[11] + (-2.0 * dnuz_ds) * ds0_dph);
-            }
-#pragma unroll
-            for (int i = 0; i < N; i++) inc[i] = 0.0f;
+            for (int i = 0; i < NA; i++) inca[i] = 0.0f;
         }
         double rk[12];
 #pragma unroll
-        for (int i = 0; i < 12; i++) rk[i] = 0.0;
+        for (int i = 0; i < 4; i++) rk[i] = yd[i] + incd[i];
 #pragma unroll
-        for (int i = 0; i < N; i++) rk[i] = (double)y[i] + (i < 4 ? (double)lo[i] : 0.0) + (double)inc[i];
+        for (int i = 0; i < 8; i++) rk[4 + i] = AMP ? (double)ya[i] + (double)yl[i] + (double)inca[i] : 0.0;
         TraceRes& o = out[r];
 #pragma unroll
         for (int i = 0; i < 12; i++) o.y[i] = rk[i];
@@ -593,8 +588,8 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
         o.steps = steps;
         o.escaped = esc ? 1 : 0;
         if (record) {
-            o.tt = tt; o.att = att; o.zmax = (double)zmax;
-            RayConst rcd{(double)rc.nx, (double)rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
+            o.tt = tt; o.att = att; o.zmax = zmax;
+            const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
             int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
             o.amp_db = AMP ? amp_db(a.knots, a, segd, rk, rcd, q.theta, q.phi, nullptr) : 0.0;
             const double ze = fmin(fmax(rk[2], a.z_lo), a.z_hi);
@@ -610,12 +605,12 @@ __global__ void __launch_bounds__(kThreadsC) trace3d_fp32c_kernel(const __grid_c
     }
 }
 
-template <bool AMP>
+template <bool AMP, bool SMEM>
 cudaError_t launch_trace_c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, cudaStream_t st,
                            SegRes* seg_out, int seg_stride, unsigned int* d_queue) {
     if (n <= 0) return cudaSuccess;
-    auto kern = trace3d_fp32c_kernel<AMP>;
-    const size_t smem = (size_t)DimF<AMP>::n * kThreadsC * sizeof(float) + (size_t)a.n_knots * kStrideF * sizeof(float);
+    auto kern = trace3d_fp32c_kernel<AMP, SMEM>;
+    const size_t smem = smem_c(a, kThreadsC, SMEM);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int grid = 0;
@@ -625,12 +620,12 @@ cudaError_t launch_trace_c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* 
     return cudaGetLastError();
 }
 
-template <bool AMP>
+template <bool AMP, bool SMEM>
 cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     // threads per block: the caller's choice (a multiple of 32 up to kThreadsC) or kThreadsC
     const int threads = a.block > 0 ? a.block : kThreadsC;
-    auto kern = fan3d_fp32c_kernel<AMP>;
-    const size_t smem = (size_t)DimF<AMP>::n * threads * sizeof(float) + (size_t)a.n_knots * kStrideF * sizeof(float);
+    auto kern = fan3d_fp32c_kernel<AMP, SMEM>;
+    const size_t smem = smem_c(a, threads, SMEM);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, n_sm = 0, per_sm = 0;
@@ -651,13 +646,18 @@ cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
 }  // namespace
 
 cudaError_t launch_fan3d_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used) {
-    return calc_amp ? launch_c<true>(a, stream, grid_used) : launch_c<false>(a, stream, grid_used);
+    if (table_in_smem(a))
+        return calc_amp ? launch_c<true, true>(a, stream, grid_used) : launch_c<false, true>(a, stream, grid_used);
+    return calc_amp ? launch_c<true, false>(a, stream, grid_used) : launch_c<false, false>(a, stream, grid_used);
 }
 
 cudaError_t launch_trace_fp32c(const Fan3DArgs& a, const TraceReq* d_req, TraceRes* d_res, int n, bool amp,
                                cudaStream_t st, unsigned int* d_queue, SegRes* seg_out, int seg_stride) {
-    return amp ? launch_trace_c<true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
-               : launch_trace_c<false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    if (table_in_smem(a))
+        return amp ? launch_trace_c<true, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+                   : launch_trace_c<false, true>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
+    return amp ? launch_trace_c<true, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue)
+               : launch_trace_c<false, false>(a, d_req, d_res, n, st, seg_out, seg_stride, d_queue);
 }
 
 }  // namespace iga

@@ -37,7 +37,7 @@ struct iga_atmo_s {
     void* d_buf = nullptr;
     size_t d_buf_bytes = 0;
     // FP32-compensated path: FP32 knot table and alpha(z) tables per frequency
-    float* d_knots_f = nullptr;
+    double* d_knots_c = nullptr;   // power-basis FP64 table of the FP32-compensated kernels
     std::mutex alpha_mu;
     struct AlphaTab { float* d = nullptr; int n = 0; double z0 = 0.0, inv_h = 0.0; };
     std::map<double, AlphaTab> alpha;   // kept until destroy (launches may still read them)

@@ -1,14 +1,17 @@
-"""FP32-compensated fan (IGA_FP32C) against the FP64 reference: error bounds
-on arrivals whose FP64 values are stable at FP32 precision, counts of the
-arrivals outside that set, and of rays whose bounce / turning classification
-flips."""
+"""FP32-compensated fan (IGA_FP32C) against FP64: the north-star bound --
+ground-intercept range within 10 m, travel time within 10 ms, amplitude within
+0.1 dB -- on every non-caustic arrival (no caustic passed by the ray up to that
+arrival), with zero violations, on every 3D golden case (against the
+reference's own output) and on the full 71,520-ray config-1 fan of each of the
+four benchmark seeds (against the FP64 kernel, which follows the reference to
+1e-9).  Classification flips (arrival count or turning layer) are counted and
+must stay rare."""
 import numpy as np
 import pytest
 
 import infraga_b200 as ig
 from infraga_b200 import synth
-from tests._cases import (case_setup, fp32c_errors, fp64_stability, load_cases, match_arrivals, parse_golden,
-                          profile_path, worst_rows)
+from tests._cases import case_setup, load_cases, match_arrivals, noncaustic_report, parse_golden, profile_path
 
 pytestmark = pytest.mark.gpu
 
@@ -30,48 +33,40 @@ def ray_ids(rows, th, ph):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_fp32c_matches_reference_cases(dev, name):
-    """Against the reference's own FP64 output (golden fixtures)."""
+def test_fp32c_north_star_bound_on_reference_cases(dev, name):
+    """Against the reference's own FP64 output (golden fixtures); the caustic
+    count of each arrival comes from the FP64 GPU run, whose arrivals are the
+    golden rows (tests/test_fan3d_gpu.py)."""
     c = CASES[name]
     th, ph, p = case_setup(c["args"])
     atmo = ig.Atmosphere.load(profile_path(c["seed"]))
-    base, stab = fp64_stability(ig, atmo, atmo.default_params(**p), th, ph)
+    r64 = ig.fan_run(atmo, atmo.default_params(**p), th, ph, with_aux=True)
     ref, _ = parse_golden(name)
-    assert base["arrivals"].shape == ref.shape
-    r = ig.fan_run(atmo, atmo.default_params(**p, precision=ig.FP32C), th, ph)
-    a, b, st, flipped = match_arrivals(r["arrivals"], r["ray_index"].astype(np.int64), ref, ray_ids(ref, th, ph),
-                                       th.size, stab)
-    ok, err = fp32c_errors(a, b, st, calc_amp=p["calc_amp"])
-    print(name, "flips", flipped.size, err)
-    print("  worst range:", worst_rows(a, b, st, 3, 3))
-    print("  worst amp:", worst_rows(a, b, st, 10, 3))
+    assert r64["arrivals"].shape == ref.shape
+    r32 = ig.fan_run(atmo, atmo.default_params(**p, precision=ig.FP32C), th, ph)
+    got, want, aux, flipped = match_arrivals(r32["arrivals"], r32["ray_index"].astype(np.int64), ref,
+                                             ray_ids(ref, th, ph), th.size, r64["aux"])
+    rep = noncaustic_report(got, want, aux[:, 3], calc_amp=bool(p["calc_amp"]))
+    print(name, "flips", flipped.size, rep)
     assert flipped.size <= max(1, th.size // 100), f"classification flips on rays {flipped}"
-    assert ok, err
-    # over every matched arrival (stable or not), <= 1000 km and 5 bounces
-    assert err["range_km_p90"] <= 0.01 and err["time_s_p90"] <= 0.03, err
+    assert rep["ok"], rep
 
 
-def test_fp32c_full_fan_vs_fp64(dev):
-    """71,520-ray fan, 10 bounces, 2000 km: FP32C against FP64 on the GPU."""
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_fp32c_north_star_bound_full_fan(dev, seed):
+    """The config-1 fan (596 x 120 = 71,520 rays, 10 bounces, 2000 km) of one
+    benchmark seed: zero violations on the non-caustic arrivals."""
     th, ph = synth.fan_angles(0.5, 60.01, 0.1, 0, 357, 3)
-    atmo = ig.Atmosphere.load(profile_path(1))
+    atmo = ig.Atmosphere.load(profile_path(seed))
     kw = dict(bounces=10, rng_max=2000.0, write_rays=0)
-    r64, stab = fp64_stability(ig, atmo, atmo.default_params(**kw), th, ph)
+    r64 = ig.fan_run(atmo, atmo.default_params(**kw), th, ph, with_aux=True)
     r32 = ig.fan_run(atmo, atmo.default_params(**kw, precision=ig.FP32C), th, ph)
-    a, b, st, flipped = match_arrivals(r32["arrivals"], r32["ray_index"].astype(np.int64),
-                                       r64["arrivals"], r64["ray_index"].astype(np.int64), th.size, stab)
-    ok, err = fp32c_errors(a, b, st)
-    frac_flip = flipped.size / th.size
+    got, want, aux, flipped = match_arrivals(r32["arrivals"], r32["ray_index"].astype(np.int64), r64["arrivals"],
+                                             r64["ray_index"].astype(np.int64), th.size, r64["aux"])
+    rep = noncaustic_report(got, want, aux[:, 3])
     steps_rel = abs(r32["total_steps"] - r64["total_steps"]) / r64["total_steps"]
-    print("full fan fp32c vs fp64: flips", flipped.size, f"({100 * frac_flip:.3f}%)", err, "steps rel", steps_rel)
-    print("  worst range:", worst_rows(a, b, st, 3, 4))
-    print("  worst amp:", worst_rows(a, b, st, 10, 4))
-    assert frac_flip < 1e-3
+    print(f"seed {seed}: flips {flipped.size} ({100 * flipped.size / th.size:.4f}%) steps rel {steps_rel:.2e}", rep)
+    assert rep["n_noncaustic"] > 1000
+    assert rep["ok"], rep
+    assert flipped.size < 1e-3 * th.size
     assert steps_rel < 1e-4
-    # The one-sided perturbation check misses some edge rays: measured 0.44%
-    # of the range-stable arrivals fall outside the bounds; at most 1% may.
-    assert err["n_range_stable_violations"] <= 1e-2 * err["n_range_stable"], err
-    assert err["n_amp_stable_violations"] <= 1e-2 * err["n_amp_stable"], err
-    # distribution over every matched arrival of the 2000 km, 10-bounce fan
-    assert err["range_km_p50"] <= 0.005 and err["range_km_p90"] <= 0.015 and err["range_km_p99"] <= 0.05, err
-    assert err["time_s_p90"] <= 0.05 and err["amp_db_p90"] <= 0.1, err
