@@ -45,8 +45,15 @@ enum iga_ray_status {
     IGA_RAY_SHORT = 3,       /* ground reached in < 2 steps (main.infraga.3d.cpp:507) */
     IGA_RAY_NONFINITE = 4,   /* state became NaN/Inf */
     IGA_RAY_STEPCAP = 5,     /* s_max/ds_min steps without a stop (prop_rk4 array bound) */
-    IGA_RAY_TIME = 6         /* travel time above time_max (spherical run_prop,
+    IGA_RAY_TIME = 6,        /* travel time above time_max (spherical run_prop,
                                 main.infraga.sph.cpp:515) */
+    /* Flag OR'ed into the reason above (status & 0xff) for IGA_FP32C rays
+     * with amplitudes that were traced again, from launch, with FP64
+     * auxiliaries: a ray whose tube Jacobian at an arrival falls below 0.2 of
+     * the largest |D| along its path before its first caustic.  Near such a
+     * focus the amplitude is ill-conditioned and FP32 auxiliaries would miss
+     * it by tenths of a dB. */
+    IGA_RAY_AUX_FP64 = 0x100
 };
 
 /* geometry / precision selectors */

@@ -66,13 +66,53 @@ void strip_extension(char* s) {
         }
 }
 
+// How the binary was started: its reference name (the serial one or the MPI
+// build's infraga-accel-* name) and, under mpirun, the process count the
+// reference's MPI summaries print as "threads".
+struct Launch {
+    bool accel = false;
+    int threads = 1;
+};
+Launch g_launch;
+
+// Rank and size of an MPI launch, from the variables the common launchers set
+// (Open MPI, MPICH / Hydra, PMIx, Slurm); 0 and 1 without one.
+int env_int(const char* const* names, int dflt) {
+    for (const char* const* n = names; *n; n++) {
+        const char* v = getenv(*n);
+        if (v && v[0]) return atoi(v);
+    }
+    return dflt;
+}
+int launch_rank() {
+    static const char* const k[] = {"OMPI_COMM_WORLD_RANK", "PMI_RANK", "PMIX_RANK", "MV2_COMM_WORLD_RANK", "SLURM_PROCID", nullptr};
+    return env_int(k, 0);
+}
+int launch_size() {
+    static const char* const k[] = {"OMPI_COMM_WORLD_SIZE", "PMI_SIZE", "MV2_COMM_WORLD_SIZE", "SLURM_NTASKS", nullptr};
+    return std::max(1, env_int(k, 1));
+}
+
 const char* variant_name(Variant v) {
+    if (g_launch.accel) {
+        switch (v) {
+            case Variant::k3D: return "infraga-accel-3d";
+            case Variant::kSph: return "infraga-accel-sph";
+            case Variant::k3DRngdep: return "infraga-accel-3d-rngdep";
+            default: return "infraga-accel-sph-rngdep";
+        }
+    }
     switch (v) {
         case Variant::k3D: return "infraga-3d";
         case Variant::kSph: return "infraga-sph";
         case Variant::k3DRngdep: return "infraga-3d-rngdep";
         default: return "infraga-sph-rngdep";
     }
+}
+
+// The MPI builds' summaries end with the process count (main.infraga.3d.mpi.cpp:322, :868).
+void threads_line(std::ostream& f, const char* lead) {
+    if (g_launch.accel) f << lead << '\t' << "threads: " << g_launch.threads << '\n';
 }
 
 bool is_sph(Variant v) { return v == Variant::kSph || v == Variant::kSphRngdep; }
@@ -476,7 +516,9 @@ int run_prop(int argc, char** argv, Variant v) {
     else results << "#" << '\t' << "topo file:" << topo << '\n';
     if (v == Variant::kSph) results << "#" << '\t' << "turn_ht_min: " << turn_ht_min << '\n';
     results << "#" << '\t' << "frequency: " << freq << '\n';
-    results << "#" << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n' << '\n';
+    results << "#" << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n';
+    threads_line(results, "#");
+    results << '\n';
     const char* cols_3d[] = {"x_0 [km]", "y_0 [km]", "arrival incl [deg]", "back az [deg]"};
     const char* cols_sph[] = {"lat_0 [deg]", "lon_0 [deg]", "inclination [deg]", "back azimuth [deg]"};
     const char** cn = sph ? cols_sph : cols_3d;
@@ -665,6 +707,10 @@ struct EigOpts {
     bool verbose = false;
     bool write_atmo = false;
     const char* output_id = nullptr;
+    // infraga-accel-* only: source and receiver list files
+    // (main.infraga.3d.mpi.cpp:639-640, :720-760)
+    const char* srcs_list = nullptr;
+    const char* rcvrs_list = nullptr;
 };
 
 // Sampled path of one eigenray for {id}.eigenray-N.dat (find_eigenray's
@@ -758,6 +804,13 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
         else if (sph && key2(a, "rcvr_lat=", "lat_rcvr=", &val)) o.rcvr[0] = atof(val);
         else if (sph && key2(a, "rcvr_lon=", "lon_rcvr=", &val)) o.rcvr[1] = atof(val);
         else if (key(a, "verbose=", &val)) o.verbose = str2bool(val);
+        else if (g_launch.accel && !direct && key2(a, "srcs_list=", "list_srcs=", &val)) o.srcs_list = val;
+        else if (g_launch.accel && !direct && key2(a, "rcvrs_list=", "list_rcvrs=", &val)) o.rcvrs_list = val;
+        // the MPI builds' sequential-source reuse and verbose receiver choice:
+        // accepted; every source here gets the full search
+        else if (g_launch.accel && !direct && key(a, "seq_srcs=", &val)) {}
+        else if (g_launch.accel && !direct && key(a, "seq_srcs_dr=", &val)) {}
+        else if (g_launch.accel && !direct && key(a, "verbose_rcvr=", &val)) {}
         else if (key(a, "iterations=", &val)) ep.iterations = (int)atof(val);
         else if (key(a, "damping=", &val)) ep.damping = atof(val);
         else if (key(a, "tolerance=", &val)) ep.tolerance = atof(val);
@@ -775,6 +828,140 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
     }
     o.write_atmo = po.write_atmo;
     return true;
+}
+
+// Rows of a source or receiver list file: file_length lines (those not
+// starting with '#', less one), `cols` numbers each (fileIO.cpp:18-35).
+bool read_list(const char* path, int cols, std::vector<double>& out) {
+    std::ifstream f(path);
+    if (!f.is_open()) return false;
+    int n = 0;
+    std::string line;
+    while (std::getline(f, line))
+        if (line.find('#') != 0) n++;
+    n -= 1;
+    if (n < 1) return false;
+    f.clear();
+    f.seekg(0);
+    out.clear();
+    for (int i = 0; i < n * cols; i++) {
+        double x;
+        if (!(f >> x)) return false;
+        out.push_back(x);
+    }
+    return true;
+}
+
+// infraga-accel-* -eig_search with srcs_list= / rcvrs_list=
+// (main.infraga.3d.mpi.cpp:556-975): every source against every receiver,
+// each source's receivers in one batched search, one arrivals file per
+// (source, receiver) named as the MPI build names them, eigenray path files
+// numbered per file from 0.  The search itself is the serial one
+// (est_eigenray / find_eigenray of geoac.eigenray.3d.cpp), as for the
+// single-pair case.
+template <class Ground>
+int run_eig_lists(Variant v, const char* profile, const char* topo, iga_atmo_t atmo, iga_eig_params& ep,
+                  const EigOpts& o, const std::string& id, Ground ground) {
+    const bool sph = is_sph(v), has_topo = topo != nullptr;
+    std::vector<double> srcs, rcvrs;
+    if (o.srcs_list) {
+        if (!read_list(o.srcs_list, 3, srcs)) {
+            std::cout << '\t' << "ERROR: cannot read source list " << o.srcs_list << '\n';
+            return 0;
+        }
+    } else {
+        srcs.assign(o.src, o.src + 3);
+    }
+    if (o.rcvrs_list) {
+        if (!read_list(o.rcvrs_list, 2, rcvrs)) {
+            std::cout << '\t' << "ERROR: cannot read receiver list " << o.rcvrs_list << '\n';
+            return 0;
+        }
+    } else {
+        rcvrs.assign(o.rcvr, o.rcvr + 2);
+    }
+    const int n_src = (int)srcs.size() / 3, n_rcv = (int)rcvrs.size() / 2;
+    for (int n = 0; n < n_src; n++) srcs[3 * n + 2] = std::max(srcs[3 * n + 2], ground(srcs[3 * n], srcs[3 * n + 1]));
+    const char* loc_s = sph ? "source location (lat, lon, alt): " : "source location: ";
+    const char* loc_r = sph ? "receiver location (lat, lon, alt): " : "receiver location: ";
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "source location(s) " << (sph ? "(lat, lon, alt):" : "(x, y, alt):") << '\n';
+    for (int n = 0; n < std::min(n_src, 10); n++)
+        std::cout << '\t' << '\t' << "(" << srcs[3 * n] << ", " << srcs[3 * n + 1] << ", " << srcs[3 * n + 2] << ")" << '\n';
+    if (n_src > 10) std::cout << '\t' << '\t' << "..." << '\n';
+    std::cout << '\t' << "receiver location(s) " << (sph ? "(lat, lon, alt):" : "(x, y, alt):") << '\n';
+    for (int i = 0; i < std::min(n_rcv, 10); i++)
+        std::cout << '\t' << '\t' << "(" << rcvrs[2 * i] << ", " << rcvrs[2 * i + 1] << ", "
+                  << ground(rcvrs[2 * i], rcvrs[2 * i + 1]) << ")" << '\n';
+    if (n_rcv > 10) std::cout << '\t' << '\t' << "..." << '\n';
+    std::cout << '\t' << "inclination range: " << ep.incl_min << ", " << ep.incl_max << '\n';
+    std::cout << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
+    if (!has_topo) std::cout << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+    std::cout << '\t' << "damping:" << ep.damping << '\n';
+    std::cout << '\t' << "frequency: " << ep.fan.freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n';
+    std::cout << '\t' << "threads: " << g_launch.threads << '\n' << '\n';
+
+    for (int n = 0; n < n_src; n++) {
+        const double* src = &srcs[3 * n];
+        std::cout << '\n' << "Searching for eigenrays from source at " << src[0] << ", " << src[1] << ", " << src[2] << '\n';
+        std::vector<iga_eig_pair> pairs(n_rcv);
+        for (int i = 0; i < n_rcv; i++) {
+            pairs[i].src[0] = src[0]; pairs[i].src[1] = src[1]; pairs[i].src[2] = src[2];
+            pairs[i].rcvr[0] = rcvrs[2 * i]; pairs[i].rcvr[1] = rcvrs[2 * i + 1];
+        }
+        int cap = 256 * n_rcv, n_out = 0;
+        std::vector<double> rows((size_t)cap * IGA_ARRIVAL_COLS);
+        std::vector<int> pidx(cap);
+        long long steps = 0;
+        int rc = iga_eig_run(atmo, &ep, pairs.data(), n_rcv, rows.data(), cap, &n_out, pidx.data(), &steps);
+        if (rc == IGA_E_TRUNCATED) {
+            cap = n_out;
+            rows.resize((size_t)cap * IGA_ARRIVAL_COLS);
+            pidx.resize(cap);
+            rc = iga_eig_run(atmo, &ep, pairs.data(), n_rcv, rows.data(), cap, &n_out, pidx.data(), &steps);
+        }
+        if (rc) return fail("eigenray search", rc);
+        for (int i = 0; i < n_rcv; i++) {
+            std::string stem = id;
+            if (n_src > 1) stem += ".src-" + std::to_string(n);
+            if (n_rcv > 1) stem += ".rcvr-" + std::to_string(i);
+            std::ofstream res((stem + ".arrivals.dat").c_str());
+            const double zr = ground(rcvrs[2 * i], rcvrs[2 * i + 1]);
+            res << "# " << variant_name(v) << " -eig_search summary:" << '\n';
+            res << "# " << '\t' << "profile: " << profile << '\n';
+            res << "# " << '\t' << loc_s << src[0] << ", " << src[1] << ", " << src[2] << '\n';
+            res << "# " << '\t' << loc_r << rcvrs[2 * i] << ", " << rcvrs[2 * i + 1] << ", " << zr << ")." << '\n';
+            res << "# " << '\t' << "inclination range: " << ep.incl_min << ", " << ep.incl_max << '\n';
+            res << "# " << '\t' << "bounces: " << ep.bnc_min << ", " << ep.bnc_max << '\n';
+            if (!has_topo) res << "#" << '\t' << "ground elevation: " << ep.fan.z_grnd << '\n';
+            else res << "#" << '\t' << "topo file:" << topo << '\n';
+            res << "# " << '\t' << "damping: " << ep.damping << '\n';
+            res << "# " << '\t' << "frequency: " << ep.fan.freq << '\n';
+            res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n';
+            res << "# " << '\t' << "threads: " << g_launch.threads << '\n' << '\n';
+            res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << (sph ? "lat_0 [deg]" : "x_0 [km]") << '\t'
+                << (sph ? "lon_0 [deg]" : "y_0 [km]") << '\t' << "time [s]" << '\t' << "cel [km/s]" << '\t'
+                << "turning ht [km]" << '\t' << "arrival incl [deg]" << '\t' << "back az [deg]" << '\t'
+                << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\n';
+            int cnt = 0;
+            for (int j = 0; j < n_out; j++) {
+                if (pidx[j] != i) continue;
+                const double* q = &rows[(size_t)j * IGA_ARRIVAL_COLS];
+                res << std::setprecision(8) << q[0] << '\t' << std::setprecision(8) << q[1] << '\t' << (int)q[2];
+                for (int col = 3; col < IGA_ARRIVAL_COLS; col++) res << '\t' << q[col];
+                res << '\n';
+                print_eigenray(q, src, o.verbose);
+                rc = write_eigenray_file(stem + ".eigenray-" + std::to_string(cnt) + ".dat", atmo, ep.fan, src, q[0], q[1],
+                                         (int)q[2], sph);
+                if (rc) return fail("eigenray path", rc);
+                cnt++;
+            }
+            std::cout << '\t' << "Identified " << cnt << " eigenray(s) to receiver at " << rcvrs[2 * i] << ", "
+                      << rcvrs[2 * i + 1] << ", " << zr << '\n';
+        }
+    }
+    return 0;
 }
 
 int run_eig(int argc, char** argv, Variant v, bool direct) {
@@ -845,6 +1032,11 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
         o.output_id = argv[2];
     }
     const std::string id = o.output_id;
+    if (!direct && (o.srcs_list || o.rcvrs_list)) {
+        rc = run_eig_lists(v, argv[2], topo, atmo, ep, o, id, ground);
+        iga_atmo_destroy(atmo);
+        return rc;
+    }
     iga_eig_pair pair;
     pair.src[0] = o.src[0]; pair.src[1] = o.src[1]; pair.src[2] = o.src[2];
     pair.rcvr[0] = o.rcvr[0]; pair.rcvr[1] = o.rcvr[1];
@@ -902,7 +1094,9 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
         res << "# " << '\t' << "damping: " << ep.damping << '\n';
         res << "# " << '\t' << "frequency: " << ep.fan.freq << '\n';
         // infraga-sph writes no blank line after the summary (main.infraga.sph.cpp:944)
-        res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n' << (sph ? "" : "\n");
+        res << "# " << '\t' << "S&B atten coeff: " << ep.fan.tweak_abs << '\n';
+        threads_line(res, "# ");
+        res << (sph ? "" : "\n");
         if (sph)
             res << "# incl [deg]" << '\t' << "az [deg]" << '\t' << "n_b" << '\t' << "lat_0 [deg]" << '\t' << "lon_0 [deg]"
                 << '\t' << "time [s]" << '\t' << "cel [km/s]" << '\t' << "turning ht [km]" << '\t' << "inclination [deg]"
@@ -1068,7 +1262,12 @@ int run_back(int argc, char** argv, Variant v) {
 
 }  // namespace
 
-int run(int argc, char** argv, Variant v) {
+int run(int argc, char** argv, Variant v, bool accel) {
+    g_launch.accel = accel;
+    if (accel) {
+        if (launch_rank() > 0) return 0;   // one GPU process does the work of the whole launch
+        g_launch.threads = launch_size();
+    }
     const int min_args = is_rngdep(v) ? 5 : 3;
     if (argc < min_args) {
         usage(v);

@@ -15,7 +15,12 @@ namespace cli {
 
 enum class Variant { k3D, kSph, k3DRngdep, kSphRngdep };
 
-// main() of one binary: option dispatch as in the reference mains.
-int run(int argc, char** argv, Variant v);
+// main() of one binary: option dispatch as in the reference mains.  accel:
+// the infraga-accel-* names the reference gives its MPI builds
+// (src/main.infraga.*.mpi.cpp), which run_infraga.py launches as
+// `mpirun -np N infraga-accel-* ...` for --cpu-cnt N >= 2.  The GPU traces the
+// whole job in the first process; the other processes of such a launch exit
+// at once.
+int run(int argc, char** argv, Variant v, bool accel = false);
 
 }  // namespace cli

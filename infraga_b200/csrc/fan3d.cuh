@@ -97,6 +97,10 @@ constexpr int kStrideC = 14;  // doubles per segment row of the FP32-compensated
 // [dB] (0 without calc_amp or in terrain mode), absorption [dB] (-2 x the
 // running sum), travel time [s], bounce.  Caustic rows: position (3), time,
 // bounce, ray, and the ray's step index of the row (for ordering).
+// Flag OR'ed into a ray's status (IGA_RAY_AUX_FP64): an FP32C ray traced
+// again with FP64 auxiliaries after a focusing arrival.
+constexpr int kRayAuxFp64 = 0x100;
+
 // Back-projection rows (kPathProj, 3D stratified flat-ground kernel only):
 // x, y, z [km], time [s], X_incl (3) [km/deg], T_incl [s/deg], X_az (3),
 // T_az, group velocity (3) [km/s].

@@ -13,11 +13,10 @@
 //     their right-hand side in FP32 and their state summed with TwoSum
 //     (hi/lo pairs), so the sum of ~1e5 small increments keeps FP64-like
 //     accuracy;
-//   * boundary-layer scaling and set_ds's exponential in FP32; Sutherland-Bass
-//     absorption from an FP64-built table of alpha(z) (a stratified profile
-//     makes alpha a function of altitude only);
-//   * travel time, absorption, ground intercept, reflection and amplitude in
-//     FP64.
+//   * Sutherland-Bass absorption from an FP64-built table of alpha(z) (a
+//     stratified profile makes alpha a function of altitude only);
+//   * boundary-layer scaling, set_ds, travel time, absorption sums, ground
+//     intercept, reflection and amplitude in FP64.
 //
 // The ray equations stay in FP64 because rays that graze a duct boundary have
 // launch sensitivities |d(range)/d(inclination)| of 1e6..7e7 km/rad: an FP32
@@ -43,16 +42,30 @@ namespace {
 constexpr int kThreadsC = IGA_FANC_THREADS;
 // Above this height X = exp(-(z-zg)/0.1) < 2e-22: S = (1-X)/(1+X) rounds to 1
 // in FP64 and the X-terms of S' and S'' vanish against the spline slopes.
-constexpr float kBlCutoffC = 5.0f;
+constexpr double kBlCutoffC = 5.0;
 
 template <bool AMP> struct AuxN { static constexpr int n = AMP ? 8 : 1; };
 
+// Focusing test.  Near a caustic the ray tube collapses: the Jacobian D at an
+// arrival falls far below the largest |D| the ray has had, and the amplitude
+// becomes ill-conditioned -- an error in the auxiliaries early on the path
+// reaches the arrival amplified by 1e4..1e5 (the same amplification shows
+// with the auxiliaries in FP64, one rounding order lower).  A ray that meets
+// an arrival with |D| < kFocusRatio * max|D| before its first caustic is
+// traced again from its launch with FP64 auxiliaries (about 1% of the rays
+// of a 10-bounce fan); every other ray keeps its FP32 auxiliaries.
+constexpr double kFocusRatio = 0.2;
+
 // Per-ray constants: nu_x, nu_y and |nu_h|^2 in FP64 for the ray equations,
-// FP32 copies and the mu_x, mu_y components for the auxiliaries.
+// copies and the mu_x, mu_y components in the auxiliaries' type T.
+template <class T>
 struct RayConstC {
     double nx, ny, nh2;
-    float nxf, nyf, mtx, mty, mpx, mpy;
+    T nxf, nyf, mtx, mty, mpx, mpy;
 };
+
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 
 __device__ __forceinline__ int seg_walk_c(const double* __restrict__ tab, int n, double z, int k) {
     while (k > 0 && z < tab[k * kStrideC]) --k;
@@ -69,32 +82,35 @@ __device__ __forceinline__ double rsqrt_c(double x) {
 }
 
 // Knuth's TwoSum: adds inc to the pair (hi, lo) and renormalises it.
-__device__ __forceinline__ void acc_pair(float& hi, float& lo, float inc) {
-    const float s = hi + inc;
-    const float bb = s - hi;
-    const float e = (hi - (s - bb)) + (inc - bb);
-    const float l = lo + e;
+template <class T>
+__device__ __forceinline__ void acc_pair(T& hi, T& lo, T inc) {
+    const T s = hi + inc;
+    const T bb = s - hi;
+    const T e = (hi - (s - bb)) + (inc - bb);
+    const T l = lo + e;
     hi = s + l;
     lo = l - (hi - s);
 }
 
 // No-slip boundary-layer scaling S = (1-X)/(1+X), X = exp(-h/bl) over flat
-// ground (bndlyr_sc / bndlyr_dsc, atmo_state.3d.strat.cpp:85-142) and its
-// first two h-derivatives, in FP32.
+// ground (bndlyr_sc / bndlyr_dsc, atmo_state.3d.strat.cpp:85-142) and its first
+// two h-derivatives, in FP64: the wind and its gradient enter the ray equations,
+// and for rays near a duct boundary an FP32 scaling shifts the intercept by
+// tens of metres.  Only the lowest kBlCutoffC km pay for the exponential.
 struct BlScale {
-    float s0, ds, dds;
+    double s0, ds, dds;
 };
 
 template <bool D2>
-__device__ __forceinline__ BlScale bl_scale_c(float hz, float inv_bl) {
-    BlScale b{1.0f, 0.0f, 0.0f};
+__device__ __forceinline__ BlScale bl_scale_c(double hz, double inv_bl) {
+    BlScale b{1.0, 0.0, 0.0};
     if (hz < kBlCutoffC) {
-        const float X = __expf(-hz * inv_bl);
-        const float iop = __fdividef(1.0f, 1.0f + X);
-        b.s0 = (1.0f - X) * iop;
-        const float dX = -X * inv_bl;
-        b.ds = -2.0f * dX * (iop * iop);
-        if (D2) b.dds = -2.0f * (X * inv_bl * inv_bl * (iop * iop) - 2.0f * dX * dX * (iop * iop * iop));
+        const double X = exp(-hz * inv_bl);
+        const double iop = 1.0 / (1.0 + X);
+        b.s0 = (1.0 - X) * iop;
+        const double dX = -X * inv_bl;
+        b.ds = -2.0 * dX * (iop * iop);
+        if (D2) b.dds = -2.0 * (X * inv_bl * inv_bl * (iop * iop) - 2.0 * dX * dX * (iop * iop * iop));
     }
     return b;
 }
@@ -102,25 +118,26 @@ __device__ __forceinline__ BlScale bl_scale_c(float hz, float inv_bl) {
 // Right-hand side at state (yd, ya): update_refs (geoac.eqset.3d.strat.cpp:
 // 225-328) + eval_src_eq (:333-389) on flat ground, the same algebra as rhs()
 // in fan3d_common.cuh; ray part fd[0..3] in FP64, auxiliaries fa[0..7]
-// (X_th, mu_th_z, X_ph, mu_ph_z) in FP32.
-template <bool AMP>
-__device__ __forceinline__ void rhs_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf, int& seg,
-                                      const double* yd, const float* ya, const RayConstC& rc, double* fd, float* fa) {
+// (X_th, mu_th_z, X_ph, mu_ph_z) in T (FP32, or FP64 for a re-traced ray).
+template <bool AMP, class T>
+__device__ __forceinline__ void rhs_c(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                      const double* yd, const T* ya, const RayConstC<T>& rc, double* fd, T* fa) {
     const double z = yd[2];
     const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
     seg = seg_walk_c(tab, a.n_knots, ze, seg);
     const double* r0 = tab + seg * kStrideC;
     const double idx = r0[1];
     const double X = (ze - r0[0]) * idx;
-    // power basis f = a0 + X (a1 + X (a2 + X a3)), f' = (a1 + X (2 a2 + 3 a3 X)) / dz
+    // power basis f = a0 + X (a1 + X (a2 + X a3)), f' = (a1 + 2X a2 + 3X^2 a3) / dz
+    const double X2 = 2.0 * X, X3 = 3.0 * X * X;
     const double c = fma(X, fma(X, fma(X, r0[5], r0[4]), r0[3]), r0[2]);
-    const double cz = fma(X, fma(3.0 * r0[5], X, 2.0 * r0[4]), r0[3]) * idx;
+    const double cz = fma(X3, r0[5], fma(X2, r0[4], r0[3])) * idx;
     const double u0 = fma(X, fma(X, fma(X, r0[9], r0[8]), r0[7]), r0[6]);
-    const double u0z = fma(X, fma(3.0 * r0[9], X, 2.0 * r0[8]), r0[7]) * idx;
+    const double u0z = fma(X3, r0[9], fma(X2, r0[8], r0[7])) * idx;
     const double v0 = fma(X, fma(X, fma(X, r0[13], r0[12]), r0[11]), r0[10]);
-    const double v0z = fma(X, fma(3.0 * r0[13], X, 2.0 * r0[12]), r0[11]) * idx;
-    const BlScale bl = bl_scale_c<AMP>((float)(z - a.z0), inv_blf);
-    const double sc0 = (double)bl.s0, dsc = (double)bl.ds;
+    const double v0z = fma(X3, r0[13], fma(X2, r0[12], r0[11])) * idx;
+    const BlScale bl = bl_scale_c<AMP>(z - a.z0, a.inv_bl);
+    const double sc0 = bl.s0, dsc = bl.ds;
     const double u = u0 * sc0, v = v0 * sc0;
     const double uz = u0z * sc0 + u0 * dsc;
     const double vz = v0z * sc0 + v0 * dsc;
@@ -139,31 +156,33 @@ __device__ __forceinline__ void rhs_c(const double* __restrict__ tab, const Fan3
     const double Kz = num * cz + rc.nx * uz + rc.ny * vz;
     fd[3] = -icg * Kz;
     if (AMP) {
-        const double idx2 = idx * idx;
-        const float czz = (float)(fma(6.0 * r0[5], X, 2.0 * r0[4]) * idx2);
-        const float u0zz = (float)(fma(6.0 * r0[9], X, 2.0 * r0[8]) * idx2);
-        const float v0zz = (float)(fma(6.0 * r0[13], X, 2.0 * r0[12]) * idx2);
-        const float uzz = u0zz * bl.s0 + 2.0f * (float)u0z * bl.ds + (float)u0 * bl.dds;
-        const float vzz = v0zz * bl.s0 + 2.0f * (float)v0z * bl.ds + (float)v0 * bl.dds;
-        const float czf = (float)cz, uzf = (float)uz, vzf = (float)vz;
-        const float inumf = (float)inum, icgf = (float)icg, numf = (float)num, Kzf = (float)Kz;
-        const float cgxf = (float)cgx, cgyf = (float)cgy, cgzf = (float)cgz, nzf = (float)nz;
-        const float cinf = (float)cin, cin2 = cinf * inumf;
-        const float Xtz = ya[2], Xpz = ya[6], mtz = ya[3], mpz = ya[7];
-        const float dc3 = Xtz * czf, dc4 = Xpz * czf;
-        const float du3 = Xtz * uzf, du4 = Xpz * uzf;
-        const float dv3 = Xtz * vzf + Xpz * vzf;   // reference's dv[3]/dv[4] accumulation (eqset.3d.strat.cpp:298)
-        const float dnu0 = (rc.nxf * rc.mtx + rc.nyf * rc.mty + nzf * mtz) * inumf;
-        const float dnu1 = (rc.nxf * rc.mpx + rc.nyf * rc.mpy + nzf * mpz) * inumf;
-        const float g0x = rc.nxf * inumf * dc3 + cinf * rc.mtx - cin2 * rc.nxf * dnu0 + du3;
-        const float g0y = rc.nyf * inumf * dc3 + cinf * rc.mty - cin2 * rc.nyf * dnu0 + dv3;
-        const float g0z = nzf * inumf * dc3 + cinf * mtz - cin2 * nzf * dnu0;
-        const float g1x = rc.nxf * inumf * dc4 + cinf * rc.mpx - cin2 * rc.nxf * dnu1 + du4;
-        const float g1y = rc.nyf * inumf * dc4 + cinf * rc.mpy - cin2 * rc.nyf * dnu1;
-        const float g1z = nzf * inumf * dc4 + cinf * mpz - cin2 * nzf * dnu1;
-        const float dm0 = (cgxf * g0x + cgyf * g0y + cgzf * g0z) * icgf;
-        const float dm1 = (cgxf * g1x + cgyf * g1y + cgzf * g1z) * icgf;
-        const float icg2 = icgf * icgf;
+        // f'' = (2 a2 + 6 X a3) / dz^2, formed in T (auxiliaries only)
+        const T idx2 = (T)(idx * idx), Xf6 = T(6) * (T)X;
+        const T czz = fma_t(Xf6, (T)r0[5], T(2) * (T)r0[4]) * idx2;
+        const T u0zz = fma_t(Xf6, (T)r0[9], T(2) * (T)r0[8]) * idx2;
+        const T v0zz = fma_t(Xf6, (T)r0[13], T(2) * (T)r0[12]) * idx2;
+        const T s0f = (T)bl.s0, dsf = (T)bl.ds, ddsf = (T)bl.dds;
+        const T uzz = u0zz * s0f + T(2) * (T)u0z * dsf + (T)u0 * ddsf;
+        const T vzz = v0zz * s0f + T(2) * (T)v0z * dsf + (T)v0 * ddsf;
+        const T czf = (T)cz, uzf = (T)uz, vzf = (T)vz;
+        const T inumf = (T)inum, icgf = (T)icg, numf = (T)num, Kzf = (T)Kz;
+        const T cgxf = (T)cgx, cgyf = (T)cgy, cgzf = (T)cgz, nzf = (T)nz;
+        const T cinf = (T)cin, cin2 = cinf * inumf;
+        const T Xtz = ya[2], Xpz = ya[6], mtz = ya[3], mpz = ya[7];
+        const T dc3 = Xtz * czf, dc4 = Xpz * czf;
+        const T du3 = Xtz * uzf, du4 = Xpz * uzf;
+        const T dv3 = Xtz * vzf + Xpz * vzf;   // reference's dv[3]/dv[4] accumulation (eqset.3d.strat.cpp:298)
+        const T dnu0 = (rc.nxf * rc.mtx + rc.nyf * rc.mty + nzf * mtz) * inumf;
+        const T dnu1 = (rc.nxf * rc.mpx + rc.nyf * rc.mpy + nzf * mpz) * inumf;
+        const T g0x = rc.nxf * inumf * dc3 + cinf * rc.mtx - cin2 * rc.nxf * dnu0 + du3;
+        const T g0y = rc.nyf * inumf * dc3 + cinf * rc.mty - cin2 * rc.nyf * dnu0 + dv3;
+        const T g0z = nzf * inumf * dc3 + cinf * mtz - cin2 * nzf * dnu0;
+        const T g1x = rc.nxf * inumf * dc4 + cinf * rc.mpx - cin2 * rc.nxf * dnu1 + du4;
+        const T g1y = rc.nyf * inumf * dc4 + cinf * rc.mpy - cin2 * rc.nyf * dnu1;
+        const T g1z = nzf * inumf * dc4 + cinf * mpz - cin2 * nzf * dnu1;
+        const T dm0 = (cgxf * g0x + cgyf * g0y + cgzf * g0z) * icgf;
+        const T dm1 = (cgxf * g1x + cgyf * g1y + cgzf * g1z) * icgf;
+        const T icg2 = icgf * icgf;
         fa[0] = g0x * icgf - cgxf * icg2 * dm0;
         fa[1] = g0y * icgf - cgyf * icg2 * dm0;
         fa[2] = g0z * icgf - cgzf * icg2 * dm0;
@@ -178,60 +197,63 @@ __device__ __forceinline__ void rhs_c(const double* __restrict__ tab, const Fan3
 }
 
 // One RK4 step (rk4solver.cpp:30-55) of size ds from (yd, ya): the increments
-// incd (FP64) and inca (FP32), and the stage-1 direction f1 = c_g/|c_g| for the
+// incd (FP64) and inca (T), and the stage-1 direction f1 = c_g/|c_g| for the
 // caustic test.
-template <bool AMP>
-__device__ __forceinline__ void rk4_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf, int& seg,
-                                      double ds, const double* yd, const float* ya, const RayConstC& rc,
-                                      double* incd, float* inca, double* f1) {
+template <bool AMP, class T>
+__device__ __forceinline__ void rk4_c(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                      double ds, const double* yd, const T* ya, const RayConstC<T>& rc,
+                                      double* incd, T* inca, double* f1) {
     constexpr int NA = AuxN<AMP>::n;
-    const float dsf = (float)ds;
+    const T dsf = (T)ds;
+    const T sixth = T(1) / T(6), third = T(1) / T(3), half = T(0.5);
     double stgd[4], fd[4];
-    float stga[NA], fa[NA];
-    rhs_c<AMP>(tab, a, inv_blf, seg, yd, ya, rc, fd, fa);
+    T stga[NA], fa[NA];
+    rhs_c<AMP>(tab, a, seg, yd, ya, rc, fd, fa);
 #pragma unroll
     for (int i = 0; i < 3; i++) f1[i] = fd[i];
 #pragma unroll
     for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] = t * (1.0 / 6.0); stgd[i] = yd[i] + t * 0.5; }
     if (AMP) {
 #pragma unroll
-        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] = t * (1.0f / 6.0f); stga[i] = ya[i] + t * 0.5f; }
+        for (int i = 0; i < NA; i++) { const T t = dsf * fa[i]; inca[i] = t * sixth; stga[i] = ya[i] + t * half; }
     }
-    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+    rhs_c<AMP>(tab, a, seg, stgd, stga, rc, fd, fa);
 #pragma unroll
     for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] += t * (1.0 / 3.0); stgd[i] = yd[i] + t * 0.5; }
     if (AMP) {
 #pragma unroll
-        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] += t * (1.0f / 3.0f); stga[i] = ya[i] + t * 0.5f; }
+        for (int i = 0; i < NA; i++) { const T t = dsf * fa[i]; inca[i] += t * third; stga[i] = ya[i] + t * half; }
     }
-    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+    rhs_c<AMP>(tab, a, seg, stgd, stga, rc, fd, fa);
 #pragma unroll
     for (int i = 0; i < 4; i++) { const double t = ds * fd[i]; incd[i] += t * (1.0 / 3.0); stgd[i] = yd[i] + t; }
     if (AMP) {
 #pragma unroll
-        for (int i = 0; i < NA; i++) { const float t = dsf * fa[i]; inca[i] += t * (1.0f / 3.0f); stga[i] = ya[i] + t; }
+        for (int i = 0; i < NA; i++) { const T t = dsf * fa[i]; inca[i] += t * third; stga[i] = ya[i] + t; }
     }
-    rhs_c<AMP>(tab, a, inv_blf, seg, stgd, stga, rc, fd, fa);
+    rhs_c<AMP>(tab, a, seg, stgd, stga, rc, fd, fa);
 #pragma unroll
     for (int i = 0; i < 4; i++) incd[i] += (ds * fd[i]) * (1.0 / 6.0);
     if (AMP) {
 #pragma unroll
-        for (int i = 0; i < NA; i++) inca[i] += (dsf * fa[i]) * (1.0f / 6.0f);
+        for (int i = 0; i < NA; i++) inca[i] += (dsf * fa[i]) * sixth;
     }
 }
 
-// set_ds (geoac.eqset.3d.strat.cpp:214-220), the exponential in FP32.
+// set_ds (geoac.eqset.3d.strat.cpp:214-220), as the FP64 kernel forms it, so
+// both precisions step through the same rows near the ground.
 __device__ __forceinline__ double step_c(const Fan3DArgs& a, double z) {
     double ds = a.ds_max;
-    if (z < a.z_bl) ds -= (a.ds_max - a.ds_min) * (double)__expf(-(float)(z - a.z0) * 5.0f);
+    if (z < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(z - a.z0) / 0.2);
     return ds;
 }
 
 // Travel-time and absorption increments of the step yd -> yd + incd at its
 // midpoint (travel_time :486-511, c, u, v in FP64; atten :688-699 with
 // alpha(z) from the FP64-built table, tweak_abs applied here).
-__device__ __forceinline__ void seg_increment_c(const double* __restrict__ tab, const Fan3DArgs& a, float inv_blf,
-                                                int& seg, const double* yd, const double* incd, const RayConstC& rc,
+template <class T>
+__device__ __forceinline__ void seg_increment_c(const double* __restrict__ tab, const Fan3DArgs& a, int& seg,
+                                                const double* yd, const double* incd, const RayConstC<T>& rc,
                                                 double& dt, double& da) {
     const double seg_ds = sqrt(incd[0] * incd[0] + incd[1] * incd[1] + incd[2] * incd[2]);
     const double zm = yd[2] + 0.5 * incd[2];
@@ -241,7 +263,7 @@ __device__ __forceinline__ void seg_increment_c(const double* __restrict__ tab, 
     const double* r0 = tab + seg * kStrideC;
     const double X = (ze - r0[0]) * r0[1];
     const double c = fma(X, fma(X, fma(X, r0[5], r0[4]), r0[3]), r0[2]);
-    const double sc = (double)bl_scale_c<false>((float)(zm - a.z0), inv_blf).s0;
+    const double sc = bl_scale_c<false>(zm - a.z0, a.inv_bl).s0;
     const double u = fma(X, fma(X, fma(X, r0[9], r0[8]), r0[7]), r0[6]) * sc;
     const double v = fma(X, fma(X, fma(X, r0[13], r0[12]), r0[11]), r0[10]) * sc;
     const double cin = c * rsqrt_c(rc.nh2 + nzm * nzm);
@@ -257,9 +279,9 @@ __device__ __forceinline__ void seg_increment_c(const double* __restrict__ tab, 
 
 // geoac::set_initial (geoac.eqset.3d.strat.cpp:58-105) from (x0, y0, src_z)
 // into the split state.
-template <bool AMP>
+template <bool AMP, class T>
 __device__ __forceinline__ void init_c(const Fan3DArgs& a, double theta, double phi, double x0, double y0, double* yd,
-                                       float* ya, float* yl, RayConstC& rc) {
+                                       T* ya, T* yl, RayConstC<T>& rc) {
     double y[12];
     RayConst r;
     ray_init<AMP>(a, theta, phi, y, r);
@@ -268,16 +290,19 @@ __device__ __forceinline__ void init_c(const Fan3DArgs& a, double theta, double 
     for (int i = 0; i < 4; i++) yd[i] = y[i];
     if (AMP) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) { ya[i] = (float)y[4 + i]; yl[i] = (float)(y[4 + i] - (double)ya[i]); }
+        for (int i = 0; i < 8; i++) { ya[i] = (T)y[4 + i]; yl[i] = (T)(y[4 + i] - (double)ya[i]); }
     }
     rc.nx = r.nx; rc.ny = r.ny; rc.nh2 = r.nx * r.nx + r.ny * r.ny;
-    rc.nxf = (float)r.nx; rc.nyf = (float)r.ny;
-    rc.mtx = (float)r.mtx; rc.mty = (float)r.mty; rc.mpx = (float)r.mpx; rc.mpy = (float)r.mpy;
+    rc.nxf = (T)r.nx; rc.nyf = (T)r.ny;
+    rc.mtx = (T)r.mtx; rc.mty = (T)r.mty; rc.mpx = (T)r.mpx; rc.mpy = (T)r.mpy;
 }
 
-// Rows k-1 (r1) and the step k-2 -> k-1 (d1) in FP64, 12-state layout.
-template <bool AMP>
-__device__ __forceinline__ void last_rows_c(const double* yd, const float* ya, const float* yl, const double* dprev,
+// Rows k-1 (r1) and the step k-2 -> k-1 (d1) in FP64, 12-state layout.  The
+// auxiliaries' step is kept in FP32 for both types: it enters only the
+// intercept extrapolation, scaled by dz_grnd / dz_k <= 1, where its rounding
+// is ~1e-10 of the state.
+template <bool AMP, class T>
+__device__ __forceinline__ void last_rows_c(const double* yd, const T* ya, const T* yl, const double* dprev,
                                             const float* dprevf, double* r1, double* d1) {
 #pragma unroll
     for (int i = 0; i < 4; i++) { r1[i] = yd[i]; d1[i] = dprev[i * blockDim.x]; }
@@ -290,9 +315,9 @@ __device__ __forceinline__ void last_rows_c(const double* yd, const float* ya, c
 
 // approx_intercept + flat-ground set_refl (geoac.eqset.3d.strat.cpp:110-209)
 // in FP64 from rows k-1 and k-2, into the split state.
-template <bool AMP>
-__device__ __forceinline__ void reflect_c(const Fan3DArgs& a, const double* r1, const double* d1, const RayConstC& rc,
-                                          double* yd, float* ya, float* yl) {
+template <bool AMP, class T>
+__device__ __forceinline__ void reflect_c(const Fan3DArgs& a, const double* r1, const double* d1, const RayConstC<T>& rc,
+                                          double* yd, T* ya, T* yl) {
     const double dz_grnd = a.z0 - r1[2];
     const double dz_k = d1[2];
     double p[12];
@@ -306,7 +331,7 @@ __device__ __forceinline__ void reflect_c(const Fan3DArgs& a, const double* r1, 
         const double q[8] = {p[4], p[5], -p[6], -p[7] + (-2.0 * dnuz_ds) * ds0_dth,
                              p[8], p[9], -p[10], -p[11] + (-2.0 * dnuz_ds) * ds0_dph};
 #pragma unroll
-        for (int i = 0; i < 8; i++) { ya[i] = (float)q[i]; yl[i] = (float)(q[i] - (double)ya[i]); }
+        for (int i = 0; i < 8; i++) { ya[i] = (T)q[i]; yl[i] = (T)(q[i] - (double)ya[i]); }
     }
 }
 
@@ -331,66 +356,58 @@ __device__ __forceinline__ const double* stage_table_c(const Fan3DArgs& a, doubl
     return s_mem;
 }
 
-template <bool AMP, bool SMEM>
-__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
+// One ray of the fan, launch to last bounce, with the auxiliaries in T.
+// Returns true, with nothing of the ray's record final, when T is FP32 and the
+// ray reaches a focusing arrival (kFocusRatio) before its first caustic: the
+// caller then traces it again with T = double.
+template <bool AMP, class T>
+__device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
+                                          float* dprevf, int ray) {
     constexpr int NA = AuxN<AMP>::n;
-    extern __shared__ double s_memc[];
-    const double* tab = stage_table_c<SMEM>(a, s_memc);
-    double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
-    double* dprev = s_lane + threadIdx.x;
-    float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
-
+    constexpr bool ESCALATE = AMP && sizeof(T) == sizeof(float);
     const int nb = a.bounces + 1;
-    const float inv_blf = (float)a.inv_bl;
-
-    int ray = (int)atomicAdd(a.queue, 1u);
-    if (ray >= a.n_rays) return;
+    const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
+    const double theta = th_deg * kPi / 180.0;
+    const double phi = kPi / 2.0 - ph_deg * kPi / 180.0;
 
     double yd[4];
-    float ya[NA], yl[NA];
-    RayConstC rc;
-    int seg, bnc, kb, na, caustics;
-    float D_prev = 0.0f;
-    long long steps;
+    T ya[NA], yl[NA];
+    RayConstC<T> rc;
+    init_c<AMP>(a, theta, phi, a.src_x, a.src_y, yd, ya, yl, rc);
+    int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+    int bnc = 0, kb = 0, na = 0, caustics = 0;
+    T D_prev = T(0), D_max = T(0);
+    long long steps = 0;
     // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
     // sums (bulk mode) or the pending last-segment increments (write_rays mode)
-    double s, tt, att, pt, pa, zmax;
-
-    auto start_ray = [&](int r) {
-        const double theta = a.theta_deg[r] * kPi / 180.0;
-        const double phi = kPi / 2.0 - a.phi_deg[r] * kPi / 180.0;
-        init_c<AMP>(a, theta, phi, a.src_x, a.src_y, yd, ya, yl, rc);
-        seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-        bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
-        s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
-        zmax = a.z0;
+    double s = 0.0, tt = 0.0, att = 0.0, pt = 0.0, pa = 0.0, zmax = a.z0;
 #pragma unroll
-        for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
-        if (AMP) {
+    for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
+    if (AMP) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
-        }
-    };
-    start_ray(ray);
+        for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
+    }
 
     while (true) {
         zmax = fmax(zmax, yd[2]);
         const double ds = step_c(a, yd[2]);
         s += ds;
         double incd[4], f1[3];
-        float inca[NA];
-        rk4_c<AMP>(tab, a, inv_blf, seg, ds, yd, ya, rc, incd, inca, f1);
-        if (AMP && a.aux && kb >= 1) {   // caustics: sign changes of D between rows 1..k-1 of the bounce
-            const float f0 = (float)f1[0], g1 = (float)f1[1], g2 = (float)f1[2];
-            const float D = f0 * (ya[1] * ya[6] - ya[5] * ya[2]) - ya[0] * (g1 * ya[6] - g2 * ya[5]) +
-                            ya[4] * (g1 * ya[2] - g2 * ya[1]);
-            if (kb >= 2 && D * D_prev < 0.0f) caustics++;
+        T inca[NA];
+        rk4_c<AMP>(tab, a, seg, ds, yd, ya, rc, incd, inca, f1);
+        if (AMP && (a.aux || ESCALATE) && kb >= 1) {
+            // caustics: sign changes of D between rows 1..k-1 of the bounce
+            const T f0 = (T)f1[0], g1 = (T)f1[1], g2 = (T)f1[2];
+            const T D = f0 * (ya[1] * ya[6] - ya[5] * ya[2]) - ya[0] * (g1 * ya[6] - g2 * ya[5]) +
+                        ya[4] * (g1 * ya[2] - g2 * ya[1]);
+            if (kb >= 2 && D * D_prev < T(0)) caustics++;
             D_prev = D;
+            if (ESCALATE) D_max = fmax(D_max, fabs(D));
         }
         kb++;
         {
             double dt, da;
-            seg_increment_c(tab, a, inv_blf, seg, yd, incd, rc, dt, da);
+            seg_increment_c(tab, a, seg, yd, incd, rc, dt, da);
             if (a.write_rays) { tt += pt; att += pa; pt = dt; pa = da; }   // main.infraga.3d.cpp:451-453
             else { pt += dt; pa += da; }                                    // :486-487
         }
@@ -412,7 +429,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             for (int i = 0; i < 4; i++) { dprev[i * blockDim.x] = incd[i]; yd[i] = nd[i]; }
             if (AMP) {
 #pragma unroll
-                for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
+                for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = (float)inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
             }
             continue;
         }
@@ -432,8 +449,14 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             last_rows_c<AMP>(yd, ya, yl, dprev, dprevf, r1, d1);
 #pragma unroll
             for (int i = 0; i < 12; i++) rk[i] = r1[i] + (i < 4 ? incd[i] : (AMP ? (double)inca[i - 4] : 0.0));
+            const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
+            double jac = 0.0, amp = 0.0;
+            if (AMP) {
+                int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+                amp = amp_db(a.knots, a, segd, rk, rcd, theta, phi, &jac);
+                if (ESCALATE && caustics == 0 && fabs(jac) < kFocusRatio * (double)D_max) return true;
+            }
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
-            const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
             const double incl = -asin(a.c_ratio * rk[3]) * 180.0 / kPi;
             double baz = 90.0 - atan2(-rc.ny, -rc.nx) * 180.0 / kPi;
             if (baz < -180.0) baz += 360.0;
@@ -449,14 +472,7 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             out[7] = zmax;
             out[8] = incl;
             out[9] = baz;
-            const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
-            double jac = 0.0;
-            if (AMP) {
-                int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-                out[10] = amp_db(a.knots, a, segd, rk, rcd, th_deg * kPi / 180.0, kPi / 2.0 - ph_deg * kPi / 180.0, &jac);
-            } else {
-                out[10] = 0.0;
-            }
+            out[10] = amp;
             out[11] = -2.0 * att;
             if (a.aux) {
                 double* ax = a.aux + ((size_t)ray * nb + na) * 4;
@@ -472,13 +488,43 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
             s = 0.0; kb = 0;
             continue;
         }
-        // ray finished: record and take the next one from the queue
+        // ray finished: its record
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
-        if (a.ray_status) a.ray_status[ray] = status;
-        ray = (int)atomicAdd(a.queue, 1u);
-        if (ray >= a.n_rays) break;
-        start_ray(ray);
+        if (a.ray_status) a.ray_status[ray] = status | (sizeof(T) == sizeof(double) ? kRayAuxFp64 : 0);
+        return false;
+    }
+}
+
+// Both traces of a ray are kept out of line: the FP64-auxiliary one so that
+// its wider state does not enlarge the register allocation of the FP32 loop,
+// the FP32 one so that the call to the other does not make the compiler
+// keep values of its loop in local memory.
+template <bool AMP>
+__device__ __noinline__ bool fan_ray_c32(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
+                                         float* dprevf, int ray) {
+    return fan_ray_c<AMP, float>(a, tab, dprev, dprevf, ray);
+}
+
+template <bool AMP>
+__device__ __noinline__ void fan_ray_c64(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
+                                         float* dprevf, int ray) {
+    fan_ray_c<AMP, double>(a, tab, dprev, dprevf, ray);
+}
+
+// Persistent fan kernel: each thread takes the next ray from the queue when
+// its ray ends, so lanes do not idle until the warp's longest ray.
+template <bool AMP, bool SMEM>
+__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
+    extern __shared__ double s_memc[];
+    const double* tab = stage_table_c<SMEM>(a, s_memc);
+    double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
+    double* dprev = s_lane + threadIdx.x;
+    float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
+    for (int ray = (int)atomicAdd(a.queue, 1u); ray < a.n_rays; ray = (int)atomicAdd(a.queue, 1u)) {
+        if (fan_ray_c32<AMP>(a, tab, dprev, dprevf, ray)) {
+            if constexpr (AMP) fan_ray_c64<AMP>(a, tab, dprev, dprevf, ray);
+        }
     }
 }
 
@@ -487,121 +533,142 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
 // trace3d_fp64_kernel in eig3d.cu, including the record mode's per-step
 // time/absorption sums and turning height from 0 over rows 1..k-1,
 // geoac.eigenray.3d.cpp:229-262).  The search's bracket and Newton updates
-// stay in FP64 on the host.
+// stay in FP64 on the host.  Sweep and Newton traces carry FP32 auxiliaries
+// (the Newton step only needs their direction); a record trace, whose
+// amplitude is the eigenray's output, carries FP64 auxiliaries.
+template <bool AMP, class T>
+__device__ __forceinline__ void trace_req_c(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
+                                            float* dprevf, const TraceReq& q, TraceRes* o_ptr, SegRes* seg_out,
+                                            int seg_stride, int r) {
+    constexpr int NA = AuxN<AMP>::n;
+    const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
+    double yd[4], incd[4] = {0.0, 0.0, 0.0, 0.0};
+    T ya[NA], yl[NA], inca[NA];
+    RayConstC<T> rc;
+    init_c<AMP>(a, q.theta, q.phi, q.x0, q.y0, yd, ya, yl, rc);
+#pragma unroll
+    for (int i = 0; i < NA; i++) inca[i] = T(0);
+    int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+    double tt = 0.0, att = 0.0, zmax = 0.0;
+    long long steps = 0;
+    bool esc = false;
+    for (int sg = 0; sg < q.n_seg; sg++) {
+        double s = 0.0, pt = 0.0, pa = 0.0;
+        int kb = 0;
+        bool capped = false;
+#pragma unroll
+        for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
+        if (AMP) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
+        }
+        while (true) {
+            if (record && kb >= 1) zmax = fmax(zmax, yd[2]);
+            const double ds = step_c(a, yd[2]);
+            s += ds;
+            double f1[3];
+            rk4_c<AMP>(tab, a, seg, ds, yd, ya, rc, incd, inca, f1);
+            kb++;
+            if (record) {
+                double dt, da;
+                seg_increment_c(tab, a, seg, yd, incd, rc, dt, da);
+                tt += pt; att += pa; pt = dt; pa = da;
+            }
+            double nd[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) nd[i] = yd[i] + incd[i];
+            const double rx = nd[0] - q.x0, ry = nd[1] - q.y0;
+            esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (nd[0] > a.x_max) ||
+                  (nd[0] < a.x_min) || (nd[1] > a.y_max) || (nd[1] < a.y_min) || (nd[2] > a.alt_max);
+            const bool gnd = !esc && (nd[2] < a.z0);
+            if (!esc && !gnd) {
+                if (kb >= a.length - 1) { capped = true; esc = true; }
+                else if (!isfinite(nd[2]) || !isfinite(nd[3])) esc = true;
+            }
+            if (!esc && !gnd) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) { dprev[i * blockDim.x] = incd[i]; yd[i] = nd[i]; }
+                if (AMP) {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = (float)inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
+                }
+                continue;
+            }
+            break;
+        }
+        steps += capped ? a.length : kb;
+        if (seg_out) {
+            SegRes& g = seg_out[(size_t)r * seg_stride + sg];
+            g.x = yd[0] + incd[0];
+            g.y = yd[1] + incd[1];
+            g.steps = steps;
+            g.escaped = esc ? 1 : 0;
+        }
+        if (sg == q.n_seg - 1 || (esc && stop)) break;
+        double r1[12], d1[12];
+        last_rows_c<AMP>(yd, ya, yl, dprev, dprevf, r1, d1);
+        reflect_c<AMP>(a, r1, d1, rc, yd, ya, yl);
+#pragma unroll
+        for (int i = 0; i < 4; i++) incd[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA; i++) inca[i] = T(0);
+    }
+    double rk[12];
+#pragma unroll
+    for (int i = 0; i < 4; i++) rk[i] = yd[i] + incd[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) rk[4 + i] = AMP ? (double)ya[i] + (double)yl[i] + (double)inca[i] : 0.0;
+    TraceRes& o = *o_ptr;
+#pragma unroll
+    for (int i = 0; i < 12; i++) o.y[i] = rk[i];
+    o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
+    o.steps = steps;
+    o.escaped = esc ? 1 : 0;
+    if (record) {
+        o.tt = tt; o.att = att; o.zmax = zmax;
+        const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
+        int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+        o.amp_db = AMP ? amp_db(a.knots, a, segd, rk, rcd, q.theta, q.phi, nullptr) : 0.0;
+        const double ze = fmin(fmax(rk[2], a.z_lo), a.z_hi);
+        segd = seg_walk(a.knots, a.n_knots, ze, segd);
+        const double* r0 = a.knots + segd * kStride;
+        const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
+        o.incl = -asin(c_k / a.c0 * rk[3]) * (180.0 / kPi);
+        double baz = 90.0 - atan2(-rcd.ny, -rcd.nx) * (180.0 / kPi);
+        while (baz > 180.0) baz -= 360.0;
+        while (baz < -180.0) baz += 360.0;
+        o.baz = baz;
+    }
+}
+
+template <bool AMP>
+__device__ __noinline__ void trace_req_c64(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
+                                           float* dprevf, const TraceReq& q, TraceRes* o_ptr, SegRes* seg_out,
+                                           int seg_stride, int r) {
+    trace_req_c<AMP, double>(a, tab, dprev, dprevf, q, o_ptr, seg_out, seg_stride, r);
+}
+
 template <bool AMP, bool SMEM>
 __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB)
     trace3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a, const TraceReq* __restrict__ reqs,
                          TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
                          SegRes* __restrict__ seg_out, int seg_stride) {
-    constexpr int NA = AuxN<AMP>::n;
     extern __shared__ double s_memc[];
     const double* tab = stage_table_c<SMEM>(a, s_memc);
     double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
     double* dprev = s_lane + threadIdx.x;
     float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
-    const float inv_blf = (float)a.inv_bl;
     // persistent: each thread takes the next request when its trace ends, so
     // lanes whose trace finished early do not idle until the warp's longest one
     for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
         const TraceReq q = reqs[r];
-        const bool record = (q.flags & kRecord) != 0, stop = (q.flags & kStopOnEscape) != 0;
-        double yd[4], incd[4] = {0.0, 0.0, 0.0, 0.0};
-        float ya[NA], yl[NA], inca[NA];
-        RayConstC rc;
-        init_c<AMP>(a, q.theta, q.phi, q.x0, q.y0, yd, ya, yl, rc);
-#pragma unroll
-        for (int i = 0; i < NA; i++) inca[i] = 0.0f;
-        int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-        double tt = 0.0, att = 0.0, zmax = 0.0;
-        long long steps = 0;
-        bool esc = false;
-        for (int sg = 0; sg < q.n_seg; sg++) {
-            double s = 0.0, pt = 0.0, pa = 0.0;
-            int kb = 0;
-            bool capped = false;
-#pragma unroll
-            for (int i = 0; i < 4; i++) dprev[i * blockDim.x] = 0.0;
-            if (AMP) {
-#pragma unroll
-                for (int i = 0; i < 8; i++) dprevf[i * blockDim.x] = 0.0f;
+        if constexpr (AMP) {
+            if (q.flags & kRecord) {
+                trace_req_c64<AMP>(a, tab, dprev, dprevf, q, out + r, seg_out, seg_stride, r);
+                continue;
             }
-            while (true) {
-                if (record && kb >= 1) zmax = fmax(zmax, yd[2]);
-                const double ds = step_c(a, yd[2]);
-                s += ds;
-                double f1[3];
-                rk4_c<AMP>(tab, a, inv_blf, seg, ds, yd, ya, rc, incd, inca, f1);
-                kb++;
-                if (record) {
-                    double dt, da;
-                    seg_increment_c(tab, a, inv_blf, seg, yd, incd, rc, dt, da);
-                    tt += pt; att += pa; pt = dt; pa = da;
-                }
-                double nd[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) nd[i] = yd[i] + incd[i];
-                const double rx = nd[0] - q.x0, ry = nd[1] - q.y0;
-                esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (nd[0] > a.x_max) ||
-                      (nd[0] < a.x_min) || (nd[1] > a.y_max) || (nd[1] < a.y_min) || (nd[2] > a.alt_max);
-                const bool gnd = !esc && (nd[2] < a.z0);
-                if (!esc && !gnd) {
-                    if (kb >= a.length - 1) { capped = true; esc = true; }
-                    else if (!isfinite(nd[2]) || !isfinite(nd[3])) esc = true;
-                }
-                if (!esc && !gnd) {
-#pragma unroll
-                    for (int i = 0; i < 4; i++) { dprev[i * blockDim.x] = incd[i]; yd[i] = nd[i]; }
-                    if (AMP) {
-#pragma unroll
-                        for (int i = 0; i < 8; i++) { dprevf[i * blockDim.x] = inca[i]; acc_pair(ya[i], yl[i], inca[i]); }
-                    }
-                    continue;
-                }
-                break;
-            }
-            steps += capped ? a.length : kb;
-            if (seg_out) {
-                SegRes& g = seg_out[(size_t)r * seg_stride + sg];
-                g.x = yd[0] + incd[0];
-                g.y = yd[1] + incd[1];
-                g.steps = steps;
-                g.escaped = esc ? 1 : 0;
-            }
-            if (sg == q.n_seg - 1 || (esc && stop)) break;
-            double r1[12], d1[12];
-            last_rows_c<AMP>(yd, ya, yl, dprev, dprevf, r1, d1);
-            reflect_c<AMP>(a, r1, d1, rc, yd, ya, yl);
-#pragma unroll
-            for (int i = 0; i < 4; i++) incd[i] = 0.0;
-#pragma unroll
-            for (int i = 0; i < NA; i++) inca[i] = 0.0f;
         }
-        double rk[12];
-#pragma unroll
-        for (int i = 0; i < 4; i++) rk[i] = yd[i] + incd[i];
-#pragma unroll
-        for (int i = 0; i < 8; i++) rk[4 + i] = AMP ? (double)ya[i] + (double)yl[i] + (double)inca[i] : 0.0;
-        TraceRes& o = out[r];
-#pragma unroll
-        for (int i = 0; i < 12; i++) o.y[i] = rk[i];
-        o.rc[0] = rc.nx; o.rc[1] = rc.ny; o.rc[2] = rc.mtx; o.rc[3] = rc.mty; o.rc[4] = rc.mpx; o.rc[5] = rc.mpy;
-        o.steps = steps;
-        o.escaped = esc ? 1 : 0;
-        if (record) {
-            o.tt = tt; o.att = att; o.zmax = zmax;
-            const RayConst rcd{rc.nx, rc.ny, (double)rc.mtx, (double)rc.mty, (double)rc.mpx, (double)rc.mpy};
-            int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
-            o.amp_db = AMP ? amp_db(a.knots, a, segd, rk, rcd, q.theta, q.phi, nullptr) : 0.0;
-            const double ze = fmin(fmax(rk[2], a.z_lo), a.z_hi);
-            segd = seg_walk(a.knots, a.n_knots, ze, segd);
-            const double* r0 = a.knots + segd * kStride;
-            const double c_k = cubic_f(r0, cubic_at(r0, ze), 2);
-            o.incl = -asin(c_k / a.c0 * rk[3]) * (180.0 / kPi);
-            double baz = 90.0 - atan2(-rcd.ny, -rcd.nx) * (180.0 / kPi);
-            while (baz > 180.0) baz -= 360.0;
-            while (baz < -180.0) baz += 360.0;
-            o.baz = baz;
-        }
+        trace_req_c<AMP, float>(a, tab, dprev, dprevf, q, out + r, seg_out, seg_stride, r);
     }
 }
 

@@ -213,6 +213,11 @@ def noncaustic_report(got, ref, caustics, calc_amp=True):
            "time_s_p50": pct(dt, 50), "time_s_p99": pct(dt, 99),
            "amp_db_p50": pct(da, 50), "amp_db_p99": pct(da, 99)}
     rep["ok"] = rep["viol_range"] == 0 and rep["viol_time"] == 0 and rep["viol_amp"] == 0
+    # the worst non-caustic rows (incl, az, bounce, range err, time err, amp err, reference amp)
+    for key, err in (("worst_range", rng), ("worst_amp", da)):
+        o = np.argsort(-np.where(nc, err, -1.0))[:4]
+        rep[key] = [(float(ref[i, 0]), float(ref[i, 1]), int(ref[i, 2]), float(rng[i]), float(dt[i]), float(da[i]),
+                     float(ref[i, 10])) for i in o if nc[i]]
     return rep
 
 
