@@ -835,10 +835,15 @@ bool parse_eig(int argc, char** argv, Variant v, bool direct, iga_eig_params& ep
 bool read_list(const char* path, int cols, std::vector<double>& out) {
     std::ifstream f(path);
     if (!f.is_open()) return false;
+    // file_length (util/fileIO.cpp:18-35): read until eof, count the lines
+    // not starting with '#', minus one -- the empty read after a final newline
+    // (a list without one loses its last entry there too)
     int n = 0;
     std::string line;
-    while (std::getline(f, line))
+    while (!f.eof()) {
+        std::getline(f, line);
         if (line.find('#') != 0) n++;
+    }
     n -= 1;
     if (n < 1) return false;
     f.clear();

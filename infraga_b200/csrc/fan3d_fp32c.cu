@@ -25,6 +25,8 @@
 // intercept, travel time and turning height follow the FP64 kernel to
 // rounding; the auxiliaries only set the amplitude, which tolerates FP32
 // arithmetic once their state is summed with compensation.
+#include <type_traits>
+
 #include "eig3d.cuh"
 #include "fan3d.cuh"
 #include "fan3d_common.cuh"
@@ -496,24 +498,11 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
     }
 }
 
-// Both traces of a ray are kept out of line: the FP64-auxiliary one so that
-// its wider state does not enlarge the register allocation of the FP32 loop,
-// the FP32 one so that the call to the other does not make the compiler
-// keep values of its loop in local memory.
-template <bool AMP>
-__device__ __noinline__ bool fan_ray_c32(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
-                                         float* dprevf, int ray) {
-    return fan_ray_c<AMP, float>(a, tab, dprev, dprevf, ray);
-}
-
-template <bool AMP>
-__device__ __noinline__ void fan_ray_c64(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
-                                         float* dprevf, int ray) {
-    fan_ray_c<AMP, double>(a, tab, dprev, dprevf, ray);
-}
-
 // Persistent fan kernel: each thread takes the next ray from the queue when
-// its ray ends, so lanes do not idle until the warp's longest ray.
+// its ray ends, so lanes do not idle until the warp's longest ray.  A ray
+// that needs FP64 auxiliaries is marked (n_arr = -1) and left to
+// fan3d_fp32c_retrace_kernel: tracing it here would hold the other 31 lanes
+// of its warp for the length of a ray.
 template <bool AMP, bool SMEM>
 __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a) {
     extern __shared__ double s_memc[];
@@ -521,11 +510,25 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
     double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
     double* dprev = s_lane + threadIdx.x;
     float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
-    for (int ray = (int)atomicAdd(a.queue, 1u); ray < a.n_rays; ray = (int)atomicAdd(a.queue, 1u)) {
-        if (fan_ray_c32<AMP>(a, tab, dprev, dprevf, ray)) {
-            if constexpr (AMP) fan_ray_c64<AMP>(a, tab, dprev, dprevf, ray);
-        }
-    }
+    for (int ray = (int)atomicAdd(a.queue, 1u); ray < a.n_rays; ray = (int)atomicAdd(a.queue, 1u))
+        if (fan_ray_c<AMP, float>(a, tab, dprev, dprevf, ray)) a.n_arr[ray] = -1;
+}
+
+// The marked rays of a fan, traced from launch with FP64 auxiliaries (about
+// 1% of a 10-bounce fan): one CTA per SM scans the fan's rays through a
+// second queue counter, so the few marked rays spread over the SMs.
+constexpr int kThreadsR = 128;
+
+template <bool SMEM>
+__global__ void __launch_bounds__(kThreadsR, 1)
+    fan3d_fp32c_retrace_kernel(const __grid_constant__ Fan3DArgs a, unsigned int* __restrict__ queue) {
+    extern __shared__ double s_memc[];
+    const double* tab = stage_table_c<SMEM>(a, s_memc);
+    double* s_lane = s_memc + (SMEM ? (size_t)a.n_knots * kStrideC : 0);
+    double* dprev = s_lane + threadIdx.x;
+    float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
+    for (int ray = (int)atomicAdd(queue, 1u); ray < a.n_rays; ray = (int)atomicAdd(queue, 1u))
+        if (a.n_arr[ray] < 0) fan_ray_c<true, double>(a, tab, dprev, dprevf, ray);
 }
 
 // Eigenray-search traces in FP32-compensated form: one request per thread,
@@ -533,9 +536,11 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB) fan3d_fp32c_kernel(c
 // trace3d_fp64_kernel in eig3d.cu, including the record mode's per-step
 // time/absorption sums and turning height from 0 over rows 1..k-1,
 // geoac.eigenray.3d.cpp:229-262).  The search's bracket and Newton updates
-// stay in FP64 on the host.  Sweep and Newton traces carry FP32 auxiliaries
-// (the Newton step only needs their direction); a record trace, whose
-// amplitude is the eigenray's output, carries FP64 auxiliaries.
+// stay in FP64 on the host.  Sweep traces carry no auxiliaries; Newton and
+// record traces carry them in FP64, so the search takes the FP64 search's
+// iterates (the Newton step reads the launch-angle derivatives of the
+// landing point, which an FP32 error moves near a fold of the fan) and the
+// eigenray's amplitude keeps FP64 conditioning.
 template <bool AMP, class T>
 __device__ __forceinline__ void trace_req_c(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
                                             float* dprevf, const TraceReq& q, TraceRes* o_ptr, SegRes* seg_out,
@@ -641,15 +646,8 @@ __device__ __forceinline__ void trace_req_c(const Fan3DArgs& a, const double* __
     }
 }
 
-template <bool AMP>
-__device__ __noinline__ void trace_req_c64(const Fan3DArgs& a, const double* __restrict__ tab, double* dprev,
-                                           float* dprevf, const TraceReq& q, TraceRes* o_ptr, SegRes* seg_out,
-                                           int seg_stride, int r) {
-    trace_req_c<AMP, double>(a, tab, dprev, dprevf, q, o_ptr, seg_out, seg_stride, r);
-}
-
 template <bool AMP, bool SMEM>
-__global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB)
+__global__ void __launch_bounds__(kThreadsC, AMP ? 1 : IGA_FANC_MINB)
     trace3d_fp32c_kernel(const __grid_constant__ Fan3DArgs a, const TraceReq* __restrict__ reqs,
                          TraceRes* __restrict__ out, int n, unsigned int* __restrict__ queue,
                          SegRes* __restrict__ seg_out, int seg_stride) {
@@ -660,16 +658,9 @@ __global__ void __launch_bounds__(kThreadsC, IGA_FANC_MINB)
     float* dprevf = reinterpret_cast<float*>(s_lane + 4 * blockDim.x) + threadIdx.x;
     // persistent: each thread takes the next request when its trace ends, so
     // lanes whose trace finished early do not idle until the warp's longest one
-    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u)) {
-        const TraceReq q = reqs[r];
-        if constexpr (AMP) {
-            if (q.flags & kRecord) {
-                trace_req_c64<AMP>(a, tab, dprev, dprevf, q, out + r, seg_out, seg_stride, r);
-                continue;
-            }
-        }
-        trace_req_c<AMP, float>(a, tab, dprev, dprevf, q, out + r, seg_out, seg_stride, r);
-    }
+    using T = typename std::conditional<AMP, double, float>::type;
+    for (int r = (int)atomicAdd(queue, 1u); r < n; r = (int)atomicAdd(queue, 1u))
+        trace_req_c<AMP, T>(a, tab, dprev, dprevf, reqs[r], out + r, seg_out, seg_stride, r);
 }
 
 template <bool AMP, bool SMEM>
@@ -707,6 +698,15 @@ cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
     kern<<<(unsigned)grid, threads, smem, stream>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess || !AMP) return e;
+    // the rays marked for FP64 auxiliaries, after the fan on the same stream;
+    // its queue is the workspace's second counter (cleared with the first)
+    auto rk = fan3d_fp32c_retrace_kernel<SMEM>;
+    const size_t smem_r = smem_c(a, kThreadsR, SMEM);
+    if ((e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r)) != cudaSuccess)
+        return e;
+    const long long grid_r = std::min<long long>(n_sm, ((long long)a.n_rays + kThreadsR - 1) / kThreadsR);
+    rk<<<(unsigned)grid_r, kThreadsR, smem_r, stream>>>(a, a.queue + 1);
     return cudaGetLastError();
 }
 

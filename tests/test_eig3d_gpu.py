@@ -85,12 +85,12 @@ def test_eigen_pair_groups_equal_one_stream(dev):
     assert many["total_steps"] == one["total_steps"]
 
 
-# FP32-compensated ray integration with FP64 bracket/Newton updates: the same
-# eigenrays within the search tolerance.  A trace's FP32 rounding moves its
-# landing point by metres, so the Newton iteration stops at a slightly
-# different launch angle (still within 0.1 km of the receiver); near
-# caustics the amplitude differs more.  Bounds for the matched rows:
-FP32C_EIG_TOL = {"incl": 0.05, "az": 0.05, "time": 0.5, "amp_db": 1.0}
+# FP32C search: sweep traces in the FP32-compensated kernel (FP64 ray
+# equations), Newton and record traces with FP64 auxiliaries, bracket and
+# Newton updates in FP64 on the host.  The sweep's landing points follow the
+# FP64 kernel to ~1e-9 km, so the search takes the FP64 search's iterates and
+# its eigenrays; bounds for the matched rows:
+FP32C_EIG_TOL = {"incl": 0.05, "az": 0.05, "time": 0.5, "amp_db": 0.1}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
