@@ -638,13 +638,15 @@ def cpu_baseline_sphr(files):
                       f"{steps} ray-steps in {wall:.1f} s"}
 
 
-def sphr_measure(steps, warmup, shapes=((1, None), (0, None), (1, 0))):
+def sphr_measure(steps, warmup, shapes=((1, None, "fp64"), (0, None, "fp64"), (1, 0, "fp64"), (1, None, "fp32c"),
+                                       (1, 0, "fp32c"))):
     """Config 2: spherical range-dependent fan over a 21x21 node grid with
-    0.05-deg fractal terrain (workloads.py), FP64.  The autotuner
-    (iga_fan_tune) picks the CTA size first; each (calc_amp, block) in
-    `shapes` (block None = the tuned one, 0 = the default 128) is timed over
-    `steps` launches with CUDA events after `warmup`, L2 flushed between.
-    Returns (legs, tuned block, seconds per tuning candidate, rays, files)."""
+    0.05-deg fractal terrain (workloads.py), FP64 and FP32-compensated.  The
+    autotuner (iga_fan_tune) picks the CTA size first (on the FP64 kernel);
+    each (calc_amp, block, precision) in `shapes` (block None = the tuned
+    one, 0 = the kernel's default) is timed over `steps` launches with CUDA
+    events after `warmup`, L2 flushed between.  Returns (legs, tuned block,
+    seconds per tuning candidate, rays, files)."""
     import torch
     import infraga_b200 as ig
     from infraga_b200 import workloads as wl
@@ -666,10 +668,10 @@ def sphr_measure(steps, warmup, shapes=((1, None), (0, None), (1, 0))):
     tp = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"], write_rays=0)
     best, tune_s = ig.fan_tune(atmo, tp, th, ph)
     legs = {}
-    for amp, block in shapes:
+    for amp, block, prec in shapes:
         block = best if block is None else block
         params = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"],
-                                     write_rays=0, calc_amp=amp)
+                                     write_rays=0, calc_amp=amp, precision=ig.FP32C if prec == "fp32c" else ig.FP64)
         params.block = block
         times, n_steps = [], 0
         for i in range(warmup + steps):
@@ -684,8 +686,10 @@ def sphr_measure(steps, warmup, shapes=((1, None), (0, None), (1, 0))):
                 times.append(e0.elapsed_time(e1) * 1e-3)
                 n_steps = int(st.sum().item())
         t = sum(times) / len(times)
-        name = ("amp" if amp else "noamp") + ("" if block == best else f"_block{block or 128}")
-        legs[name] = {"ray_steps": n_steps, "s_per_fan": t, "value": n_steps / t, "block": block or 128}
+        name = ("fp32c_" if prec == "fp32c" else "") + ("amp" if amp else "noamp") + \
+            ("" if block == best else f"_block{block or 128}")
+        legs[name] = {"ray_steps": n_steps, "s_per_fan": t, "value": n_steps / t, "block": block or 128,
+                      "precision": prec}
     atmo.close()
     return legs, best, tune_s, n, files
 
@@ -819,11 +823,14 @@ def extra_configs(gpu_id):
     out = {}
     sampler = ClockSampler(gpu_id)
     sampler.start()
-    legs, best, tune_s, n, _ = sphr_measure(2, 1, shapes=((1, None),))
+    legs, best, tune_s, n, _ = sphr_measure(2, 1, shapes=((1, None, "fp64"), (1, None, "fp32c")))
     out["config2"] = {"metric": METRIC, "unit": UNIT, "value": legs["amp"]["value"], "dtype": "f64",
+                      "fp32c_value": legs["fp32c_amp"]["value"],
+                      "fp32c_over_fp64": legs["fp32c_amp"]["value"] / legs["amp"]["value"],
                       "workload": f"sph-rngdep-fan-{n}rays-21x21grid-401x401terrain-20bnc-3000km",
                       "timing": "CUDA events, mean of 2 launches after 1 warm-up, L2 flushed",
-                      "block": best, "s_per_fan": legs["amp"]["s_per_fan"], "clocks": sampler.stop()}
+                      "block": best, "s_per_fan": legs["amp"]["s_per_fan"],
+                      "fp32c_s_per_fan": legs["fp32c_amp"]["s_per_fan"], "clocks": sampler.stop()}
     sampler = ClockSampler(gpu_id)
     sampler.start()
     legs3, err, _, _ = eigen_measure([1])

@@ -99,6 +99,16 @@ int upload_rngdep(iga_atmo_s* h) {
     buf.insert(buf.end(), g.z.begin(), g.z.end());
     IGA_CUDA(cudaMalloc(&h->d_hyb, buf.size() * sizeof(double)), "cudaMalloc(hybrid tables)");
     IGA_CUDA(cudaMemcpy(h->d_hyb, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(hybrid)");
+    {   // FP32 copies of the second-derivative blocks (c, u, v) for the FP32C kernel
+        const size_t n_rec = (size_t)g.nx * g.ny * g.nz;
+        std::vector<float> x32(n_rec * iga::kHybX32, 0.0f);
+        for (size_t r = 0; r < n_rec; r++)
+            for (int k = 0; k < 3 * iga::kHybX; k++)
+                x32[r * iga::kHybX32 + k] = (float)g.table[r * iga::kHybRec + iga::kHybXOff + k];
+        IGA_CUDA(cudaMalloc(&h->d_hyb_x32, x32.size() * sizeof(float)), "cudaMalloc(hybrid FP32 blocks)");
+        IGA_CUDA(cudaMemcpy(h->d_hyb_x32, x32.data(), x32.size() * sizeof(float), cudaMemcpyHostToDevice),
+                 "cudaMemcpy(hybrid FP32 blocks)");
+    }
     int rc = upload_terrain(h);
     if (rc) return rc;
     IGA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -160,10 +170,6 @@ int validate(const iga_fan_params* p, int n_rays) {
     if (p->geometry != IGA_GEOM_3D && p->geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
     if (p->precision != IGA_FP64 && p->precision != IGA_FP32C) return IGA_E_INVALID;
     if (p->geometry == IGA_GEOM_SPH) {
-        if (p->precision != IGA_FP64) {
-            g_cuda_err = "spherical geometry: FP64 only";
-            return IGA_E_UNSUPPORTED;
-        }
         if (!(std::fabs(p->src[0]) < 90.0) || !std::isfinite(p->src[1])) return IGA_E_INVALID;
         if (!(p->time_max > 0.0)) return IGA_E_INVALID;
     }
@@ -509,8 +515,13 @@ namespace {
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st, int grid_cap = 0, const PathSpec* ps = nullptr) {
-    if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) || p->precision != IGA_FP64)) {
-        g_cuda_err = "range-dependent atmosphere: FP64, with the geometry it was loaded for";
+    if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) ||
+                         (p->precision != IGA_FP64 && !(h->kind == 1 && p->precision == IGA_FP32C)))) {
+        g_cuda_err = "range-dependent atmosphere: the geometry it was loaded for; FP32C on the spherical grid only";
+        return IGA_E_UNSUPPORTED;
+    }
+    if (p->geometry == IGA_GEOM_SPH && p->precision == IGA_FP32C && h->kind != 1) {
+        g_cuda_err = "spherical geometry: FP32C on range-dependent node grids only";
         return IGA_E_UNSUPPORTED;
     }
     NvtxRange nv(ps ? "iga_fan_paths launch" : "iga_fan launch");
@@ -530,16 +541,19 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         a.path_rows = ps->rows; a.path_off = ps->off; a.path_n = ps->n; a.path_mode = ps->mode;
         a.caus_rows = ps->caus; a.caus_count = ps->caus_count; a.caus_cap = ps->caus_cap;
     }
-    if (p->precision == IGA_FP32C) {
+    if (p->precision == IGA_FP32C && h->kind == 0) {
         iga_atmo_s::AlphaTab t;
         rc = ensure_alpha(h, p->freq, t);
         if (rc) return rc;
         a.knots_c = h->d_knots_c;
         a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
     }
+    if (p->precision == IGA_FP32C && h->kind == 1) a.hyb_x32 = h->d_hyb_x32;
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    if (h->kind == 1)
+    if (h->kind == 1 && p->precision == IGA_FP32C && a.hyb_tab != nullptr)
+        IGA_CUDA(iga::launch_fansphr_fp32c(a, p->calc_amp != 0, st, nullptr), "fansphr fp32c kernel launch");
+    else if (h->kind == 1)
         IGA_CUDA(iga::launch_fansphr_fp64(a, p->calc_amp != 0, st, nullptr), "fansphr kernel launch");
     else if (h->kind == 2)
         IGA_CUDA(iga::launch_fan3dr_fp64(a, p->calc_amp != 0, st, nullptr), "fan3dr kernel launch");
@@ -782,6 +796,7 @@ int iga_atmo_destroy(iga_atmo_t h) {
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->d_knots_c) cudaFree(h->d_knots_c);
     if (h->d_hyb) cudaFree(h->d_hyb);
+    if (h->d_hyb_x32) cudaFree(h->d_hyb_x32);
     if (h->d_topo) cudaFree(h->d_topo);
     for (auto& kv : h->alpha) cudaFree(kv.second.d);
     delete h;

@@ -88,19 +88,23 @@ struct Fan3DArgs {
     const float* alpha_tab;  // Sutherland-Bass alpha(z) [dB/km, tweak_abs = 1] on a uniform grid
     int alpha_n;
     double alpha_z0, alpha_inv_h;
+    const float* hyb_x32;    // [nx][ny][nz][kHybX32] FP32 copies of the hybrid records'
+                             // second-derivative blocks (c, u, v: 9 values each)
 };
 
+constexpr int kHybX32 = 32;   // floats per record of hyb_x32 (3 x 9 used)
+
 constexpr int kStrideC = 14;  // doubles per segment row of the FP32-compensated path's power-basis table
+
+// Flag OR'ed into a ray's status (IGA_RAY_AUX_FP64): an FP32C ray traced
+// again with FP64 auxiliaries after a focusing arrival.
+constexpr int kRayAuxFp64 = 0x100;
 
 // Sampled output rows.  Path rows: horizontal position (x, y [km] or lat, lon
 // [deg]), altitude [km] (terrain mode: the ground height there), amplitude
 // [dB] (0 without calc_amp or in terrain mode), absorption [dB] (-2 x the
 // running sum), travel time [s], bounce.  Caustic rows: position (3), time,
 // bounce, ray, and the ray's step index of the row (for ordering).
-// Flag OR'ed into a ray's status (IGA_RAY_AUX_FP64): an FP32C ray traced
-// again with FP64 auxiliaries after a focusing arrival.
-constexpr int kRayAuxFp64 = 0x100;
-
 // Back-projection rows (kPathProj, 3D stratified flat-ground kernel only):
 // x, y, z [km], time [s], X_incl (3) [km/deg], T_incl [s/deg], X_az (3),
 // T_az, group velocity (3) [km/s].
@@ -138,6 +142,11 @@ cudaError_t launch_fan3dr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t s
 
 // Spherical range-dependent fan with optional terrain, FP64 (fansphr_fp64.cu).
 cudaError_t launch_fansphr_fp64(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
+
+// Spherical range-dependent fan with optional terrain, FP32-compensated
+// (fansphr_fp32c.cu): the fan kernel and the FP64-auxiliary re-trace of its
+// focusing rays, on `stream`.
+cudaError_t launch_fansphr_fp32c(const Fan3DArgs& a, bool calc_amp, cudaStream_t stream, int* grid_used);
 
 constexpr double kEarthRadiusKm = 6370.0;   // globe::r0 (util/globe.cpp:10)
 

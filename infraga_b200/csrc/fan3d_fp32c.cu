@@ -35,8 +35,11 @@ namespace iga {
 
 namespace {
 
+// 256 threads x 2 CTAs per SM caps the fan kernel at 128 registers: 16
+// resident warps per SM (168 registers and 12 warps at 192 x 2 ran 9% slower,
+// its few spills notwithstanding)
 #ifndef IGA_FANC_THREADS
-#define IGA_FANC_THREADS 192
+#define IGA_FANC_THREADS 256
 #endif
 #ifndef IGA_FANC_MINB
 #define IGA_FANC_MINB 2
@@ -368,14 +371,13 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
     constexpr int NA = AuxN<AMP>::n;
     constexpr bool ESCALATE = AMP && sizeof(T) == sizeof(float);
     const int nb = a.bounces + 1;
-    const double th_deg = a.theta_deg[ray], ph_deg = a.phi_deg[ray];
-    const double theta = th_deg * kPi / 180.0;
-    const double phi = kPi / 2.0 - ph_deg * kPi / 180.0;
+    const double theta0 = a.theta_deg[ray] * kPi / 180.0;
+    const double phi0 = kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0;
 
     double yd[4];
     T ya[NA], yl[NA];
     RayConstC<T> rc;
-    init_c<AMP>(a, theta, phi, a.src_x, a.src_y, yd, ya, yl, rc);
+    init_c<AMP>(a, theta0, phi0, a.src_x, a.src_y, yd, ya, yl, rc);
     int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
     int bnc = 0, kb = 0, na = 0, caustics = 0;
     T D_prev = T(0), D_max = T(0);
@@ -455,6 +457,8 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
             double jac = 0.0, amp = 0.0;
             if (AMP) {
                 int segd = seg_guess(fmin(fmax(rk[2], a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
+                const double theta = a.theta_deg[ray] * kPi / 180.0;
+                const double phi = kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0;
                 amp = amp_db(a.knots, a, segd, rk, rcd, theta, phi, &jac);
                 if (ESCALATE && caustics == 0 && fabs(jac) < kFocusRatio * (double)D_max) return true;
             }
@@ -464,8 +468,8 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
             if (baz < -180.0) baz += 360.0;
             else if (baz > 180.0) baz -= 360.0;
             const double ex = rk[0] - a.src_x, ey = rk[1] - a.src_y;
-            out[0] = th_deg;
-            out[1] = ph_deg;
+            out[0] = a.theta_deg[ray];
+            out[1] = a.phi_deg[ray];
             out[2] = (double)bnc;
             out[3] = rk[0];
             out[4] = rk[1];

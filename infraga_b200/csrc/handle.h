@@ -27,6 +27,7 @@ struct iga_atmo_s {
     iga::Terrain topo;
     bool has_topo = false;
     double* d_hyb = nullptr;  // hybrid node records, then node lat, lon, z
+    float* d_hyb_x32 = nullptr;   // FP32 second-derivative blocks of the hybrid records (FP32C)
     double* d_topo = nullptr; // terrain node records, then node lat, lon
     double* d_knots = nullptr;
     // stream of the host-buffer entry points: one per handle, so calls on

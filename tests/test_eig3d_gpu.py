@@ -1,6 +1,8 @@
 """GPU eigenray search (iga_eig_run) against the reference's own
 est_eigenray/find_eigenray output (tests/golden/3d_eig_*, written by the
 reference with 8 significant digits)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -87,10 +89,16 @@ def test_eigen_pair_groups_equal_one_stream(dev):
 
 # FP32C search: sweep traces in the FP32-compensated kernel (FP64 ray
 # equations), Newton and record traces with FP64 auxiliaries, bracket and
-# Newton updates in FP64 on the host.  The sweep's landing points follow the
-# FP64 kernel to ~1e-9 km, so the search takes the FP64 search's iterates and
-# its eigenrays; bounds for the matched rows:
-FP32C_EIG_TOL = {"incl": 0.05, "az": 0.05, "time": 0.5, "amp_db": 0.1}
+# Newton updates in FP64 on the host.  Its eigenrays are the reference's
+# within the search tolerance: the Newton iteration stops anywhere within
+# 0.1 km of the receiver, so rounding differences of 1e-9 km can end it at a
+# slightly different launch angle, and where the amplitude changes fast with
+# the launch angle (the middle branch of a triplication, between two
+# caustics) the reference's and the FP32C eigenray then differ by up to a few
+# dB while both are correct to the search tolerance.  The amplitude is
+# therefore checked against an FP64 fan ray launched at the FP32C eigenray's
+# own angles (the arithmetic error), and against the reference only in bulk.
+FP32C_EIG_TOL = {"incl": 0.05, "az": 0.05, "time": 0.5, "amp_db_same_angle": 0.1, "amp_db_ref": 3.0}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -111,5 +119,16 @@ def test_fp32c_eigenrays_match_reference(dev, name):
         m = cand[j]
         assert abs(m[0] - row[0]) < FP32C_EIG_TOL["incl"] and abs(m[1] - row[1]) < FP32C_EIG_TOL["az"], (m[:3], row[:3])
         assert abs(m[5] - row[5]) < FP32C_EIG_TOL["time"]
-        assert abs(m[10] - row[10]) < FP32C_EIG_TOL["amp_db"]
+        assert abs(m[10] - row[10]) < FP32C_EIG_TOL["amp_db_ref"]
         assert np.hypot(m[3] - rcvr[0], m[4] - rcvr[1]) < params.tolerance + 1e-3
+    # every FP32C eigenray against an FP64 ray at its own launch angles
+    for m in got:
+        pf = ig.FanParams.from_buffer_copy(params.fan)
+        pf.precision, pf.bounces, pf.write_rays, pf.calc_amp = ig.FP64, int(m[2]), 0, 1
+        pf.src = (ctypes.c_double * 3)(*src)
+        f = ig.fan_run(atmo, pf, np.array([m[0]]), np.array([m[1]]))
+        a = f["arrivals"][f["arrivals"][:, 2] == m[2]]
+        assert a.shape[0] == 1, m[:3]
+        assert np.hypot(a[0, 3] - m[3], a[0, 4] - m[4]) < 1e-4, (a[0, 3:5], m[3:5])
+        if np.isfinite(a[0, 10]):
+            assert abs(a[0, 10] - m[10]) < FP32C_EIG_TOL["amp_db_same_angle"], (a[0, 10], m[10], m[:3])

@@ -79,7 +79,7 @@ def test_sphr_region_and_defaults(dev):
 
 def test_sphr_rejects_unsupported(dev):
     a = atmo(False)
-    for over in (dict(geometry=ig.GEOM_3D), dict(geometry=ig.GEOM_SPH, precision=ig.FP32C)):
+    for over in (dict(geometry=ig.GEOM_3D),):
         p = a.default_params(**over)
         with pytest.raises(ig.IgaError):
             ig.fan_run(a, p, np.array([10.0]), np.array([90.0]))
