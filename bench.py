@@ -43,7 +43,8 @@ FAN = dict(incl=(0.5, 60.01, 0.1), az=(0.0, 357.0, 3.0), bounces=10, rng_max=200
 # holds the counts, the weights and the sample they came from.
 with open(os.path.join(ROOT, "roofline.json")) as _f:
     ROOFLINE = json.load(_f)
-FLOPS_PER_STEP = {"fp64": ROOFLINE["variants"]["fp64_amp"], "fp32c": ROOFLINE["variants"]["fp32c_amp"]}
+FLOPS_PER_STEP = {"fp64": ROOFLINE["variants"]["fp64_amp"], "fp32c": ROOFLINE["variants"]["fp32c_amp"],
+                  "fp32c_flagged": ROOFLINE["variants"]["fp32c_amp"]}
 # The FP32C kernel runs two classes of work on two pipes: the ray equations
 # (the no-amplitude count) in FP64 and the Jacobian auxiliaries (the rest) in
 # FP32, issued from the same schedulers, so its peak is the serial mix of the
@@ -58,8 +59,14 @@ def mixed_peak(p64, p32):
     return FLOPS_PER_STEP["fp32c"] / (FP32C_SPLIT["fp64"] / p64 + FP32C_SPLIT["fp32"] / p32)
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per fan launch of the dominant kernel, from the ncu
-# captures summarised in profiles/ (None until captured).
-TRAFFIC = {"fp64": None, "fp32c": None}
+# captures of the full 71,520-ray fan cut to one bounce (bench.py --profile-case
+# fan3d_fp32c / fan3d_fp64, summarised in profiles/): the tables, launch angles
+# and code are read once per launch and the state stays in registers, so the
+# bytes do not grow with the steps of the 10-bounce launch, whose extra
+# arrival rows (<= 76 MB) are written into the 126 MB L2.
+TRAFFIC = {"fp64": 1366016 + 540672, "fp32c": 2059264 + 278784}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, 71,520-ray fan at 1 bounce "
+                  "(profiles/fan3d_*_ncu_full_71520rays_1bnc.md)")
 
 
 def config_dict(extra=None):
@@ -317,9 +324,11 @@ def run_ours(args):
     atmos = [ig.Atmosphere.load(m) for m in mets]
     th, ph = fan_angles()
     n = th.size
-    precs = {"fp64": ig.FP64, "fp32c": ig.FP32C}
+    precs = {"fp64": ig.FP64, "fp32c": ig.FP32C, "fp32c_flagged": ig.FP32C_FLAGGED}
     head = "fp32c" if args.precision in ("fp32c", "both") else "fp64"
     legs = [p_ for p_ in ("fp32c", "fp64") if args.precision in (p_, "both")]
+    if args.precision == "both":   # the fan kernel without the re-trace pass (focusing rays flagged)
+        legs.append("fp32c_flagged")
     all_params = {k: [a.default_params(bounces=FAN["bounces"], rng_max=FAN["rng_max"], write_rays=0,
                                        precision=precs[k]) for a in atmos] for k in legs}
     nb = FAN["bounces"] + 1
@@ -349,6 +358,7 @@ def run_ours(args):
     if not args.no_peak:
         gemm = {"fp64": fp64_peak_tflops(torch), "fp32": fp32_peak_tflops(torch)}
         peaks = {"fp64": gemm["fp64"], "fp32c": mixed_peak(gemm["fp64"], gemm["fp32"])}
+        peaks["fp32c_flagged"] = peaks["fp32c"]
 
     props = torch.cuda.get_device_properties(dev)
     gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
@@ -452,7 +462,7 @@ def run_ours(args):
             # FP32C: the fan kernel and the FP64-auxiliary re-trace kernel per fan
             "gpu_launches": args.steps * len(atmos) * (2 if head == "fp32c" else 1),
             "roofline": {"bound": "fp64+fp32" if head == "fp32c" else "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": TRAFFIC.get(head),
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": TRAFFIC.get(head), "traffic_source": TRAFFIC_SOURCE,
                          "peak_source": ("measured in this run: cuBLAS DGEMM and SGEMM (TF32 off) 8192^3 via "
                                          "torch.matmul, best of 5; FP32C peak = flops_per_step / (fp64 part / DGEMM "
                                          "+ fp32 part / SGEMM)" if head == "fp32c" else
@@ -469,6 +479,8 @@ def run_ours(args):
         }
         if "fp32c" in res and "fp64" in res:
             line["fp32c_over_fp64"] = res["fp32c"]["value"] / res["fp64"]["value"]
+        if "fp32c_flagged" in res and "fp64" in res:
+            line["fp32c_flagged_over_fp64"] = res["fp32c_flagged"]["value"] / res["fp64"]["value"]
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(mets[0])
         if world == 1 and not args.no_extra:
@@ -639,7 +651,7 @@ def cpu_baseline_sphr(files):
 
 
 def sphr_measure(steps, warmup, shapes=((1, None, "fp64"), (0, None, "fp64"), (1, 0, "fp64"), (1, None, "fp32c"),
-                                       (1, 0, "fp32c"))):
+                                       (1, None, "fp32c_flagged"), (0, None, "fp32c"))):
     """Config 2: spherical range-dependent fan over a 21x21 node grid with
     0.05-deg fractal terrain (workloads.py), FP64 and FP32-compensated.  The
     autotuner (iga_fan_tune) picks the CTA size first (on the FP64 kernel);
@@ -671,7 +683,8 @@ def sphr_measure(steps, warmup, shapes=((1, None, "fp64"), (0, None, "fp64"), (1
     for amp, block, prec in shapes:
         block = best if block is None else block
         params = atmo.default_params(geometry=ig.GEOM_SPH, bounces=f["bounces"], rng_max=f["rng_max"],
-                                     write_rays=0, calc_amp=amp, precision=ig.FP32C if prec == "fp32c" else ig.FP64)
+                                     write_rays=0, calc_amp=amp,
+                                     precision={"fp64": ig.FP64, "fp32c": ig.FP32C, "fp32c_flagged": ig.FP32C_FLAGGED}[prec])
         params.block = block
         times, n_steps = [], 0
         for i in range(warmup + steps):
@@ -686,7 +699,7 @@ def sphr_measure(steps, warmup, shapes=((1, None, "fp64"), (0, None, "fp64"), (1
                 times.append(e0.elapsed_time(e1) * 1e-3)
                 n_steps = int(st.sum().item())
         t = sum(times) / len(times)
-        name = ("fp32c_" if prec == "fp32c" else "") + ("amp" if amp else "noamp") + \
+        name = ("" if prec == "fp64" else prec + "_") + ("amp" if amp else "noamp") + \
             ("" if block == best else f"_block{block or 128}")
         legs[name] = {"ray_steps": n_steps, "s_per_fan": t, "value": n_steps / t, "block": block or 128,
                       "precision": prec}
@@ -823,14 +836,16 @@ def extra_configs(gpu_id):
     out = {}
     sampler = ClockSampler(gpu_id)
     sampler.start()
-    legs, best, tune_s, n, _ = sphr_measure(2, 1, shapes=((1, None, "fp64"), (1, None, "fp32c")))
+    legs, best, tune_s, n, _ = sphr_measure(2, 1, shapes=((1, None, "fp64"), (1, None, "fp32c"),
+                                                          (1, None, "fp32c_flagged")))
     out["config2"] = {"metric": METRIC, "unit": UNIT, "value": legs["amp"]["value"], "dtype": "f64",
                       "fp32c_value": legs["fp32c_amp"]["value"],
                       "fp32c_over_fp64": legs["fp32c_amp"]["value"] / legs["amp"]["value"],
                       "workload": f"sph-rngdep-fan-{n}rays-21x21grid-401x401terrain-20bnc-3000km",
                       "timing": "CUDA events, mean of 2 launches after 1 warm-up, L2 flushed",
                       "block": best, "s_per_fan": legs["amp"]["s_per_fan"],
-                      "fp32c_s_per_fan": legs["fp32c_amp"]["s_per_fan"], "clocks": sampler.stop()}
+                      "fp32c_s_per_fan": legs["fp32c_amp"]["s_per_fan"],
+                      "fp32c_flagged_value": legs["fp32c_flagged_amp"]["value"], "clocks": sampler.stop()}
     sampler = ClockSampler(gpu_id)
     sampler.start()
     legs3, err, _, _ = eigen_measure([1])
@@ -860,16 +875,28 @@ def _profile_case(name):
         prec = ig.FP32C if name.endswith("fp32c") else ig.FP64
         p = atmo.default_params(bounces=1, rng_max=600.0, write_rays=0, precision=prec)
         return lambda: ig.fan_run(atmo, p, th, ph)
+    if name in ("config2_fp32c", "config2_fp64"):
+        # the config-2 fan itself (14,328 rays, 21x21 grid with terrain, 20
+        # bounces, 3000 km): one launch of several seconds, for launch lists
+        # (gpu__time_duration only) of the fan and re-trace kernels
+        f = wl.sphr_files()
+        atmo = ig.Atmosphere.load_rngdep(f[0], f[1], f[2], topo_file=f[3], geometry=ig.GEOM_SPH)
+        th, ph = wl.sphr_angles()
+        s = wl.SPHR_FAN
+        p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=s["bounces"], rng_max=s["rng_max"], write_rays=0,
+                                precision=ig.FP32C if name.endswith("fp32c") else ig.FP64)
+        return lambda: ig.fan_run(atmo, p, th, ph)
     if name == "fansph":       # spherical stratified fan (fansph_fp64_kernel): 1,440 rays
         atmo = ig.Atmosphere.load(wl.profile_met(1))
         th, ph = synth.fan_angles(0.5, 60.0, 0.5, 0.0, 330.0, 30.0)
         p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=5, rng_max=2000.0, src=(30.0, 0.0, 0.0))
         return lambda: ig.fan_run(atmo, p, th, ph)
-    if name == "fansphr":      # 21x21 grid with terrain (fansphr_fp64_kernel): 408 rays, 1 bounce, 600 km
+    if name in ("fansphr", "fansphr_fp32c"):   # 21x21 grid with terrain: 408 rays, 1 bounce, 600 km
         f = wl.sphr_files()
         atmo = ig.Atmosphere.load_rngdep(f[0], f[1], f[2], topo_file=f[3], geometry=ig.GEOM_SPH)
         th, ph = synth.fan_angles(0.5, 50.0, 3.0, 0.0, 345.0, 15.0)
-        p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=1, rng_max=600.0)
+        p = atmo.default_params(geometry=ig.GEOM_SPH, bounces=1, rng_max=600.0,
+                                precision=ig.FP32C if name.endswith("fp32c") else ig.FP64)
         return lambda: ig.fan_run(atmo, p, th, ph)
     if name == "fan3dr":       # committed 5x5 grid with terrain (fan3dr_fp64_kernel): 1,080 rays
         d = os.path.join(golden, "rngdep3d")
@@ -898,7 +925,7 @@ def _profile_case(name):
     raise SystemExit(f"unknown profiling case {name!r} (one of {', '.join(PROFILE_CASES)})")
 
 
-PROFILE_CASES = ("fan3d_fp32c", "fan3d_fp64", "fansph", "fansphr", "fan3dr", "paths", "eig3d", "eigsph")
+PROFILE_CASES = ("fan3d_fp32c", "fan3d_fp64", "config2_fp32c", "config2_fp64", "fansph", "fansphr_fp32c", "fansphr", "fan3dr", "paths", "eig3d", "eigsph")
 
 
 def run_profile_case(args):

@@ -53,12 +53,22 @@ enum iga_ray_status {
      * the largest |D| along its path before its first caustic.  Near such a
      * focus the amplitude is ill-conditioned and FP32 auxiliaries would miss
      * it by tenths of a dB. */
-    IGA_RAY_AUX_FP64 = 0x100
+    IGA_RAY_AUX_FP64 = 0x100,
+    /* Flag OR'ed into the reason for IGA_FP32C_FLAGGED rays that met such a
+     * focusing arrival and were not traced again. */
+    IGA_RAY_FOCUS = 0x200
 };
 
 /* geometry / precision selectors */
 enum iga_geometry { IGA_GEOM_3D = 0, IGA_GEOM_SPH = 1 };
-enum iga_precision { IGA_FP64 = 0, IGA_FP32C = 1 };
+/* IGA_FP32C: FP32-compensated form (FP64 ray equations, FP32 Jacobian
+ * auxiliaries summed with compensation); rays that reach a focusing arrival
+ * before their first caustic are traced again with FP64 auxiliaries
+ * (IGA_RAY_AUX_FP64).  IGA_FP32C_FLAGGED: the same without that second pass:
+ * such rays keep their FP32 auxiliaries and carry IGA_RAY_FOCUS instead (their
+ * amplitudes from the focusing arrival on are ill-conditioned, off by up to a
+ * few tenths of a dB); the other arrivals are the same as with IGA_FP32C. */
+enum iga_precision { IGA_FP64 = 0, IGA_FP32C = 1, IGA_FP32C_FLAGGED = 2 };
 
 /* Columns of an arrival row, in the reference's .arrivals.dat order
  * (main.infraga.3d.cpp:362-374): incl, az, n_b, x_0, y_0, time, cel,
@@ -98,7 +108,7 @@ typedef struct iga_profile {
  * topo::z0 ground height and the run_prop locals (main.infraga.3d.cpp:206-215). */
 typedef struct iga_fan_params {
     int geometry;            /* IGA_GEOM_3D or IGA_GEOM_SPH */
-    int precision;           /* IGA_FP64 or IGA_FP32C */
+    int precision;           /* IGA_FP64, IGA_FP32C or IGA_FP32C_FLAGGED */
     int bounces;             /* reflections to follow (>= 0) */
     int calc_amp;            /* 1: 18 equations with the Jacobian auxiliaries */
     int write_rays;          /* 1: sum time/absorption per step like the CLI's

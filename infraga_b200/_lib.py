@@ -18,11 +18,14 @@ AUX_COLS = 4
 IGA_OK, IGA_E_INVALID, IGA_E_IO, IGA_E_NOMEM, IGA_E_CUDA, IGA_E_NODEVICE, IGA_E_TRUNCATED, IGA_E_UNSUPPORTED = \
     0, -1, -2, -3, -4, -5, -6, -7
 GEOM_3D, GEOM_SPH = 0, 1
-FP64, FP32C = 0, 1
+FP64, FP32C, FP32C_FLAGGED = 0, 1, 2
 RAY_STATUS = {0: "bounces", 1: "escaped", 2: "low_turn", 3: "short", 4: "nonfinite", 5: "stepcap", 6: "time_max"}
 # flag OR'ed into an FP32C ray's status: traced again with FP64 auxiliaries
 # after a focusing arrival (IGA_RAY_AUX_FP64); status & 0xff is the reason
 RAY_AUX_FP64 = 0x100
+# flag OR'ed into an FP32C_FLAGGED ray's status: met a focusing arrival and kept
+# its FP32 auxiliaries (IGA_RAY_FOCUS)
+RAY_FOCUS = 0x200
 
 
 class NativeLibraryError(RuntimeError):

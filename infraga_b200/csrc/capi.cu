@@ -168,7 +168,8 @@ namespace iga_internal {
 int validate(const iga_fan_params* p, int n_rays) {
     if (!p || n_rays < 0) return IGA_E_INVALID;
     if (p->geometry != IGA_GEOM_3D && p->geometry != IGA_GEOM_SPH) return IGA_E_INVALID;
-    if (p->precision != IGA_FP64 && p->precision != IGA_FP32C) return IGA_E_INVALID;
+    if (p->precision != IGA_FP64 && p->precision != IGA_FP32C && p->precision != IGA_FP32C_FLAGGED)
+        return IGA_E_INVALID;
     if (p->geometry == IGA_GEOM_SPH) {
         if (!(std::fabs(p->src[0]) < 90.0) || !std::isfinite(p->src[1])) return IGA_E_INVALID;
         if (!(p->time_max > 0.0)) return IGA_E_INVALID;
@@ -515,12 +516,13 @@ namespace {
 int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const double* d_ph, int n_rays,
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st, int grid_cap = 0, const PathSpec* ps = nullptr) {
+    const bool f32c = p->precision == IGA_FP32C || p->precision == IGA_FP32C_FLAGGED;
     if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) ||
-                         (p->precision != IGA_FP64 && !(h->kind == 1 && p->precision == IGA_FP32C)))) {
+                         (p->precision != IGA_FP64 && !(h->kind == 1 && f32c)))) {
         g_cuda_err = "range-dependent atmosphere: the geometry it was loaded for; FP32C on the spherical grid only";
         return IGA_E_UNSUPPORTED;
     }
-    if (p->geometry == IGA_GEOM_SPH && p->precision == IGA_FP32C && h->kind != 1) {
+    if (p->geometry == IGA_GEOM_SPH && f32c && h->kind != 1) {
         g_cuda_err = "spherical geometry: FP32C on range-dependent node grids only";
         return IGA_E_UNSUPPORTED;
     }
@@ -541,17 +543,18 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         a.path_rows = ps->rows; a.path_off = ps->off; a.path_n = ps->n; a.path_mode = ps->mode;
         a.caus_rows = ps->caus; a.caus_count = ps->caus_count; a.caus_cap = ps->caus_cap;
     }
-    if (p->precision == IGA_FP32C && h->kind == 0) {
+    a.retrace = p->precision == IGA_FP32C ? 1 : 0;
+    if (f32c && h->kind == 0) {
         iga_atmo_s::AlphaTab t;
         rc = ensure_alpha(h, p->freq, t);
         if (rc) return rc;
         a.knots_c = h->d_knots_c;
         a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
     }
-    if (p->precision == IGA_FP32C && h->kind == 1) a.hyb_x32 = h->d_hyb_x32;
+    if (f32c && h->kind == 1) a.hyb_x32 = h->d_hyb_x32;
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    if (h->kind == 1 && p->precision == IGA_FP32C && a.hyb_tab != nullptr)
+    if (h->kind == 1 && f32c && a.hyb_tab != nullptr)
         IGA_CUDA(iga::launch_fansphr_fp32c(a, p->calc_amp != 0, st, nullptr), "fansphr fp32c kernel launch");
     else if (h->kind == 1)
         IGA_CUDA(iga::launch_fansphr_fp64(a, p->calc_amp != 0, st, nullptr), "fansphr kernel launch");
@@ -559,7 +562,7 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         IGA_CUDA(iga::launch_fan3dr_fp64(a, p->calc_amp != 0, st, nullptr), "fan3dr kernel launch");
     else if (p->geometry == IGA_GEOM_SPH)
         IGA_CUDA(iga::launch_fansph_fp64(a, p->calc_amp != 0, st, nullptr), "fansph kernel launch");
-    else if (p->precision == IGA_FP32C)
+    else if (f32c)
         IGA_CUDA(iga::launch_fan3d_fp32c(a, p->calc_amp != 0, st, nullptr), "fan3d fp32c kernel launch");
     else
         IGA_CUDA(iga::launch_fan3d_fp64(a, p->calc_amp != 0, st, nullptr), "fan3d kernel launch");

@@ -514,7 +514,7 @@ int eig_search(iga_atmo_s* h, const iga_eig_params* P, const iga_eig_pair* pairs
         iga::spline_eval(h->prof.z, h->prof.c, h->prof.cs, h->prof.z.front(), f, d1, d2);
         c_incl_src = f;
     }
-    const bool f32 = fp.precision == IGA_FP32C;
+    const bool f32 = fp.precision == IGA_FP32C || fp.precision == IGA_FP32C_FLAGGED;
     if (f32 && (rc = fp32c_setup(h, fp.freq, a))) return rc;
 
     Settings S;

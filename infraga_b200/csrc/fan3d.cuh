@@ -90,6 +90,8 @@ struct Fan3DArgs {
     double alpha_z0, alpha_inv_h;
     const float* hyb_x32;    // [nx][ny][nz][kHybX32] FP32 copies of the hybrid records'
                              // second-derivative blocks (c, u, v: 9 values each)
+    int retrace;             // FP32C: 1 = mark focusing rays for the FP64-auxiliary re-trace,
+                             // 0 = flag them (kRayFocus) and keep tracing
 };
 
 constexpr int kHybX32 = 32;   // floats per record of hyb_x32 (3 x 9 used)
@@ -99,6 +101,9 @@ constexpr int kStrideC = 14;  // doubles per segment row of the FP32-compensated
 // Flag OR'ed into a ray's status (IGA_RAY_AUX_FP64): an FP32C ray traced
 // again with FP64 auxiliaries after a focusing arrival.
 constexpr int kRayAuxFp64 = 0x100;
+// Flag OR'ed into a ray's status (IGA_RAY_FOCUS): an FP32C ray that met a
+// focusing arrival and, without the re-trace pass, kept its FP32 auxiliaries.
+constexpr int kRayFocus = 0x200;
 
 // Sampled output rows.  Path rows: horizontal position (x, y [km] or lat, lon
 // [deg]), altitude [km] (terrain mode: the ground height there), amplitude

@@ -380,6 +380,7 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
     init_c<AMP>(a, theta0, phi0, a.src_x, a.src_y, yd, ya, yl, rc);
     int seg = seg_guess(fmin(fmax(a.src_z, a.z_lo), a.z_hi), a.z_lo, a.inv_dz, a.n_knots);
     int bnc = 0, kb = 0, na = 0, caustics = 0;
+    bool focused = false;
     T D_prev = T(0), D_max = T(0);
     long long steps = 0;
     // tt/att: the ray's time and absorption sums; pt/pa: the bounce's partial
@@ -460,7 +461,10 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
                 const double theta = a.theta_deg[ray] * kPi / 180.0;
                 const double phi = kPi / 2.0 - a.phi_deg[ray] * kPi / 180.0;
                 amp = amp_db(a.knots, a, segd, rk, rcd, theta, phi, &jac);
-                if (ESCALATE && caustics == 0 && fabs(jac) < kFocusRatio * (double)D_max) return true;
+                if (ESCALATE && !focused && caustics == 0 && fabs(jac) < kFocusRatio * (double)D_max) {
+                    if (a.retrace) return true;
+                    focused = true;
+                }
             }
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
             const double incl = -asin(a.c_ratio * rk[3]) * 180.0 / kPi;
@@ -497,7 +501,8 @@ __device__ __forceinline__ bool fan_ray_c(const Fan3DArgs& a, const double* __re
         // ray finished: its record
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
-        if (a.ray_status) a.ray_status[ray] = status | (sizeof(T) == sizeof(double) ? kRayAuxFp64 : 0);
+        if (a.ray_status)
+            a.ray_status[ray] = status | (sizeof(T) == sizeof(double) ? kRayAuxFp64 : 0) | (focused ? kRayFocus : 0);
         return false;
     }
 }
@@ -702,7 +707,7 @@ cudaError_t launch_c(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
     kern<<<(unsigned)grid, threads, smem, stream>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess || !AMP) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess || !AMP || !a.retrace) return e;
     // the rays marked for FP64 auxiliaries, after the fan on the same stream;
     // its queue is the workspace's second counter (cleared with the first)
     auto rk = fan3d_fp32c_retrace_kernel<SMEM>;

@@ -12,11 +12,9 @@
 //     scaling over the terrain in FP64;
 //   * the twelve Jacobian auxiliaries (R_th, mu_th, R_ph, mu_ph) in FP32, their
 //     state summed with TwoSum; the Hessians of c, u, v they read are formed
-//     in FP32 from an FP32 copy of the records' second-derivative blocks
-//     (hyb_x32: half the bytes of the largest part of a record read) and from
-//     the FP64 value blocks with the cell's first corner value taken out
-//     before the conversion (the derivative bases annihilate constants, so
-//     FP32 keeps the digits of the horizontal variation);
+//     partly in FP32 from an FP32 copy of the records' second-derivative
+//     blocks (hyb_x32: half the bytes of the largest part of a record read),
+//     the entries formed from the value blocks in FP64;
 //   * travel time, Sutherland-Bass absorption, reflection and amplitude in
 //     FP64, at the same points as the FP64 kernel;
 //   * focusing escalation as in the 3D kernel: a ray reaching an arrival with
@@ -62,81 +60,93 @@ __device__ __forceinline__ float herm_val_f(float v0, float s0, float v1, float 
     return v0 + X * (df + (1.0f - X) * (A * (1.0f - X) + B * X));
 }
 
-__device__ __forceinline__ float patch_f(const float (&c)[4][4], const float (&bx)[4], const float (&by)[4]) {
-    // bx/by = {h0, h1, g0, g1}, corners as in patch() (rngdep_eval.cuh)
-    float s = 0.0f;
+// Horizontal Hermite bases of a cell (value and d/dx, d/dy forms), in FP64
+// and FP32, formed once per evaluation point for the three fields.
+struct CellBasis {
+    double hx[2], gx[2], hy[2], gy[2], dhx[2], dgx[2], dhy[2], dgy[2];
+    float fhx[2], fgx[2], fhy[2], fgy[2], fdhx[2], fdhy[2];
+};
+
+__device__ __forceinline__ CellBasis cell_basis(const HybLoc& L) {
+    const Basis1 bx = basis_val(L.tx), by = basis_val(L.ty);
+    const Basis1 dbx = basis_der(L.tx, 1.0 / L.dx), dby = basis_der(L.ty, 1.0 / L.dy);
+    CellBasis c;
+    c.hx[0] = bx.h0; c.hx[1] = bx.h1; c.gx[0] = bx.g0; c.gx[1] = bx.g1;
+    c.hy[0] = by.h0; c.hy[1] = by.h1; c.gy[0] = by.g0; c.gy[1] = by.g1;
+    c.dhx[0] = dbx.h0; c.dhx[1] = dbx.h1; c.dgx[0] = dbx.g0; c.dgx[1] = dbx.g1;
+    c.dhy[0] = dby.h0; c.dhy[1] = dby.h1; c.dgy[0] = dby.g0; c.dgy[1] = dby.g1;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        c.fhx[k] = (float)c.hx[k]; c.fgx[k] = (float)c.gx[k]; c.fhy[k] = (float)c.hy[k]; c.fgy[k] = (float)c.gy[k];
+        c.fdhx[k] = (float)c.dhx[k]; c.fdhy[k] = (float)c.dhy[k];
+    }
+    return c;
+}
+
+// Field fld (0 c, 1 u, 2 v) at L (interp::eval_all, interpolation.cpp:
+// 1544-1788, as hyb_f2): f, the gradient and the Hessian entries formed from
+// the FP64 value blocks (d2/dz2, d2/dz dlat, d2/dz dlon, d2/dlat dlon) in
+// FP64, the two formed from the second-derivative blocks (d2/dlat2,
+// d2/dlon2) in FP32 from their FP32 copies (hyb_x32).  The patches are summed
+// corner by corner as the corner data are formed, so no corner array is held.
+__device__ __forceinline__ void hyb_f2_c(const HybView& g, const float* __restrict__ x32, const HybLoc& L,
+                                         const CellBasis& B, int fld, HybF1& o, float (&dd)[3][3]) {
+    const float Xf = (float)L.zq.X, hf = (float)L.zq.h;
+    const double dxdy = L.dx * L.dy;
+    const float dxf = (float)L.dx, dyf = (float)L.dy, dxdyf = (float)dxdy;
+    double f = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, h00 = 0.0, h01 = 0.0, h02 = 0.0, h12 = 0.0;
+    float h11 = 0.0f, h22 = 0.0f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int a = q & 1, b = q >> 1;
-        s += c[q][0] * bx[a] * by[b] + c[q][1] * bx[2 + a] * by[b] + c[q][2] * bx[a] * by[2 + b] +
-             c[q][3] * bx[2 + a] * by[2 + b];
-    }
-    return s;
-}
-
-// Field fld (0 c, 1 u, 2 v) at L: f and gradient in FP64 (interp::eval_all,
-// interpolation.cpp:1544-1616, as hyb_f1), Hessian in FP32 (:1618-1788, as
-// hyb_f2) from the FP64 value blocks and the FP32 second-derivative blocks.
-__device__ __forceinline__ void hyb_f2_c(const HybView& g, const float* __restrict__ x32, const HybLoc& L, int fld,
-                                         HybF1& o, float (&dd)[3][3]) {
-    double cv[4][4], cz[4][4];
-    float czz[4][4], cq[4][4], cr[4][4];
-    const float Xf = (float)L.zq.X, hf = (float)L.zq.h;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int ix = L.kx + (q & 1), iy = L.ky + (q >> 1);
+        const int ix = L.kx + a, iy = L.ky + b;
         const size_t rec = (size_t)(ix * g.ny + iy) * g.nz + L.kz;
         const double* p0 = g.tab + rec * kRecLen + fld * kRecP;
         const double* p1 = p0 + kRecLen;
         const float* x0 = x32 + rec * kHybX32 + fld * kRecX;
         const float* x1 = x0 + kHybX32;
+        double cv[4], cz[4], czz[4];
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            cv[q][m] = herm_val(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq);
-            cz[q][m] = herm_der(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq);
-            czz[q][m] = (float)herm_der2(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq_raw);
+            cv[m] = herm_val(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq);
+            cz[m] = herm_der(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq);
+            czz[m] = herm_der2(p0[2 * m], p0[2 * m + 1], p1[2 * m], p1[2 * m + 1], L.zq_raw);
         }
-        cq[q][0] = herm_val_f((float)p0[2], x0[0], (float)p1[2], x1[0], Xf, hf);
-        cq[q][1] = herm_val_f(x0[1], x0[2], x1[1], x1[2], Xf, hf);
-        cq[q][2] = (float)cv[q][3];
-        cq[q][3] = herm_val_f(x0[3], x0[4], x1[3], x1[4], Xf, hf);
-        cr[q][0] = herm_val_f((float)p0[4], x0[0], (float)p1[4], x1[0], Xf, hf);
-        cr[q][1] = (float)cv[q][3];
-        cr[q][2] = herm_val_f(x0[5], x0[6], x1[5], x1[6], Xf, hf);
-        cr[q][3] = herm_val_f(x0[7], x0[8], x1[7], x1[8], Xf, hf);
-        const double dxdy = L.dx * L.dy;
-        cv[q][1] *= L.dx; cv[q][2] *= L.dy; cv[q][3] *= dxdy;
-        cz[q][1] *= L.dx; cz[q][2] *= L.dy; cz[q][3] *= dxdy;
-        const float dxf = (float)L.dx, dyf = (float)L.dy, dxdyf = (float)dxdy;
-        czz[q][1] *= dxf; czz[q][2] *= dyf; czz[q][3] *= dxdyf;
-        cq[q][1] *= dxf; cq[q][2] *= dyf; cq[q][3] *= dxdyf;
-        cr[q][1] *= dxf; cr[q][2] *= dyf; cr[q][3] *= dxdyf;
+        const float cv3f = (float)cv[3];
+        const float q0 = herm_val_f((float)p0[2], x0[0], (float)p1[2], x1[0], Xf, hf);
+        const float q1 = herm_val_f(x0[1], x0[2], x1[1], x1[2], Xf, hf) * dxf;
+        const float q2 = cv3f * dyf;
+        const float q3 = herm_val_f(x0[3], x0[4], x1[3], x1[4], Xf, hf) * dxdyf;
+        const float r0 = herm_val_f((float)p0[4], x0[0], (float)p1[4], x1[0], Xf, hf);
+        const float r1 = cv3f * dxf;
+        const float r2 = herm_val_f(x0[5], x0[6], x1[5], x1[6], Xf, hf) * dyf;
+        const float r3 = herm_val_f(x0[7], x0[8], x1[7], x1[8], Xf, hf) * dxdyf;
+        cv[1] *= L.dx; cv[2] *= L.dy; cv[3] *= dxdy;
+        cz[1] *= L.dx; cz[2] *= L.dy; cz[3] *= dxdy;
+        czz[1] *= L.dx; czz[2] *= L.dy; czz[3] *= dxdy;
+        const double hx = B.hx[a], gx = B.gx[a], hy = B.hy[b], gy = B.gy[b];
+        const double dhx = B.dhx[a], dgx = B.dgx[a], dhy = B.dhy[b], dgy = B.dgy[b];
+        f += cv[0] * hx * hy + cv[1] * gx * hy + cv[2] * hx * gy + cv[3] * gx * gy;
+        d1 += cv[0] * dhx * hy + cv[1] * dgx * hy + cv[2] * dhx * gy + cv[3] * dgx * gy;
+        d2 += cv[0] * hx * dhy + cv[1] * gx * dhy + cv[2] * hx * dgy + cv[3] * gx * dgy;
+        d0 += cz[0] * hx * hy + cz[1] * gx * hy + cz[2] * hx * gy + cz[3] * gx * gy;
+        h12 += cv[0] * dhx * dhy + cv[1] * dgx * dhy + cv[2] * dhx * dgy + cv[3] * dgx * dgy;
+        h01 += cz[0] * dhx * hy + cz[1] * dgx * hy + cz[2] * dhx * gy + cz[3] * dgx * gy;
+        h02 += cz[0] * hx * dhy + cz[1] * gx * dhy + cz[2] * hx * dgy + cz[3] * gx * dgy;
+        h00 += czz[0] * hx * hy + czz[1] * gx * hy + czz[2] * hx * gy + czz[3] * gx * gy;
+        const float fhx = B.fhx[a], fgx = B.fgx[a], fhy = B.fhy[b], fgy = B.fgy[b];
+        const float fdhx = B.fdhx[a], fdhy = B.fdhy[b];
+        const float fdgx = (float)dgx, fdgy = (float)dgy;
+        h11 += q0 * fdhx * fhy + q1 * fdgx * fhy + q2 * fdhx * fgy + q3 * fdgx * fgy;
+        h22 += r0 * fhx * fdhy + r1 * fgx * fdhy + r2 * fhx * fdgy + r3 * fgx * fdgy;
     }
-    const Basis1 bx = basis_val(L.tx), by = basis_val(L.ty);
-    const Basis1 dbx = basis_der(L.tx, 1.0 / L.dx), dby = basis_der(L.ty, 1.0 / L.dy);
-    o.f = patch(cv, bx, by);
-    o.d[1] = patch(cv, dbx, by);
-    o.d[2] = patch(cv, bx, dby);
-    o.d[0] = patch(cz, bx, by);
-    // the Hessian: corner values relative to corner 0 (derivative bases sum to zero)
-    float cvf[4][4], czf[4][4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        cvf[q][0] = (float)(cv[q][0] - cv[0][0]);
-        czf[q][0] = (float)(cz[q][0] - cz[0][0]);
-#pragma unroll
-        for (int m = 1; m < 4; m++) { cvf[q][m] = (float)cv[q][m]; czf[q][m] = (float)cz[q][m]; }
-    }
-    const float fbx[4] = {(float)bx.h0, (float)bx.h1, (float)bx.g0, (float)bx.g1};
-    const float fby[4] = {(float)by.h0, (float)by.h1, (float)by.g0, (float)by.g1};
-    const float fdbx[4] = {(float)dbx.h0, (float)dbx.h1, (float)dbx.g0, (float)dbx.g1};
-    const float fdby[4] = {(float)dby.h0, (float)dby.h1, (float)dby.g0, (float)dby.g1};
-    dd[1][2] = dd[2][1] = patch_f(cvf, fdbx, fdby);
-    dd[0][1] = dd[1][0] = patch_f(czf, fdbx, fby);
-    dd[0][2] = dd[2][0] = patch_f(czf, fbx, fdby);
-    dd[0][0] = patch_f(czz, fbx, fby);
-    dd[1][1] = patch_f(cq, fdbx, fby);
-    dd[2][2] = patch_f(cr, fbx, fdby);
+    o.f = f; o.d[0] = d0; o.d[1] = d1; o.d[2] = d2;
+    dd[0][0] = (float)h00;
+    dd[0][1] = dd[1][0] = (float)h01;
+    dd[0][2] = dd[2][0] = (float)h02;
+    dd[1][1] = h11;
+    dd[1][2] = dd[2][1] = (float)h12;
+    dd[2][2] = h22;
 }
 
 // atm_full (fansphr_common.cuh) with the Hessians in T: for T = double the
@@ -161,9 +171,10 @@ __device__ __forceinline__ void atm_full_c(const Fan3DArgs& a, const Views& vw, 
         hyb_locate(vw.hyb, lat, lon, r - a.r_earth, L, cl.hx, cl.hy, cl.hz);
         HybF1 c1, u1, v1;
         float cdd[3][3], udd[3][3], vdd[3][3];
-        hyb_f2_c(vw.hyb, a.hyb_x32, L, 0, c1, cdd);
-        hyb_f2_c(vw.hyb, a.hyb_x32, L, 1, u1, udd);
-        hyb_f2_c(vw.hyb, a.hyb_x32, L, 2, v1, vdd);
+        const CellBasis B = cell_basis(L);
+        hyb_f2_c(vw.hyb, a.hyb_x32, L, B, 0, c1, cdd);
+        hyb_f2_c(vw.hyb, a.hyb_x32, L, B, 1, u1, udd);
+        hyb_f2_c(vw.hyb, a.hyb_x32, L, B, 2, v1, vdd);
         // boundary-layer scaling over the terrain (or flat ground), as atm_full
         const double zr = r - a.r_earth;
         double zg = a.r_grnd, dzg[2] = {0.0, 0.0}, ddzg[3] = {0.0, 0.0, 0.0};
@@ -368,6 +379,7 @@ __device__ __forceinline__ bool fan_ray_sc(const Fan3DArgs& a, const Views& vw, 
     }
     Cells cl{0, 0, 0, 0, 0};
     int bnc = 0, kb = 0, na = 0, caustics = 0;
+    bool focused = false;
     T D_prev = T(0), D_max = T(0);
     long long steps = 0;
     double s = 0.0, tt = 0.0, att = 0.0, pt = 0.0, pa = 0.0, rmax = 0.0;
@@ -460,9 +472,11 @@ __device__ __forceinline__ bool fan_ray_sc(const Fan3DArgs& a, const Views& vw, 
                 amp = amp_db_sphr<false>(a, vw, cl, rk, a.theta_deg[ray] * (kPi / 180.0),
                                          kPi / 2.0 - a.phi_deg[ray] * (kPi / 180.0), &jac);
                 // jac = r^2 cos(lat) x the determinant D of the caustic test
-                if (ESCALATE && caustics == 0 &&
-                    fabs(jac) < kFocusRatioS * (double)D_max * rk[0] * rk[0] * cos(rk[1]))
-                    return true;
+                if (ESCALATE && !focused && caustics == 0 &&
+                    fabs(jac) < kFocusRatioS * (double)D_max * rk[0] * rk[0] * cos(rk[1])) {
+                    if (a.retrace) return true;
+                    focused = true;
+                }
             }
             double* out = a.arrivals + ((size_t)ray * nb + na) * 12;
             AtmPt mk;
@@ -516,7 +530,8 @@ __device__ __forceinline__ bool fan_ray_sc(const Fan3DArgs& a, const Views& vw, 
         }
         a.n_arr[ray] = na;
         a.ray_steps[ray] = steps;
-        if (a.ray_status) a.ray_status[ray] = status | (sizeof(T) == sizeof(double) && AMP ? kRayAuxFp64 : 0);
+        if (a.ray_status)
+            a.ray_status[ray] = status | (sizeof(T) == sizeof(double) && AMP ? kRayAuxFp64 : 0) | (focused ? kRayFocus : 0);
         return false;
     }
 }
@@ -593,7 +608,7 @@ cudaError_t launch_sc(const Fan3DArgs& a, cudaStream_t stream, int* grid_used) {
     if (grid < 1) grid = 1;
     if (grid_used) *grid_used = (int)grid;
     kern<<<(unsigned)grid, threads, smem, stream>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess || !AMP) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess || !AMP || !a.retrace) return e;
     auto rk = fansphr_fp32c_retrace_kernel;
     const size_t smem_r = smem_sphr_c(a, kThreadsSR);
     if ((e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r)) != cudaSuccess)

@@ -89,3 +89,31 @@ def test_fp32c_north_star_bound_full_fan(dev, seed):
     assert nc2.sum() > 0
     assert np.abs(g2[nc2, 10] - w2[nc2, 10]).max() < 1e-3
     assert np.hypot(g2[nc2, 3] - w2[nc2, 3], g2[nc2, 4] - w2[nc2, 4]).max() < 1e-4
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_fp32c_flagged_form(dev, seed):
+    """IGA_FP32C_FLAGGED: the fan kernel alone.  Rays that met a focusing arrival
+    carry IGA_RAY_FOCUS (the rays the default form re-traces); every other ray
+    is bit-identical to the default form, and the north-star bound holds on
+    its non-caustic arrivals."""
+    th, ph = synth.fan_angles(0.5, 60.01, 0.1, 0, 357, 3)
+    atmo = ig.Atmosphere.load(profile_path(seed))
+    kw = dict(bounces=10, rng_max=2000.0, write_rays=0)
+    r64 = ig.fan_run(atmo, atmo.default_params(**kw), th, ph, with_aux=True)
+    r32 = ig.fan_run(atmo, atmo.default_params(**kw, precision=ig.FP32C), th, ph)
+    rf = ig.fan_run(atmo, atmo.default_params(**kw, precision=ig.FP32C_FLAGGED), th, ph)
+    redo = (r32["ray_status"] & ig.RAY_AUX_FP64) != 0
+    foc = (rf["ray_status"] & ig.RAY_FOCUS) != 0
+    np.testing.assert_array_equal(foc, redo)
+    np.testing.assert_array_equal(rf["ray_status"] & 0xFF, r32["ray_status"] & 0xFF)
+    keep = np.where(~foc)[0]
+    s32, sf = np.isin(r32["ray_index"], keep), np.isin(rf["ray_index"], keep)
+    np.testing.assert_array_equal(rf["arrivals"][sf], r32["arrivals"][s32])
+    s64 = np.isin(r64["ray_index"], keep)
+    got, want, aux, flipped = match_arrivals(rf["arrivals"][sf], rf["ray_index"][sf].astype(np.int64),
+                                             r64["arrivals"][s64], r64["ray_index"][s64].astype(np.int64), th.size,
+                                             r64["aux"][s64])
+    rep = noncaustic_report(got, want, aux[:, 3])
+    print(f"seed {seed}: flagged {foc.sum()} rays", rep)
+    assert rep["ok"], rep
