@@ -72,15 +72,15 @@ __global__ void __launch_bounds__(kSphTraceThreads) tracesph_fp64_kernel(const _
                 rhs_sph<AMP>(tab, a, seg, y, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-                rhs_sph<AMP>(tab, a, seg, stg, f);
+                // stages 2..4 with one copy of the right-hand side (instruction-cache footprint)
+#pragma unroll 1
+                for (int st = 0; st < 3; st++) {
+                    rhs_sph<AMP>(tab, a, seg, stg, f);
+                    const double w = st < 2 ? c_third : c_sixth;
+                    const double c = st == 0 ? 0.5 : 1.0;
 #pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-                rhs_sph<AMP>(tab, a, seg, stg, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-                rhs_sph<AMP>(tab, a, seg, stg, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+                    for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * w; stg[i] = y[i] + t * c; }
+                }
                 kb++;
                 // s_max and break_check (in-place longitude wrap first), ground_check
                 esc = s > a.s_max;

@@ -112,15 +112,15 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         }
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-        rhs<AMP>(tab, a, seg, stg, rc, f);
+        // stages 2..4 with one copy of the right-hand side (instruction-cache footprint)
+#pragma unroll 1
+        for (int st = 0; st < 3; st++) {
+            rhs<AMP>(tab, a, seg, stg, rc, f);
+            const double w = st < 2 ? c_third : c_sixth;
+            const double c = st == 0 ? 0.5 : 1.0;
 #pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-        rhs<AMP>(tab, a, seg, stg, rc, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-        rhs<AMP>(tab, a, seg, stg, rc, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * w; stg[i] = y[i] + t * c; }
+        }
         kb++;
 
         double dt, da;

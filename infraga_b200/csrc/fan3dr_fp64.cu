@@ -494,15 +494,15 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         }
 #pragma unroll
         for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
+        // stages 2..4 with one copy of the right-hand side (instruction-cache footprint)
+#pragma unroll 1
+        for (int st = 0; st < 3; st++) {
+            rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
+            const double w = st < 2 ? c_third : c_sixth;
+            const double c = st == 0 ? 0.5 : 1.0;
 #pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-        rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
-#pragma unroll
-        for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+            for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * w; stg[i] = y[i] + t * c; }
+        }
         kb++;
 
         // s_max, break_check (eqset.3d.rngdep.cpp:434-442), ground_check (:444-451)
@@ -703,15 +703,15 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) trace3dr_fp64_kernel(c
                 rhs_3dr<AMP, ST>(a, vw, cl, y, f);
 #pragma unroll
                 for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] = y[i] + t * c_sixth; stg[i] = y[i] + t * 0.5; }
-                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
+                // stages 2..4 with one copy of the right-hand side (instruction-cache footprint)
+#pragma unroll 1
+                for (int st = 0; st < 3; st++) {
+                    rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
+                    const double w = st < 2 ? c_third : c_sixth;
+                    const double c = st == 0 ? 0.5 : 1.0;
 #pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t * 0.5; }
-                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_third; stg[i] = y[i] + t; }
-                rhs_3dr<AMP, ST>(a, vw, cl, stg, f);
-#pragma unroll
-                for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * c_sixth; }
+                    for (int i = 0; i < N; i++) { const double t = ds * f[i]; acc[i] += t * w; stg[i] = y[i] + t * c; }
+                }
                 kb++;
                 const double rx = acc[0] - a.src_x, ry = acc[1] - a.src_y;
                 esc = (s > a.s_max) || (sqrt(rx * rx + ry * ry) > a.rng_max) || (acc[0] > a.x_max) || (acc[0] < a.x_min) ||
