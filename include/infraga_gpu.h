@@ -304,7 +304,9 @@ enum iga_path_mode {
     IGA_PATH_RAYS = 0,       /* rows m == 1 and m % 15 == 0 of every bounce (write_rays) */
     IGA_PATH_TERRAIN = 1,    /* rows m % 10 == 1 (write_topo) */
     IGA_PATH_PROJ = 2,       /* rows m == 1 and m % 5 == 0, IGA_PROJ_COLS wide (-back_proj);
-                                3D stratified flat-ground handles, calc_amp = 1, no caustics */
+                                3D stratified flat-ground and 3D range-dependent handles
+                                (run_back_proj of main.infraga.3d.cpp:559-770 and
+                                main.infraga.3d.rngdep.cpp:548-750), calc_amp = 1, no caustics */
     IGA_PATH_RESID = 3       /* one row per bounce segment (prop_rk4 call) at its row k - 1
                                 (print_resid, main.infraga.3d.cpp:437-441): eikonal residual,
                                 auxiliary-parameter residual, bounce, then zeros

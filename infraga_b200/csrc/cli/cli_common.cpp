@@ -160,10 +160,11 @@ void usage(Variant v) {
     std::cout << '\t' << "Common: freq, abs_coeff, z_grnd, prof_format, reverse_winds, output_id, calc_amp, max_alt, max_rng,"
               << '\n' << '\t' << "        " << (sph ? "min_lat, max_lat, min_lon, max_lon, max_time" : "min_x, max_x, min_y, max_y")
               << ", min_ds, max_ds, max_s, topo_file" << '\n';
-    if (v == Variant::k3D)
+    const bool back = v == Variant::k3D || v == Variant::k3DRngdep;
+    if (back)
         std::cout << '\t' << "-back_proj   one ray from (rcvr_x, rcvr_y) at (inclination, azimuth) through the reversed"
                   << " winds (bounces)" << '\n';
-    std::cout << '\t' << (v == Variant::k3D ? "" : "-back_proj, ")
+    std::cout << '\t' << (back ? "" : "-back_proj, ")
               << "-wnl_wvfrm and the reference's MPI builds are not provided by the GPU front end." << '\n' << '\n';
 }
 
@@ -188,11 +189,11 @@ struct PropOpts {
 // Loads the atmosphere of argv (first pass: prof_format, reverse_winds,
 // topo_file; z_grnd there is overwritten by set_limits) and prints set_region's
 // messages.  Returns null on failure (messages printed).
-iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_out) {
+iga_atmo_t load_atmosphere(Variant v, int argc, char** argv, const char** topo_out, bool force_rev = false) {
     const int first = is_rngdep(v) ? 5 : 3;
     const char* fmt = "zTuvdp";
     const char* topo = nullptr;
-    bool rev = false;
+    bool rev = force_rev;
     const char* val;
     for (int i = first; i < argc; i++) {
         if (key(argv[i], "prof_format=", &val)) fmt = val;
@@ -1151,7 +1152,12 @@ int run_eig(int argc, char** argv, Variant v, bool direct) {
 // holds its rows m == 1 and m % 5 == 0 with the inclination / azimuth
 // derivatives of position and travel time and the group velocity
 // (iga_fan_paths, IGA_PATH_PROJ), the console the arrival at the last bounce.
+int run_back_3dr(int argc, char** argv, Variant v);
+void write_projection(const std::string& id, const std::vector<double>& rows, long long np);
+void print_back_arrival(const std::vector<double>& arr, int n_out, int nb);
+
 int run_back(int argc, char** argv, Variant v) {
+    if (v == Variant::k3DRngdep) return run_back_3dr(argc, argv, v);
     if (v != Variant::k3D) {
         std::cout << "-back_proj is not provided by the GPU front end." << '\n';
         return 0;
@@ -1234,6 +1240,14 @@ int run_back(int argc, char** argv, Variant v) {
     rc = iga_fan_paths(atmo, &p, &incl, &az, 1, IGA_PATH_PROJ, &st, rows.data(), cap, &np, nullptr, nullptr, 0, nullptr,
                        nullptr);
     if (rc) return fail("back projection rows", rc);
+    write_projection(id, rows, np);
+    print_back_arrival(arr, n_out, nb);
+    iga_atmo_destroy(atmo);
+    return 0;
+}
+
+// {id}.projection.dat of run_back_proj: header and the np rows
+void write_projection(const std::string& id, const std::vector<double>& rows, long long np) {
     std::ofstream f((id + ".projection.dat").c_str());
     f << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "time [s]" << '\t' << "X^{(incl)} [km/deg]" << '\t'
       << "Y^{(incl)} [km/deg]" << '\t' << "Z^{(incl)} [km/deg]" << '\t' << "T^{(incl)} [s/deg]" << '\t'
@@ -1245,7 +1259,10 @@ int run_back(int argc, char** argv, Variant v) {
         for (int c = 1; c < IGA_PROJ_COLS; c++) f << '\t' << q[c];
         f << '\n';
     }
-    // the arrival after the last bounce, as run_back_proj prints it
+}
+
+// the arrival after the last bounce, as run_back_proj prints it
+void print_back_arrival(const std::vector<double>& arr, int n_out, int nb) {
     if (n_out == nb) {
         const double* q = &arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS];
         std::cout << '\t' << "Back projected arrival:" << '\n';
@@ -1261,6 +1278,87 @@ int run_back(int argc, char** argv, Variant v) {
     } else {
         std::cout << '\n' << '\t' << '\t' << "Ray path does not return to the ground." << '\n' << '\n';
     }
+}
+
+// -back_proj of infraga-3d-rngdep (run_back_proj, main.infraga.3d.rngdep.cpp:548-750):
+// one ray from the receiver through the reversed winds of the node grid, flat
+// ground (topo::z = 0) or terrain; {id}.projection.dat rows m == 1 and m % 5
+// == 0 with the altitude held at the terrain, the console the arrival at the
+// last bounce.
+int run_back_3dr(int argc, char** argv, Variant v) {
+    banner(v, "Back Projection");
+    const char* topo = nullptr;
+    iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo, true);   // set_region(..., true): winds reversed
+    if (!atmo) return 0;
+    const bool has_topo = topo != nullptr;
+    iga_fan_params p;
+    int rc = iga_fan_params_init(atmo, IGA_GEOM_3D, &p);
+    if (rc) return fail("parameters", rc);
+    print_region(v, p);
+    PropOpts o;
+    double incl = 15.0, az = 90.0, xr = 0.0, yr = 0.0, freq = 0.1;
+    if (has_topo) {   // the receiver defaults to the centre of the region (main.infraga.3d.rngdep.cpp:585-588)
+        xr = (p.x_max + p.x_min) / 2.0;
+        yr = (p.y_max + p.y_min) / 2.0;
+    }
+    int bounces = 0;
+    const char* val;
+    for (int i = 5; i < argc; i++) {
+        const char* a = argv[i];
+        if (key(a, "inclination=", &val)) incl = atof(val);
+        else if (key(a, "azimuth=", &val)) az = atof(val);
+        else if (key(a, "bounces=", &val)) bounces = std::max(0, atoi(val));
+        else if (key2(a, "rcvr_x=", "x_rcvr=", &val)) xr = atof(val);
+        else if (key2(a, "rcvr_y=", "y_rcvr=", &val)) yr = atof(val);
+        else if (common_key(v, a, p, o, has_topo, freq)) {}
+        else if (!confirm_unknown(a, false)) return 0;
+    }
+    if (o.use_blw) {
+        std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
+        return 0;
+    }
+    double zr = 0.0;   // z_rcvr = max(topo::z(x, y), 0); topo::z = 0 without terrain
+    if (has_topo) {
+        double zz = 0.0;
+        iga_atmo_terrain(atmo, xr, yr, &zz, nullptr, nullptr);
+        zr = std::max(zz, 0.0);
+    }
+    if (o.write_atmo && (rc = write_atmo_file(atmo, p, xr, yr, Pi / 2.0 - az * (Pi / 180.0))))
+        return fail("write_atmo", rc);
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "inclination: " << incl * (Pi / 180.0) * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "azimuth: " << 90.0 - (Pi / 2.0 - az * (Pi / 180.0)) * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "bounces: " << bounces << '\n';
+    std::cout << '\t' << "receiver location: " << xr << ", " << yr << ", " << zr << '\n';
+    if (!has_topo) std::cout << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    std::cout << '\t' << "frequency: " << freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n' << '\n';
+    if (!o.output_id) {
+        strip_extension(argv[2]);
+        o.output_id = argv[2];
+    }
+    const std::string id = o.output_id;
+    p.bounces = bounces;
+    p.calc_amp = 1;
+    p.write_rays = 1;
+    p.src[0] = xr; p.src[1] = yr; p.src[2] = zr;
+    p.freq = freq;
+    p.turn_ht_min = -1.0e30;   // run_back_proj has no turning-height cut
+    p.precision = IGA_FP64;
+    const int nb = bounces + 1;
+    std::vector<double> arr((size_t)nb * IGA_ARRIVAL_COLS);
+    long long st = 0;
+    int n_out = 0;
+    rc = iga_fan_run(atmo, &p, &incl, &az, 1, arr.data(), nb, &n_out, nullptr, &st, nullptr, nullptr, nullptr);
+    if (rc) return fail("back projection", rc);
+    const long long cap = (long long)nb + st / 5 + 1;
+    std::vector<double> rows((size_t)cap * IGA_PROJ_COLS);
+    long long np = 0;
+    rc = iga_fan_paths(atmo, &p, &incl, &az, 1, IGA_PATH_PROJ, &st, rows.data(), cap, &np, nullptr, nullptr, 0, nullptr,
+                       nullptr);
+    if (rc) return fail("back projection rows", rc);
+    write_projection(id, rows, np);
+    print_back_arrival(arr, n_out, nb);
     iga_atmo_destroy(atmo);
     return 0;
 }

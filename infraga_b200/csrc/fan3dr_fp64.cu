@@ -266,6 +266,92 @@ __device__ __forceinline__ void seg_increment_3dr(const Fan3DArgs& a, const View
     da_out = sb_alpha_cart(m.c, m.rho, zm, a.freq, a.tweak_abs, a.sb) * ds;
 }
 
+// travel_time_var of one segment (geoac.eqset.3d.rngdep.cpp:595-660, the
+// (tt, .., k1, k2) form run_back_proj calls): the inclination / azimuth
+// variations of the travel time at the segment midpoint, with atmo::c, dc, u,
+// du, v, dv as atmo_state.3d.rngdep.cpp:148-230 return them (the
+// boundary-layer scaling only below z_bndlyr, topo::bndlyr_sc / bndlyr_dsc
+// :83-103), w = 0.  Kept with the reference's sign (the sums are decremented)
+// and its product in the dot product (dcg[1] * cg[1] * dcg[2] * cg[2]).
+template <bool ST>
+__device__ __forceinline__ void seg_time_var_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y0,
+                                                 const double* y1, double& dvar_t, double& dvar_p) {
+    const double dx = y1[0] - y0[0], dy = y1[1] - y0[1], dz = y1[2] - y0[2];
+    const double xm = y0[0] + dx / 2.0, ym = y0[1] + dy / 2.0, zm = y0[2] + dz / 2.0;
+    const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+    double nu[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) nu[i] = y0[3 + i] + (y1[3 + i] - y0[3 + i]) / 2.0;
+    const double num = sqrt(nu[0] * nu[0] + nu[1] * nu[1] + nu[2] * nu[2]);
+    // c, u, v and their x, y, z derivatives before the boundary-layer scaling
+    double c, dc[3], u, du[3], v, dv[3];
+    if (ST) {
+        Cubic q;
+        const double* r0 = strat_at(a, cl, zm, q);
+        cubic_f1(r0, q, 2, c, dc[2]);
+        cubic_f1(r0, q, 4, u, du[2]);
+        cubic_f1(r0, q, 6, v, dv[2]);
+        dc[0] = dc[1] = du[0] = du[1] = dv[0] = dv[1] = 0.0;
+    } else {
+        HybLoc L;
+        hyb_locate(vw.hyb, xm, ym, zm, L, cl.hx, cl.hy, cl.hz);
+        L.zq_raw = L.zq;
+        HybF1 t;
+        hyb_f1(vw.hyb, L, 0, t); c = t.f;
+#pragma unroll
+        for (int n = 0; n < 3; n++) dc[n] = t.d[hix(n)];
+        hyb_f1(vw.hyb, L, 1, t); u = t.f;
+#pragma unroll
+        for (int n = 0; n < 3; n++) du[n] = t.d[hix(n)];
+        hyb_f1(vw.hyb, L, 2, t); v = t.f;
+#pragma unroll
+        for (int n = 0; n < 3; n++) dv[n] = t.d[hix(n)];
+    }
+    double sc = 1.0, dsc[3] = {0.0, 0.0, 0.0};
+    if (zm < a.z_bl) {
+        double zg = 0.0, dzg[2] = {0.0, 0.0};
+        if (vw.has_topo) {
+            TopoVal tv;
+            topo_eval(vw.topo, xm, ym, 1, tv, cl.tx, cl.ty);
+            zg = tv.z; dzg[0] = tv.d[0]; dzg[1] = tv.d[1];
+        }
+        const double X = exp(-(zm - zg) * a.inv_bl);
+        sc = (1.0 - X) / (1.0 + X);
+        const double dX[3] = {X * a.inv_bl * dzg[0], X * a.inv_bl * dzg[1], -X * a.inv_bl};
+#pragma unroll
+        for (int n = 0; n < 3; n++) dsc[n] = -2.0 * dX[n] / ((1.0 + X) * (1.0 + X));
+    }
+#pragma unroll
+    for (int n = 0; n < 3; n++) {
+        du[n] = du[n] * sc + u * dsc[n];
+        dv[n] = dv[n] * sc + v * dsc[n];
+    }
+    const double cg[3] = {c * nu[0] / num + u * sc, c * nu[1] / num + v * sc, c * nu[2] / num};
+    const double cgm = sqrt(cg[0] * cg[0] + cg[1] * cg[1] + cg[2] * cg[2]);
+    const double den = cgm * cgm * cgm;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int o = 6 * j;   // X at 6..8 / 12..14, mu at 9..11 / 15..17
+        double X[3], mu[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            X[i] = y0[6 + o + i] + (y1[6 + o + i] - y0[6 + o + i]) / 2.0;
+            mu[i] = y0[9 + o + i] + (y1[9 + o + i] - y0[9 + o + i]) / 2.0;
+        }
+        double s = X[0] * dc[0];
+        s += X[1] * dc[1];
+        s += X[2] * dc[2];
+        s -= c / (num * num) * (mu[0] * nu[0] + mu[1] * nu[1] + mu[2] * nu[2]);
+        double dcg[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) dcg[i] = nu[i] / num * s + c / num * mu[i];
+        dcg[0] += X[0] * du[0] + X[1] * du[1] + X[2] * du[2];
+        dcg[1] += X[0] * dv[0] + X[1] * dv[1] + X[2] * dv[2];
+        const double var = -((dcg[0] * cg[0] + dcg[1] * cg[1] * dcg[2] * cg[2]) / den * ds);
+        if (j == 0) dvar_t = var; else dvar_p = var;
+    }
+}
+
 // geoac::amp with geoac::jacobian at the below-ground row (eqset.3d.rngdep.cpp:704-748)
 template <bool ST>
 __device__ __noinline__ double amp_db_3dr(const Fan3DArgs& a, const Views& vw, Cells& cl, const double* y, double theta,
@@ -455,6 +541,9 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
     long long steps;
     double s, tt, att, pt, pa, zmax;
     long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
+    // PATHS, back projection: travel-time variations (sums and pending increments as tt / pt)
+    double tvt = 0.0, tvp = 0.0, ptvt = 0.0, ptvp = 0.0;
+    const bool proj = PATHS && AMP && a.path_rows && a.path_mode == kPathProj;
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
@@ -462,6 +551,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         ray_init_3dr<AMP>(a, theta, phi, y);
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
+        tvt = tvp = ptvt = ptvp = 0.0;
         zmax = ST ? a.z0 : 0.0;   // run_prop's z_max = topo::z0 (0 in the range-dependent main)
         if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
@@ -515,6 +605,11 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         seg_increment_3dr<ST>(a, vw, cl, y, acc, dt, da);
         if (a.write_rays) { tt += pt; att += pa; pt = dt; pa = da; }
         else { pt += dt; pa += da; }
+        if (proj) {   // run_back_proj sums travel_time_var per segment the same way (main.infraga.3d.rngdep.cpp:684-686)
+            double vt, vp;
+            seg_time_var_3dr<ST>(a, vw, cl, y, acc, vt, vp);
+            tvt += ptvt; tvp += ptvp; ptvt = vt; ptvp = vp;
+        }
 
         bool capped = false, bad = false;
         if (!esc && !gnd) {
@@ -524,7 +619,25 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         if (!esc && !gnd) {
 #pragma unroll
             for (int i = 0; i < N; i++) { prev[i * blockDim.x] = y[i]; y[i] = acc[i]; }
-            if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
+            if (proj && path_sampled(a.path_mode, kb)) {
+                // projection row (main.infraga.3d.rngdep.cpp:688-714): position with the
+                // altitude held at the terrain, derivatives per degree, group velocity
+                if (p_n < p_cap) {
+                    double* o = a.path_rows + (p_base + p_n) * kProjCols;
+                    Cells c2 = cl;
+                    const double d2r = kPi / 180.0;
+                    o[0] = y[0]; o[1] = y[1]; o[2] = fmax(y[2], topo_z(vw, c2, y[0], y[1])); o[3] = tt + pt;
+                    o[4] = y[6] * d2r; o[5] = y[7] * d2r; o[6] = y[8] * d2r; o[7] = (tvt + ptvt) * d2r;
+                    o[8] = y[12] * d2r; o[9] = y[13] * d2r; o[10] = y[14] * d2r; o[11] = (tvp + ptvp) * d2r;
+                    const double num = sqrt(y[3] * y[3] + y[4] * y[4] + y[5] * y[5]);
+                    AtmPt mp;
+                    atm_point<ST>(a, vw, c2, y[0], y[1], y[2], mp);
+                    o[12] = mp.c * y[3] / num + mp.u;
+                    o[13] = mp.c * y[4] / num + mp.v;
+                    o[14] = mp.c * y[5] / num;
+                }
+                p_n++;
+            } else if (PATHS && a.path_rows && path_sampled(a.path_mode, kb)) {
                 if (p_n < p_cap) {
                     double* o = a.path_rows + (p_base + p_n) * kPathCols;
                     Cells c2 = cl;
@@ -547,6 +660,7 @@ __global__ void __launch_bounds__(kThreads, IGA_3DR_MINB) fan3dr_fp64_kernel(con
         steps += K;
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
+        ptvt = 0.0; ptvp = 0.0;
         int status = -1;
         if (a.topo_tab == nullptr && zmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);

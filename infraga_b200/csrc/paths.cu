@@ -69,10 +69,10 @@ extern "C" int iga_fan_paths(iga_atmo_t h, const iga_fan_params* p, const double
         return IGA_E_INVALID;
     }
     if (p->precision != IGA_FP64) return IGA_E_UNSUPPORTED;
-    if (path_mode == IGA_PATH_PROJ) {   // run_back_proj exists here for the 3D stratified flat-ground solver
+    if (path_mode == IGA_PATH_PROJ) {   // run_back_proj of infraga-3d (flat ground) and infraga-3d-rngdep
         if (want_caus || !p->calc_amp) return IGA_E_INVALID;
-        if (h->kind != 0 || p->geometry != IGA_GEOM_3D) {
-            g_err = "back projection rows: 3D stratified flat-ground atmospheres only";
+        if (!(h->kind == 0 || h->kind == 2) || p->geometry != IGA_GEOM_3D || (h->kind == 0 && h->has_topo)) {
+            g_err = "back projection rows: 3D stratified flat-ground or 3D range-dependent atmospheres only";
             return IGA_E_UNSUPPORTED;
         }
     }

@@ -76,6 +76,12 @@ CASES = {
     "3dr_eig": ("infraga-3d-rngdep", "3dr", 0,
                 ["-eig_search", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "rcvr_x=210",
                  "rcvr_y=0", "incl_min=12", "incl_max=24"]),
+    "3dr_back_proj": ("infraga-3d-rngdep", "3dr", 0,
+                      ["-back_proj", "grid/node", "grid/x.dat", "grid/y.dat", "inclination=12", "azimuth=60",
+                       "bounces=1", "rcvr_x=40", "rcvr_y=-30", "max_ds=0.25"]),
+    "3dr_back_proj_topo": ("infraga-3d-rngdep", "3dr", 0,
+                           ["-back_proj", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat",
+                            "inclination=16", "azimuth=250", "bounces=2", "max_ds=0.25", "output_id=bp"]),
     "3dr_direct": ("infraga-3d-rngdep", "3dr", 0,
                    ["-eig_direct", "grid/node", "grid/x.dat", "grid/y.dat", "topo_file=topo.dat", "rcvr_x=210",
                     "rcvr_y=0", "incl_est=18", "az_est=90", "bounces=0", "output_id=direct"]),

@@ -43,16 +43,18 @@ def test_unsupported_modes_say_so(bins):
     r = subprocess.run([os.path.join(bins, "infraga-3d"), "-wnl_wvfrm", "x.met"], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode == 0 and "not provided" in r.stdout
-    # back projection: infraga-3d over flat ground only; the others refuse before loading anything
-    for name in ("infraga-sph", "infraga-3d-rngdep", "infraga-sph-rngdep"):
+    # back projection: infraga-3d over flat ground and infraga-3d-rngdep; the spherical ones refuse
+    # before loading anything
+    for name in ("infraga-sph", "infraga-sph-rngdep"):
         r = subprocess.run([os.path.join(bins, name), "-back_proj", "a", "b", "c", "d"], capture_output=True, text=True,
                            timeout=60)
         assert r.returncode == 0 and "-back_proj is not provided" in r.stdout, name
     r = subprocess.run([os.path.join(bins, "infraga-3d"), "-b", "x.met", "topo_file=t.dat"], capture_output=True,
                        text=True, timeout=60)
     assert r.returncode == 0 and "over terrain is not provided" in r.stdout
-    r = subprocess.run([os.path.join(bins, "infraga-3d")], capture_output=True, text=True, timeout=60)
-    assert "-back_proj   one ray" in r.stdout
+    for name in ("infraga-3d", "infraga-3d-rngdep"):
+        r = subprocess.run([os.path.join(bins, name)], capture_output=True, text=True, timeout=60)
+        assert "-back_proj   one ray" in r.stdout, name
 
 
 def test_cli_fixtures_complete():
