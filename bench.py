@@ -57,6 +57,8 @@ def mixed_peak(p64, p32):
     if not p64 or not p32:
         return None
     return FLOPS_PER_STEP["fp32c"] / (FP32C_SPLIT["fp64"] / p64 + FP32C_SPLIT["fp32"] / p32)
+
+
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per fan launch of the dominant kernel, from the ncu
 # captures of the full 71,520-ray fan cut to one bounce (bench.py --profile-case
@@ -64,7 +66,7 @@ L2_FLUSH_BYTES = 256 << 20
 # and code are read once per launch and the state stays in registers, so the
 # bytes do not grow with the steps of the 10-bounce launch, whose extra
 # arrival rows (<= 76 MB) are written into the 126 MB L2.
-TRAFFIC = {"fp64": 1366016 + 540672, "fp32c": 2059264 + 278784}
+TRAFFIC = {"fp64": 1453568 + 414720, "fp32c": 2059264 + 278784, "fp32c_flagged": 2059264 + 278784}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, 71,520-ray fan at 1 bounce "
                   "(profiles/fan3d_*_ncu_full_71520rays_1bnc.md)")
 

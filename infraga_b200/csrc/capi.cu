@@ -517,12 +517,14 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
                double* d_arr, int* d_n, long long* d_steps, int* d_status, double* d_aux, void* d_ws,
                cudaStream_t st, int grid_cap = 0, const PathSpec* ps = nullptr) {
     const bool f32c = p->precision == IGA_FP32C || p->precision == IGA_FP32C_FLAGGED;
+    const bool sph_grid = h->kind == 1 && !h->strat_topo;   // a spherical node grid (not a profile over terrain)
     if (h->kind != 0 && (p->geometry != (h->kind == 1 ? IGA_GEOM_SPH : IGA_GEOM_3D) ||
-                         (p->precision != IGA_FP64 && !(h->kind == 1 && f32c)))) {
-        g_cuda_err = "range-dependent atmosphere: the geometry it was loaded for; FP32C on the spherical grid only";
+                         (p->precision != IGA_FP64 && !(sph_grid && f32c)))) {
+        g_cuda_err = "range-dependent or terrain atmosphere: the geometry it was loaded for; FP32C on a spherical "
+                     "node grid only";
         return IGA_E_UNSUPPORTED;
     }
-    if (p->geometry == IGA_GEOM_SPH && f32c && h->kind != 1) {
+    if (p->geometry == IGA_GEOM_SPH && f32c && !sph_grid) {
         g_cuda_err = "spherical geometry: FP32C on range-dependent node grids only";
         return IGA_E_UNSUPPORTED;
     }
@@ -551,10 +553,10 @@ int run_device(iga_atmo_s* h, const iga_fan_params* p, const double* d_th, const
         a.knots_c = h->d_knots_c;
         a.alpha_tab = t.d; a.alpha_n = t.n; a.alpha_z0 = t.z0; a.alpha_inv_h = t.inv_h;
     }
-    if (f32c && h->kind == 1) a.hyb_x32 = h->d_hyb_x32;
+    if (f32c && sph_grid) a.hyb_x32 = h->d_hyb_x32;
     IGA_CUDA(cudaMemsetAsync(d_ws, 0, iga_fan_workspace_bytes(), st), "cudaMemsetAsync(workspace)");
     if (n_rays == 0) return IGA_OK;
-    if (h->kind == 1 && f32c && a.hyb_tab != nullptr)
+    if (sph_grid && f32c)
         IGA_CUDA(iga::launch_fansphr_fp32c(a, p->calc_amp != 0, st, nullptr), "fansphr fp32c kernel launch");
     else if (h->kind == 1)
         IGA_CUDA(iga::launch_fansphr_fp64(a, p->calc_amp != 0, st, nullptr), "fansphr kernel launch");
