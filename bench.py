@@ -830,10 +830,11 @@ def run_eigen(args):
 
 
 def extra_configs(gpu_id):
-    """Compact measurements of configs 2 and 3 carried in the default line,
-    each with the clocks sampled during it: the config-2 fan at the tuned CTA
-    size (2 timed launches after 1 warm-up) and one config-3 seed (128 pairs,
-    bounces 0..8) at both precisions."""
+    """Compact measurements of configs 2 and 3 and of the waveform mode carried
+    in the default line, each with the clocks sampled during it: the config-2
+    fan at the tuned CTA size (2 timed launches after 1 warm-up), one config-3
+    seed (128 pairs, bounces 0..8) at both precisions, and the -wnl_wvfrm fan
+    (576 rays, 2 timed calls after 1 warm-up)."""
     from infraga_b200 import workloads as wl
     out = {}
     sampler = ClockSampler(gpu_id)
@@ -855,7 +856,100 @@ def extra_configs(gpu_id):
                       "workload": f"3d-strat-eigen-1seed-x-{wl.EIG['pairs']}pairs-bnc0-{wl.EIG['bnc_max']}",
                       "timing": "wall clock of iga_eig_run", "legs": legs3, "fp32c_vs_fp64": err,
                       "clocks": sampler.stop()}
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    w = wnl_measure(2)
+    w["clocks"] = sampler.stop()
+    out["wnl"] = w
     return out
+
+
+# ---------------------------------------------------------------- weakly non-linear waveforms
+# -wnl_wvfrm over a fan: 16 inclinations x 36 azimuths (576 rays, about four
+# per SM), the reference's default 8192-sample impulse, one bounce.
+WNL = dict(incl=(4.0, 34.0, 16), az=(0.0, 350.0, 36), bounces=1, len=8192, seed=1, ref_rays=2)
+
+
+def wnl_waveform(n):
+    """wvfrm::build_wvfrm's built-in impulse with its defaults (p0 10 Pa, t0 0.1 s,
+    alpha 4, N_rise 10, N_period 40; waveforms.cpp:67-84)."""
+    import math
+    p0, t0, alpha = 10.0, 0.1, 4.0
+    dur = t0 * n * max(((1.0 + alpha) - math.sqrt(1.0 + alpha)) / 10, 2.0 * 3.14159 * math.sqrt(1 + alpha) / 40)
+    t = np.array([-dur / 2.0 + dur * i / n for i in range(n)])
+    xp = (alpha + 1.0) - math.sqrt(alpha + 1.0)
+    norm = xp ** alpha * (1.0 - xp / (1.0 + alpha)) * math.exp(-xp)
+    x = np.where(t >= 0, t / t0, 0.0)
+    pw = np.where(t >= 0, p0 * (x ** alpha * (1.0 - x / (1.0 + alpha)) * np.exp(-x)) / norm, 0.0)
+    return t, pw
+
+
+def wnl_fan():
+    th = np.repeat(np.linspace(*WNL["incl"]), WNL["az"][2])
+    ph = np.tile(np.linspace(*WNL["az"]), WNL["incl"][2])
+    return th, ph
+
+
+def wnl_cpu_reference(met, th, ph):
+    """The reference's waveform mode (oracle/_ref/infraga-3d-wnl, built from its
+    sources over oracle/fftshim) on one host core for a few rays of the fan:
+    seconds per waveform."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "infraga-3d-wnl")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/infraga-3d-wnl not built"}
+    tot = 0.0
+    n = WNL["ref_rays"]
+    idx = np.linspace(0, th.size - 1, n).astype(int)
+    with tempfile.TemporaryDirectory() as d:
+        shutil.copy(met, os.path.join(d, "atmo.met"))
+        for i in idx:
+            t0 = time.perf_counter()
+            subprocess.run([exe, "-wnl_wvfrm", "atmo.met", f"inclination={th[i]!r}", f"azimuth={ph[i]!r}",
+                            f"bounces={WNL['bounces']}"], cwd=d, stdout=subprocess.DEVNULL, check=True, timeout=600)
+            tot += time.perf_counter() - t0
+    return {"value": n / tot, "unit": "waveforms/s", "cores": 1, "kind": "reference",
+            "sample": f"{n} rays of the fan (indices {idx.tolist()}), one process each, wall clock"}
+
+
+def wnl_measure(reps=2, cpu=True):
+    """Waveforms per second through iga_wnl_run (host buffers in and out: the
+    trace, the step-count pass and the waveform kernel), with the Heun steps
+    per second of the waveform kernel's work, and the reference on the host."""
+    import infraga_b200 as ig
+    from infraga_b200 import workloads as wl
+    met = wl.profile_met(WNL["seed"])
+    atmo = ig.Atmosphere.load(met)
+    p = ig.wnl_params(atmo, bounces=WNL["bounces"])
+    th, ph = wnl_fan()
+    t, pw = wnl_waveform(WNL["len"])
+    ig.wnl_run(atmo, p, th[:8], ph[:8], t, pw)   # warm-up (kernel loading, allocator)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = ig.wnl_run(atmo, p, th, ph, t, pw)
+        times.append(time.perf_counter() - t0)
+    sec = statistics.mean(times)
+    steps = float(np.sum(r["steps"]))
+    out = {"metric": "waveforms/s", "unit": "waveforms/s", "value": th.size / sec, "dtype": "f64",
+           "workload": f"3d-strat-wnl-{th.size}rays-{WNL['len']}samples-{WNL['bounces']}bnc-impulse",
+           "timing": f"wall clock of iga_wnl_run, mean of {reps} calls after 1 warm-up",
+           "s_per_call": sec, "heun_steps": steps, "heun_steps_per_s": steps / sec,
+           "rays_ok": int(np.sum(r["status"] == 0))}
+    if cpu:
+        out["cpu_reference"] = wnl_cpu_reference(met, th, ph)
+    atmo.close()
+    return out
+
+
+def run_wnl(args):
+    import torch
+    torch.cuda.set_device(0)
+    sampler = ClockSampler(0)
+    sampler.start()
+    out = wnl_measure(max(args.steps, 1), cpu=not args.no_cpu)
+    out["clocks"] = sampler.stop()
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 # ---------------------------------------------------------------- profiling cases
@@ -914,6 +1008,13 @@ def _profile_case(name):
         p = atmo.default_params(bounces=3, rng_max=1000.0, write_rays=1)
         steps = ig.fan_run(atmo, p, th, ph)["ray_steps"]
         return lambda: ig.fan_paths(atmo, p, th, ph, caustics=True, ray_steps=steps)
+    if name == "wnl3d":        # waveforms of 148 rays, 8192 samples, no bounce (wnl3d_kernel: one CTA per ray)
+        atmo = ig.Atmosphere.load(wl.profile_met(1))
+        th = np.repeat(np.linspace(4.0, 34.0, 4), 37)
+        ph = np.tile(np.linspace(0.0, 360.0, 37), 4)
+        p = ig.wnl_params(atmo, bounces=0)
+        t, pw = wnl_waveform(8192)
+        return lambda: ig.wnl_run(atmo, p, th, ph, t, pw)
     if name == "eig3d":        # 3D eigenray search, 16 pairs (trace3d_fp64_kernel)
         atmo = ig.Atmosphere.load(wl.profile_met(1))
         pairs = wl.eig_pairs(1, 16)
@@ -927,7 +1028,8 @@ def _profile_case(name):
     raise SystemExit(f"unknown profiling case {name!r} (one of {', '.join(PROFILE_CASES)})")
 
 
-PROFILE_CASES = ("fan3d_fp32c", "fan3d_fp64", "config2_fp32c", "config2_fp64", "fansph", "fansphr_fp32c", "fansphr", "fan3dr", "paths", "eig3d", "eigsph")
+PROFILE_CASES = ("fan3d_fp32c", "fan3d_fp64", "config2_fp32c", "config2_fp64", "fansph", "fansphr_fp32c", "fansphr",
+                 "fan3dr", "paths", "wnl3d", "eig3d", "eigsph")
 
 
 def run_profile_case(args):
@@ -975,6 +1077,8 @@ def main():
                     help="time the spherical range-dependent fan with terrain (config 2) instead")
     ap.add_argument("--eigen", action="store_true",
                     help="time the batched 3D eigenray search (config 3, FP64 and FP32C) instead")
+    ap.add_argument("--wnl", action="store_true",
+                    help="time the weakly non-linear waveform mode over a 576-ray fan instead")
     ap.add_argument("--profile-case", choices=PROFILE_CASES,
                     help="run one small profiling workload of a single kernel (for ncu captures) instead")
     ap.add_argument("--reps", type=int, default=1, help="repetitions of --profile-case")
@@ -989,6 +1093,8 @@ def main():
         return run_sphr(args)
     if args.eigen:
         return run_eigen(args)
+    if args.wnl:
+        return run_wnl(args)
     if args.az_step != FAN["az"][2]:
         FAN["az"] = (FAN["az"][0], FAN["az"][1], args.az_step)
     if args.impl == "reference":

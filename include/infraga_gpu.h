@@ -349,6 +349,79 @@ int iga_fan_paths(iga_atmo_t atmo, const iga_fan_params* params,
                   double* path_rows, long long path_cap, long long* n_path, long long* path_start,
                   double* caustic_rows, long long caustic_cap, long long* n_caustic, int* caustic_ray);
 
+/* ---- weakly non-linear waveform (-wnl_wvfrm) ---- */
+
+/* Settings of run_wnl_wvfrm (main.infraga.3d.cpp:1087-1184) beyond the ray's:
+ * fan carries the propagation settings (bounces, source, ds, limits, ground,
+ * frequency of the absorption column, abs_coeff); its calc_amp and write_rays
+ * are taken as 1, precision as IGA_FP64, and turn_ht_min is ignored (the
+ * waveform driver has no turning-height cut). */
+typedef struct iga_wnl_params {
+    iga_fan_params fan;
+    double ds_wvfrm;             /* geoac::ds_wvfrm: step scale of the Burgers solver (0.5) */
+    double wvfrm_ref;            /* km of ray length where the source waveform is given (1.0) */
+    double out_step;             /* km; below 1e4: a spectrum / waveform snapshot each time the
+                                    ray length crosses a multiple of it (1e10: none) */
+    double filt1_g, filt1_n1, filt1_n2;   /* wvfrm::filt1_* low-pass of the non-linear term (0.5, 4, 0.5) */
+    double filt2_g, filt2_n1, filt2_n2;   /* wvfrm::filt2_* low-pass of the spectrum (0.75, 2, 1) */
+    long long max_steps;         /* Heun steps per ray after which the ray is given up (status 2);
+                                    no counterpart in the reference, whose loop is unbounded
+                                    (1000000; 0 = that default) */
+} iga_wnl_params;
+
+/* Per-ray summary (info rows of IGA_WNL_INFO doubles, in this order). */
+#define IGA_WNL_INFO 17
+enum iga_wnl_info {
+    IGA_WNL_STATUS = 0,     /* 0: waveform computed; 1: the ray never reached wvfrm_ref (u_out = 0);
+                               2: max_steps reached (u_out: the waveform where it stopped) */
+    IGA_WNL_STEPS = 1,      /* Heun steps of the Burgers solver over all bounces */
+    IGA_WNL_SHIFTS = 2,     /* caustic phase shifts applied ("Caustic encountered.") */
+    IGA_WNL_EVENTS = 3,     /* event rows produced (may exceed event_cap) */
+    IGA_WNL_SNAPS = 4,      /* snapshots produced (may exceed snap_cap) */
+    IGA_WNL_T_REF = 5,      /* travel time to the reference row: the time offset of .wvfrm_init.dat */
+    IGA_WNL_P0 = 6,         /* max |p| of the source waveform [Pa] */
+    IGA_WNL_SCALE = 7,      /* amplitude factor at the last row: p(t) = u_out * p0 * scale */
+    IGA_WNL_LENGTH = 8,     /* ray length the waveform was carried along [km] (the reference's running sum) */
+    IGA_WNL_C0 = 9, IGA_WNL_RHO0 = 10, IGA_WNL_NU0 = 11, IGA_WNL_CG0 = 12, IGA_WNL_D0 = 13,
+                            /* sound speed, density, |nu|, |c_g| and Jacobian at the reference row */
+    IGA_WNL_OOB = 14,       /* spline look-ups outside the ray's knots (the reference prints
+                               "Cannot interpolate outside of given bounds" for each) */
+    IGA_WNL_BETA0 = 15,     /* the non-linearity coefficient beta0 */
+    IGA_WNL_TIME = 16       /* travel time summed per bounce to its row k - 1 (the driver's
+                               travel_time_sum; the arrival row's time when the ray lands) */
+};
+/* Event row: type (0: the "Computing waveform at ray length" line of every
+ * 10 km, 1: "Caustic encountered."), ray length [km], altitude [km], beta. */
+#define IGA_WNL_EVENT_COLS 4
+
+/* Defaults of run_wnl_wvfrm after set_region (fan as iga_fan_params_default). */
+int iga_wnl_params_default(iga_atmo_t atmo, iga_wnl_params* params);
+
+/* Replaces run_wnl_wvfrm's bounce loop with geoac::wnl_wvfrm
+ * (src/main.infraga.3d.cpp:1281-1347, src/geoac/geoac.eqset.3d.strat.cpp:753-1045)
+ * for n_rays rays of a 3D stratified flat-ground atmosphere at once: each ray
+ * is traced (FP64, calc_amp), the source waveform (wv_t, wv_p: len samples of
+ * t [s] and p [Pa]; len a power of two from 16 to 8192) is given at ray length
+ * wvfrm_ref and carried to the end of the last bounce by the reference's
+ * Heun / FFT Burgers scheme with absorption, caustic phase shifts and filters.
+ *   u_out       [n_rays][len] waveform at the end scaled by 1 / p0; the
+ *               reference's .wvfrm_out.dat column is u_out * p0 * scale at
+ *               t = (arrival time) + wv_t
+ *   info        [n_rays][IGA_WNL_INFO] (iga_wnl_info)
+ *   arrivals    nullable: [n_rays][bounces + 1][IGA_ARRIVAL_COLS] the fan's
+ *               arrival rows (time / absorption summed per step, as the
+ *               waveform driver does); n_arr, ray_status nullable [n_rays]
+ *   events      nullable: [n_rays][event_cap][IGA_WNL_EVENT_COLS]
+ *   snaps       nullable: [n_rays][snap_cap][1 + len + 2 (len / 2 + 1)]:
+ *               the ray length label, u (scaled), then the spectrum U as
+ *               (re, im) pairs (sc_waveform / sc_spectrum of out_step)
+ * Returns IGA_E_TRUNCATED when events or snapshots had too little room (info
+ * holds the counts needed). */
+int iga_wnl_run(iga_atmo_t atmo, const iga_wnl_params* params, const double* theta_deg, const double* phi_deg,
+                int n_rays, const double* wv_t, const double* wv_p, int len, double* u_out, double* info,
+                double* arrivals, int* n_arr, int* ray_status, double* events, int event_cap, double* snaps,
+                int snap_cap);
+
 /* ---- eigenray search ---- */
 
 /* One source-receiver pair of an eigenray search (receiver on the ground).

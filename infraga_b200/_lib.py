@@ -65,6 +65,21 @@ class EigParams(ctypes.Structure):
                 ("chunk", ctypes.c_int), ("streams", ctypes.c_int)]
 
 
+class WnlParams(ctypes.Structure):
+    """Mirror of iga_wnl_params."""
+    _fields_ = [("fan", FanParams), ("ds_wvfrm", ctypes.c_double), ("wvfrm_ref", ctypes.c_double),
+                ("out_step", ctypes.c_double),
+                ("filt1_g", ctypes.c_double), ("filt1_n1", ctypes.c_double), ("filt1_n2", ctypes.c_double),
+                ("filt2_g", ctypes.c_double), ("filt2_n1", ctypes.c_double), ("filt2_n2", ctypes.c_double),
+                ("max_steps", ctypes.c_longlong)]
+
+
+WNL_INFO = 17
+WNL_INFO_NAMES = ("status", "steps", "shifts", "events", "snaps", "t_ref", "p0", "scale", "length", "c0", "rho0",
+                  "nu0", "cg0", "D0", "oob", "beta0", "time")
+WNL_EVENT_COLS = 4
+
+
 class EigPair(ctypes.Structure):
     _fields_ = [("src", ctypes.c_double * 3), ("rcvr", ctypes.c_double * 2)]
 
@@ -135,6 +150,9 @@ _SIGS = {
                            _P(_D), _LL, _P(_LL), _P(_I)]),
     "iga_atmo_terrain": (_I, [_VP, _D, _D, _P(_D), _P(_D), _P(_D)]),
     "iga_fan_tune": (_I, [_VP, _P(FanParams), _P(_D), _P(_D), _I, _P(_I), _P(_D)]),
+    "iga_wnl_params_default": (_I, [_VP, _P(WnlParams)]),
+    "iga_wnl_run": (_I, [_VP, _P(WnlParams), _P(_D), _P(_D), _I, _P(_D), _P(_D), _I, _P(_D), _P(_D), _P(_D), _P(_I),
+                         _P(_I), _P(_D), _I, _P(_D), _I]),
 }
 
 
@@ -516,3 +534,53 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def wnl_params(atmo: "Atmosphere", **overrides) -> WnlParams:
+    """iga_wnl_params_default, then fields by name (fan fields too: bounces=, src=, freq= ...)."""
+    p = WnlParams()
+    _check(lib().iga_wnl_params_default(atmo.handle, ctypes.byref(p)), "iga_wnl_params_default")
+    for k, v in overrides.items():
+        if hasattr(p, k) and k != "fan":
+            setattr(p, k, v)
+        elif k == "src":
+            for i in range(3):
+                p.fan.src[i] = float(v[i])
+        else:
+            setattr(p.fan, k, v)
+    return p
+
+
+def wnl_run(atmo: "Atmosphere", params: WnlParams, theta_deg, phi_deg, wv_t, wv_p, event_cap: int = 0,
+            snap_cap: int = 0):
+    """Weakly non-linear waveforms along rays (iga_wnl_run).  Returns a dict:
+    ``u`` [n, len] (p = u * p0 * scale), ``info`` [n, WNL_INFO] (also by name),
+    ``arrivals`` [n, bounces + 1, 12], ``n_arr``, ``ray_status`` and, with
+    caps, ``events`` / ``snaps``."""
+    th = np.ascontiguousarray(np.atleast_1d(theta_deg), dtype=np.float64)
+    ph = np.ascontiguousarray(np.atleast_1d(phi_deg), dtype=np.float64)
+    t = np.ascontiguousarray(wv_t, dtype=np.float64)
+    pw = np.ascontiguousarray(wv_p, dtype=np.float64)
+    n, N = th.size, t.size
+    nb = params.fan.bounces + 1
+    u = np.zeros((n, N))
+    info = np.zeros((n, WNL_INFO))
+    arr = np.zeros((n, nb, ARRIVAL_COLS))
+    n_arr = np.zeros(n, dtype=np.int32)
+    status = np.zeros(n, dtype=np.int32)
+    ev = np.zeros((n, max(event_cap, 1), WNL_EVENT_COLS))
+    snap_w = 1 + N + 2 * (N // 2 + 1)
+    sn = np.zeros((n, max(snap_cap, 1), snap_w))
+    rc = lib().iga_wnl_run(atmo.handle, ctypes.byref(params), _dptr(th), _dptr(ph), n, _dptr(t), _dptr(pw), N,
+                           _dptr(u), _dptr(info), _dptr(arr), n_arr.ctypes.data_as(_P(_I)),
+                           status.ctypes.data_as(_P(_I)), _dptr(ev) if event_cap else None, int(event_cap),
+                           _dptr(sn) if snap_cap else None, int(snap_cap))
+    _check(rc, "iga_wnl_run")
+    out = {"u": u, "info": info, "arrivals": arr, "n_arr": n_arr, "ray_status": status}
+    for i, name in enumerate(WNL_INFO_NAMES):
+        out[name] = info[:, i]
+    if event_cap:
+        out["events"] = ev
+    if snap_cap:
+        out["snaps"] = sn
+    return out

@@ -22,6 +22,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -165,7 +166,8 @@ void usage(Variant v) {
         std::cout << '\t' << "-back_proj   one ray from (rcvr_x, rcvr_y) at (inclination, azimuth) through the reversed"
                   << " winds (bounces)" << '\n';
     std::cout << '\t' << (back ? "" : "-back_proj, ")
-              << "-wnl_wvfrm and the reference's MPI builds are not provided by the GPU front end." << '\n' << '\n';
+              << (v == Variant::k3D ? "" : "-wnl_wvfrm, ")
+              << "the reference's MPI builds are not provided by the GPU front end." << '\n' << '\n';
 }
 
 void version() {
@@ -1363,6 +1365,336 @@ int run_back_3dr(int argc, char** argv, Variant v) {
     return 0;
 }
 
+// ------------------------------------------------------------------------
+// -wnl_wvfrm (infraga-3d, flat ground): run_wnl_wvfrm, main.infraga.3d.cpp:1087-1420
+// ------------------------------------------------------------------------
+
+// wvfrm:: settings (util/waveforms.cpp:21-37)
+struct WaveOpts {
+    double p0 = 10.0, t0 = 0.1, alpha = 4.0;
+    long len = 8192;
+    int N_rise = 10, N_period = 40;
+    const char* file = "none";
+    const char* opt = "impulse";
+};
+
+// wvfrm::impulse and wvfrm::n_wave (waveforms.cpp:42-62)
+double wv_impulse(const WaveOpts& w, double t) {
+    if (t < 0.0) return 0.0;
+    const double x = t / w.t0, x_pk = (w.alpha + 1.0) - sqrt(w.alpha + 1.0);
+    double r = pow(x, w.alpha) * (1.0 - x / (1.0 + w.alpha)) * exp(-x);
+    r /= pow(x_pk, w.alpha) * (1.0 - x_pk / (1.0 + w.alpha)) * exp(-x_pk);
+    return r;
+}
+double wv_nwave(const WaveOpts& w, double t) { return fabs(t) <= w.t0 ? t / w.t0 : 0.0; }
+
+// wvfrm::build_wvfrm / load_wvfrm (waveforms.cpp:67-147): t [s], p [Pa]
+bool make_waveform(WaveOpts& w, std::vector<double>& t, std::vector<double>& pw) {
+    if (strncmp(w.file, "none", 4) != 0) {
+        std::cout << '\t' << "Loading waveform from file: " << w.file << "." << '\n';
+        std::ifstream f(w.file);
+        if (!f.is_open()) return false;
+        long len = 0;   // file_length: lines not starting with '#', minus one
+        std::string line;
+        while (!f.eof()) {
+            std::getline(f, line);
+            if (line.find('#') != 0) len++;
+        }
+        len -= 1;
+        if (len < 2) return false;
+        f.clear();
+        f.seekg(0);
+        w.len = len;
+        t.assign(len, 0.0); pw.assign(len, 0.0);
+        long n = 0;
+        while (!f.eof() && n < len) {
+            std::getline(f, line);
+            if (line.find('#') != 0) {
+                std::stringstream ss(line);
+                ss >> t[n];
+                ss >> pw[n];
+                n++;
+            }
+        }
+        return true;
+    }
+    const long len = w.len;
+    t.resize(len); pw.resize(len);
+    const char* o = w.opt;
+    double duration;
+    if (strncmp(o, "impulse", 7) == 0) {
+        w.alpha = std::max(w.alpha, 0.01);
+        duration = w.t0 * len * std::max(((1.0 + w.alpha) - sqrt(1.0 + w.alpha)) / w.N_rise,
+                                         2.0 * 3.14159 * sqrt(1 + w.alpha) / w.N_period);
+        std::cout << '\t' << "Defining waveform from built in impulse with shaping parameter = " << w.alpha << "." << '\n';
+        for (long n = 0; n < len; n++) {
+            t[n] = -duration / 2.0 + duration * n / len;
+            pw[n] = w.p0 * wv_impulse(w, t[n]);
+        }
+    } else if (strncmp(o, "Uwave", 5) == 0 || strncmp(o, "u-wave", 6) == 0 || strncmp(o, "U-wave", 6) == 0) {
+        w.alpha = std::max(w.alpha, 2.0);
+        duration = w.t0 * len * std::max(((1.0 + w.alpha) - sqrt(1.0 + w.alpha)) / w.N_rise,
+                                         2.0 * 3.14159 * sqrt(1 + w.alpha) / w.N_period);
+        std::cout << '\t' << "Defining waveform from built in U-wave with shaping parameter = " << w.alpha << "." << '\n';
+        const double eps = 1.0e-2;
+        for (long n = 0; n < len; n++) {
+            t[n] = -duration / 2.0 + duration * n / len;
+            pw[n] = w.p0 * (wv_impulse(w, t[n] + eps) - wv_impulse(w, t[n] - eps)) / (2.0 * eps);
+            pw[n] /= 1.126 * (wv_impulse(w, eps) - wv_impulse(w, -eps)) / (2.0 * eps);
+        }
+    } else if (strncmp(o, "Nwave", 5) == 0 || strncmp(o, "n-wave", 6) == 0 || strncmp(o, "N-wave", 6) == 0) {
+        duration = (w.t0 / w.N_period) * len;
+        std::cout << '\t' << "Defining waveform from built in N-wave." << '\n';
+        for (long n = 0; n < len; n++) {
+            t[n] = -duration / 2.0 + duration * n / len;
+            pw[n] = -w.p0 * wv_nwave(w, t[n] - w.t0 / 2.0);
+        }
+    } else {
+        // the fallback takes the shorter of the two time scales (waveforms.cpp:127-130)
+        w.alpha = std::max(w.alpha, 0.01);
+        duration = w.t0 * len * std::min(((1.0 + w.alpha) - sqrt(1.0 + w.alpha)) / w.N_rise,
+                                         2.0 * 3.14159 * sqrt(1 + w.alpha) / w.N_period);
+        std::cout << '\t' << "Warning!!  Unrecognized option in waveform.  Options are 'impulse', 'Uwave', and 'Nwave'  Using "
+                  << "impulse with shaping parameter " << w.alpha << "." << '\n';
+        for (long n = 0; n < len; n++) {
+            t[n] = -duration / 2.0 + duration * n / len;
+            pw[n] = w.p0 * wv_impulse(w, t[n]);
+        }
+    }
+    return true;
+}
+
+int run_wnl(int argc, char** argv, Variant v) {
+    if (v != Variant::k3D) {
+        std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
+        return 0;
+    }
+    std::cout << '\n';
+    std::cout << '\t' << "##########################################" << '\n';
+    std::cout << '\t' << "####        Running infraga-3d        ####" << '\n';
+    std::cout << '\t' << "####    Weakly Non-Linear Waveform    ####" << '\n';
+    std::cout << '\t' << "##########################################" << '\n' << '\n';
+    const char* topo = nullptr;
+    const char* val;
+    for (int i = 3; i < argc; i++)
+        if (key(argv[i], "topo_file=", &val)) topo = val;
+    if (topo) {
+        std::cout << '\t' << "ERROR: -wnl_wvfrm over terrain is not provided by the GPU front end" << '\n';
+        return 0;
+    }
+    iga_atmo_t atmo = load_atmosphere(v, argc, argv, &topo);
+    if (!atmo) return 0;
+    iga_wnl_params wp;
+    int rc = iga_wnl_params_default(atmo, &wp);
+    if (rc) return fail("parameters", rc);
+    iga_fan_params& p = wp.fan;
+    print_region(v, p);
+    PropOpts o;
+    WaveOpts w;
+    double incl = 15.0, az = 90.0, xs = 0.0, ys = 0.0, zs = 0.0, freq = 0.1;
+    int bounces = 0;
+    bool write_rays = false;
+    for (int i = 3; i < argc; i++) {
+        const char* a = argv[i];
+        if (key(a, "inclination=", &val)) incl = atof(val);
+        else if (key(a, "azimuth=", &val)) az = atof(val);
+        else if (key(a, "bounces=", &val)) bounces = std::max(0, atoi(val));
+        else if (key2(a, "src_x=", "x_src=", &val)) xs = atof(val);
+        else if (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val)) ys = atof(val);
+        else if (key2(a, "src_alt=", "alt_src=", &val)) zs = atof(val);
+        else if (key(a, "write_ray=", &val)) write_rays = str2bool(val);
+        else if (key(a, "wvfrm_file=", &val)) w.file = val;
+        else if (key(a, "wvfrm_opt=", &val)) w.opt = val;
+        else if (key(a, "wvfrm_p0=", &val)) w.p0 = atof(val);
+        else if (key(a, "wvfrm_t0=", &val)) w.t0 = atof(val);
+        else if (key(a, "wvfrm_alpha=", &val)) w.alpha = atof(val);
+        else if (key(a, "wvfrm_ref=", &val)) wp.wvfrm_ref = atof(val);
+        else if (key(a, "wvfrm_out_step=", &val)) wp.out_step = atof(val);
+        else if (key(a, "wvfrm_ds=", &val)) wp.ds_wvfrm = atof(val);
+        // the reference reads N_rise from 15 characters in (its key has 13)
+        else if (match(a, "wvfrm_N_rise=", 13, 15, &val)) w.N_rise = (int)atof(a + std::min<size_t>(15, strlen(a)));
+        else if (key(a, "wvfrm_N_period=", &val)) w.N_period = (int)atof(val);
+        else if (key(a, "wvfrm_len=", &val)) w.len = (long)atof(val);
+        else if (key(a, "wvfrm_filt1_g=", &val)) wp.filt1_g = atof(val);
+        else if (key(a, "wvfrm_filt1_n1=", &val)) wp.filt1_n1 = atof(val);
+        else if (key(a, "wvfrm_filt1_n2=", &val)) wp.filt1_n2 = atof(val);
+        else if (key(a, "wvfrm_filt2_g=", &val)) wp.filt2_g = atof(val);
+        else if (key(a, "wvfrm_filt2_n1=", &val)) wp.filt2_n1 = atof(val);
+        else if (key(a, "wvfrm_filt2_n2=", &val)) wp.filt2_n2 = atof(val);
+        else if (common_key(v, a, p, o, false, freq)) {}
+        else if (!confirm_unknown(a, false)) { iga_atmo_destroy(atmo); return 0; }
+    }
+    if (o.use_blw) {
+        std::cout << '\t' << "ERROR: topo_use_BLw (boundary-layer vertical winds) is not provided by the GPU front end" << '\n';
+        iga_atmo_destroy(atmo);
+        return 0;
+    }
+    zs = std::max(p.z_grnd, zs);   // z_src = max(topo::z(x_src, y_src), z_src)
+    const double theta = incl * (Pi / 180.0), phi = Pi / 2.0 - az * (Pi / 180.0);
+    if (o.write_atmo && (rc = write_atmo_file(atmo, p, xs, ys, phi))) return fail("write_atmo", rc);
+    const double alpha_in = w.alpha;
+    std::cout << '\n' << "Parameter summary:" << '\n';
+    std::cout << '\t' << "inclination: " << theta * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "azimuth: " << 90.0 - phi * (180.0 / Pi) << '\n';
+    std::cout << '\t' << "bounces: " << bounces << '\n';
+    std::cout << '\t' << "source location: " << xs << ", " << ys << ", " << zs << '\n';
+    std::cout << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    std::cout << '\t' << "frequency: " << freq << '\n';
+    std::cout << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n';
+    if (strncmp(w.file, "none", 4) != 0) {
+        std::cout << '\t' << "waveform source file: " << w.file << '\n';
+    } else {
+        std::cout << '\t' << "waveform option: " << w.opt << '\n';
+        std::cout << '\t' << "waveform p0: " << w.p0 << '\n';
+        std::cout << '\t' << "waveform t0: " << w.t0 << '\n';
+        std::cout << '\t' << "waveform alpha: " << alpha_in << '\n';
+    }
+    std::cout << '\t' << "waveform reference location: " << wp.wvfrm_ref << '\n' << '\n';
+    if (!o.output_id) {
+        strip_extension(argv[2]);
+        o.output_id = argv[2];
+    }
+    const std::string id = o.output_id;
+    p.bounces = bounces;
+    p.src[0] = xs; p.src[1] = ys; p.src[2] = zs;
+    p.freq = freq;
+    p.turn_ht_min = -1.0e30;
+    std::cout << "Calculating ray path geometry and weakly non-linear waveform evolution..." << '\n';
+    std::vector<double> wt, wpr;
+    if (!make_waveform(w, wt, wpr)) {
+        std::cout << '\t' << "ERROR: cannot read the waveform file " << w.file << '\n';
+        iga_atmo_destroy(atmo);
+        return 0;
+    }
+    const int N = (int)w.len;
+    if (write_rays) {   // {id}.raypaths.dat rows m == 1 and m % 15 == 0 (main.infraga.3d.cpp:1287-1309)
+        iga_fan_params q = p;
+        q.calc_amp = 1; q.write_rays = 1; q.precision = IGA_FP64;
+        std::vector<double> arr((size_t)(bounces + 1) * IGA_ARRIVAL_COLS);
+        long long st = 0;
+        int n_out = 0;
+        if ((rc = iga_fan_run(atmo, &q, &incl, &az, 1, arr.data(), bounces + 1, &n_out, nullptr, &st, nullptr, nullptr,
+                              nullptr)))
+            return fail("ray path", rc);
+        const long long cap = (long long)(bounces + 1) + st / 15 + 1;
+        std::vector<double> rows((size_t)cap * IGA_PATH_COLS);
+        long long np = 0;
+        if ((rc = iga_fan_paths(atmo, &q, &incl, &az, 1, IGA_PATH_RAYS, &st, rows.data(), cap, &np, nullptr, nullptr, 0,
+                                nullptr, nullptr)))
+            return fail("ray path rows", rc);
+        std::ofstream raypath((id + ".raypaths.dat").c_str());
+        raypath << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "trans. coeff. [dB]" << '\t'
+                << "absorption [dB]" << '\t' << "time [s]" << '\n';
+        for (long long j = 0; j < np; j++) {
+            const double* r = &rows[(size_t)j * IGA_PATH_COLS];
+            raypath << r[0] << '\t' << r[1] << '\t' << r[2] << '\t' << r[3] << '\t' << r[4] << '\t' << r[5] << '\n';
+        }
+    }
+    // the waveform along the ray: events first sized by the ray length bound,
+    // grown once if the kernel reports more
+    const int nb = bounces + 1;
+    const int M1 = N / 2 + 1;
+    const size_t snap_w = 1 + (size_t)N + 2 * (size_t)M1;
+    std::vector<double> u(N), info(IGA_WNL_INFO), arr((size_t)nb * IGA_ARRIVAL_COLS);
+    int n_arr = 0, status = 0;
+    int ev_cap = 4096, sn_cap = wp.out_step < 1.0e4 ? 64 : 0;
+    std::vector<double> ev, sn;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        ev.assign((size_t)ev_cap * IGA_WNL_EVENT_COLS, 0.0);
+        sn.assign((size_t)sn_cap * snap_w, 0.0);
+        rc = iga_wnl_run(atmo, &wp, &incl, &az, 1, wt.data(), wpr.data(), N, u.data(), info.data(), arr.data(), &n_arr,
+                         &status, ev.data(), ev_cap, sn_cap ? sn.data() : nullptr, sn_cap);
+        if (rc != IGA_E_TRUNCATED) break;
+        ev_cap = std::max(ev_cap, (int)info[IGA_WNL_EVENTS]);
+        sn_cap = std::max(sn_cap, (int)info[IGA_WNL_SNAPS]);
+    }
+    if (rc) {
+        fail("waveform", rc);
+        iga_atmo_destroy(atmo);
+        return 0;
+    }
+    const bool started = info[IGA_WNL_STATUS] == 0.0;
+    std::ofstream wout;   // one stream for both files, as the reference (its precision carries over)
+    if (started) {
+        wout.open((id + ".wvfrm_init.dat").c_str());
+        wout << "# t [sec]" << '\t' << "p(t) [Pa]" << '\n';
+        for (int n = 0; n < N; n++) wout << std::setprecision(8) << info[IGA_WNL_T_REF] + wt[n] << '\t' << wpr[n] << '\n';
+        wout.close();
+    }
+    const int n_ev = std::min((int)info[IGA_WNL_EVENTS], ev_cap);
+    const int n_sn = std::min((int)info[IGA_WNL_SNAPS], sn_cap);
+    const double dt = wt[1] - wt[0];
+    char buf[512];
+    for (int j = 0; j < n_ev; j++) {
+        const double* e = &ev[(size_t)j * IGA_WNL_EVENT_COLS];
+        if (e[0] == 0.0)
+            std::cout << '\t' << "Computing waveform at ray length: " << e[1] << '\t' << "altitude: " << e[2] << '\t'
+                      << "scaled non-linearity factor: " << e[3] << '\n';
+        else
+            std::cout << '\t' << "Caustic encountered." << '\n';
+    }
+    for (int j = 0; j < n_sn; j++) {   // sc_spectrum / sc_waveform files (geoac.eqset.3d.strat.cpp:874-887)
+        const double* q = &sn[(size_t)j * snap_w];
+        snprintf(buf, sizeof(buf), "sc_spectrum-%04g.dat", q[0]);
+        std::ofstream fs(buf);
+        for (int k = 0; k < M1; k++)
+            fs << 1.0 / dt * k / N << '\t' << q[1 + N + 2 * k] << '\t' << q[2 + N + 2 * k] << '\n';
+        fs.close();
+        snprintf(buf, sizeof(buf), "sc_waveform-%04g.dat", q[0]);
+        std::ofstream fw(buf);
+        for (int n = 0; n < N; n++) fw << wt[n] << '\t' << q[1 + n] << '\n';
+    }
+    const bool landed = (status == 0) && n_arr == nb;
+    const double tt = landed ? arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS + 5] : info[IGA_WNL_TIME];
+    if (landed) {
+        const double* q = &arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS];
+        std::cout << '\n';
+        std::cout << '\t' << "Arrival summary:" << '\n';
+        std::cout << '\t' << '\t' << "x [km E-W] = " << q[3] << '\n';
+        std::cout << '\t' << '\t' << "y [km N-S] = " << q[4] << '\n';
+        std::cout << '\t' << '\t' << "time [s] = " << q[5] << '\n';
+        std::cout << '\t' << '\t' << "celerity [km/s] = " << q[6] << '\n';
+        std::cout << '\t' << '\t' << "turning height [km] = " << q[7] << '\n';
+        std::cout << '\t' << '\t' << "arrival inclination [deg] = " << q[8] << '\n';
+        std::cout << '\t' << '\t' << "back azimuth = " << q[9] << '\n';
+        std::cout << '\t' << '\t' << "attenuation (geometric) [dB] = " << q[10] << '\n';
+        std::cout << '\t' << '\t' << "absorption [dB] = " << q[11] << '\n' << '\n';
+    } else {
+        std::cout << '\n';
+        std::cout << '\t' << '\t' << "Ray path does not return to the ground." << '\n' << '\n';
+    }
+    if (!started)
+        std::cout << '\t' << "Note: the ray is shorter than wvfrm_ref; no waveform was carried along it." << '\n';
+    wout.open((id + ".wvfrm_out.dat").c_str());
+    wout << "# infraga-3d -wnl_wvfrm summary:" << '\n';
+    wout << "#" << '\t' << "profile: " << argv[2] << '\n';
+    wout << "#" << '\t' << "inclination: " << theta * (180.0 / Pi) << '\n';
+    wout << "#" << '\t' << "azimuth: " << phi * (180.0 / Pi) << '\n';
+    wout << "#" << '\t' << "bounces: " << bounces << '\n';
+    wout << "#" << '\t' << "source location: " << xs << ", " << ys << ", " << zs << '\n';
+    wout << "#" << '\t' << "ground elevation: " << p.z_grnd << '\n';
+    wout << "#" << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n';
+    if (strncmp(w.file, "none", 4) != 0) {
+        wout << "#" << '\t' << "waveform source file: " << w.file << '\n';
+    } else {
+        wout << "#" << '\t' << "waveform option: " << w.opt << '\n';
+        wout << "#" << '\t' << "waveform p0: " << w.p0 << '\n';
+        wout << "#" << '\t' << "waveform t0: " << w.t0 << '\n';
+        wout << "#" << '\t' << "waveform alpha: " << w.alpha << '\n';
+    }
+    wout << "#" << '\t' << "waveform reference location: " << wp.wvfrm_ref << '\n' << '\n';
+    wout << "# t [sec]" << '\t' << "p(t) [Pa]" << '\n';
+    const double p0 = info[IGA_WNL_P0], sc = info[IGA_WNL_SCALE];
+    for (int n = 0; n < N; n++) {
+        wout << std::setprecision(8) << tt + wt[n];
+        wout << '\t' << (started ? u[n] * p0 * sc : 0.0);
+        wout << '\n';
+    }
+    wout.close();
+    iga_atmo_destroy(atmo);
+    return 0;
+}
+
 }  // namespace
 
 int run(int argc, char** argv, Variant v, bool accel) {
@@ -1387,7 +1719,7 @@ int run(int argc, char** argv, Variant v, bool accel) {
     } else if (strncmp(o, "-eig_direct", 11) == 0 || strncmp(o, "-d", 2) == 0) {
         return run_eig(argc, argv, v, true);
     } else if (strncmp(o, "-wnl_wvfrm", 10) == 0 || strncmp(o, "-w", 2) == 0)
-        std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
+        return run_wnl(argc, argv, v);
     else
         std::cout << "Unrecognized option." << '\n';
     return 0;

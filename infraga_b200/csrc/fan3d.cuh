@@ -120,18 +120,27 @@ constexpr int kPathRays = 0;      // rows m == 1 and m % 15 == 0 of each bounce 
 constexpr int kPathTerrain = 1;   // rows m % 10 == 1 (terrain under the ray)
 constexpr int kPathProj = 2;      // rows m == 1 and m % 5 == 0 (back projection)
 constexpr int kPathResid = 3;     // one row per bounce segment: residuals at its row k - 1 (print_resid)
+constexpr int kPathWnl = 4;       // every row m = 0..k of each bounce (weakly non-linear waveform), kWnlCols wide
+// Waveform trace rows (kPathWnl, 3D stratified flat-ground kernel, calc_amp):
+// x, y, z [km], nu_x, nu_y, nu_z, the ray-tube Jacobian D (geoac::jacobian),
+// the travel time from the bounce's row 0 to this row (geoac::travel_time(solution, m)),
+// bounce, m.
+constexpr int kWnlCols = 10;
 
 __host__ __device__ inline bool path_sampled(int mode, int m) {
-    if (mode == kPathResid) return false;   // written at the segment end, not per step
+    if (mode == kPathResid || mode == kPathWnl) return false;   // written by their own branches
     return mode == kPathRays ? (m == 1 || m % 15 == 0) : (mode == kPathTerrain ? (m % 10 == 1) : (m == 1 || m % 5 == 0));
 }
 
-__host__ __device__ inline int path_cols(int mode) { return mode == kPathProj ? kProjCols : kPathCols; }
+__host__ __device__ inline int path_cols(int mode) {
+    return mode == kPathProj ? kProjCols : (mode == kPathWnl ? kWnlCols : kPathCols);
+}
 
 // Upper bound on the path rows of a ray that took `steps` RK4 steps over at
 // most `segments` bounce segments: each segment of K rows samples m in 1..K-1.
 inline long long path_rows_bound(int mode, long long steps, int segments) {
     if (mode == kPathResid) return segments;
+    if (mode == kPathWnl) return steps + segments;   // K + 1 rows per segment of K steps
     return (long long)segments + steps / (mode == kPathRays ? 15 : (mode == kPathTerrain ? 10 : 5)) + 1;
 }
 

@@ -244,6 +244,27 @@ static __device__ __noinline__ double amp_db(const double* __restrict__ tab, con
     return 20.0 * log10(sqrt(fabs(numr / den)));
 }
 
+// geoac::jacobian (geoac.eqset.3d.strat.cpp:703-723) at state y: the unit
+// group-velocity direction from c, u, v at the row's altitude and the
+// position derivatives X_th, X_ph (the determinant amp_db also takes).
+static __device__ __noinline__ double row_jacobian(const double* __restrict__ tab, const Fan3DArgs& a, int seg,
+                                                   const double* y, const RayConst& rc) {
+    const double zk = y[2];
+    const double ze = fmin(fmax(zk, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    const double c = cubic_f(r0, q, 2);
+    const double sc = bl_scale(a, zk);
+    const double wx = cubic_f(r0, q, 4) * sc, wy = cubic_f(r0, q, 6) * sc;
+    const double nz = y[3];
+    const double num = sqrt(rc.nx * rc.nx + rc.ny * rc.ny + nz * nz);
+    const double cgx = c * rc.nx / num + wx, cgy = c * rc.ny / num + wy, cgz = c * nz / num;
+    const double cgm = sqrt(cgx * cgx + cgy * cgy + cgz * cgz);
+    const double ex = cgx / cgm, ey = cgy / cgm, ez = cgz / cgm;
+    const double Xt[3] = {y[4], y[5], y[6]}, Xp[3] = {y[8], y[9], y[10]};
+    return ex * (Xt[1] * Xp[2] - Xp[1] * Xt[2]) - Xt[0] * (ey * Xp[2] - ez * Xp[1]) + Xp[0] * (ey * Xt[2] - ez * Xt[1]);
+}
 
 // geoac::eval_eikonal and geoac::eval_eikonal_deriv (geoac.eqset.3d.strat.cpp:
 // 393-432) at state y (12-state layout) over flat ground, the print_resid

@@ -73,6 +73,20 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
     // PATHS, back projection: travel-time variations (sums and pending increments as tt / pt)
     double tvt = 0.0, tvp = 0.0, ptvt = 0.0, ptvp = 0.0;
     const bool proj = PATHS && AMP && a.path_rows && a.path_mode == kPathProj;
+    // PATHS, waveform trace rows: every row of every bounce, with the bounce's
+    // travel time from its row 0 (ttb)
+    const bool wnl = PATHS && AMP && a.path_rows && a.path_mode == kPathWnl;
+    double ttb = 0.0;
+    auto wnl_row = [&](const double* yr, int m) {
+        if (p_n < p_cap) {
+            double* o = a.path_rows + (p_base + p_n) * kWnlCols;
+            o[0] = yr[0]; o[1] = yr[1]; o[2] = yr[2];
+            o[3] = rc.nx; o[4] = rc.ny; o[5] = yr[3];
+            o[6] = row_jacobian(tab, a, seg, yr, rc);
+            o[7] = ttb; o[8] = (double)bnc; o[9] = (double)m;
+        }
+        p_n++;
+    };
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * kPi / 180.0;
@@ -83,12 +97,14 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         zmax = a.z0;
         tvt = tvp = ptvt = ptvp = 0.0;
+        ttb = 0.0;
         if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
 
     while (true) {
         // ---- one RK4 step (rk4solver.cpp:30-55) ----
+        if (wnl) wnl_row(y, kb);
         zmax = fmax(zmax, y[2]);
         double ds = a.ds_max;   // set_ds (geoac.eqset.3d.strat.cpp:214-220)
         if (y[2] < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[2] - a.z0) / 0.2);
@@ -125,6 +141,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
 
         double dt, da;
         seg_increment(tab, a, seg, y, acc, rc, dt, da);
+        if (wnl) ttb += dt;
         if (a.write_rays) {   // all segments but the bounce's last (main.infraga.3d.cpp:451-453)
             tt += pt; att += pa; pt = dt; pa = da;
             if (proj) {       // run_back_proj sums travel_time_var the same way (main.infraga.3d.cpp:706-708)
@@ -191,6 +208,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         // ---- end of a bounce segment (main.infraga.3d.cpp:436-538) ----
         const int K = capped ? a.length : kb;
         steps += K;
+        if (wnl) wnl_row(acc, kb);   // row k: the first row beyond the segment's end
         if (PATHS && a.path_rows && a.path_mode == kPathResid) {
             // print_resid (main.infraga.3d.cpp:437-441): residuals at row k - 1
             if (p_n < p_cap) {
@@ -203,6 +221,7 @@ __global__ void __launch_bounds__(kThreads, IGA_FAN_MINB) fan3d_fp64_kernel(cons
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
         ptvt = 0.0; ptvp = 0.0;
+        ttb = 0.0;
         int status = -1;
         if (zmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);

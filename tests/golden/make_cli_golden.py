@@ -140,6 +140,62 @@ STDOUT_CASES = {
 }
 RESID_MARKERS = ("Calculating ray path", "Residuals at Ray Termination", "Eikonal residual", "Aux. param. residual")
 
+# -wnl_wvfrm cases: the reference's infraga-3d built against oracle/fftshim
+# (oracle/_ref/infraga-3d-wnl, ``make -C oracle wnl``) writes the fixtures;
+# the GPU front end runs as bin/infraga-3d.  Every output file is kept with
+# the waveform console lines (WNL_MARKERS) as cli/NAME/stdout.txt; the
+# argument lists go to cli/wnl_cases.json.  Kind "1dw" also stages wave.dat,
+# a source waveform file (wave_file()).
+WNL_CASES = {
+    "3d_wnl": ("infraga-3d-wnl", "1d", 0,
+               ["-wnl_wvfrm", "atmo.met", "inclination=12", "azimuth=60", "bounces=0", "wvfrm_len=2048"]),
+    "3d_wnl_dflt": ("infraga-3d-wnl", "1d", 2, ["-w", "atmo.met"]),
+    "3d_wnl_strong": ("infraga-3d-wnl", "1d", 1,
+                      ["-wnl_wvfrm", "atmo.met", "inclination=20", "azimuth=-30", "bounces=1", "wvfrm_len=1024",
+                       "wvfrm_p0=500", "wvfrm_opt=Uwave", "write_ray=true", "freq=0.5"]),
+    "3d_wnl_nwave": ("infraga-3d-wnl", "1d", 0,
+                     ["-wnl_wvfrm", "atmo.met", "inclination=8", "azimuth=60", "bounces=1", "wvfrm_opt=Nwave",
+                      "wvfrm_len=1024", "wvfrm_ref=5", "wvfrm_out_step=100", "output_id=nw"]),
+    "3d_wnl_file": ("infraga-3d-wnl", "1dw", 3,
+                    ["-wnl_wvfrm", "atmo.met", "inclination=18", "azimuth=0", "wvfrm_file=wave.dat", "bounces=0",
+                     "z_grnd=0.2", "src_alt=0.5", "abs_coeff=2"]),
+}
+WNL_MARKERS = ("Defining waveform", "Loading waveform", "Computing waveform", "Caustic encountered", "Arrival summary",
+               "[km E-W]", "[km N-S]", "time [s] =", "celerity", "turning height", "arrival inclination",
+               "back azimuth", "attenuation (geometric)", "absorption [dB]", "does not return")
+
+
+def wave_file() -> str:
+    """A 512-sample source waveform file (a Gaussian-windowed two-cycle pulse)
+    with a comment header, read through load_wvfrm."""
+    import math
+    lines = ["# t [s]\tp [Pa]"]
+    n = 512
+    for i in range(n):
+        t = -4.0 + 8.0 * i / n
+        p = 25.0 * math.exp(-(t / 0.35) ** 2) * math.sin(2.0 * math.pi * t / 0.4)
+        lines.append(f"{t:.10g}\t{p:.10g}")
+    return "\n".join(lines) + "\n"
+
+
+def wnl_lines(stdout: str) -> list[str]:
+    return [ln for ln in stdout.splitlines() if any(m in ln for m in WNL_MARKERS)]
+
+
+def run_case_wnl(binary_dir: str, spec, binary: str | None = None) -> tuple[dict[str, str], str]:
+    """Runs one -wnl_wvfrm case; returns ({relative path: text}, console lines)."""
+    ref_binary, kind, seed, argv = spec
+    with tempfile.TemporaryDirectory() as work:
+        stage(work, kind, seed)
+        before = inputs(work)
+        r = subprocess.run([os.path.join(binary_dir, binary or ref_binary), *argv], cwd=work, stdin=subprocess.DEVNULL,
+                           capture_output=True, text=True, check=True, timeout=600)
+        files = {}
+        for rel in sorted(inputs(work) - before):
+            with open(os.path.join(work, rel)) as f:
+                files[rel] = f.read()
+        return files, "\n".join(wnl_lines(r.stdout)) + "\n"
+
 
 def resid_lines(stdout: str) -> list[str]:
     return [ln for ln in stdout.splitlines() if any(m in ln for m in RESID_MARKERS)]
@@ -157,9 +213,12 @@ def run_case_stdout(binary_dir: str, spec) -> str:
 
 def stage(work: str, kind: str, seed: int) -> None:
     """Input files of a case in `work` under fixed relative names."""
-    if kind in ("1d", "1dt", "1dts"):
+    if kind in ("1d", "1dt", "1dts", "1dw"):
         shutil.copy(os.path.join(HERE, "profiles", f"gen{seed}.met"), os.path.join(work, "atmo.met"))
-        if kind != "1d":
+        if kind == "1dw":
+            with open(os.path.join(work, "wave.dat"), "w") as f:
+                f.write(wave_file())
+        elif kind != "1d":
             shutil.copy(os.path.join(HERE, "rngdep3d" if kind == "1dt" else "rngdep", "topo.dat"),
                         os.path.join(work, "topo.dat"))
         return
@@ -226,6 +285,26 @@ def main(names: list[str]) -> None:
     os.makedirs(OUT, exist_ok=True)
     with open(meta_path, "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)
+    wnl_path = os.path.join(OUT, "wnl_cases.json")
+    wmeta = json.load(open(wnl_path)) if os.path.exists(wnl_path) else {}
+    for name, spec in WNL_CASES.items():
+        if names and name not in names:
+            continue
+        files, text = run_case_wnl(REF, spec)
+        d = os.path.join(OUT, name)
+        if os.path.isdir(d):
+            shutil.rmtree(d)
+        os.makedirs(d)
+        for rel, body in files.items():
+            with open(os.path.join(d, rel), "w") as f:
+                f.write(body)
+        with open(os.path.join(d, "stdout.txt"), "w") as f:
+            f.write(text)
+        wmeta[name] = {"binary": "infraga-3d", "ref_binary": spec[0], "kind": spec[1], "seed": spec[2],
+                       "argv": spec[3], "files": sorted(files)}
+        print(name, sorted(files), sum(len(t) for t in files.values()), "bytes,", text.count("\n"), "console lines")
+    with open(wnl_path, "w") as f:
+        json.dump(wmeta, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

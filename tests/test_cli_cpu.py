@@ -40,9 +40,14 @@ def test_usage_and_version(bins, name):
 
 
 def test_unsupported_modes_say_so(bins):
-    r = subprocess.run([os.path.join(bins, "infraga-3d"), "-wnl_wvfrm", "x.met"], capture_output=True, text=True,
-                       timeout=60)
-    assert r.returncode == 0 and "not provided" in r.stdout
+    # the waveform mode: infraga-3d over flat ground; the other binaries and terrain refuse before loading
+    for name in ("infraga-sph", "infraga-3d-rngdep", "infraga-sph-rngdep"):
+        r = subprocess.run([os.path.join(bins, name), "-wnl_wvfrm", "a", "b", "c", "d"], capture_output=True, text=True,
+                           timeout=60)
+        assert r.returncode == 0 and "-wnl_wvfrm is not provided" in r.stdout, name
+    r = subprocess.run([os.path.join(bins, "infraga-3d"), "-w", "x.met", "topo_file=t.dat"], capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 0 and "-wnl_wvfrm over terrain is not provided" in r.stdout
     # back projection: infraga-3d over flat ground and infraga-3d-rngdep; the spherical ones refuse
     # before loading anything
     for name in ("infraga-sph", "infraga-sph-rngdep"):
@@ -55,6 +60,19 @@ def test_unsupported_modes_say_so(bins):
     for name in ("infraga-3d", "infraga-3d-rngdep"):
         r = subprocess.run([os.path.join(bins, name)], capture_output=True, text=True, timeout=60)
         assert "-back_proj   one ray" in r.stdout, name
+
+
+def test_wnl_fixtures_complete():
+    """The -wnl_wvfrm fixtures (reference waveform mode over oracle/fftshim) match
+    make_cli_golden.WNL_CASES, and each waveform file holds its samples."""
+    cases = json.load(open(os.path.join(CLI, "wnl_cases.json")))
+    assert set(cases) == set(mk.WNL_CASES)
+    for name, c in cases.items():
+        assert c["argv"] == mk.WNL_CASES[name][3]
+        assert any(f.endswith(".wvfrm_out.dat") for f in c["files"]), name
+        for rel in c["files"]:
+            assert os.path.getsize(os.path.join(CLI, name, rel)) > 0, (name, rel)
+        assert "Computing waveform at ray length" in open(os.path.join(CLI, name, "stdout.txt")).read()
 
 
 def test_cli_fixtures_complete():
