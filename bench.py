@@ -944,7 +944,7 @@ def wnl_measure(reps=2, cpu=True):
 def run_wnl(args):
     import torch
     torch.cuda.set_device(0)
-    sampler = ClockSampler(0)
+    sampler = ClockSampler("0")
     sampler.start()
     out = wnl_measure(max(args.steps, 1), cpu=not args.no_cpu)
     out["clocks"] = sampler.stop()

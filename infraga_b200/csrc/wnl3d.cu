@@ -7,8 +7,9 @@
 // Then one CTA per ray runs the whole waveform evolution without returning
 // to the host: the waveform u(t) (N samples), its spectrum U(f) and one
 // complex work array live in shared memory, and each Heun step is
-//   one thread: the linear splines along the ray (interp::linear_spline_1D
-//               with each spline's cached segment), beta, the step size,
+//   one thread: the linear splines along the ray (interp::linear_spline_1D;
+//               the six share their knots, so one segment walk serves all),
+//               beta, the step size,
 //               the caustic test and the frequency-independent part of the
 //               Sutherland-Bass absorption at the step's point;
 //   all threads: the non-linear source term, one real FFT of it, the spectral
@@ -169,28 +170,23 @@ struct WnlArgs {
     int snap_cap;
 };
 
-// interp::find_segment (interpolation.cpp:14-48) over the s column of the
-// scratch table (stride 3): the spline's cached segment `prev` first, then
-// its neighbours, then a search from both ends; outside the knots the cached
-// segment is kept (the reference prints a warning; counted in `oob`).
-__device__ __forceinline__ int find_seg(double x, const double* S, int L, int& prev, int& oob) {
-    if (x > S[(L - 1) * 3] || x < S[0]) { oob++; return prev; }
-    if (x >= S[prev * 3] && x <= S[(prev + 1) * 3]) return prev;
-    if (prev + 2 <= L - 1 && x >= S[(prev + 1) * 3] && x <= S[(prev + 2) * 3]) return ++prev;
-    if (prev - 1 >= 0 && x >= S[(prev - 1) * 3] && x <= S[prev * 3]) return --prev;
-    for (int n = 0; n + 1 < L; n++) {
-        if (x >= S[n * 3] && x <= S[(n + 1) * 3]) { prev = n; break; }
-        const int m = (L - 1) - (n + 1);
-        if (x >= S[m * 3] && x < S[(m + 1) * 3]) { prev = m; break; }
-    }
-    return prev;
+// Segment of x on the shared knots of the six splines (the s column of the
+// scratch table, stride 3): a forward walk from `k` (s only grows within a
+// bounce).  For x inside the knots this is the segment interp::find_segment
+// (interpolation.cpp:14-48) returns from any cached index, except when x
+// equals a knot, where the two neighbouring segments give the same value up
+// to rounding; outside the knots the segment is kept (the reference keeps its
+// cached one and prints a warning; counted in `oob`).
+__device__ __forceinline__ int seg_of(double x, const double* S, int L, int k, int& oob) {
+    if (!(x <= S[(L - 1) * 3] && x >= S[0])) { oob++; return k; }
+    while (k < L - 2 && S[(k + 1) * 3] < x) k++;
+    while (k > 0 && S[k * 3] > x) k--;
+    return k;
 }
 
-// interp::eval_f of a linear spline whose knots are the s column and whose
-// values sit at F[i * stride]; the slope (interp::set) from the same two knots.
-__device__ __forceinline__ double lin_eval(double x, const double* S, const double* F, int stride, int L, int& prev,
-                                           int& oob) {
-    const int k = find_seg(x, S, L, prev, oob);
+// interp::eval_f of a linear spline on segment k, knots s and values at
+// F[i * stride]; the slope (interp::set) from the same two knots.
+__device__ __forceinline__ double lin_at(double x, const double* S, const double* F, int stride, int k) {
     const double s0 = S[k * 3], s1 = S[(k + 1) * 3];
     const double f0 = F[(size_t)k * stride], f1 = F[(size_t)(k + 1) * stride];
     return f0 + (x - s0) * ((f1 - f0) / (s1 - s0));
@@ -283,7 +279,7 @@ struct WnlScal {
     SBPoint sp;
     long long steps;
     int shifts, snap, L, oob, n_ev, n_snap, started;
-    int aD, aB, aBc, aX, aY, aZ;   // cached segments of the six splines
+    int ks;                        // segment of s on the splines' knots
 };
 
 // atmo::c / rho / u / v at altitude z (clamped to the profile as
@@ -439,7 +435,7 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
             fm = block_max(fm, red);
             if (tid == 0) {
                 S.Uf_max = fm; S.s = 0.0; S.ds = A.ds_wvfrm;
-                S.aD = S.aB = S.aBc = S.aX = S.aY = S.aZ = 0;
+                S.ks = 0;
             }
             __syncthreads();
             // ---- Heun steps (:871-995), at most max_steps over the ray ----
@@ -454,9 +450,10 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                         S.snap = 1;
                         S.snap_label = A.out_step * ceil((s + sp) / A.out_step);
                     }
-                    const double Ds = lin_eval(s, sx, Rs + 6, kWnlCols, L, S.aD, oob);
-                    const double bc = fabs(Ds) >= 0.5 ? lin_eval(s, sx, Ts + 1, 3, L, S.aB, oob)
-                                                      : lin_eval(s, sx, Ts + 2, 3, L, S.aBc, oob);
+                    const int ks = seg_of(s, sx, L, S.ks, oob);
+                    S.ks = ks;
+                    const double Ds = lin_at(s, sx, Rs + 6, kWnlCols, ks);
+                    const double bc = fabs(Ds) >= 0.5 ? lin_at(s, sx, Ts + 1, 3, ks) : lin_at(s, sx, Ts + 2, 3, ks);
                     // std::min / std::max as the reference calls them: a NaN step stays NaN
                     // (and ends the loop through s)
                     double ds = A.ds_wvfrm / (kPi * S.Uf_max * bc);
@@ -464,11 +461,11 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                     ds = (ds < 1.0e-5) ? 1.0e-5 : ds;
                     const double s_last = sx[(size_t)(L - 1) * 3];
                     const double sn = (s_last < s + ds) ? s_last : s + ds;
-                    const double Dn = lin_eval(sn, sx, Rs + 6, kWnlCols, L, S.aD, oob);
-                    const double bn = fabs(Dn) >= 0.5 ? lin_eval(sn, sx, Ts + 1, 3, L, S.aB, oob)
-                                                      : lin_eval(sn, sx, Ts + 2, 3, L, S.aBc, oob);
+                    const int kn = seg_of(sn, sx, L, ks, oob);
+                    const double Dn = lin_at(sn, sx, Rs + 6, kWnlCols, kn);
+                    const double bn = fabs(Dn) >= 0.5 ? lin_at(sn, sx, Ts + 1, 3, kn) : lin_at(sn, sx, Ts + 2, 3, kn);
                     if (fabs(10.0 * ceil((s + sp + ds) / 10.0) - 10.0 * ceil((s + sp) / 10.0)) > 0.0) {
-                        const double zs = lin_eval(s, sx, Rs + 2, kWnlCols, L, S.aZ, oob);
+                        const double zs = lin_at(s, sx, Rs + 2, kWnlCols, ks);
                         if (ev && S.n_ev < A.event_cap) {
                             double* o = ev + (size_t)S.n_ev * kWnlEventCols;
                             o[0] = 0.0; o[1] = 10.0 * ceil((s + sp) / 10.0); o[2] = zs; o[3] = bc;
@@ -477,8 +474,8 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                     }
                     int shift = 0;
                     if (s + ds <= S.s_tot) {
-                        const double D0s = lin_eval(s, sx, Rs + 6, kWnlCols, L, S.aD, oob);
-                        const double D1s = lin_eval(s + ds, sx, Rs + 6, kWnlCols, L, S.aD, oob);
+                        const double D1s = lin_at(s + ds, sx, Rs + 6, kWnlCols, seg_of(s + ds, sx, L, ks, oob));
+                        const double D0s = Ds;
                         if (D0s * D1s <= 0.0) {
                             shift = 1;
                             if (ev && S.n_ev < A.event_cap) {
@@ -490,10 +487,8 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                         }
                     }
                     // absorption point (the reference evaluates it inside the bin loop)
-                    const double xs = lin_eval(s, sx, Rs + 0, kWnlCols, L, S.aX, oob);
-                    const double ys = lin_eval(s, sx, Rs + 1, kWnlCols, L, S.aY, oob);
-                    const double zs = lin_eval(s, sx, Rs + 2, kWnlCols, L, S.aZ, oob);
-                    (void)xs; (void)ys;
+                    // (x and y do not enter a stratified atmosphere)
+                    const double zs = lin_at(s, sx, Rs + 2, kWnlCols, ks);
                     const AtmoPt p = atmo_at(a, zs);
                     S.sp = sb_point(p.c, p.rho, zs, a.tweak_abs, a.sb);
                     S.fac = -p.c / S.c0;
