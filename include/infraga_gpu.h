@@ -394,12 +394,16 @@ enum iga_wnl_info {
  * 10 km, 1: "Caustic encountered."), ray length [km], altitude [km], beta. */
 #define IGA_WNL_EVENT_COLS 4
 
-/* Defaults of run_wnl_wvfrm after set_region (fan as iga_fan_params_default). */
+/* Defaults of run_wnl_wvfrm after set_region (fan as iga_fan_params_default; for
+ * infraga-sph's waveform mode set fan with iga_fan_params_init(atmo,
+ * IGA_GEOM_SPH, &params->fan) afterwards). */
 int iga_wnl_params_default(iga_atmo_t atmo, iga_wnl_params* params);
 
 /* Replaces run_wnl_wvfrm's bounce loop with geoac::wnl_wvfrm
- * (src/main.infraga.3d.cpp:1281-1347, src/geoac/geoac.eqset.3d.strat.cpp:753-1045)
- * for n_rays rays of a 3D stratified flat-ground atmosphere at once: each ray
+ * (src/main.infraga.3d.cpp:1281-1347, src/geoac/geoac.eqset.3d.strat.cpp:753-1045;
+ * with fan.geometry = IGA_GEOM_SPH, src/main.infraga.sph.cpp:1270-1325 and
+ * geoac.eqset.sph.strat.cpp:855-1130, source latitude / longitude in degrees)
+ * for n_rays rays of a stratified flat-ground atmosphere at once: each ray
  * is traced (FP64, calc_amp), the source waveform (wv_t, wv_p: len samples of
  * t [s] and p [Pa]; len a power of two from 16 to 8192) is given at ray length
  * wvfrm_ref and carried to the end of the last bounce by the reference's

@@ -536,10 +536,13 @@ class Server:
             pass
 
 
-def wnl_params(atmo: "Atmosphere", **overrides) -> WnlParams:
-    """iga_wnl_params_default, then fields by name (fan fields too: bounces=, src=, freq= ...)."""
+def wnl_params(atmo: "Atmosphere", geometry: int = GEOM_3D, **overrides) -> WnlParams:
+    """iga_wnl_params_default (fan from iga_fan_params_init for GEOM_SPH), then
+    fields by name (fan fields too: bounces=, src=, freq= ...)."""
     p = WnlParams()
     _check(lib().iga_wnl_params_default(atmo.handle, ctypes.byref(p)), "iga_wnl_params_default")
+    if geometry != GEOM_3D:
+        _check(lib().iga_fan_params_init(atmo.handle, int(geometry), ctypes.byref(p.fan)), "iga_fan_params_init")
     for k, v in overrides.items():
         if hasattr(p, k) and k != "fan":
             setattr(p, k, v)

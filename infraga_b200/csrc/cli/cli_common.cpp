@@ -166,7 +166,7 @@ void usage(Variant v) {
         std::cout << '\t' << "-back_proj   one ray from (rcvr_x, rcvr_y) at (inclination, azimuth) through the reversed"
                   << " winds (bounces)" << '\n';
     std::cout << '\t' << (back ? "" : "-back_proj, ")
-              << (v == Variant::k3D ? "" : "-wnl_wvfrm, ")
+              << (v == Variant::k3D || v == Variant::kSph ? "" : "-wnl_wvfrm, ")
               << "the reference's MPI builds are not provided by the GPU front end." << '\n' << '\n';
 }
 
@@ -1465,15 +1465,23 @@ bool make_waveform(WaveOpts& w, std::vector<double>& t, std::vector<double>& pw)
 }
 
 int run_wnl(int argc, char** argv, Variant v) {
-    if (v != Variant::k3D) {
+    if (v != Variant::k3D && v != Variant::kSph) {
         std::cout << "-wnl_wvfrm is not provided by the GPU front end." << '\n';
         return 0;
     }
+    const bool sph = v == Variant::kSph;   // run_wnl_wvfrm of main.infraga.sph.cpp:1142-1480
     std::cout << '\n';
-    std::cout << '\t' << "##########################################" << '\n';
-    std::cout << '\t' << "####        Running infraga-3d        ####" << '\n';
-    std::cout << '\t' << "####    Weakly Non-Linear Waveform    ####" << '\n';
-    std::cout << '\t' << "##########################################" << '\n' << '\n';
+    if (sph) {
+        std::cout << '\t' << "###########################################" << '\n';
+        std::cout << '\t' << "####        Running infraga-sph        ####" << '\n';
+        std::cout << '\t' << "####     Weakly Non-Linear Waveform    ####" << '\n';
+        std::cout << '\t' << "###########################################" << '\n' << '\n';
+    } else {
+        std::cout << '\t' << "##########################################" << '\n';
+        std::cout << '\t' << "####        Running infraga-3d        ####" << '\n';
+        std::cout << '\t' << "####    Weakly Non-Linear Waveform    ####" << '\n';
+        std::cout << '\t' << "##########################################" << '\n' << '\n';
+    }
     const char* topo = nullptr;
     const char* val;
     for (int i = 3; i < argc; i++)
@@ -1486,12 +1494,13 @@ int run_wnl(int argc, char** argv, Variant v) {
     if (!atmo) return 0;
     iga_wnl_params wp;
     int rc = iga_wnl_params_default(atmo, &wp);
+    if (!rc && sph) rc = iga_fan_params_init(atmo, IGA_GEOM_SPH, &wp.fan);
     if (rc) return fail("parameters", rc);
     iga_fan_params& p = wp.fan;
     print_region(v, p);
     PropOpts o;
     WaveOpts w;
-    double incl = 15.0, az = 90.0, xs = 0.0, ys = 0.0, zs = 0.0, freq = 0.1;
+    double incl = 15.0, az = 90.0, xs = sph ? 30.0 : 0.0, ys = 0.0, zs = 0.0, freq = 0.1;
     int bounces = 0;
     bool write_rays = false;
     for (int i = 3; i < argc; i++) {
@@ -1499,8 +1508,10 @@ int run_wnl(int argc, char** argv, Variant v) {
         if (key(a, "inclination=", &val)) incl = atof(val);
         else if (key(a, "azimuth=", &val)) az = atof(val);
         else if (key(a, "bounces=", &val)) bounces = std::max(0, atoi(val));
-        else if (key2(a, "src_x=", "x_src=", &val)) xs = atof(val);
-        else if (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val)) ys = atof(val);
+        else if (!sph && key2(a, "src_x=", "x_src=", &val)) xs = atof(val);
+        else if (!sph && (key(a, "src_y=", &val) || match(a, "y_src_y=", 6, 6, &val))) ys = atof(val);
+        else if (sph && key2(a, "src_lat=", "lat_src=", &val)) xs = atof(val);
+        else if (sph && key2(a, "src_lon=", "lon_src=", &val)) ys = atof(val);
         else if (key2(a, "src_alt=", "alt_src=", &val)) zs = atof(val);
         else if (key(a, "write_ray=", &val)) write_rays = str2bool(val);
         else if (key(a, "wvfrm_file=", &val)) w.file = val;
@@ -1529,15 +1540,19 @@ int run_wnl(int argc, char** argv, Variant v) {
         iga_atmo_destroy(atmo);
         return 0;
     }
-    zs = std::max(p.z_grnd, zs);   // z_src = max(topo::z(x_src, y_src), z_src)
+    if (sph) std::cout << "s_max --> " << p.s_max << '\n';
+    zs = std::max(p.z_grnd, zs);   // z_src = max(topo::z(src), z_src) over flat ground
     const double theta = incl * (Pi / 180.0), phi = Pi / 2.0 - az * (Pi / 180.0);
+    // the spherical driver keeps the source in radians and echoes it back in degrees
+    const double xe = sph ? xs * (Pi / 180.0) * (180.0 / Pi) : xs, ye = sph ? ys * (Pi / 180.0) * (180.0 / Pi) : ys;
     if (o.write_atmo && (rc = write_atmo_file(atmo, p, xs, ys, phi))) return fail("write_atmo", rc);
     const double alpha_in = w.alpha;
     std::cout << '\n' << "Parameter summary:" << '\n';
     std::cout << '\t' << "inclination: " << theta * (180.0 / Pi) << '\n';
     std::cout << '\t' << "azimuth: " << 90.0 - phi * (180.0 / Pi) << '\n';
     std::cout << '\t' << "bounces: " << bounces << '\n';
-    std::cout << '\t' << "source location: " << xs << ", " << ys << ", " << zs << '\n';
+    std::cout << '\t' << (sph ? "source location (lat, lon, alt): " : "source location: ") << xe << ", " << ye << ", "
+              << zs << '\n';
     std::cout << '\t' << "ground elevation: " << p.z_grnd << '\n';
     std::cout << '\t' << "frequency: " << freq << '\n';
     std::cout << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n';
@@ -1559,6 +1574,16 @@ int run_wnl(int argc, char** argv, Variant v) {
     p.src[0] = xs; p.src[1] = ys; p.src[2] = zs;
     p.freq = freq;
     p.turn_ht_min = -1.0e30;
+    if (sph) p.time_max = 1.0e30;
+    std::ofstream raypath;   // opened before the trace, as the reference does
+    if (write_rays) {
+        raypath.open((id + ".raypaths.dat").c_str());
+        if (sph)
+            raypath << "# z [km]" << '\t' << "lat [deg]" << '\t' << "lon [deg]";
+        else
+            raypath << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]";
+        raypath << '\t' << "trans. coeff. [dB]" << '\t' << "absorption [dB]" << '\t' << "time [s]" << '\n';
+    }
     std::cout << "Calculating ray path geometry and weakly non-linear waveform evolution..." << '\n';
     std::vector<double> wt, wpr;
     if (!make_waveform(w, wt, wpr)) {
@@ -1582,12 +1607,11 @@ int run_wnl(int argc, char** argv, Variant v) {
         if ((rc = iga_fan_paths(atmo, &q, &incl, &az, 1, IGA_PATH_RAYS, &st, rows.data(), cap, &np, nullptr, nullptr, 0,
                                 nullptr, nullptr)))
             return fail("ray path rows", rc);
-        std::ofstream raypath((id + ".raypaths.dat").c_str());
-        raypath << "# x [km]" << '\t' << "y [km]" << '\t' << "z [km]" << '\t' << "trans. coeff. [dB]" << '\t'
-                << "absorption [dB]" << '\t' << "time [s]" << '\n';
         for (long long j = 0; j < np; j++) {
             const double* r = &rows[(size_t)j * IGA_PATH_COLS];
-            raypath << r[0] << '\t' << r[1] << '\t' << r[2] << '\t' << r[3] << '\t' << r[4] << '\t' << r[5] << '\n';
+            if (sph) raypath << std::setprecision(8) << r[0] << '\t' << std::setprecision(8) << r[1];
+            else raypath << r[0] << '\t' << r[1];
+            raypath << '\t' << r[2] << '\t' << r[3] << '\t' << r[4] << '\t' << r[5] << '\n';
         }
     }
     // the waveform along the ray: events first sized by the ray length bound,
@@ -1628,8 +1652,8 @@ int run_wnl(int argc, char** argv, Variant v) {
     for (int j = 0; j < n_ev; j++) {
         const double* e = &ev[(size_t)j * IGA_WNL_EVENT_COLS];
         if (e[0] == 0.0)
-            std::cout << '\t' << "Computing waveform at ray length: " << e[1] << '\t' << "altitude: " << e[2] << '\t'
-                      << "scaled non-linearity factor: " << e[3] << '\n';
+            std::cout << '\t' << (sph ? "Generating" : "Computing") << " waveform at ray length: " << e[1] << '\t'
+                      << "altitude: " << e[2] << '\t' << "scaled non-linearity factor: " << e[3] << '\n';
         else
             std::cout << '\t' << "Caustic encountered." << '\n';
     }
@@ -1646,7 +1670,20 @@ int run_wnl(int argc, char** argv, Variant v) {
     }
     const bool landed = (status == 0) && n_arr == nb;
     const double tt = landed ? arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS + 5] : info[IGA_WNL_TIME];
-    if (landed) {
+    if (landed && sph) {   // the latitude's setprecision(8) stays on the stream
+        const double* q = &arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS];
+        std::cout << '\n';
+        std::cout << '\t' << "Arrival summary:" << '\n';
+        std::cout << '\t' << '\t' << "latitude [deg] = " << std::setprecision(8) << q[3] << '\n';
+        std::cout << '\t' << '\t' << "longitude [deg] = " << std::setprecision(8) << q[4] << '\n';
+        std::cout << '\t' << '\t' << "time [s] = " << q[5] << '\n';
+        std::cout << '\t' << '\t' << "celerity [km/s] = " << q[6] << '\n';
+        std::cout << '\t' << '\t' << "turning height [km] = " << q[7] << '\n';
+        std::cout << '\t' << '\t' << "arrival inclination [deg] = " << q[8] << '\n';
+        std::cout << '\t' << '\t' << "back azimuth [deg] = " << q[9] << '\n';
+        std::cout << '\t' << '\t' << "trans. coeff. [dB] = " << q[10] << '\n';
+        std::cout << '\t' << '\t' << "absorption [dB] = " << q[11] << '\n' << '\n';
+    } else if (landed) {
         const double* q = &arr[(size_t)(nb - 1) * IGA_ARRIVAL_COLS];
         std::cout << '\n';
         std::cout << '\t' << "Arrival summary:" << '\n';
@@ -1666,12 +1703,13 @@ int run_wnl(int argc, char** argv, Variant v) {
     if (!started)
         std::cout << '\t' << "Note: the ray is shorter than wvfrm_ref; no waveform was carried along it." << '\n';
     wout.open((id + ".wvfrm_out.dat").c_str());
-    wout << "# infraga-3d -wnl_wvfrm summary:" << '\n';
+    wout << (sph ? "# infraga-sph -wnl_wvfrm summary:" : "# infraga-3d -wnl_wvfrm summary:") << '\n';
     wout << "#" << '\t' << "profile: " << argv[2] << '\n';
     wout << "#" << '\t' << "inclination: " << theta * (180.0 / Pi) << '\n';
     wout << "#" << '\t' << "azimuth: " << phi * (180.0 / Pi) << '\n';
     wout << "#" << '\t' << "bounces: " << bounces << '\n';
-    wout << "#" << '\t' << "source location: " << xs << ", " << ys << ", " << zs << '\n';
+    wout << "#" << '\t' << (sph ? "source (lat, lon, alt): " : "source location: ") << xe << ", " << ye << ", " << zs
+         << '\n';
     wout << "#" << '\t' << "ground elevation: " << p.z_grnd << '\n';
     wout << "#" << '\t' << "S&B atten coeff: " << p.tweak_abs << '\n';
     if (strncmp(w.file, "none", 4) != 0) {

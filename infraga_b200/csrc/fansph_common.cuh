@@ -276,6 +276,33 @@ static __device__ __noinline__ double amp_db_sph(const double* __restrict__ tab,
     return 20.0 * log10(sqrt(fabs(numr / den)));
 }
 
+// geoac::jacobian (geoac.eqset.sph.strat.cpp:800-822) at state y (18-state
+// layout): the unit group-velocity direction in (r, lat, lon) rates and the
+// position derivatives, scaled by r^2 cos(lat) (the determinant amp_db_sph
+// also takes).
+static __device__ __noinline__ double row_jacobian_sph(const double* __restrict__ tab, const Fan3DArgs& a, int seg,
+                                                       const double* y) {
+    const double r = y[0];
+    const double ze = fmin(fmax(r - a.r_earth, a.z_lo), a.z_hi);
+    seg = seg_walk(tab, a.n_knots, ze, seg);
+    const double* r0 = tab + seg * kStride;
+    const Cubic q = cubic_at(r0, ze);
+    const double c = cubic_f(r0, q, 2);
+    const double sc = bl_scale_sph(a, r);
+    const double u = cubic_f(r0, q, 4) * sc, v = cubic_f(r0, q, 6) * sc;
+    const double n0 = y[3], n1 = y[4], n2 = y[5];
+    const double nm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    const double j0 = c * n0 / nm, j1 = c * n1 / nm + v, j2 = c * n2 / nm + u;
+    const double jm = sqrt(j0 * j0 + j1 * j1 + j2 * j2);
+    const double cl = cos(y[1]);
+    const double dr_ds = j0 / jm, dt_ds = 1.0 / r * j1 / jm, dp_ds = 1.0 / (r * cl) * j2 / jm;
+    const double* Rt = y + 6;
+    const double* Rp = y + 12;
+    return r * r * cl *
+           (dr_ds * (Rt[1] * Rp[2] - Rp[1] * Rt[2]) - Rt[0] * (dt_ds * Rp[2] - dp_ds * Rp[1]) +
+            Rp[0] * (dt_ds * Rt[2] - dp_ds * Rt[1]));
+}
+
 // Per-arrival diagnostics (18-state layout): launch-angle derivatives of the
 // ground intercept as the spherical find_eigenray forms them
 // (geoac.eigenray.sph.cpp:351-359, flat ground), as ground distance per

@@ -60,6 +60,20 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
     long long steps;
     double s, tt, att, pt, pa, rmax;
     long long p_base = 0, p_cap = 0, p_n = 0;   // PATHS: this ray's row range and rows produced
+    // PATHS, waveform trace rows: every row of every bounce (r, lat, lon, nu,
+    // D, the bounce's travel time from its row 0, bounce, m)
+    const bool wnl = PATHS && AMP && a.path_rows && a.path_mode == kPathWnl;
+    double ttb = 0.0;
+    auto wnl_row = [&](const double* yr, int m) {
+        if (p_n < p_cap) {
+            double* o = a.path_rows + (p_base + p_n) * kWnlCols;
+            o[0] = yr[0]; o[1] = yr[1]; o[2] = yr[2];
+            o[3] = yr[3]; o[4] = yr[4]; o[5] = yr[5];
+            o[6] = row_jacobian_sph(tab, a, seg, yr);
+            o[7] = ttb; o[8] = (double)bnc; o[9] = (double)m;
+        }
+        p_n++;
+    };
 
     auto start_ray = [&](int r) {
         const double theta = a.theta_deg[r] * (kPi / 180.0);
@@ -69,12 +83,14 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
         bnc = 0; kb = 0; na = 0; steps = 0; caustics = 0;
         s = 0.0; tt = 0.0; att = 0.0; pt = 0.0; pa = 0.0;
         rmax = 0.0;
+        ttb = 0.0;
         if (PATHS && a.path_rows) { p_base = a.path_off[r]; p_cap = a.path_off[r + 1] - p_base; p_n = 0; }
     };
     start_ray(ray);
 
     while (true) {
         // ---- one RK4 step (rk4solver.cpp:30-55) ----
+        if (wnl) wnl_row(y, kb);
         rmax = fmax(rmax, y[0] - a.r_earth);
         double ds = a.ds_max;   // set_ds (geoac.eqset.sph.strat.cpp:216-222)
         if (y[0] - a.r_earth < a.z_bl) ds -= (a.ds_max - a.ds_min) * exp(-(y[0] - a.r_grnd) / 0.2);
@@ -124,6 +140,7 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
 
         double dt, da;
         seg_increment_sph(tab, a, seg, y, acc, dt, da);
+        if (wnl) ttb += dt;
         if (a.write_rays) {   // all segments but the bounce's last (main.infraga.sph.cpp:466-468)
             tt += pt; att += pa; pt = dt; pa = da;
         } else {              // per-bounce sum added at the end (main.infraga.sph.cpp:496-497)
@@ -158,8 +175,10 @@ __global__ void __launch_bounds__(kThreads, IGA_SPH_MINB) fansph_fp64_kernel(con
         // ---- end of a bounce segment (main.infraga.sph.cpp:459-548) ----
         const int K = capped ? a.length : kb;
         steps += K;
+        if (wnl) wnl_row(acc, kb);   // row k: the first row beyond the segment's end
         if (!a.write_rays) { tt += pt; att += pa; }
         pt = 0.0; pa = 0.0;
+        ttb = 0.0;
         int status = -1;
         if (rmax < a.z0 + a.turn_ht_min) status = 2;
         else if (esc) status = bad ? 4 : (capped ? 5 : 1);

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "fan3d_common.cuh"
+#include "fansph_common.cuh"
 #include "handle.h"
 #include "nvtx.h"
 
@@ -42,8 +43,9 @@ constexpr int kWnlMaxLen = 8192;
 constexpr int kWnlInfo = 17;      // doubles of per-ray summary (IGA_WNL_INFO order)
 constexpr int kWnlEventCols = 4;  // type, value, altitude, beta
 
-// The frequency-independent part of sb_alpha<false> at one point
-// (atmo_state.abs.cart.cpp:12-142): what the per-bin part below needs.
+// The frequency-independent part of sb_alpha<SPH> at one point
+// (atmo_state.abs.cart.cpp:12-142, atmo_state.abs.sph.cpp:11-147): what the
+// per-bin part below needs.
 struct SBPoint {
     double cs, mu, P_z3;   // sound speed [m/s], viscosity, 3 P_z
     double nn;             // (4/5) sqrt(3/7) Z_rot
@@ -53,6 +55,7 @@ struct SBPoint {
     double tweak;
 };
 
+template <bool SPH>
 __device__ __forceinline__ SBPoint sb_point(double c_kms, double rho_gcc, double z, double tweak_abs, const SBConst& k) {
     SBPoint P;
     const double mu_o = 18.192e-6, T_o = 293.15, P_o = 101325.0, S = 117.0;
@@ -70,7 +73,7 @@ __device__ __forceinline__ SBPoint sb_point(double c_kms, double rho_gcc, double
     const double X4 = iga_exp10(z > 95.0 ? (-3.2456 + (4.6642e-2 * z) - (2.6894e-4 * z2) + (5.264e-7 * z3))
                                      : (-11.195 + (1.5408e-1 * z) - (1.4348e-3 * z2) + (1.0166e-5 * z3)));
     // the Cartesian N-profile polynomial's z^2 where z^4 is meant (cart line 78)
-    const double X5 = iga_exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * z2) + (4.2609e-10 * z5));
+    const double X5 = iga_exp10(-53.746 + (1.5439 * z) - (1.8824e-2 * z2) + (1.1587e-4 * z3) - (3.5399e-7 * (SPH ? z4 : z2)) + (4.2609e-10 * z5));
     const double X6 = iga_exp10(z > 30.0 ? (-4.2563 + (7.6245e-2 * z) - (2.1824e-3 * z2) - (2.3010e-6 * z3) + (2.4265e-7 * z4) - (1.2500e-9 * z5))
                                      : (-1.7491 + (4.4986e-2 * z) - (6.8549e-2 * z2) + (5.4639e-3 * z3) - (1.5539e-4 * z4) + (1.5063e-6 * z5)));
     const double Tm13 = iga_rcbrt(T_z);
@@ -117,8 +120,9 @@ __device__ __forceinline__ SBPoint sb_point(double c_kms, double rho_gcc, double
     return P;
 }
 
-// sb_alpha<false>(c, rho, z, freq) given sb_point(c, rho, z): the same
+// sb_alpha<SPH>(c, rho, z, freq) given sb_point<SPH>(c, rho, z): the same
 // operations in the same order.
+template <bool SPH>
 __device__ __forceinline__ double sb_bin(const SBPoint& P, double freq) {
     const double sigma = 5.0 / sqrt(21.0);
     const double nu = (8.0 * kPi * freq * P.mu) / P.P_z3;
@@ -127,12 +131,19 @@ __device__ __forceinline__ double sb_bin(const SBPoint& P, double freq) {
     const double beta_0 = 2.0 * kPi * freq / P.cs;
     const double nu2 = nu * nu, sq = sqrt(1.0 + nu2);
     const double cc2 = cchi * cchi, sc2 = (sigma * cchi) * (sigma * cchi);
-    const double beta_1 = sqrt(0.5 * (sq + 1.0) / (1.0 + nu2));
-    const double beta_2 = sqrt((1.0 + cc2) / (1.0 + sc2));
-    const double alpha_1 = beta_0 * sqrt(0.5 * (sq - 1.0) / (1.0 + nu2));
-    const double alpha_2 = beta_0 * (((sigma / 2.0 - 1.0 / (2.0 * sigma)) * chi) / (sqrt((1.0 + cc2) * (1.0 + sc2))));
-    const double a_cl = alpha_1 * beta_2;
-    const double a_rot = alpha_2 * beta_1 * P.X_ON;
+    double a_cl, a_rot;
+    if (SPH) {
+        a_cl = beta_0 * sqrt(0.5 * (sq - 1.0) * (1.0 + cc2) / ((1.0 + nu2) * (1.0 + sc2)));
+        a_rot = beta_0 * P.X_ON * ((sigma * sigma - 1.0) * chi / (2.0 * sigma)) *
+                sqrt(0.5 * (sq + 1.0) / ((1.0 + nu2) * (1.0 + cc2)));
+    } else {
+        const double beta_1 = sqrt(0.5 * (sq + 1.0) / (1.0 + nu2));
+        const double beta_2 = sqrt((1.0 + cc2) / (1.0 + sc2));
+        const double alpha_1 = beta_0 * sqrt(0.5 * (sq - 1.0) / (1.0 + nu2));
+        const double alpha_2 = beta_0 * (((sigma / 2.0 - 1.0 / (2.0 * sigma)) * chi) / (sqrt((1.0 + cc2) * (1.0 + sc2))));
+        a_cl = alpha_1 * beta_2;
+        a_rot = alpha_2 * beta_1 * P.X_ON;
+    }
     const double f2 = freq * freq;
     double a_vib = 0.0;
 #pragma unroll
@@ -140,6 +151,7 @@ __device__ __forceinline__ double sb_bin(const SBPoint& P, double freq) {
         const double q = freq / P.fv[m];
         a_vib += P.Acs[m] * ((2.0 * f2 / P.fv[m]) / (1.0 + q * q));
     }
+    if (SPH) return (a_cl + a_rot + 0.003 * a_cl + a_vib) * P.tweak * 8.685889e3;
     return (a_cl * 1.003 + a_rot + a_vib) * P.tweak * 8.685889e3;
 }
 
@@ -282,15 +294,19 @@ struct WnlScal {
     int ks;                        // segment of s on the splines' knots
 };
 
-// atmo::c / rho / u / v at altitude z (clamped to the profile as
-// atmo_state.3d.strat.cpp:148-180 does; u, v with the boundary-layer scaling)
+// atmo::c / rho / u / v at a row's height coordinate (3D: altitude z; SPH:
+// radius r, altitude r - r_earth), clamped to the profile as
+// atmo_state.3d.strat.cpp:148-180 and atmo_state.sph.strat.cpp do; u, v with
+// the boundary-layer scaling.
 struct AtmoPt { double c, rho, u, v; };
-__device__ __forceinline__ AtmoPt atmo_at(const Fan3DArgs& a, double z) {
+template <bool SPH>
+__device__ __forceinline__ AtmoPt atmo_at(const Fan3DArgs& a, double h) {
+    const double z = SPH ? h - a.r_earth : h;
     const double ze = fmin(fmax(z, a.z_lo), a.z_hi);
     const int sg = seg_walk(a.knots, a.n_knots, ze, seg_guess(ze, a.z_lo, a.inv_dz, a.n_knots));
     const double* r0 = a.knots + sg * kStride;
     const Cubic q = cubic_at(r0, ze);
-    const double sc = bl_scale(a, z);
+    const double sc = SPH ? bl_scale_sph(a, h) : bl_scale(a, z);
     AtmoPt p;
     p.c = cubic_f(r0, q, 2);
     p.u = cubic_f(r0, q, 4) * sc;
@@ -303,6 +319,35 @@ __device__ __forceinline__ double nu_mag(const double* r) {
     return sqrt(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
 }
 
+// |c_g| at a row from c nu / |nu| plus the winds: 3D (x, y, z) takes (u, v, 0),
+// SPH (r, lat, lon) takes (w = 0, v, u) (main.infraga.3d.cpp:1321-1325,
+// main.infraga.sph.cpp:1303-1307).
+template <bool SPH>
+__device__ __forceinline__ double group_speed(const double* r, const AtmoPt& p, double nu) {
+    const double g0 = p.c * r[3] / nu + (SPH ? 0.0 : p.u);
+    const double g1 = p.c * r[4] / nu + p.v;
+    const double g2 = p.c * r[5] / nu + (SPH ? p.u : 0.0);
+    return sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+}
+
+// Chord between rows r0 and r1: wnl_wvfrm's spline knots (3D: Euclidean;
+// SPH: dr, r0 dlat, r0 cos(lat0) dlon, geoac.eqset.sph.strat.cpp:907-911) or,
+// with MID, run_wnl_wvfrm's search for the reference row (SPH: at the
+// segment's midpoint radius and latitude, main.infraga.sph.cpp:1294-1299).
+template <bool SPH, bool MID>
+__device__ __forceinline__ double chord(const double* r0, const double* r1) {
+    const double d0 = r1[0] - r0[0], d1 = r1[1] - r0[1], d2 = r1[2] - r0[2];
+    if (!SPH) return sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    const double r = MID ? r0[0] + d0 / 2.0 : r0[0];
+    const double t = MID ? r0[1] + d1 / 2.0 : r0[1];
+    const double a1 = r * d1, a2 = r * cos(t) * d2;
+    return sqrt(d0 * d0 + a1 * a1 + a2 * a2);
+}
+
+// SPH: infraga-sph's wnl_wvfrm (geoac.eqset.sph.strat.cpp:855-1130) with its
+// differences: spherical chords, a 1e-7 km step floor (1e-5 in 3D), strict
+// caustic tests (s + ds < s_tot, D(s) D(s + ds) < 0), the spherical absorption.
+template <bool SPH>
 __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_constant__ WnlArgs A) {
     extern __shared__ double sm[];
     const int N = A.len, M = N >> 1, logm = A.logm;
@@ -346,16 +391,13 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                 for (int j = 0; j < K; j++) {
                     const double* r0 = R + (b + j) * kWnlCols;
                     const double* r1 = r0 + kWnlCols;
-                    const double dx = r1[0] - r0[0], dy = r1[1] - r0[1], dz = r1[2] - r0[2];
-                    S.ray_length += sqrt(dx * dx + dy * dy + dz * dz);
+                    S.ray_length += chord<SPH, true>(r0, r1);
                     if (S.ray_length >= A.wvfrm_ref) {
                         // reference quantities at row j + 1
-                        const AtmoPt p = atmo_at(a, r1[2]);
+                        const AtmoPt p = atmo_at<SPH>(a, r1[SPH ? 0 : 2]);
                         S.c0 = p.c; S.rho0 = p.rho;
                         S.nu0 = nu_mag(r1);
-                        const double gx = S.c0 * r1[3] / S.nu0 + p.u, gy = S.c0 * r1[4] / S.nu0 + p.v;
-                        const double gz = S.c0 * r1[5] / S.nu0;
-                        S.cg0 = sqrt(gx * gx + gy * gy + gz * gz);
+                        S.cg0 = group_speed<SPH>(r1, p, S.nu0);
                         S.D0 = r1[6];
                         S.t_ref = r1[7];
                         S.started = 1;
@@ -392,9 +434,7 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
             for (int i = tid; i < L; i += T) {   // chord to the next row, summed below
                 if (i + 1 < L) {
                     const double* r0 = Rs + (size_t)i * kWnlCols;
-                    const double* r1 = r0 + kWnlCols;
-                    const double dx = r1[0] - r0[0], dy = r1[1] - r0[1], dz = r1[2] - r0[2];
-                    Ts[(size_t)(i + 1) * 3] = sqrt(dx * dx + dy * dy + dz * dz);
+                    Ts[(size_t)(i + 1) * 3] = chord<SPH, false>(r0, r0 + kWnlCols);
                 }
             }
             __syncthreads();
@@ -410,7 +450,7 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                 const double k2 = S.c0 * (S.nu0 * S.nu0 * S.nu0);
                 for (int i = tid; i < L; i += T) {
                     const double* r = Rs + (size_t)i * kWnlCols;
-                    const AtmoPt p = atmo_at(a, r[2]);
+                    const AtmoPt p = atmo_at<SPH>(a, r[SPH ? 0 : 2]);
                     const double nu = nu_mag(r);
                     const double c3 = p.c * p.c * p.c, n3 = nu * nu * nu;
                     Ts[(size_t)i * 3 + 1] = S.beta0 * sqrt(fabs(k0 / (r[6] * p.rho * c3) * (p.c * n3) / k2));
@@ -458,14 +498,15 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                     // (and ends the loop through s)
                     double ds = A.ds_wvfrm / (kPi * S.Uf_max * bc);
                     ds = (1.0 < ds) ? 1.0 : ds;
-                    ds = (ds < 1.0e-5) ? 1.0e-5 : ds;
+                    ds = (ds < (SPH ? 1.0e-7 : 1.0e-5)) ? (SPH ? 1.0e-7 : 1.0e-5) : ds;
                     const double s_last = sx[(size_t)(L - 1) * 3];
                     const double sn = (s_last < s + ds) ? s_last : s + ds;
                     const int kn = seg_of(sn, sx, L, ks, oob);
                     const double Dn = lin_at(sn, sx, Rs + 6, kWnlCols, kn);
                     const double bn = fabs(Dn) >= 0.5 ? lin_at(sn, sx, Ts + 1, 3, kn) : lin_at(sn, sx, Ts + 2, 3, kn);
                     if (fabs(10.0 * ceil((s + sp + ds) / 10.0) - 10.0 * ceil((s + sp) / 10.0)) > 0.0) {
-                        const double zs = lin_at(s, sx, Rs + 2, kWnlCols, ks);
+                        const double zs = SPH ? lin_at(s, sx, Rs + 0, kWnlCols, ks) - a.r_earth
+                                              : lin_at(s, sx, Rs + 2, kWnlCols, ks);
                         if (ev && S.n_ev < A.event_cap) {
                             double* o = ev + (size_t)S.n_ev * kWnlEventCols;
                             o[0] = 0.0; o[1] = 10.0 * ceil((s + sp) / 10.0); o[2] = zs; o[3] = bc;
@@ -473,10 +514,10 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                         S.n_ev++;
                     }
                     int shift = 0;
-                    if (s + ds <= S.s_tot) {
+                    if (SPH ? (s + ds < S.s_tot) : (s + ds <= S.s_tot)) {
                         const double D1s = lin_at(s + ds, sx, Rs + 6, kWnlCols, seg_of(s + ds, sx, L, ks, oob));
                         const double D0s = Ds;
-                        if (D0s * D1s <= 0.0) {
+                        if (SPH ? (D0s * D1s < 0.0) : (D0s * D1s <= 0.0)) {
                             shift = 1;
                             if (ev && S.n_ev < A.event_cap) {
                                 double* o = ev + (size_t)S.n_ev * kWnlEventCols;
@@ -487,10 +528,10 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                         }
                     }
                     // absorption point (the reference evaluates it inside the bin loop)
-                    // (x and y do not enter a stratified atmosphere)
-                    const double zs = lin_at(s, sx, Rs + 2, kWnlCols, ks);
-                    const AtmoPt p = atmo_at(a, zs);
-                    S.sp = sb_point(p.c, p.rho, zs, a.tweak_abs, a.sb);
+                    // (the horizontal coordinates do not enter a stratified atmosphere)
+                    const double hs = lin_at(s, sx, Rs + (SPH ? 0 : 2), kWnlCols, ks);
+                    const AtmoPt p = atmo_at<SPH>(a, hs);
+                    S.sp = sb_point<SPH>(p.c, p.rho, SPH ? hs - a.r_earth : hs, a.tweak_abs, a.sb);
                     S.fac = -p.c / S.c0;
                     S.ds = ds; S.beta_c = bc; S.beta_n = bn;
                     S.w1 = ds * (bc + bn) / 2.0;
@@ -542,7 +583,7 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
                     const double pf = kPi * fr;
                     X.x -= pf * Q.y * A.filt1[k];
                     X.y += pf * Q.x * A.filt1[k];
-                    const double absorp = iga_exp10(fac * sb_bin(sp, fr) * ds / 10.0);
+                    const double absorp = iga_exp10(fac * sb_bin<SPH>(sp, fr) * ds / 10.0);
                     const double g = absorp * A.filt2[k];
                     X.x *= g; X.y *= g;
                     U[k] = X;
@@ -577,10 +618,9 @@ __global__ void __launch_bounds__(kWnlThreads, 1) wnl3d_kernel(const __grid_cons
         double scale_sq = 0.0;
         if (last_row >= 0 && S.started) {
             const double* r = R + last_row * kWnlCols;
-            const AtmoPt p = atmo_at(a, r[2]);
+            const AtmoPt p = atmo_at<SPH>(a, r[SPH ? 0 : 2]);
             const double nu = sqrt(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
-            const double gx = p.c * r[3] / nu + p.u, gy = p.c * r[4] / nu + p.v, gz = p.c * r[5] / nu;
-            const double cg = sqrt(gx * gx + gy * gy + gz * gz);
+            const double cg = group_speed<SPH>(r, p, nu);
             scale_sq = sqrt(fabs((p.rho * (p.c * p.c * p.c) * nu) / (S.rho0 * (S.c0 * S.c0 * S.c0) * S.nu0) *
                                  (S.cg0 * S.D0) / (cg * r[6])));
         }
@@ -667,16 +707,18 @@ extern "C" int iga_wnl_run(iga_atmo_t h, const iga_wnl_params* wp, const double*
         g_cuda_err = "waveform length: a power of two from 16 to 8192 samples";
         return IGA_E_UNSUPPORTED;
     }
-    if (h->kind != 0 || h->has_topo || wp->fan.geometry != IGA_GEOM_3D) {
-        g_cuda_err = "weakly non-linear waveform: 3D stratified flat-ground atmospheres only";
+    if (h->kind != 0 || h->has_topo) {
+        g_cuda_err = "weakly non-linear waveform: stratified flat-ground atmospheres only (3D or spherical geometry)";
         return IGA_E_UNSUPPORTED;
     }
+    const bool sph = wp->fan.geometry == IGA_GEOM_SPH;
     if (!(wp->ds_wvfrm > 0.0)) return IGA_E_INVALID;
     iga_fan_params q = wp->fan;
     q.calc_amp = 1;
     q.write_rays = 1;               // run_wnl_wvfrm sums time and absorption per step (:1296-1299)
     q.precision = IGA_FP64;
     q.turn_ht_min = -1.0e30;        // no turning-height cut in run_wnl_wvfrm
+    if (sph) q.time_max = 1.0e30;   // nor the spherical run_prop's travel-time cap
     int rc = validate(&q, n_rays);
     if (rc) return rc;
     if (n_rays == 0) return IGA_OK;
@@ -772,9 +814,9 @@ extern "C" int iga_wnl_run(iga_atmo_t h, const iga_wnl_params* wp, const double*
     A.snaps = d_sn; A.snap_cap = snap_cap;
     const size_t smem = sizeof(double) * ((size_t)N + 2 * (size_t)(M + 1) + 2 * (size_t)M) + sizeof(iga::WnlScal) +
                         40 * sizeof(double);
-    IGA_CUDA(cudaFuncSetAttribute(iga::wnl3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "wnl smem attribute");
-    iga::wnl3d_kernel<<<n_rays, iga::kWnlThreads, smem, st>>>(A);
+    auto kern = sph ? iga::wnl3d_kernel<true> : iga::wnl3d_kernel<false>;
+    IGA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "wnl smem attribute");
+    kern<<<n_rays, iga::kWnlThreads, smem, st>>>(A);
     IGA_CUDA(cudaGetLastError(), "wnl kernel launch");
 
     IGA_CUDA(cudaMemcpyAsync(u_out, d_u, sizeof(double) * n * N, cudaMemcpyDeviceToHost, st), "D2H wnl waveforms");

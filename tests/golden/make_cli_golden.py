@@ -140,9 +140,9 @@ STDOUT_CASES = {
 }
 RESID_MARKERS = ("Calculating ray path", "Residuals at Ray Termination", "Eikonal residual", "Aux. param. residual")
 
-# -wnl_wvfrm cases: the reference's infraga-3d built against oracle/fftshim
-# (oracle/_ref/infraga-3d-wnl, ``make -C oracle wnl``) writes the fixtures;
-# the GPU front end runs as bin/infraga-3d.  Every output file is kept with
+# -wnl_wvfrm cases: the reference's infraga-3d and infraga-sph built against
+# oracle/fftshim (oracle/_ref/infraga-{3d,sph}-wnl, ``make -C oracle wnl``)
+# write the fixtures; the GPU front end runs as bin/infraga-3d / infraga-sph.  Every output file is kept with
 # the waveform console lines (WNL_MARKERS) as cli/NAME/stdout.txt; the
 # argument lists go to cli/wnl_cases.json.  Kind "1dw" also stages wave.dat,
 # a source waveform file (wave_file()).
@@ -159,10 +159,18 @@ WNL_CASES = {
     "3d_wnl_file": ("infraga-3d-wnl", "1dw", 3,
                     ["-wnl_wvfrm", "atmo.met", "inclination=18", "azimuth=0", "wvfrm_file=wave.dat", "bounces=0",
                      "z_grnd=0.2", "src_alt=0.5", "abs_coeff=2"]),
+    "sph_wnl": ("infraga-sph-wnl", "1d", 0,
+                ["-wnl_wvfrm", "atmo.met", "inclination=12", "azimuth=60", "bounces=1", "wvfrm_len=1024"]),
+    "sph_wnl_nwave": ("infraga-sph-wnl", "1d", 1,
+                      ["-wnl_wvfrm", "atmo.met", "src_lat=40", "src_lon=-100", "inclination=20", "azimuth=-30",
+                       "bounces=0", "wvfrm_opt=Nwave", "wvfrm_len=2048", "wvfrm_p0=200", "write_ray=true",
+                       "wvfrm_out_step=150", "output_id=sw"]),
 }
-WNL_MARKERS = ("Defining waveform", "Loading waveform", "Computing waveform", "Caustic encountered", "Arrival summary",
-               "[km E-W]", "[km N-S]", "time [s] =", "celerity", "turning height", "arrival inclination",
-               "back azimuth", "attenuation (geometric)", "absorption [dB]", "does not return")
+WNL_MARKERS = ("Defining waveform", "Loading waveform", "Computing waveform", "Generating waveform",
+               "Caustic encountered", "Arrival summary", "[km E-W]", "[km N-S]", "latitude [deg] =",
+               "longitude [deg] =", "time [s] =", "celerity", "turning height", "arrival inclination",
+               "back azimuth", "attenuation (geometric)", "trans. coeff. [dB] =", "absorption [dB]",
+               "does not return")
 
 
 def wave_file() -> str:
@@ -300,7 +308,7 @@ def main(names: list[str]) -> None:
                 f.write(body)
         with open(os.path.join(d, "stdout.txt"), "w") as f:
             f.write(text)
-        wmeta[name] = {"binary": "infraga-3d", "ref_binary": spec[0], "kind": spec[1], "seed": spec[2],
+        wmeta[name] = {"binary": spec[0].replace("-wnl", ""), "ref_binary": spec[0], "kind": spec[1], "seed": spec[2],
                        "argv": spec[3], "files": sorted(files)}
         print(name, sorted(files), sum(len(t) for t in files.values()), "bytes,", text.count("\n"), "console lines")
     with open(wnl_path, "w") as f:

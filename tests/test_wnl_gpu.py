@@ -1,8 +1,9 @@
-"""infraga-3d -wnl_wvfrm on the GPU (iga_wnl_run, infraga_b200/csrc/wnl3d.cu)
-against the reference's own waveform mode: oracle/_ref/infraga-3d-wnl is the
-unmodified reference built against oracle/fftshim (a working FFT behind the
-FFTW API subset it calls), and its output files for the cases of
-tests/golden/make_cli_golden.py WNL_CASES are the fixtures.
+"""infraga-3d and infraga-sph -wnl_wvfrm on the GPU (iga_wnl_run,
+infraga_b200/csrc/wnl3d.cu) against the reference's own waveform mode:
+oracle/_ref/infraga-{3d,sph}-wnl are the unmodified reference binaries built
+against oracle/fftshim (a working FFT behind the FFTW API subset they call),
+and their output files for the cases of tests/golden/make_cli_golden.py
+WNL_CASES are the fixtures.
 
 Tolerances.  Time columns: the printed 8 significant digits, within one unit
 of the last digit (the FP64 travel-time sums of the GPU and the CPU can
@@ -93,7 +94,7 @@ def _compare_console(got, ref):
     g, r = got.splitlines(), ref.splitlines()
     assert len(g) == len(r), f"{len(g)} console lines, reference {len(r)}:\n" + "\n".join(g[-5:])
     for lg, lr in zip(g, r):
-        if "Computing waveform" in lr:
+        if "Computing waveform" in lr or "Generating waveform" in lr:
             fg, fr = lg.split("\t"), lr.split("\t")
             assert fg[1] == fr[1], (lg, lr)   # ray length label
             for a, b in zip(fg[2:], fr[2:]):
